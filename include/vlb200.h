@@ -1,0 +1,96 @@
+/* vlb200.h -- extension entry points of the B200 GMM / Fisher-vector library.
+ *
+ * These are NOT VLFeat names.  The reference's API (vl/gmm.h, vl/fisher.h)
+ * takes host pointers, which bounds throughput by host<->device copies
+ * (320 B per D=80 float descriptor).  The entry points below take device
+ * pointers, encode many images in one call, and select the arithmetic used
+ * on the GPU.  All pointers marked "device" must be CUDA device (or managed)
+ * memory of the current device; "stream" is a cudaStream_t (NULL = the
+ * calling thread's library stream).  Every function returns 0 on success and
+ * a VL_ERR_* code on failure, with the message in vl_get_last_error_message().
+ */
+#ifndef VLB200_H
+#define VLB200_H
+
+#include "vl/generic.h"
+#include "vl/gmm.h"
+
+/* Arithmetic used on the GPU.
+ *  EXACT      direct (x-mu)^2/sigma^2 evaluation in the data type on CUDA cores
+ *             (float or double), the reference's own formulation
+ *             (vl/gmm.c:762-775, vl/fisher.c:442-447).
+ *  FP32       tensor cores: E-step and statistics contractions in bf16x3
+ *             split precision with fp32 accumulation (FP32-grade results).
+ *  BF16       tensor cores: bf16x3 E-step, single-pass bf16 statistics.
+ *  BF16_ROUTER  learned router picks candidate components; exact posteriors
+ *             on the candidates only; bf16 statistics; full E-step fallback
+ *             for descriptors whose predicted candidate mass is < 0.99.
+ * DEFAULT resolves to the process-wide mode (vlb200_set_precision), which
+ * starts as EXACT.  VL_TYPE_DOUBLE calls always run EXACT in double. */
+#define VLB200_PREC_DEFAULT 0
+#define VLB200_PREC_EXACT 1
+#define VLB200_PREC_FP32 2
+#define VLB200_PREC_BF16 3
+#define VLB200_PREC_BF16_ROUTER 4
+
+VL_EXPORT int vlb200_set_precision(int precision);
+VL_EXPORT int vlb200_get_precision(void);
+
+/* Library / device information. */
+VL_EXPORT char const *vlb200_version(void);
+VL_EXPORT int vlb200_device_ok(void); /* 1 if a usable CUDA device is present */
+
+/* Count of kernels this library has launched in this process (all threads). */
+VL_EXPORT vl_uint64 vlb200_launch_count(void);
+
+/* Kernel timing.  When enabled, every launch is bracketed by CUDA events on
+ * its own stream; vlb200_profile_read() synchronises and reports, per kernel
+ * name, the number of launches and the summed device time in ms. */
+VL_EXPORT void vlb200_profile_enable(int on);
+VL_EXPORT int vlb200_profile_read(char *names, vl_size nameStride, double *ms,
+                                  vl_uint64 *launches, vl_size maxEntries);
+VL_EXPORT void vlb200_profile_reset(void);
+
+/* E-step on device data (vl_get_gmm_data_posteriors_f, vl/gmm.h:94-103, with
+ * device pointers).  posteriors: numData x numClusters, device.  *ll receives
+ * the log-likelihood (host pointer). */
+VL_EXPORT int vlb200_gmm_posteriors_device(float *posteriors, vl_size numClusters,
+                                           vl_size numData, float const *priors,
+                                           float const *means, vl_size dimension,
+                                           float const *covariances, float const *data,
+                                           int precision, double *ll, void *stream);
+
+/* EM on device-resident data: the vl_gmm_em loop (vl/gmm.c:1220-1308) with
+ * the data already in device memory.  The model's parameters stay the host
+ * copies visible through vl_gmm_get_*; posteriors are fetched lazily. */
+VL_EXPORT double vlb200_gmm_em_device(VlGMM *self, float const *data, vl_size numData,
+                                      int precision);
+
+/* Per-iteration log-likelihood trace of the last EM run (up to maxEntries
+ * values; returns the number written). */
+VL_EXPORT vl_size vlb200_gmm_get_ll_trace(VlGMM const *self, double *trace, vl_size maxEntries);
+/* Number of empty modes re-seeded in the last EM run. */
+VL_EXPORT vl_size vlb200_gmm_get_num_restarts(VlGMM const *self);
+
+/* Fisher encoding of one image with device pointers (vl_fisher_encode,
+ * vl/fisher.h:48-54).  enc: 2*D*K floats, device.  numTerms: host pointer or
+ * NULL. */
+VL_EXPORT int vlb200_fisher_encode_device(float *enc, float const *means, vl_size dimension,
+                                          vl_size numClusters, float const *covariances,
+                                          float const *priors, float const *data,
+                                          vl_size numData, int flags, int precision,
+                                          vl_uint64 *numTerms, void *stream);
+
+/* Batched Fisher encoding of many images of uneven size in one call.
+ * data: total x D floats (device), image j owns rows offsets[j] ..
+ * offsets[j+1]-1; offsets: numImages+1 int64 (host).  enc: numImages x 2DK
+ * floats (device), image-major.  numTerms: numImages uint64 (device) or NULL.
+ * Equivalent to numImages calls of vl_fisher_encode. */
+VL_EXPORT int vlb200_fisher_encode_batch_device(float *enc, float const *means, vl_size dimension,
+                                                vl_size numClusters, float const *covariances,
+                                                float const *priors, float const *data,
+                                                vl_int64 const *offsets, vl_size numImages,
+                                                int flags, int precision, vl_uint64 *numTerms,
+                                                void *stream);
+
+#endif /* VLB200_H */

@@ -1,0 +1,143 @@
+"""Generate the golden fixtures in this directory from VLFeat's own CPU code.
+
+Run where the reference sources exist:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Every output comes from ``oracle/_ref/libvl_ref.so`` (the reference compiled
+from its own sources by ``oracle/Makefile``) through VLFeat's C API, run with
+one thread so the M-step merge order (vl/gmm.c:1152-1166) is fixed.  Inputs are
+seeded and stored beside the outputs, so the tests need neither the reference
+nor the generators.  The reference ships no golden vectors of its own; the
+Fisher known-answer case restates the setup of toolbox/xtest/vl_test_fisher.m:9-20
+(D=5, N=21, K=3, unit variances, uniform priors) with seeded NumPy data.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle.oracle import (FLAG_FAST, FLAG_IMPROVED, FLAG_NORMALIZED,  # noqa: E402
+                           FLAG_SQUARE_ROOT, Reference)
+from vlfeat_b200 import workloads as W  # noqa: E402
+
+FLAG_SETS = [0, FLAG_SQUARE_ROOT, FLAG_NORMALIZED, FLAG_IMPROVED, FLAG_IMPROVED | FLAG_FAST, FLAG_FAST]
+
+
+def rng(seed):
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def fisher_kat(ref, out):
+    r = rng(1)
+    D, N, K = 5, 21, 3
+    x = r.standard_normal((N, D))
+    mu = r.standard_normal((K, D))
+    cv = np.ones((K, D))
+    pr = np.full(K, 1.0 / K)
+    out.update(kat_data=x, kat_means=mu, kat_covs=cv, kat_priors=pr)
+    for dt, tag in ((np.float32, "f"), (np.float64, "d")):
+        for fl in FLAG_SETS:
+            enc, nt = ref.fisher(x.astype(dt), mu.astype(dt), cv.astype(dt), pr.astype(dt), fl)
+            out[f"kat_enc_{tag}_{fl}"] = enc
+            out[f"kat_nterms_{tag}_{fl}"] = np.int64(nt)
+
+
+def posteriors_case(ref, out):
+    D, N, K = 16, 500, 8
+    x = W.mixture_data(N, D, K, seed=11)
+    pr, mu, cv = W.custom_init(x, K, seed=12)
+    pr = rng(13).dirichlet(np.ones(K))
+    pr[3] = 5e-7  # below the 1e-6 prior floor: log-weight -inf (vl/gmm.c:746-747)
+    pr /= pr.sum()
+    out.update(post_data=x, post_priors=pr, post_means=mu.astype(np.float64), post_covs=cv.astype(np.float64))
+    for dt, tag in ((np.float32, "f"), (np.float64, "d")):
+        q, ll = ref.posteriors(x.astype(dt), pr.astype(dt), mu.astype(dt), cv.astype(dt))
+        out[f"post_q_{tag}"] = q
+        out[f"post_ll_{tag}"] = np.float64(ll)
+
+
+def em_case(ref, out):
+    """EM with an initial mean far from the data, so that mode empties and the
+    restart path (vl/gmm.c:814-999) fires.  Snapshots after t = 0..T
+    iterations come from separate vl_gmm_cluster calls with maxNumIterations = t
+    from the same custom initialisation (exact, restarts included)."""
+    D, N, K, T = 24, 3000, 12, 8
+    x = W.mixture_data(N, D, 10, seed=21)
+    pr, mu, cv = W.custom_init(x, K, seed=22)
+    mu = mu.astype(np.float64)
+    mu[5] = mu[5] + 60.0  # far outlier mean -> empty mode -> restart at iteration 2
+    cv = cv.astype(np.float64)
+    pr = pr.astype(np.float64)
+    lb = np.full(D, 1e-3)
+    out.update(em_data=x, em_priors0=pr, em_means0=mu, em_covs0=cv, em_lb=lb)
+    out["em_T"] = np.int64(T)
+    for dt, tag in ((np.float32, "f"), (np.float64, "d")):
+        lls, P, M, S = [], [], [], []
+        for t in range(T + 1):
+            r = ref.em(x.astype(dt), pr.astype(dt), mu.astype(dt), cv.astype(dt), lb, t,
+                       want_posteriors=(t == T))
+            lls.append(r["ll"])
+            P.append(r["priors"])
+            M.append(r["means"])
+            S.append(r["covs"])
+            if t == T:
+                out[f"em_post_{tag}"] = r["posteriors"]
+        out[f"em_ll_{tag}"] = np.array(lls)
+        out[f"em_priors_{tag}"] = np.stack(P)
+        out[f"em_means_{tag}"] = np.stack(M)
+        out[f"em_covs_{tag}"] = np.stack(S)
+
+
+def fv_case(ref, out):
+    D, K, N = 32, 16, 400
+    pr, mu, cv = W.fv_gmm(K, D, seed=31, dtype=np.float64)
+    pr[2] = 3e-7  # component skipped by the encoder (vl/fisher.c:436)
+    pr /= pr.sum()
+    x = W.pca_like(N, D, seed=32)
+    out.update(fv_data=x, fv_priors=pr, fv_means=mu, fv_covs=cv)
+    for dt, tag in ((np.float32, "f"), (np.float64, "d")):
+        for fl in FLAG_SETS:
+            enc, nt = ref.fisher(x.astype(dt), mu.astype(dt), cv.astype(dt), pr.astype(dt), fl)
+            out[f"fv_enc_{tag}_{fl}"] = enc
+            out[f"fv_nterms_{tag}_{fl}"] = np.int64(nt)
+
+
+def edge_cases(ref, out):
+    D, K = 7, 5
+    pr, mu, cv = W.fv_gmm(K, D, seed=41, dtype=np.float64)
+    x = W.pca_like(3, D, seed=42)
+    out.update(edge_priors=pr, edge_means=mu, edge_covs=cv, edge_data=x)
+    for dt, tag in ((np.float32, "f"), (np.float64, "d")):
+        for n in (0, 1, 3):
+            enc, nt = ref.fisher(x[:n].astype(dt), mu.astype(dt), cv.astype(dt), pr.astype(dt), FLAG_IMPROVED)
+            out[f"edge_enc_{tag}_n{n}"] = enc
+            out[f"edge_nterms_{tag}_n{n}"] = np.int64(nt)
+        # K = 1 and D = 1
+        enc, nt = ref.fisher(x.astype(dt), mu[:1].astype(dt), cv[:1].astype(dt), np.ones(1, dt), FLAG_IMPROVED)
+        out[f"edge_enc_{tag}_k1"] = enc
+        enc, nt = ref.fisher(x[:, :1].copy().astype(dt), mu[:, :1].copy().astype(dt), cv[:, :1].copy().astype(dt),
+                             pr.astype(dt), FLAG_IMPROVED)
+        out[f"edge_enc_{tag}_d1"] = enc
+
+
+def main():
+    ref = Reference(threads=1)
+    out: dict = {}
+    fisher_kat(ref, out)
+    posteriors_case(ref, out)
+    em_case(ref, out)
+    fv_case(ref, out)
+    edge_cases(ref, out)
+    path = os.path.join(HERE, "golden.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,91 @@
+"""CPU tests of the drop-in boundary: the library loads, exports every symbol
+the public headers declare, and reports failures through VLFeat's
+last-error channel instead of aborting (no kernel runs here)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+HEADERS = ["include/vl/generic.h", "include/vl/gmm.h", "include/vl/fisher.h", "include/vlb200.h"]
+
+
+def declared_symbols():
+    names = set()
+    for h in HEADERS:
+        src = open(os.path.join(ROOT, h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"VL_EXPORT[^;(]*?\b(\w+)\s*\(", src):
+            names.add(m.group(1))
+    return names
+
+
+@pytest.fixture(scope="module")
+def libpath():
+    from vlfeat_b200 import build
+    return build.build()
+
+
+def test_header_declarations_found():
+    names = declared_symbols()
+    assert {"vl_gmm_new", "vl_gmm_cluster", "vl_fisher_encode", "vl_get_gmm_data_posteriors_f",
+            "vlb200_fisher_encode_batch_device"} <= names
+    assert len(names) > 60
+
+
+def test_exports_every_declared_symbol(libpath):
+    out = subprocess.run(["nm", "-D", "--defined-only", libpath], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+    missing = declared_symbols() - exported
+    assert not missing, f"declared but not exported: {sorted(missing)}"
+
+
+def test_loads_and_binds(libpath):
+    from vlfeat_b200 import capi
+    L = capi.lib()
+    assert L.vl_get_version_string()
+    assert L.vlb200_version().startswith(b"vlfeat-b200")
+
+
+def test_model_state_without_gpu(libpath):
+    """Object lifecycle, setters and getters are host-only and match the
+    reference defaults (vl/gmm.c:353-382)."""
+    import numpy as np
+    from vlfeat_b200 import capi
+    g = capi.GMM(5, 3)
+    L = capi.lib()
+    assert L.vl_gmm_get_max_num_iterations(g._h) == 50
+    assert L.vl_gmm_get_num_repetitions(g._h) == 1
+    assert L.vl_gmm_get_initialization(g._h) == capi.INIT_RAND
+    lb = np.ctypeslib.as_array(C.cast(L.vl_gmm_get_covariance_lower_bounds(g._h),
+                                      C.POINTER(C.c_double)), shape=(5,))
+    assert np.all(lb == 1e-4)
+    g.set_means(np.arange(15, dtype=np.float32).reshape(3, 5))
+    assert np.array_equal(g.means, np.arange(15, dtype=np.float32).reshape(3, 5))
+    g.set_covariance_lower_bound(0.5)
+    assert np.all(np.ctypeslib.as_array(C.cast(L.vl_gmm_get_covariance_lower_bounds(g._h),
+                                               C.POINTER(C.c_double)), shape=(5,)) == 0.5)
+
+
+def test_bad_arguments_set_last_error(libpath):
+    import numpy as np
+    from vlfeat_b200 import capi
+    L = capi.lib()
+    enc = np.zeros(4, np.float32)
+    nt = L.vl_fisher_encode(enc.ctypes.data_as(C.c_void_p), 7, None, 1, 1, None, None, None, 0, 0)
+    assert nt == 0 and L.vl_get_last_error() == 3  # VL_ERR_BAD_ARG
+    assert L.vlb200_set_precision(99) == 3
+
+
+def test_without_gpu_reports_error(libpath):
+    import numpy as np
+    from vlfeat_b200 import capi
+    if capi.device_ok():
+        pytest.skip("a GPU is present; the failure path is exercised only without one")
+    with pytest.raises(capi.VLError):
+        capi.fisher_encode(np.zeros((3, 2), np.float32), np.zeros((1, 2), np.float32),
+                           np.ones((1, 2), np.float32), np.ones(1, np.float32))

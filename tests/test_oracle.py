@@ -1,0 +1,96 @@
+"""CPU tests: the C restatement (oracle/) is pinned against the golden vectors
+produced by VLFeat's own code (tests/golden/make_golden.py), and the FP64
+NumPy statement of the Fisher vector pins the known-answer case the way
+toolbox/xtest/vl_test_fisher.m does (absTol 1e-10 in double)."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from oracle.oracle import FLAG_FAST, FLAG_IMPROVED, FLAG_NORMALIZED, FLAG_SQUARE_ROOT, simple_fisher
+
+FLAG_SETS = [0, FLAG_SQUARE_ROOT, FLAG_NORMALIZED, FLAG_IMPROVED, FLAG_IMPROVED | FLAG_FAST, FLAG_FAST]
+TOL = {"f": 2e-5, "d": 1e-12}
+DT = {"f": np.float32, "d": np.float64}
+
+
+@pytest.mark.parametrize("tag", ["f", "d"])
+@pytest.mark.parametrize("flags", FLAG_SETS)
+def test_fisher_known_answer(golden, restatement, tag, flags):
+    g = golden
+    args = [g["kat_data"].astype(DT[tag]), g["kat_means"], g["kat_covs"], g["kat_priors"]]
+    enc, nt = restatement.fisher(args[0], *[a.astype(DT[tag]) for a in args[1:]], flags)
+    ref = g[f"kat_enc_{tag}_{flags}"]
+    assert rel_err(enc, ref) < TOL[tag]
+    assert nt == int(g[f"kat_nterms_{tag}_{flags}"])
+    if tag == "d":
+        s = simple_fisher(g["kat_data"], g["kat_means"], g["kat_covs"], g["kat_priors"], flags)
+        assert np.max(np.abs(s - ref)) < 1e-10
+
+
+@pytest.mark.parametrize("tag", ["f", "d"])
+def test_posteriors(golden, restatement, tag):
+    g = golden
+    dt = DT[tag]
+    q, ll = restatement.posteriors(g["post_data"].astype(dt), g["post_priors"].astype(dt),
+                                   g["post_means"].astype(dt), g["post_covs"].astype(dt))
+    assert rel_err(q, g[f"post_q_{tag}"]) < TOL[tag]
+    assert abs(ll - float(g[f"post_ll_{tag}"])) <= TOL[tag] * abs(float(g[f"post_ll_{tag}"]))
+    assert np.all(q[:, 3] == 0)  # prior below 1e-6 -> log-weight -inf
+
+
+@pytest.mark.parametrize("tag", ["f", "d"])
+def test_em_iterations(golden, restatement, tag):
+    """Per-iteration parameters after t = 0..T EM iterations, restart included."""
+    g = golden
+    dt = DT[tag]
+    T = int(g["em_T"])
+    tol = {"f": 2e-4, "d": 1e-10}[tag]
+    for t in range(T + 1):
+        r = restatement.em(g["em_data"].astype(dt), g["em_priors0"], g["em_means0"], g["em_covs0"],
+                           g["em_lb"], t)
+        assert abs(r["ll"] - g[f"em_ll_{tag}"][t]) <= tol * abs(g[f"em_ll_{tag}"][t])
+        for name in ("priors", "means", "covs"):
+            assert rel_err(r[name], g[f"em_{name}_{tag}"][t]) < tol, (t, name)
+        if t == T:
+            assert r["restarts"] >= 1  # the seeded outlier mode is re-seeded
+            assert rel_err(r["posteriors"], g[f"em_post_{tag}"]) < tol
+
+
+@pytest.mark.parametrize("tag", ["f", "d"])
+@pytest.mark.parametrize("flags", FLAG_SETS)
+def test_fisher_case(golden, restatement, tag, flags):
+    g = golden
+    dt = DT[tag]
+    enc, nt = restatement.fisher(g["fv_data"].astype(dt), g["fv_means"].astype(dt),
+                                 g["fv_covs"].astype(dt), g["fv_priors"].astype(dt), flags)
+    assert rel_err(enc, g[f"fv_enc_{tag}_{flags}"]) < TOL[tag]
+    assert nt == int(g[f"fv_nterms_{tag}_{flags}"])
+    K, D = g["fv_means"].shape
+    assert np.all(enc[2 * D:3 * D] == 0) and np.all(enc[K * D + 2 * D:K * D + 3 * D] == 0)
+
+
+@pytest.mark.parametrize("tag", ["f", "d"])
+def test_fisher_edges(golden, restatement, tag):
+    g = golden
+    dt = DT[tag]
+    x, mu, cv, pr = (g["edge_data"], g["edge_means"], g["edge_covs"], g["edge_priors"])
+    for n in (0, 1, 3):
+        enc, _ = restatement.fisher(x[:n].astype(dt), mu.astype(dt), cv.astype(dt), pr.astype(dt),
+                                    FLAG_IMPROVED)
+        assert rel_err(enc, g[f"edge_enc_{tag}_n{n}"]) < TOL[tag]
+        if n == 0:
+            assert np.all(enc == 0)
+    enc, _ = restatement.fisher(x.astype(dt), mu[:1].astype(dt), cv[:1].astype(dt), np.ones(1, dt),
+                                FLAG_IMPROVED)
+    assert rel_err(enc, g[f"edge_enc_{tag}_k1"]) < TOL[tag]
+    enc, _ = restatement.fisher(x[:, :1].copy().astype(dt), mu[:, :1].copy().astype(dt),
+                                cv[:, :1].copy().astype(dt), pr.astype(dt), FLAG_IMPROVED)
+    assert rel_err(enc, g[f"edge_enc_{tag}_d1"]) < TOL[tag]
+
+
+def test_oracle_is_deterministic(golden, restatement):
+    g = golden
+    a = restatement.em(g["em_data"], g["em_priors0"], g["em_means0"], g["em_covs0"], g["em_lb"], 4)
+    b = restatement.em(g["em_data"], g["em_priors0"], g["em_means0"], g["em_covs0"], g["em_lb"], 4)
+    for n in ("priors", "means", "covs", "posteriors"):
+        assert np.array_equal(a[n], b[n])

@@ -1,0 +1,393 @@
+"""Python mirror of VLFeat's GMM / Fisher-vector C API over the B200 library.
+
+Everything here calls ``vlfeat_b200/lib/libvl.so`` through ctypes: the
+reference's own entry points (vl/gmm.h, vl/fisher.h) with host arrays, and
+the ``vlb200_*`` extensions with device tensors.  There is no CPU fallback:
+if the library is missing, :func:`lib` raises; if a call fails on the GPU,
+the library's last-error message is raised as :class:`VLError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libvl.so")
+
+VL_TYPE_FLOAT = 1
+VL_TYPE_DOUBLE = 2
+FLAG_SQUARE_ROOT = 1 << 0
+FLAG_NORMALIZED = 1 << 1
+FLAG_IMPROVED = FLAG_SQUARE_ROOT | FLAG_NORMALIZED
+FLAG_FAST = 1 << 2
+INIT_KMEANS, INIT_RAND, INIT_CUSTOM = 0, 1, 2  # VlGMMInitialization, vl/gmm.h:21-26
+
+PREC_DEFAULT, PREC_EXACT, PREC_FP32, PREC_BF16, PREC_BF16_ROUTER = 0, 1, 2, 3, 4
+PRECISIONS = {"default": 0, "exact": 1, "fp32": 2, "bf16": 3, "bf16_router": 4}
+
+_vp = C.c_void_p
+_sz = C.c_uint64
+
+
+class VLError(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def _decl(L):
+    def f(name, res, *args):
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = list(args)
+
+    f("vl_gmm_new", _vp, C.c_uint32, _sz, _sz)
+    f("vl_gmm_new_copy", _vp, _vp)
+    f("vl_gmm_delete", None, _vp)
+    f("vl_gmm_reset", None, _vp)
+    f("vl_gmm_cluster", C.c_double, _vp, _vp, _sz)
+    f("vl_gmm_em", C.c_double, _vp, _vp, _sz)
+    f("vl_gmm_init_with_rand_data", None, _vp, _vp, _sz)
+    f("vl_gmm_init_with_kmeans", None, _vp, _vp, _sz, _vp)
+    for n in ("means", "covariances", "priors"):
+        f("vl_gmm_set_" + n, None, _vp, _vp)
+        f("vl_gmm_get_" + n, _vp, _vp)
+    f("vl_gmm_get_posteriors", _vp, _vp)
+    f("vl_gmm_set_num_repetitions", None, _vp, _sz)
+    f("vl_gmm_set_max_num_iterations", None, _vp, _sz)
+    f("vl_gmm_set_verbosity", None, _vp, C.c_int)
+    f("vl_gmm_set_initialization", None, _vp, C.c_int)
+    f("vl_gmm_set_kmeans_init_object", None, _vp, _vp)
+    f("vl_gmm_set_covariance_lower_bounds", None, _vp, _vp)
+    f("vl_gmm_set_covariance_lower_bound", None, _vp, C.c_double)
+    f("vl_gmm_get_data_type", C.c_uint32, _vp)
+    for n in ("dimension", "num_repetitions", "num_data", "num_clusters", "max_num_iterations"):
+        f("vl_gmm_get_" + n, _sz, _vp)
+    f("vl_gmm_get_loglikelihood", C.c_double, _vp)
+    f("vl_gmm_get_verbosity", C.c_int, _vp)
+    f("vl_gmm_get_initialization", C.c_int, _vp)
+    f("vl_gmm_get_kmeans_init_object", _vp, _vp)
+    f("vl_gmm_get_covariance_lower_bounds", _vp, _vp)
+    for s in ("_f", "_d"):
+        f("vl_get_gmm_data_posteriors" + s, C.c_double, _vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp)
+    f("vl_fisher_encode", _sz, _vp, C.c_uint32, _vp, _sz, _sz, _vp, _vp, _vp, _sz, C.c_int)
+    f("vl_get_last_error", C.c_int)
+    f("vl_get_last_error_message", C.c_char_p)
+    f("vl_set_last_error", C.c_int, C.c_int, C.c_char_p)
+    f("vl_set_num_threads", None, _sz)
+    f("vl_get_max_threads", _sz)
+    f("vl_get_version_string", C.c_char_p)
+    f("vlb200_version", C.c_char_p)
+    f("vlb200_device_ok", C.c_int)
+    f("vlb200_set_precision", C.c_int, C.c_int)
+    f("vlb200_get_precision", C.c_int)
+    f("vlb200_launch_count", C.c_uint64)
+    f("vlb200_profile_enable", None, C.c_int)
+    f("vlb200_profile_reset", None)
+    f("vlb200_profile_read", C.c_int, C.c_char_p, _sz, _vp, _vp, _sz)
+    f("vlb200_gmm_posteriors_device", C.c_int, _vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp, C.c_int,
+      C.POINTER(C.c_double), _vp)
+    f("vlb200_gmm_em_device", C.c_double, _vp, _vp, _sz, C.c_int)
+    f("vlb200_gmm_get_ll_trace", _sz, _vp, _vp, _sz)
+    f("vlb200_gmm_get_num_restarts", _sz, _vp)
+    f("vlb200_fisher_encode_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _sz, C.c_int,
+      C.c_int, C.POINTER(C.c_uint64), _vp)
+    f("vlb200_fisher_encode_batch_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _sz,
+      C.c_int, C.c_int, _vp, _vp)
+
+
+def lib(path: str = LIB_PATH):
+    """Load the library (once).  Raises if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise VLError(f"{path} is missing: build it with `python -m vlfeat_b200.build`")
+        L = C.CDLL(path)
+        _decl(L)
+        _LIB = L
+    return _LIB
+
+
+def _raise_last(what: str):
+    L = lib()
+    msg = L.vl_get_last_error_message().decode(errors="replace")
+    raise VLError(f"{what}: {msg} (code {L.vl_get_last_error()})")
+
+
+def _clear():
+    lib().vl_set_last_error(0, None)
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(_vp)
+
+
+def _dt(dtype):
+    dt = np.dtype(dtype)
+    if dt == np.float32:
+        return VL_TYPE_FLOAT
+    if dt == np.float64:
+        return VL_TYPE_DOUBLE
+    raise TypeError("data must be float32 or float64")
+
+
+def _prec(p) -> int:
+    return PRECISIONS[p] if isinstance(p, str) else int(p)
+
+
+def set_precision(p) -> None:
+    if lib().vlb200_set_precision(_prec(p)):
+        _raise_last("vlb200_set_precision")
+
+
+def get_precision() -> int:
+    return int(lib().vlb200_get_precision())
+
+
+def device_ok() -> bool:
+    return bool(lib().vlb200_device_ok())
+
+
+def launch_count() -> int:
+    return int(lib().vlb200_launch_count())
+
+
+def profile_enable(on: bool = True) -> None:
+    lib().vlb200_profile_enable(1 if on else 0)
+
+
+def profile_reset() -> None:
+    lib().vlb200_profile_reset()
+
+
+def profile_read(max_entries: int = 64):
+    """{kernel name: (launches, total device ms)} since the last reset."""
+    stride = 64
+    names = C.create_string_buffer(stride * max_entries)
+    ms = np.zeros(max_entries, np.float64)
+    cnt = np.zeros(max_entries, np.uint64)
+    n = lib().vlb200_profile_read(names, stride, _np_ptr(ms), _np_ptr(cnt), max_entries)
+    out = {}
+    for i in range(min(n, max_entries)):
+        nm = names.raw[i * stride:(i + 1) * stride].split(b"\0", 1)[0].decode()
+        out[nm] = (int(cnt[i]), float(ms[i]))
+    return out
+
+
+# ------------------------------------------------------------------ GMM
+class GMM:
+    """``VlGMM`` (vl/gmm.h) on the GPU.  Arrays are NumPy, row-major:
+    data (N, D), means/covariances (K, D), priors (K,)."""
+
+    def __init__(self, dimension: int, num_clusters: int, dtype=np.float32):
+        self.dtype = np.dtype(dtype)
+        self.D, self.K = int(dimension), int(num_clusters)
+        _clear()
+        self._h = lib().vl_gmm_new(_dt(self.dtype), self.D, self.K)
+        if not self._h:
+            _raise_last("vl_gmm_new")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _LIB is not None:
+            _LIB.vl_gmm_delete(h)
+            self._h = None
+
+    def _arr(self, a, shape):
+        a = np.ascontiguousarray(a, self.dtype)
+        if a.shape != shape:
+            raise ValueError(f"expected shape {shape}, got {a.shape}")
+        return a
+
+    def set_means(self, m):
+        lib().vl_gmm_set_means(self._h, _np_ptr(self._arr(m, (self.K, self.D))))
+
+    def set_covariances(self, c):
+        lib().vl_gmm_set_covariances(self._h, _np_ptr(self._arr(c, (self.K, self.D))))
+
+    def set_priors(self, p):
+        lib().vl_gmm_set_priors(self._h, _np_ptr(self._arr(p, (self.K,))))
+
+    def set_initialization(self, init):
+        init = {"kmeans": INIT_KMEANS, "rand": INIT_RAND, "custom": INIT_CUSTOM}.get(init, init)
+        lib().vl_gmm_set_initialization(self._h, int(init))
+
+    def set_max_num_iterations(self, n):
+        lib().vl_gmm_set_max_num_iterations(self._h, int(n))
+
+    def set_num_repetitions(self, n):
+        lib().vl_gmm_set_num_repetitions(self._h, int(n))
+
+    def set_verbosity(self, v):
+        lib().vl_gmm_set_verbosity(self._h, int(v))
+
+    def set_covariance_lower_bound(self, b):
+        lb = np.asarray(b, np.float64)
+        if lb.ndim == 0:
+            lib().vl_gmm_set_covariance_lower_bound(self._h, float(lb))
+        else:
+            lb = np.ascontiguousarray(lb, np.float64).reshape(self.D)
+            lib().vl_gmm_set_covariance_lower_bounds(self._h, _np_ptr(lb))
+
+    def _data(self, data):
+        data = np.ascontiguousarray(data, self.dtype)
+        if data.ndim != 2 or data.shape[1] != self.D:
+            raise ValueError("data must be (N, D)")
+        return data
+
+    def cluster(self, data) -> float:
+        data = self._data(data)
+        _clear()
+        ll = lib().vl_gmm_cluster(self._h, _np_ptr(data), data.shape[0])
+        if lib().vl_get_last_error():
+            _raise_last("vl_gmm_cluster")
+        return ll
+
+    def em(self, data) -> float:
+        data = self._data(data)
+        _clear()
+        ll = lib().vl_gmm_em(self._h, _np_ptr(data), data.shape[0])
+        if lib().vl_get_last_error():
+            _raise_last("vl_gmm_em")
+        return ll
+
+    def em_device(self, data_t, precision="default") -> float:
+        """EM on a (N, D) float32 CUDA tensor (vlb200_gmm_em_device)."""
+        _clear()
+        ll = lib().vlb200_gmm_em_device(self._h, data_t.data_ptr(), data_t.shape[0], _prec(precision))
+        if lib().vl_get_last_error():
+            _raise_last("vlb200_gmm_em_device")
+        return ll
+
+    def _get(self, fn, n):
+        ct = C.c_float if self.dtype == np.float32 else C.c_double
+        p = fn(self._h)
+        if not p:
+            _raise_last("getter")
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape=(n,)).copy()
+
+    @property
+    def means(self):
+        return self._get(lib().vl_gmm_get_means, self.K * self.D).reshape(self.K, self.D)
+
+    @property
+    def covariances(self):
+        return self._get(lib().vl_gmm_get_covariances, self.K * self.D).reshape(self.K, self.D)
+
+    @property
+    def priors(self):
+        return self._get(lib().vl_gmm_get_priors, self.K)
+
+    @property
+    def posteriors(self):
+        n = int(lib().vl_gmm_get_num_data(self._h))
+        return self._get(lib().vl_gmm_get_posteriors, n * self.K).reshape(n, self.K)
+
+    @property
+    def loglikelihood(self) -> float:
+        return float(lib().vl_gmm_get_loglikelihood(self._h))
+
+    @property
+    def num_data(self) -> int:
+        return int(lib().vl_gmm_get_num_data(self._h))
+
+    @property
+    def ll_trace(self):
+        buf = np.zeros(4096, np.float64)
+        n = lib().vlb200_gmm_get_ll_trace(self._h, _np_ptr(buf), buf.size)
+        return buf[:n].copy()
+
+    @property
+    def num_restarts(self) -> int:
+        return int(lib().vlb200_gmm_get_num_restarts(self._h))
+
+
+def get_gmm_data_posteriors(data, priors, means, covariances):
+    """vl_get_gmm_data_posteriors_{f,d} (vl/gmm.h:94-112) -> (posteriors, LL)."""
+    data = np.ascontiguousarray(data)
+    dt = data.dtype
+    N, D = data.shape
+    K = len(priors)
+    post = np.zeros((N, K), dt)
+    fn = lib().vl_get_gmm_data_posteriors_f if dt == np.float32 else lib().vl_get_gmm_data_posteriors_d
+    _dt(dt)
+    _clear()
+    ll = fn(_np_ptr(post), K, N, _np_ptr(np.ascontiguousarray(priors, dt)),
+            _np_ptr(np.ascontiguousarray(means, dt)), D,
+            _np_ptr(np.ascontiguousarray(covariances, dt)), _np_ptr(data))
+    if lib().vl_get_last_error():
+        _raise_last("vl_get_gmm_data_posteriors")
+    return post, ll
+
+
+def fisher_encode(data, means, covariances, priors, flags=FLAG_IMPROVED):
+    """vl_fisher_encode (vl/fisher.h:48-54) -> (enc of 2KD, numTerms)."""
+    data = np.ascontiguousarray(data)
+    dt = data.dtype
+    typ = _dt(dt)
+    N, D = data.shape
+    K = len(priors)
+    enc = np.zeros(2 * K * D, dt)
+    _clear()
+    nt = lib().vl_fisher_encode(_np_ptr(enc), typ, _np_ptr(np.ascontiguousarray(means, dt)), D, K,
+                                _np_ptr(np.ascontiguousarray(covariances, dt)),
+                                _np_ptr(np.ascontiguousarray(priors, dt)), _np_ptr(data), N,
+                                int(flags))
+    if lib().vl_get_last_error():
+        _raise_last("vl_fisher_encode")
+    return enc, int(nt)
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def gmm_posteriors_device(post_t, priors_t, means_t, covs_t, data_t, precision="default",
+                          stream=None) -> float:
+    ll = C.c_double(0)
+    N, D = data_t.shape
+    K = priors_t.shape[0]
+    _clear()
+    rc = lib().vlb200_gmm_posteriors_device(post_t.data_ptr(), K, N, priors_t.data_ptr(),
+                                            means_t.data_ptr(), D, covs_t.data_ptr(),
+                                            data_t.data_ptr(), _prec(precision), C.byref(ll),
+                                            _stream(stream))
+    if rc:
+        _raise_last("vlb200_gmm_posteriors_device")
+    return ll.value
+
+
+def fisher_encode_device(enc_t, means_t, covs_t, priors_t, data_t, flags=FLAG_IMPROVED,
+                         precision="default", stream=None) -> int:
+    N, D = data_t.shape
+    K = priors_t.shape[0]
+    nt = C.c_uint64(0)
+    _clear()
+    rc = lib().vlb200_fisher_encode_device(enc_t.data_ptr(), means_t.data_ptr(), D, K,
+                                           covs_t.data_ptr(), priors_t.data_ptr(),
+                                           data_t.data_ptr(), N, int(flags), _prec(precision),
+                                           C.byref(nt), _stream(stream))
+    if rc:
+        _raise_last("vlb200_fisher_encode_device")
+    return int(nt.value)
+
+
+def fisher_encode_batch_device(enc_t, means_t, covs_t, priors_t, data_t, offsets,
+                               flags=FLAG_IMPROVED, precision="default", nterms_t=None,
+                               stream=None) -> None:
+    """Encode len(offsets)-1 images in one call; enc_t is (numImages, 2KD)."""
+    offs = np.ascontiguousarray(offsets, np.int64)
+    D = data_t.shape[1]
+    K = priors_t.shape[0]
+    _clear()
+    rc = lib().vlb200_fisher_encode_batch_device(
+        enc_t.data_ptr(), means_t.data_ptr(), D, K, covs_t.data_ptr(), priors_t.data_ptr(),
+        data_t.data_ptr(), _np_ptr(offs), len(offs) - 1, int(flags), _prec(precision),
+        nterms_t.data_ptr() if nterms_t is not None else None, _stream(stream))
+    if rc:
+        _raise_last("vlb200_fisher_encode_batch_device")

@@ -1,0 +1,110 @@
+// Internal plumbing shared by the host-side API files and the kernel files:
+// CUDA error handling, per-thread streams, grow-only device scratch, launch
+// accounting and optional per-kernel event timing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+extern "C" {
+#include "vl/generic.h"
+}
+
+namespace vlb {
+
+// An error that the C boundary turns into vl_set_last_error + a sentinel.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char *what, const char *file, int line);
+
+#define VLB_CUDA(x)                                                   \
+  do {                                                                \
+    cudaError_t e_ = (x);                                             \
+    if (e_ != cudaSuccess) ::vlb::throw_cuda(e_, #x, __FILE__, __LINE__); \
+  } while (0)
+
+#define VLB_CHECK(cond, code, msg)                     \
+  do {                                                 \
+    if (!(cond)) throw ::vlb::Error((code), (msg));   \
+  } while (0)
+
+// The calling thread's library stream (non-blocking, created on first use).
+cudaStream_t thread_stream();
+inline cudaStream_t pick_stream(void *s) { return s ? (cudaStream_t)s : thread_stream(); }
+
+// Launch accounting: every kernel launch of the library goes through
+// launch_begin/launch_end (the LAUNCH macro below).
+void launch_begin(const char *name, cudaStream_t s);
+void launch_end(const char *name, cudaStream_t s);
+
+#define VLB_LAUNCH(name, stream, ...)           \
+  do {                                          \
+    ::vlb::launch_begin((name), (stream));      \
+    __VA_ARGS__;                                \
+    VLB_CUDA(cudaGetLastError());               \
+    ::vlb::launch_end((name), (stream));        \
+  } while (0)
+
+// Grow-only device buffer.  Contents are not preserved across growth.
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    // Kernels still queued may read the old buffer: drain the device first.
+    if (p) {
+      cudaDeviceSynchronize();
+      cudaFree(p);
+    }
+    p = nullptr;
+    cap = 0;
+  }
+  template <typename T>
+  T *get(size_t count) {
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    if (bytes > cap) {
+      release();
+      size_t want = bytes + bytes / 8;
+      cudaError_t e = cudaMalloc(&p, want);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        throw Error(VL_ERR_ALLOC, std::string("cudaMalloc of ") + std::to_string(want) +
+                                      " bytes failed: " + cudaGetErrorString(e));
+      }
+      cap = want;
+    }
+    return static_cast<T *>(p);
+  }
+};
+
+// Per-thread scratch arena: named slots reused across calls on one thread.
+struct Scratch {
+  DevBuf slot[32];
+  DevBuf host_pinned_unused;
+};
+Scratch &thread_scratch();
+
+// Pinned host staging buffer (per thread), for host-pointer API calls.
+void *pinned_host(size_t bytes);
+
+// Process-wide precision default (VLB200_PREC_*).
+int default_precision();
+int resolve_precision(int precision, bool is_double);
+
+// Host-side printf through the VLFeat hook.
+#define VLB_PRINTF(...) ((*vl_get_printf_func())(__VA_ARGS__))
+
+}  // namespace vlb

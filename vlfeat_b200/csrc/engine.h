@@ -1,0 +1,93 @@
+// Device-side engine of the GMM / Fisher-vector path.  Everything here takes
+// device pointers and a stream; the C API files (gmm_api.cpp, fisher_api.cpp)
+// stage host data and call these.
+//
+// Layouts (VLFeat's, vl/gmm.c:711-798): data[i*D + d], means/covs[k*D + d],
+// priors[k], posteriors q[i*K + k]; Fisher vector [u_1..u_K | v_1..v_K].
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "common.h"
+
+namespace vlb {
+
+using i64 = long long;
+
+// Model parameters on the device, data type T.
+template <typename T>
+struct DevModel {
+  const T *means = nullptr, *covs = nullptr, *priors = nullptr;
+  i64 K = 0, D = 0;
+};
+
+// Derived per-component constants for the exact E-step (vl/gmm.c:741-756):
+// inv = 1/sigma^2, cst = log w - (D/2) log 2pi - (1/2) sum log sigma^2
+// (-inf when the prior is below 1e-6), sis = sqrt(1/sigma^2) (vl/fisher.c:388).
+template <typename T>
+struct DevDerived {
+  T *inv = nullptr;
+  double *cst = nullptr;
+  T *sis = nullptr;
+};
+
+// ---------------------------------------------------------------- exact path
+template <typename T>
+void exact_prepare(const DevModel<T> &m, DevDerived<T> &der, cudaStream_t s);
+
+// E-step over rows [0, N): q (N x K) receives posteriors; per-block LL partials
+// go to ll_part (size >= estep_ll_parts(N)); if fast, q is replaced by the
+// one-hot arg-max (vl/fisher.c:398-417).
+i64 estep_ll_parts(i64 N);
+template <typename T>
+void exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,
+                 double *ll_part, bool fast, cudaStream_t s);
+
+// Deterministic sum of n doubles into *out (device).
+void sum_doubles(const double *part, i64 n, double *out, cudaStream_t s);
+
+// M-step (vl/gmm.c:1036-1213) in place on means/covs/priors (device, type T):
+// thresholded sufficient statistics, old-mean correction, bounds, prior
+// normalisation.  lb: D doubles (device).
+template <typename T>
+void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i64 K, i64 D,
+                 const double *lb, cudaStream_t s);
+
+// Un-thresholded posterior mass per component (vl/gmm.c:835-844), K doubles.
+template <typename T>
+void column_mass(const T *q, i64 N, i64 K, double *mass, cudaStream_t s);
+
+// Hard split of mode `best` into empty mode `icl` along dimension `dim`
+// (vl/gmm.c:969-989).
+template <typename T>
+void restart_split(T *q, const T *X, i64 N, i64 K, i64 D, i64 icl, i64 best, i64 dim, T cut,
+                   cudaStream_t s);
+
+// Variance floor applied on device (vl/gmm.c:1005-1030).
+template <typename T>
+void apply_bounds(T *covs, i64 K, i64 D, const double *lb, cudaStream_t s);
+
+// --------------------------------------------------------------- Fisher
+// One image segment: rows [row0, row1) of image `image`; q rows are indexed
+// relative to the chunk's first row.
+struct Segment {
+  i64 image, row0, row1;
+};
+
+// Batched Fisher encoding with the exact path.  h_offsets: numImages+1 host
+// array.  enc: numImages x 2KD (device).  nterms: numImages (device) or null.
+template <typename T>
+void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const DevModel<T> &m,
+                        T *enc, unsigned long long *nterms, int flags, cudaStream_t s);
+
+// ------------------------------------------------------- tensor-core path
+// Implemented in k_tc.cu.  Available for float data only.
+bool tc_supported(i64 K, i64 D);
+void tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
+              bool fast, int precision, cudaStream_t s);
+void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages,
+                     const DevModel<float> &m, float *enc, unsigned long long *nterms, int flags,
+                     int precision, cudaStream_t s);
+
+}  // namespace vlb

@@ -1,0 +1,537 @@
+// VLFeat's GMM object and EM driver (vl/gmm.h) on the GPU.
+//
+// The object keeps VLFeat's host-memory contract: means / covariances /
+// priors / posteriors are host arrays owned by the object, getters return
+// borrowed pointers (vl/gmm.c:430-675), setters copy in.  EM runs on the GPU:
+// the data is staged to device memory once per call, parameters live on the
+// device during the loop and are copied back at the end; posteriors are
+// copied back lazily on the first vl_gmm_get_posteriors() call.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+
+extern "C" {
+#include "vl/gmm.h"
+#include "vlb200.h"
+}
+
+using vlb::i64;
+
+struct _VlGMM {
+  vl_type dataType = VL_TYPE_FLOAT;
+  vl_size dimension = 0, numClusters = 0, numData = 0;
+  vl_size maxNumIterations = 50, numRepetitions = 1;  // defaults, vl/gmm.c:365-380
+  int verbosity = 0;
+  void *means = nullptr, *covariances = nullptr, *priors = nullptr;
+  void *posteriors = nullptr;
+  vl_size posteriorsCap = 0;  // rows the host posterior buffer can hold
+  double *sigmaLowBound = nullptr;
+  VlGMMInitialization initialization = VlGMMRand;
+  VlKMeans *kmeansInit = nullptr;
+  double LL = 0;
+  // GPU state.
+  bool postOnDevice = false;  // the device buffer holds the current posteriors
+  vlb::DevBuf dX, dq, dmeans, dcovs, dpriors, dlb, dtmp;
+  std::vector<double> llTrace;
+  vl_size numRestarts = 0;
+};
+
+namespace {
+
+size_t tsize(vl_type t) { return t == VL_TYPE_DOUBLE ? 8 : 4; }
+
+void check_type(vl_type t) {
+  VLB_CHECK(t == VL_TYPE_FLOAT || t == VL_TYPE_DOUBLE, VL_ERR_BAD_ARG,
+            "data type must be VL_TYPE_FLOAT or VL_TYPE_DOUBLE");
+}
+
+template <typename F>
+auto guarded(F &&f, decltype(f()) sentinel) -> decltype(f()) {
+  try {
+    return f();
+  } catch (const vlb::Error &e) {
+    vl_set_last_error(e.code, "%s", e.what());
+  } catch (const std::exception &e) {
+    vl_set_last_error(VL_ERR_ALLOC, "%s", e.what());
+  }
+  return sentinel;
+}
+
+// Host copy of the posteriors, refreshed from the device when stale.
+void sync_posteriors(VlGMM *self) {
+  if (!self->postOnDevice) return;
+  const size_t bytes = tsize(self->dataType) * self->numData * self->numClusters;
+  if (self->posteriorsCap < self->numData || !self->posteriors) {
+    vl_free(self->posteriors);
+    self->posteriors = vl_malloc(bytes ? bytes : 1);
+    self->posteriorsCap = self->numData;
+  }
+  cudaStream_t s = vlb::thread_stream();
+  if (bytes) VLB_CUDA(cudaMemcpyAsync(self->posteriors, self->dq.p, bytes, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  self->postOnDevice = false;
+}
+
+template <typename T>
+double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int precision,
+                    bool fast, cudaStream_t s) {
+  vlb::Scratch &sc = vlb::thread_scratch();
+  double *llp = sc.slot[15].get<double>(vlb::estep_ll_parts(N));
+  double *dll = sc.slot[16].get<double>(1);
+  bool done = false;
+  if constexpr (sizeof(T) == 4) {
+    if (precision != VLB200_PREC_EXACT && vlb::tc_supported(m.K, m.D)) {
+      vlb::tc_estep(dX, N, m, dq, llp, fast, precision, s);
+      done = true;
+    }
+  }
+  if (!done) {
+    vlb::DevDerived<T> der;
+    der.inv = sc.slot[17].get<T>(m.K * m.D);
+    der.sis = sc.slot[18].get<T>(m.K * m.D);
+    der.cst = sc.slot[19].get<double>(m.K);
+    vlb::exact_prepare(m, der, s);
+    vlb::exact_estep(dX, N, m, der, dq, llp, fast, s);
+  }
+  if (N <= 0) return 0.0;
+  vlb::sum_doubles(llp, vlb::estep_ll_parts(N), dll, s);
+  double ll = 0;
+  VLB_CUDA(cudaMemcpyAsync(&ll, dll, sizeof(double), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  return ll;
+}
+
+// Empty-mode restarts, vl/gmm.c:814-999, with the posteriors and parameters
+// on the device and the (cheap) selection logic on the host.
+template <typename T>
+vl_size restart_empty_modes(VlGMM *self, const T *dX, i64 N, T *dq, T *dmeans, T *dcovs,
+                            T *dpriors, const double *dlb, cudaStream_t s) {
+  const i64 K = (i64)self->numClusters, D = (i64)self->dimension;
+  if (K <= 1) return 0;
+  double *dmass = self->dtmp.get<double>(K);
+  vlb::column_mass(dq, N, K, dmass, s);
+  std::vector<double> mass(K);
+  VLB_CUDA(cudaMemcpyAsync(mass.data(), dmass, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  const double cutoff = 1e-2 * std::max(1.0, (double)N / (double)K);
+  vl_size nsplit = 0;
+  std::vector<T> pr(K), cv(K * D), mu(K * D);
+  bool have = false;
+  for (i64 icl = 0; icl < K; ++icl) {
+    if (mass[icl] >= cutoff) continue;
+    if (self->verbosity) VLB_PRINTF("gmm: mode %d is nearly empty (mass %f)\n", (int)icl, mass[icl]);
+    if (!have) {
+      VLB_CUDA(cudaMemcpyAsync(pr.data(), dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaMemcpyAsync(cv.data(), dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaMemcpyAsync(mu.data(), dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaStreamSynchronize(s));
+      have = true;
+    }
+    // Mode with the largest entropy contribution, vl/gmm.c:920-939.
+    double bestScore = -INFINITY;
+    i64 best = -1;
+    for (i64 j = 0; j < K; ++j) {
+      if ((double)pr[j] < 1e-6) continue;
+      double sc = 0.5 * (double)D * (1.0 + log(2 * 3.141592653589793));
+      for (i64 d = 0; d < D; ++d) sc += 0.5 * log((double)cv[j * D + d]);
+      sc = (double)pr[j] * (sc - log((double)pr[j]));
+      if (sc > bestScore) {
+        bestScore = sc;
+        best = j;
+      }
+    }
+    if (best == icl || best < 0) {
+      if (self->verbosity)
+        VLB_PRINTF("gmm: mode %d is empty, but no other mode to split could be found\n", (int)icl);
+      continue;
+    }
+    if (self->verbosity)
+      VLB_PRINTF("gmm: reinitializing empty mode %d with mode %d (prior %f, mass %f, score %f)\n",
+                 (int)icl, (int)best, (double)pr[best], mass[best], bestScore);
+    // Largest-variance dimension, vl/gmm.c:958-966.
+    double bv = -INFINITY;
+    i64 bd = -1;
+    for (i64 d = 0; d < D; ++d)
+      if ((double)cv[best * D + d] > bv) {
+        bv = (double)cv[best * D + d];
+        bd = d;
+      }
+    vlb::restart_split<T>(dq, dX, N, K, D, icl, best, bd, mu[best * D + bd], s);
+    vlb::exact_mstep<T>(dX, N, dq, dmeans, dcovs, dpriors, K, D, dlb, s);
+    VLB_CUDA(cudaMemcpyAsync(pr.data(), dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaMemcpyAsync(cv.data(), dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaMemcpyAsync(mu.data(), dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+    ++nsplit;
+  }
+  return nsplit;
+}
+
+// The EM loop, vl/gmm.c:1220-1308, on device-resident data dX (N x D).
+template <typename T>
+double em_device(VlGMM *self, const T *dX, i64 N, int precision) {
+  cudaStream_t s = vlb::thread_stream();
+  const i64 K = (i64)self->numClusters, D = (i64)self->dimension;
+  T *dmeans = self->dmeans.get<T>(K * D);
+  T *dcovs = self->dcovs.get<T>(K * D);
+  T *dpriors = self->dpriors.get<T>(K);
+  double *dlb = self->dlb.get<double>(D);
+  T *dq = self->dq.get<T>(std::max<i64>(1, N) * K);
+  VLB_CUDA(cudaMemcpyAsync(dmeans, self->means, sizeof(T) * K * D, cudaMemcpyHostToDevice, s));
+  VLB_CUDA(cudaMemcpyAsync(dcovs, self->covariances, sizeof(T) * K * D, cudaMemcpyHostToDevice, s));
+  VLB_CUDA(cudaMemcpyAsync(dpriors, self->priors, sizeof(T) * K, cudaMemcpyHostToDevice, s));
+  VLB_CUDA(cudaMemcpyAsync(dlb, self->sigmaLowBound, sizeof(double) * D, cudaMemcpyHostToDevice, s));
+  self->numData = (vl_size)N;  // _vl_gmm_prepare_for_data, vl/gmm.c:336-344
+  self->llTrace.clear();
+  self->numRestarts = 0;
+
+  vlb::DevModel<T> m;
+  m.means = dmeans;
+  m.covs = dcovs;
+  m.priors = dpriors;
+  m.K = K;
+  m.D = D;
+
+  vlb::apply_bounds<T>(dcovs, K, D, dlb, s);  // vl/gmm.c:1233
+  double prevLL = -INFINITY, LL = -INFINITY;
+  for (vl_size it = 0;; ++it) {
+    LL = device_estep<T>(dX, N, m, dq, precision, false, s);
+    self->llTrace.push_back(LL);
+    if (self->verbosity)
+      VLB_PRINTF("gmm: em: iteration %d: loglikelihood = %f (variation = %f)\n", (int)it, LL,
+                 LL - prevLL);
+    if (it >= self->maxNumIterations) {
+      if (self->verbosity)
+        VLB_PRINTF("gmm: em: terminating because the maximum number of iterations (%d) has been reached.\n",
+                   (int)self->maxNumIterations);
+      break;
+    }
+    const double eps = fabs((LL - prevLL) / LL);
+    if (it > 0 && eps < 0.00001) {
+      if (self->verbosity)
+        VLB_PRINTF("gmm: em: terminating because the algorithm fully converged (log-likelihood variation = %f).\n",
+                   eps);
+      break;
+    }
+    prevLL = LL;
+    if (it > 1) {
+      vl_size r = restart_empty_modes<T>(self, dX, N, dq, dmeans, dcovs, dpriors, dlb, s);
+      self->numRestarts += r;
+      if (r > 0 && self->verbosity)
+        VLB_PRINTF("gmm: em: %d Gaussian modes restarted because they had become empty.\n", (int)r);
+    }
+    vlb::exact_mstep<T>(dX, N, dq, dmeans, dcovs, dpriors, K, D, dlb, s);
+  }
+  VLB_CUDA(cudaMemcpyAsync(self->means, dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaMemcpyAsync(self->covariances, dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaMemcpyAsync(self->priors, dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  self->postOnDevice = true;
+  return LL;
+}
+
+template <typename T>
+const T *stage_data(VlGMM *self, const void *data, i64 N) {
+  const i64 D = (i64)self->dimension;
+  T *dX = self->dX.get<T>(std::max<i64>(1, N) * D);
+  if (N > 0) {
+    cudaStream_t s = vlb::thread_stream();
+    VLB_CUDA(cudaMemcpyAsync(dX, data, sizeof(T) * N * D, cudaMemcpyHostToDevice, s));
+  }
+  return dX;
+}
+
+double em_host(VlGMM *self, const void *data, vl_size N) {
+  const int prec = vlb::resolve_precision(VLB200_PREC_DEFAULT, self->dataType == VL_TYPE_DOUBLE);
+  if (self->dataType == VL_TYPE_FLOAT)
+    return em_device<float>(self, stage_data<float>(self, data, (i64)N), (i64)N, prec);
+  return em_device<double>(self, stage_data<double>(self, data, (i64)N), (i64)N, prec);
+}
+
+}  // namespace
+
+extern "C" {
+
+VlGMM *vl_gmm_new(vl_type dataType, vl_size dimension, vl_size numComponents) {
+  return guarded(
+      [&]() -> VlGMM * {
+        check_type(dataType);
+        VlGMM *self = new VlGMM();
+        const size_t sz = tsize(dataType);
+        self->dataType = dataType;
+        self->dimension = dimension;
+        self->numClusters = numComponents;
+        self->priors = vl_calloc(numComponents ? numComponents : 1, sz);
+        self->means = vl_calloc(numComponents * dimension ? numComponents * dimension : 1, sz);
+        self->covariances = vl_calloc(numComponents * dimension ? numComponents * dimension : 1, sz);
+        self->sigmaLowBound = (double *)vl_calloc(dimension ? dimension : 1, sizeof(double));
+        for (vl_size i = 0; i < dimension; ++i) self->sigmaLowBound[i] = 1e-4;
+        return self;
+      },
+      (VlGMM *)nullptr);
+}
+
+VlGMM *vl_gmm_new_copy(VlGMM const *self) {
+  VlGMM *g = vl_gmm_new(self->dataType, self->dimension, self->numClusters);
+  if (!g) return g;
+  const size_t sz = tsize(self->dataType);
+  g->initialization = self->initialization;
+  g->maxNumIterations = self->maxNumIterations;
+  g->numRepetitions = self->numRepetitions;
+  g->verbosity = self->verbosity;
+  g->LL = self->LL;
+  memcpy(g->means, self->means, sz * self->numClusters * self->dimension);
+  memcpy(g->covariances, self->covariances, sz * self->numClusters * self->dimension);
+  memcpy(g->priors, self->priors, sz * self->numClusters);
+  return g;
+}
+
+void vl_gmm_reset(VlGMM *self) {
+  if (self->posteriors) {
+    vl_free(self->posteriors);
+    self->posteriors = nullptr;
+    self->posteriorsCap = 0;
+  }
+  self->numData = 0;
+  self->postOnDevice = false;
+  self->kmeansInit = nullptr;
+}
+
+void vl_gmm_delete(VlGMM *self) {
+  if (!self) return;
+  vl_free(self->means);
+  vl_free(self->covariances);
+  vl_free(self->priors);
+  vl_free(self->posteriors);
+  vl_free(self->sigmaLowBound);
+  delete self;
+}
+
+// -------------------------------------------------------------- getters
+vl_type vl_gmm_get_data_type(VlGMM const *self) { return self->dataType; }
+vl_size vl_gmm_get_num_clusters(VlGMM const *self) { return self->numClusters; }
+vl_size vl_gmm_get_num_data(VlGMM const *self) { return self->numData; }
+double vl_gmm_get_loglikelihood(VlGMM const *self) { return self->LL; }
+int vl_gmm_get_verbosity(VlGMM const *self) { return self->verbosity; }
+void vl_gmm_set_verbosity(VlGMM *self, int v) { self->verbosity = v; }
+void const *vl_gmm_get_means(VlGMM const *self) { return self->means; }
+void const *vl_gmm_get_covariances(VlGMM const *self) { return self->covariances; }
+void const *vl_gmm_get_priors(VlGMM const *self) { return self->priors; }
+void const *vl_gmm_get_posteriors(VlGMM const *self) {
+  VlGMM *m = const_cast<VlGMM *>(self);
+  guarded(
+      [&]() -> int {
+        sync_posteriors(m);
+        return 0;
+      },
+      0);
+  return m->posteriors;
+}
+vl_size vl_gmm_get_max_num_iterations(VlGMM const *self) { return self->maxNumIterations; }
+void vl_gmm_set_max_num_iterations(VlGMM *self, vl_size n) { self->maxNumIterations = n; }
+vl_size vl_gmm_get_num_repetitions(VlGMM const *self) { return self->numRepetitions; }
+void vl_gmm_set_num_repetitions(VlGMM *self, vl_size n) {
+  if (n < 1) {
+    vl_set_last_error(VL_ERR_BAD_ARG, "vl_gmm_set_num_repetitions: must be >= 1");
+    return;
+  }
+  self->numRepetitions = n;
+}
+vl_size vl_gmm_get_dimension(VlGMM const *self) { return self->dimension; }
+VlGMMInitialization vl_gmm_get_initialization(VlGMM const *self) { return self->initialization; }
+void vl_gmm_set_initialization(VlGMM *self, VlGMMInitialization init) { self->initialization = init; }
+VlKMeans *vl_gmm_get_kmeans_init_object(VlGMM const *self) { return self->kmeansInit; }
+void vl_gmm_set_kmeans_init_object(VlGMM *self, VlKMeans *k) { self->kmeansInit = k; }
+double const *vl_gmm_get_covariance_lower_bounds(VlGMM const *self) { return self->sigmaLowBound; }
+void vl_gmm_set_covariance_lower_bounds(VlGMM *self, double const *b) {
+  memcpy(self->sigmaLowBound, b, sizeof(double) * self->dimension);
+}
+void vl_gmm_set_covariance_lower_bound(VlGMM *self, double b) {
+  for (vl_size i = 0; i < self->dimension; ++i) self->sigmaLowBound[i] = b;
+}
+
+// -------------------------------------------------------------- setters
+void vl_gmm_set_means(VlGMM *self, void const *means) {
+  memcpy(self->means, means, self->dimension * self->numClusters * tsize(self->dataType));
+}
+void vl_gmm_set_covariances(VlGMM *self, void const *covs) {
+  memcpy(self->covariances, covs, self->dimension * self->numClusters * tsize(self->dataType));
+}
+void vl_gmm_set_priors(VlGMM *self, void const *priors) {
+  memcpy(self->priors, priors, self->numClusters * tsize(self->dataType));
+}
+
+// -------------------------------------------------------- processing
+void vl_gmm_init_with_rand_data(VlGMM *self, void const *, vl_size) {
+  vl_set_last_error(VL_ERR_BAD_ARG,
+                    "vl_gmm_init_with_rand_data: random (kmeans++) initialisation is not "
+                    "available in the GPU library; use VlGMMCustom");
+  (void)self;
+}
+
+void vl_gmm_init_with_kmeans(VlGMM *self, void const *, vl_size, VlKMeans *) {
+  vl_set_last_error(VL_ERR_BAD_ARG,
+                    "vl_gmm_init_with_kmeans: k-means initialisation is not available in the GPU "
+                    "library; use VlGMMCustom");
+  (void)self;
+}
+
+double vl_gmm_em(VlGMM *self, void const *data, vl_size numData) {
+  return guarded([&]() -> double { return em_host(self, data, numData); }, (double)NAN);
+}
+
+// vl_gmm_cluster, vl/gmm.c:1557-1648.  With VlGMMCustom every repetition
+// starts from the parameters present at entry (the reference reuses buffers
+// whose contents are undefined after the first repetition).
+double vl_gmm_cluster(VlGMM *self, void const *data, vl_size numData) {
+  return guarded(
+      [&]() -> double {
+        VLB_CHECK(self->initialization == VlGMMCustom, VL_ERR_BAD_ARG,
+                  "vl_gmm_cluster: only VlGMMCustom initialisation is available in the GPU "
+                  "library");
+        const size_t sz = tsize(self->dataType);
+        const size_t nKD = self->numClusters * self->dimension;
+        std::vector<char> m0((char *)self->means, (char *)self->means + sz * nKD);
+        std::vector<char> c0((char *)self->covariances, (char *)self->covariances + sz * nKD);
+        std::vector<char> p0((char *)self->priors, (char *)self->priors + sz * self->numClusters);
+        std::vector<char> bm, bc, bp;
+        double bestLL = -INFINITY;
+        bool bestOnDevice = false;
+        const int prec = vlb::resolve_precision(VLB200_PREC_DEFAULT, self->dataType == VL_TYPE_DOUBLE);
+        const void *dX = self->dataType == VL_TYPE_FLOAT
+                             ? (const void *)stage_data<float>(self, data, (i64)numData)
+                             : (const void *)stage_data<double>(self, data, (i64)numData);
+        for (vl_size rep = 0; rep < self->numRepetitions; ++rep) {
+          if (self->verbosity)
+            VLB_PRINTF("gmm: clustering: starting repetition %d of %d\n", (int)rep + 1,
+                       (int)self->numRepetitions);
+          if (rep > 0) {
+            memcpy(self->means, m0.data(), m0.size());
+            memcpy(self->covariances, c0.data(), c0.size());
+            memcpy(self->priors, p0.data(), p0.size());
+          }
+          double LL = self->dataType == VL_TYPE_FLOAT
+                          ? em_device<float>(self, (const float *)dX, (i64)numData, prec)
+                          : em_device<double>(self, (const double *)dX, (i64)numData, prec);
+          if (LL > bestLL || rep == 0) {
+            bestLL = LL;
+            bm.assign((char *)self->means, (char *)self->means + m0.size());
+            bc.assign((char *)self->covariances, (char *)self->covariances + c0.size());
+            bp.assign((char *)self->priors, (char *)self->priors + p0.size());
+            // Posteriors of the best repetition: only the last repetition's are
+            // on the device; materialise earlier winners on the host now.
+            if (self->numRepetitions > 1) {
+              sync_posteriors(self);
+              bestOnDevice = false;
+            } else {
+              bestOnDevice = true;
+            }
+          }
+        }
+        if (self->numRepetitions > 1) {
+          memcpy(self->means, bm.data(), bm.size());
+          memcpy(self->covariances, bc.data(), bc.size());
+          memcpy(self->priors, bp.data(), bp.size());
+        }
+        self->postOnDevice = bestOnDevice;  // else the host copy holds the winner's
+        self->LL = bestLL;
+        if (self->verbosity)
+          VLB_PRINTF("gmm: all repetitions terminated with final loglikelihood %f\n", self->LL);
+        return bestLL;
+      },
+      (double)NAN);
+}
+
+// Stand-alone E-step with host pointers, vl/gmm.c:711-798.
+static double posteriors_host(vl_type t, void *post, vl_size K, vl_size N, const void *priors,
+                              const void *means, vl_size D, const void *covs, const void *data) {
+  return guarded(
+      [&]() -> double {
+        VLB_CHECK(K >= 1 && D >= 1, VL_ERR_BAD_ARG, "numClusters and dimension must be >= 1");
+        cudaStream_t s = vlb::thread_stream();
+        vlb::Scratch &sc = vlb::thread_scratch();
+        const size_t sz = tsize(t);
+        char *dX = sc.slot[20].get<char>(sz * std::max<vl_size>(1, N) * D);
+        char *dm = sc.slot[21].get<char>(sz * K * D);
+        char *dc = sc.slot[22].get<char>(sz * K * D);
+        char *dp = sc.slot[23].get<char>(sz * K);
+        char *dq = sc.slot[24].get<char>(sz * std::max<vl_size>(1, N) * K);
+        if (N) VLB_CUDA(cudaMemcpyAsync(dX, data, sz * N * D, cudaMemcpyHostToDevice, s));
+        VLB_CUDA(cudaMemcpyAsync(dm, means, sz * K * D, cudaMemcpyHostToDevice, s));
+        VLB_CUDA(cudaMemcpyAsync(dc, covs, sz * K * D, cudaMemcpyHostToDevice, s));
+        VLB_CUDA(cudaMemcpyAsync(dp, priors, sz * K, cudaMemcpyHostToDevice, s));
+        double ll;
+        if (t == VL_TYPE_FLOAT) {
+          vlb::DevModel<float> m;
+          m.means = (float *)dm; m.covs = (float *)dc; m.priors = (float *)dp;
+          m.K = (i64)K; m.D = (i64)D;
+          ll = device_estep<float>((float *)dX, (i64)N, m, (float *)dq,
+                                   vlb::resolve_precision(VLB200_PREC_DEFAULT, false), false, s);
+        } else {
+          vlb::DevModel<double> m;
+          m.means = (double *)dm; m.covs = (double *)dc; m.priors = (double *)dp;
+          m.K = (i64)K; m.D = (i64)D;
+          ll = device_estep<double>((double *)dX, (i64)N, m, (double *)dq, VLB200_PREC_EXACT,
+                                    false, s);
+        }
+        if (N) VLB_CUDA(cudaMemcpyAsync(post, dq, sz * N * K, cudaMemcpyDeviceToHost, s));
+        VLB_CUDA(cudaStreamSynchronize(s));
+        return ll;
+      },
+      (double)NAN);
+}
+
+double vl_get_gmm_data_posteriors_f(float *posteriors, vl_size numClusters, vl_size numData,
+                                    float const *priors, float const *means, vl_size dimension,
+                                    float const *covariances, float const *data) {
+  return posteriors_host(VL_TYPE_FLOAT, posteriors, numClusters, numData, priors, means,
+                         dimension, covariances, data);
+}
+
+double vl_get_gmm_data_posteriors_d(double *posteriors, vl_size numClusters, vl_size numData,
+                                    double const *priors, double const *means, vl_size dimension,
+                                    double const *covariances, double const *data) {
+  return posteriors_host(VL_TYPE_DOUBLE, posteriors, numClusters, numData, priors, means,
+                         dimension, covariances, data);
+}
+
+// ---------------------------------------------------------- extensions
+int vlb200_gmm_posteriors_device(float *posteriors, vl_size K, vl_size N, float const *priors,
+                                 float const *means, vl_size D, float const *covariances,
+                                 float const *data, int precision, double *ll, void *stream) {
+  return guarded(
+      [&]() -> int {
+        VLB_CHECK(K >= 1 && D >= 1, VL_ERR_BAD_ARG, "numClusters and dimension must be >= 1");
+        vlb::DevModel<float> m;
+        m.means = means; m.covs = covariances; m.priors = priors;
+        m.K = (i64)K; m.D = (i64)D;
+        double v = device_estep<float>(data, (i64)N, m, posteriors,
+                                       vlb::resolve_precision(precision, false), false,
+                                       vlb::pick_stream(stream));
+        if (ll) *ll = v;
+        return 0;
+      },
+      (int)VL_ERR_BAD_ARG);
+}
+
+double vlb200_gmm_em_device(VlGMM *self, float const *data, vl_size numData, int precision) {
+  return guarded(
+      [&]() -> double {
+        VLB_CHECK(self->dataType == VL_TYPE_FLOAT, VL_ERR_BAD_ARG,
+                  "vlb200_gmm_em_device: the model must be VL_TYPE_FLOAT");
+        return em_device<float>(self, data, (i64)numData, vlb::resolve_precision(precision, false));
+      },
+      (double)NAN);
+}
+
+vl_size vlb200_gmm_get_ll_trace(VlGMM const *self, double *trace, vl_size maxEntries) {
+  vl_size n = std::min<vl_size>(maxEntries, self->llTrace.size());
+  for (vl_size i = 0; i < n; ++i) trace[i] = self->llTrace[i];
+  return n;
+}
+
+vl_size vlb200_gmm_get_num_restarts(VlGMM const *self) { return self->numRestarts; }
+
+}  // extern "C"

@@ -1,0 +1,651 @@
+// Exact-arithmetic kernels (CUDA cores, float or double).  These evaluate the
+// reference's own formulation -- sum_d (x-mu)^2 / sigma^2 per (descriptor,
+// component), thresholded statistics, etc. -- and serve VL_TYPE_DOUBLE calls,
+// the EXACT precision mode and the M-step / restart machinery of EM.
+//
+// Determinism: every reduction runs in a fixed order (per-block partials,
+// then a fixed-shape final reduction), so results are bitwise reproducible
+// run to run, unlike the reference's OpenMP critical-section merge
+// (vl/gmm.c:1152-1166).
+#include <cmath>
+#include <cstring>
+
+#include "engine.h"
+
+namespace vlb {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ float dexp(float x) { return expf(x); }
+__device__ __forceinline__ double dexp(double x) { return exp(x); }
+
+// ------------------------------------------------------------ prepare
+// Per-component constants, vl/gmm.c:741-756 and vl/fisher.c:386-390.
+template <typename T>
+__global__ void k_prepare(const T *__restrict__ priors, const T *__restrict__ covs, int K, int D,
+                          T halfDimLog2Pi, T *__restrict__ inv, double *__restrict__ cst,
+                          T *__restrict__ sis) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  T acc = 0;
+  for (int d = 0; d < D; ++d) {
+    T c = covs[(i64)k * D + d];
+    acc += (T)log((double)c);
+    inv[(i64)k * D + d] = (T)1 / c;
+    sis[(i64)k * D + d] = (T)sqrt(1.0 / (double)c);
+  }
+  T logw = ((double)priors[k] < 1e-6) ? (T)(-INFINITY) : (T)log((double)priors[k]);
+  cst[k] = (double)(T)(logw - halfDimLog2Pi) - 0.5 * (double)acc;
+}
+
+// ------------------------------------------------------------ E-step
+// Log-densities of a TM x TK tile of (descriptor, component) pairs.  The
+// dimension is streamed through shared memory in chunks of DC.  Each thread
+// owns one component and RPT descriptors.
+template <typename T, int TM, int TK, int DC>
+__global__ void __launch_bounds__(kThreads) k_logp(const T *__restrict__ X, i64 N, int D, int K,
+                                                  const T *__restrict__ means,
+                                                  const T *__restrict__ inv,
+                                                  const double *__restrict__ cst,
+                                                  T *__restrict__ q) {
+  constexpr int RPT = TM * TK / kThreads;
+  __shared__ T sx[DC][TM + 1];
+  __shared__ T smu[DC][TK + 1];
+  __shared__ T siv[DC][TK + 1];
+  const int tid = threadIdx.x;
+  const int tk = tid % TK, tg = tid / TK;
+  const i64 i0 = (i64)blockIdx.x * TM;
+  const int k0 = blockIdx.y * TK;
+  T acc[RPT];
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) acc[r] = 0;
+
+  for (int d0 = 0; d0 < D; d0 += DC) {
+    for (int e = tid; e < TM * DC; e += kThreads) {
+      int r = e / DC, dd = e % DC;
+      i64 i = i0 + r;
+      int d = d0 + dd;
+      sx[dd][r] = (i < N && d < D) ? X[i * D + d] : (T)0;
+    }
+    for (int e = tid; e < TK * DC; e += kThreads) {
+      int c = e / DC, dd = e % DC;
+      int k = k0 + c, d = d0 + dd;
+      bool ok = (k < K && d < D);
+      smu[dd][c] = ok ? means[(i64)k * D + d] : (T)0;
+      siv[dd][c] = ok ? inv[(i64)k * D + d] : (T)0;
+    }
+    __syncthreads();
+    const int dl = min(DC, D - d0);
+    for (int dd = 0; dd < dl; ++dd) {
+      const T m = smu[dd][tk], iv = siv[dd][tk];
+#pragma unroll
+      for (int r = 0; r < RPT; ++r) {
+        T diff = sx[dd][tg * RPT + r] - m;
+        acc[r] += diff * diff * iv;
+      }
+    }
+    __syncthreads();
+  }
+  const int k = k0 + tk;
+  if (k < K) {
+    const double c = cst[k];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+      i64 i = i0 + tg * RPT + r;
+      if (i < N) q[i * K + k] = (T)(c - 0.5 * (double)acc[r]);
+    }
+  }
+}
+
+// Row-wise log-sum-exp normalisation (vl/gmm.c:776-790), one warp per row,
+// plus the optional FAST one-hot (vl/fisher.c:398-417: first arg-max wins).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_normalize(T *__restrict__ q, i64 N, int K, int fast,
+                                                       double *__restrict__ ll_part) {
+  constexpr int W = kThreads / 32;
+  __shared__ double sll[W];
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const i64 i = (i64)blockIdx.x * W + w;
+  double llrow = 0;
+  if (i < N) {
+    T *row = q + i * K;
+    T mx = (T)(-INFINITY);
+    for (int k = lane; k < K; k += 32) mx = max(mx, row[k]);
+    mx = warp_max(mx);
+    T sum = 0;
+    for (int k = lane; k < K; k += 32) {
+      T e = dexp(row[k] - mx);
+      row[k] = e;
+      sum += e;
+    }
+    sum = warp_sum(sum);
+    llrow = log((double)sum) + (double)mx;
+    T bv = (T)(-INFINITY);
+    int bi = 0x7fffffff;
+    for (int k = lane; k < K; k += 32) {
+      T v = row[k] / sum;
+      row[k] = v;
+      if (v > bv) { bv = v; bi = k; }
+    }
+    if (fast) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if (bi == 0x7fffffff) bi = 0;  // all-NaN row: the reference keeps index 0
+      for (int k = lane; k < K; k += 32) row[k] = (T)(k == bi);
+    }
+  }
+  if (lane == 0) sll[w] = llrow;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int j = 0; j < W; ++j) s += sll[j];
+    ll_part[blockIdx.x] = s;
+  }
+}
+
+__global__ void k_sum_doubles(const double *__restrict__ part, i64 n, double *__restrict__ out) {
+  __shared__ double sh[kThreads];
+  double s = 0;
+  for (i64 j = threadIdx.x; j < n; j += kThreads) s += part[j];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = kThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+// ------------------------------------------------------------ M-step
+// Thresholded sufficient statistics over one slab of rows for TKC components
+// and a block of 8*JMAX dimensions (vl/gmm.c:1093-1149):
+//   mass = sum q, S1 = sum q x, S2 = sum q (x - mu_old)^2, with q < 1e-2/K
+//   skipped.  Partials are written per slab in double.
+template <typename T, int TKC, int RC, int JMAX>
+__global__ void __launch_bounds__(kThreads) k_mstep_stats(
+    const T *__restrict__ X, const T *__restrict__ q, i64 N, int K, int D, i64 rowsPerSlab,
+    const T *__restrict__ oldMeans, double *__restrict__ pmass, double *__restrict__ ps1,
+    double *__restrict__ ps2) {
+  constexpr int DB = 8 * JMAX;
+  __shared__ T sx[RC][DB];
+  __shared__ T sq[RC][TKC];
+  __shared__ T smo[DB][TKC + 1];
+  const int tid = threadIdx.x, c = tid % TKC, dg = tid / TKC;
+  const int slab = blockIdx.x, k0 = blockIdx.y * TKC, dbase = blockIdx.z * DB;
+  const i64 r0 = (i64)slab * rowsPerSlab;
+  const i64 r1 = min(N, r0 + rowsPerSlab);
+  const double thr = 1e-2 / (double)K;
+  for (int e = tid; e < TKC * DB; e += kThreads) {
+    int cc = e / DB, dd = e % DB;
+    int k = k0 + cc, d = dbase + dd;
+    smo[dd][cc] = (k < K && d < D) ? oldMeans[(i64)k * D + d] : (T)0;
+  }
+  T s1[JMAX], s2[JMAX], mass = 0;
+#pragma unroll
+  for (int j = 0; j < JMAX; ++j) s1[j] = s2[j] = 0;
+  for (i64 rb = r0; rb < r1; rb += RC) {
+    const int rc = (int)min((i64)RC, r1 - rb);
+    __syncthreads();
+    for (int e = tid; e < RC * DB; e += kThreads) {
+      int r = e / DB, dd = e % DB, d = dbase + dd;
+      sx[r][dd] = (r < rc && d < D) ? X[(rb + r) * D + d] : (T)0;
+    }
+    for (int e = tid; e < RC * TKC; e += kThreads) {
+      int r = e / TKC, cc = e % TKC, k = k0 + cc;
+      T v = (r < rc && k < K) ? q[(rb + r) * K + k] : (T)0;
+      sq[r][cc] = ((double)v < thr) ? (T)0 : v;
+    }
+    __syncthreads();
+    for (int r = 0; r < rc; ++r) {
+      const T p = sq[r][c];
+      if (p == (T)0) continue;
+      mass += p;
+#pragma unroll
+      for (int j = 0; j < JMAX; ++j) {
+        const int dd = dg + 8 * j;
+        const T x = sx[r][dd];
+        const T diff = x - smo[dd][c];
+        s1[j] += p * x;
+        s2[j] += p * (diff * diff);
+      }
+    }
+  }
+  const int k = k0 + c;
+  if (k < K) {
+    const i64 base = ((i64)slab * K + k) * D;
+#pragma unroll
+    for (int j = 0; j < JMAX; ++j) {
+      const int d = dbase + dg + 8 * j;
+      if (d < D) {
+        ps1[base + d] = (double)s1[j];
+        ps2[base + d] = (double)s2[j];
+      }
+    }
+    if (dg == 0 && blockIdx.z == 0) pmass[(i64)slab * K + k] = (double)mass;
+  }
+}
+
+// Normalisation, old-to-new mean correction and bounds (vl/gmm.c:1169-1194);
+// priors receive the mass, normalised by k_normalize_priors.
+template <typename T>
+__global__ void k_mstep_finalize(int nslab, int K, int D, const double *__restrict__ pmass,
+                                 const double *__restrict__ ps1, const double *__restrict__ ps2,
+                                 const double *__restrict__ lb, T *__restrict__ means,
+                                 T *__restrict__ covs, T *__restrict__ priors) {
+  i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (i64)K * D) return;
+  const int k = (int)(idx / D), d = (int)(idx % D);
+  double mass = 0, S1 = 0, S2 = 0;
+  for (int s = 0; s < nslab; ++s) {
+    mass += pmass[(i64)s * K + k];
+    S1 += ps1[((i64)s * K + k) * D + d];
+    S2 += ps2[((i64)s * K + k) * D + d];
+  }
+  const double oldmu = (double)means[idx];
+  double mu = S1, v = S2;
+  if (mass >= 1e-6 / (double)K) {
+    mu = S1 / mass;
+    v = S2 / mass;
+    const double df = mu - oldmu;
+    v -= df * df;
+  }
+  T vt = (T)v;
+  if ((double)vt < lb[d]) vt = (T)lb[d];
+  means[idx] = (T)mu;
+  covs[idx] = vt;
+  if (d == 0) priors[k] = (T)mass;
+}
+
+template <typename T>
+__global__ void k_normalize_priors(T *__restrict__ priors, int K) {
+  __shared__ double sh[kThreads];
+  double s = 0;
+  for (int k = threadIdx.x; k < K; k += kThreads) s += (double)priors[k];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = kThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  double tot = sh[0];
+  if (tot < 1e-12) tot = 1e-12;
+  for (int k = threadIdx.x; k < K; k += kThreads) priors[k] = (T)((double)priors[k] / tot);
+}
+
+template <typename T>
+__global__ void k_apply_bounds(T *__restrict__ covs, i64 n, int D, const double *__restrict__ lb) {
+  i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int d = (int)(idx % D);
+  if ((double)covs[idx] < lb[d]) covs[idx] = (T)lb[d];
+}
+
+// Column sums of the posteriors per slab (vl/gmm.c:835-844).
+template <typename T>
+__global__ void k_colmass(const T *__restrict__ q, i64 N, int K, i64 rowsPerSlab,
+                          double *__restrict__ part) {
+  const i64 r0 = (i64)blockIdx.x * rowsPerSlab, r1 = min(N, r0 + rowsPerSlab);
+  for (int k = threadIdx.x; k < K; k += kThreads) {
+    double s = 0;
+    for (i64 i = r0; i < r1; ++i) s += (double)q[i * K + k];
+    part[(i64)blockIdx.x * K + k] = s;
+  }
+}
+
+__global__ void k_sum_slabs(const double *__restrict__ part, int nslab, int K,
+                            double *__restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  double s = 0;
+  for (int j = 0; j < nslab; ++j) s += part[(i64)j * K + k];
+  out[k] = s;
+}
+
+template <typename T>
+__global__ void k_restart_split(T *__restrict__ q, const T *__restrict__ X, i64 N, int K, int D,
+                                int icl, int best, int dim, T cut) {
+  i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  T p = q[i * K + best], r = q[i * K + icl];
+  if (X[i * D + dim] < cut) {
+    q[i * K + icl] = p + r;
+    q[i * K + best] = 0;
+  } else {
+    q[i * K + icl] = 0;
+    q[i * K + best] = p + r;
+  }
+}
+
+// ------------------------------------------------------------ Fisher
+// Fisher statistics of one segment for TKC components and a block of
+// 8*JMAX dimensions (vl/fisher.c:419-449): for pi_k >= 1e-6 and q >= 1e-6,
+// u += q (x-mu) s, v += q ((x-mu)^2 s^2 - 1); counts the accumulated terms.
+template <typename T, int TKC, int RC, int JMAX>
+__global__ void __launch_bounds__(kThreads) k_fisher_stats(
+    const T *__restrict__ X, const T *__restrict__ q, i64 qbase, int K, int D,
+    const Segment *__restrict__ segs, const T *__restrict__ means, const T *__restrict__ sis,
+    const T *__restrict__ priors, double *__restrict__ pu, double *__restrict__ pv,
+    unsigned long long *__restrict__ pnt) {
+  constexpr int DB = 8 * JMAX;
+  __shared__ T sx[RC][DB];
+  __shared__ T sq[RC][TKC];
+  __shared__ T smu[DB][TKC + 1];
+  __shared__ T ssi[DB][TKC + 1];
+  const int tid = threadIdx.x, c = tid % TKC, dg = tid / TKC;
+  const int sidx = blockIdx.x, k0 = blockIdx.y * TKC, dbase = blockIdx.z * DB;
+  const Segment sg = segs[sidx];
+  for (int e = tid; e < TKC * DB; e += kThreads) {
+    int cc = e / DB, dd = e % DB;
+    int k = k0 + cc, d = dbase + dd;
+    bool ok = (k < K && d < D);
+    smu[dd][cc] = ok ? means[(i64)k * D + d] : (T)0;
+    ssi[dd][cc] = ok ? sis[(i64)k * D + d] : (T)0;
+  }
+  const int k = k0 + c;
+  const bool active = (k < K) && ((double)priors[k] >= 1e-6);
+  T u[JMAX], v[JMAX];
+#pragma unroll
+  for (int j = 0; j < JMAX; ++j) u[j] = v[j] = 0;
+  unsigned long long nt = 0;
+  for (i64 rb = sg.row0; rb < sg.row1; rb += RC) {
+    const int rc = (int)min((i64)RC, sg.row1 - rb);
+    __syncthreads();
+    for (int e = tid; e < RC * DB; e += kThreads) {
+      int r = e / DB, dd = e % DB, d = dbase + dd;
+      sx[r][dd] = (r < rc && d < D) ? X[(rb + r) * D + d] : (T)0;
+    }
+    for (int e = tid; e < RC * TKC; e += kThreads) {
+      int r = e / TKC, cc = e % TKC, kk = k0 + cc;
+      T val = (r < rc && kk < K) ? q[(rb + r - qbase) * K + kk] : (T)0;
+      sq[r][cc] = ((double)val < 1e-6) ? (T)0 : val;
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int r = 0; r < rc; ++r) {
+      const T p = sq[r][c];
+      if (p == (T)0) continue;
+      ++nt;
+#pragma unroll
+      for (int j = 0; j < JMAX; ++j) {
+        const int dd = dg + 8 * j;
+        const T df = (sx[r][dd] - smu[dd][c]) * ssi[dd][c];
+        u[j] += p * df;
+        v[j] += p * (df * df - (T)1);
+      }
+    }
+  }
+  if (k < K) {
+    const i64 base = ((i64)sidx * K + k) * D;
+#pragma unroll
+    for (int j = 0; j < JMAX; ++j) {
+      const int d = dbase + dg + 8 * j;
+      if (d < D) {
+        pu[base + d] = (double)u[j];
+        pv[base + d] = (double)v[j];
+      }
+    }
+    if (dg == 0 && blockIdx.z == 0) pnt[(i64)sidx * K + k] = nt;
+  }
+}
+
+// Per-image Fisher finalisation (vl/fisher.c:450-485): sum the image's
+// segment partials, scale u by 1/(N sqrt pi) and v by 1/(N sqrt(2 pi)),
+// signed square root, global L2 normalisation.  One block per image.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_fisher_finalize(
+    int K, int D, const int *__restrict__ imgSegBegin, const i64 *__restrict__ imgRows,
+    const double *__restrict__ pu, const double *__restrict__ pv,
+    const unsigned long long *__restrict__ pnt, const T *__restrict__ priors, int flags,
+    i64 imgBase, T *__restrict__ enc, unsigned long long *__restrict__ nterms) {
+  __shared__ double sh[kThreads];
+  __shared__ unsigned long long shn[kThreads];
+  const int img = blockIdx.x;
+  const int s0 = imgSegBegin[img], s1 = imgSegBegin[img + 1];
+  const i64 n = imgRows[img];
+  const i64 KD = (i64)K * D;
+  T *out = enc + (imgBase + img) * 2 * KD;
+  double sq = 0;
+  for (i64 e = threadIdx.x; e < 2 * KD; e += kThreads) {
+    const bool isv = e >= KD;
+    const i64 kd = isv ? e - KD : e;
+    const int k = (int)(kd / D);
+    double acc = 0;
+    for (int s = s0; s < s1; ++s) acc += isv ? pv[(i64)s * KD + kd] : pu[(i64)s * KD + kd];
+    const double pk = (double)priors[k];
+    double z = 0;
+    if (pk >= 1e-6 && n > 0) {
+      z = isv ? acc * (1.0 / ((double)n * sqrt(2.0 * pk))) : acc * (1.0 / ((double)n * sqrt(pk)));
+    }
+    T zt = (T)z;
+    if (flags & 1) zt = zt >= (T)0 ? (T)sqrt((double)zt) : -(T)sqrt(-(double)zt);
+    out[e] = zt;
+    sq += (double)zt * (double)zt;
+  }
+  unsigned long long nt = 0;
+  for (i64 e = threadIdx.x; e < K; e += kThreads)
+    for (int s = s0; s < s1; ++s) nt += pnt[(i64)s * K + e];
+  sh[threadIdx.x] = sq;
+  shn[threadIdx.x] = nt;
+  __syncthreads();
+  for (int o = kThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sh[threadIdx.x] += sh[threadIdx.x + o];
+      shn[threadIdx.x] += shn[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && nterms) nterms[imgBase + img] = shn[0];
+  if (flags & 2) {
+    double nrm = sqrt(sh[0]);
+    if (nrm < 1e-12) nrm = 1e-12;
+    const T nt_ = (T)nrm;
+    for (i64 e = threadIdx.x; e < 2 * KD; e += kThreads) out[e] = out[e] / nt_;
+  }
+}
+
+template <typename T>
+T half_dim_log_2pi(i64 D) {
+  return (T)(((double)D / 2.0) * log(2.0 * 3.141592653589793));
+}
+
+inline unsigned grid1(i64 n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+// ================================================================ launchers
+
+template <typename T>
+void exact_prepare(const DevModel<T> &m, DevDerived<T> &der, cudaStream_t s) {
+  VLB_LAUNCH("exact_prepare", s,
+             k_prepare<T><<<grid1(m.K, 128), 128, 0, s>>>(m.priors, m.covs, (int)m.K, (int)m.D,
+                                                          half_dim_log_2pi<T>(m.D), der.inv,
+                                                          der.cst, der.sis));
+}
+
+i64 estep_ll_parts(i64 N) { return (N + 7) / 8 + 1; }
+
+template <typename T>
+void exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,
+                 double *ll_part, bool fast, cudaStream_t s) {
+  if (N <= 0) return;
+  constexpr int TM = 32, TK = 64, DC = 32;
+  dim3 g(grid1(N, TM), grid1(m.K, TK));
+  VLB_LAUNCH("exact_logp", s,
+             (k_logp<T, TM, TK, DC><<<g, kThreads, 0, s>>>(X, N, (int)m.D, (int)m.K, m.means,
+                                                           der.inv, der.cst, q)));
+  VLB_LAUNCH("exact_normalize", s,
+             k_normalize<T><<<grid1(N, 8), kThreads, 0, s>>>(q, N, (int)m.K, fast ? 1 : 0,
+                                                             ll_part));
+}
+
+void sum_doubles(const double *part, i64 n, double *out, cudaStream_t s) {
+  VLB_LAUNCH("sum_doubles", s, k_sum_doubles<<<1, kThreads, 0, s>>>(part, n, out));
+}
+
+namespace {
+i64 pick_slab_rows(i64 N) {
+  // About 2 slabs per SM for large N; at least 256 rows per slab.
+  i64 slabs = 296;
+  i64 r = (N + slabs - 1) / slabs;
+  if (r < 256) r = 256;
+  return r;
+}
+}  // namespace
+
+template <typename T>
+void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i64 K, i64 D,
+                 const double *lb, cudaStream_t s) {
+  constexpr int TKC = 32, RC = 32, JMAX = sizeof(T) == 8 ? 8 : 16, DB = 8 * JMAX;
+  const i64 rps = pick_slab_rows(N > 0 ? N : 1);
+  const int nslab = (int)((N + rps - 1) / rps > 0 ? (N + rps - 1) / rps : 1);
+  Scratch &sc = thread_scratch();
+  double *pmass = sc.slot[10].get<double>((size_t)nslab * K);
+  double *ps1 = sc.slot[11].get<double>((size_t)nslab * K * D);
+  double *ps2 = sc.slot[12].get<double>((size_t)nslab * K * D);
+  if (N > 0) {
+    dim3 g(nslab, grid1(K, TKC), grid1(D, DB));
+    VLB_LAUNCH("exact_mstep_stats", s,
+               (k_mstep_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
+                   X, q, N, (int)K, (int)D, rps, means, pmass, ps1, ps2)));
+  } else {
+    VLB_CUDA(cudaMemsetAsync(pmass, 0, sizeof(double) * nslab * K, s));
+    VLB_CUDA(cudaMemsetAsync(ps1, 0, sizeof(double) * nslab * K * D, s));
+    VLB_CUDA(cudaMemsetAsync(ps2, 0, sizeof(double) * nslab * K * D, s));
+  }
+  VLB_LAUNCH("exact_mstep_finalize", s,
+             k_mstep_finalize<T><<<grid1(K * D, kThreads), kThreads, 0, s>>>(
+                 nslab, (int)K, (int)D, pmass, ps1, ps2, lb, means, covs, priors));
+  VLB_LAUNCH("normalize_priors", s, k_normalize_priors<T><<<1, kThreads, 0, s>>>(priors, (int)K));
+}
+
+template <typename T>
+void column_mass(const T *q, i64 N, i64 K, double *mass, cudaStream_t s) {
+  const i64 rps = pick_slab_rows(N > 0 ? N : 1);
+  const int nslab = (int)((N + rps - 1) / rps > 0 ? (N + rps - 1) / rps : 1);
+  double *part = thread_scratch().slot[13].get<double>((size_t)nslab * K);
+  if (N > 0) {
+    VLB_LAUNCH("column_mass", s, k_colmass<T><<<nslab, kThreads, 0, s>>>(q, N, (int)K, rps, part));
+  } else {
+    VLB_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * nslab * K, s));
+  }
+  VLB_LAUNCH("sum_slabs", s, k_sum_slabs<<<grid1(K, 128), 128, 0, s>>>(part, nslab, (int)K, mass));
+}
+
+template <typename T>
+void restart_split(T *q, const T *X, i64 N, i64 K, i64 D, i64 icl, i64 best, i64 dim, T cut,
+                   cudaStream_t s) {
+  if (N <= 0) return;
+  VLB_LAUNCH("restart_split", s,
+             k_restart_split<T><<<grid1(N, kThreads), kThreads, 0, s>>>(
+                 q, X, N, (int)K, (int)D, (int)icl, (int)best, (int)dim, cut));
+}
+
+template <typename T>
+void apply_bounds(T *covs, i64 K, i64 D, const double *lb, cudaStream_t s) {
+  VLB_LAUNCH("apply_bounds", s,
+             k_apply_bounds<T><<<grid1(K * D, kThreads), kThreads, 0, s>>>(covs, K * D, (int)D, lb));
+}
+
+// Batched Fisher encoding with the exact kernels.  Images are processed in
+// chunks bounded by a row budget; each image is cut into segments of at most
+// kSegRows rows so long images still spread over many blocks.
+template <typename T>
+void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const DevModel<T> &m,
+                        T *enc, unsigned long long *nterms, int flags, cudaStream_t s) {
+  const i64 K = m.K, D = m.D;
+  constexpr int TKC = 32, RC = 32, JMAX = sizeof(T) == 8 ? 5 : 10, DB = 8 * JMAX;
+  constexpr i64 kSegRows = 2048;
+  const i64 kRowBudget = std::max<i64>(4096, (i64)(1u << 30) / (K * (i64)sizeof(T)));
+  const i64 kSegBudget = std::max<i64>(64, (i64)(256u << 20) / (2 * K * D * 8));
+  Scratch &sc = thread_scratch();
+  DevDerived<T> der;
+  der.inv = sc.slot[0].get<T>(K * D);
+  der.sis = sc.slot[1].get<T>(K * D);
+  der.cst = sc.slot[2].get<double>(K);
+  exact_prepare(m, der, s);
+
+  i64 img = 0;
+  while (img < numImages) {
+    // Form one chunk of images.
+    std::vector<Segment> segs;
+    std::vector<int> segBegin;
+    std::vector<i64> rows;
+    const i64 chunkImg0 = img, row0 = h_offsets[img];
+    while (img < numImages) {
+      const i64 a = h_offsets[img], b = h_offsets[img + 1];
+      const i64 nseg = std::max<i64>(1, (b - a + kSegRows - 1) / kSegRows);
+      if (!segs.empty() && ((b - row0) > kRowBudget || (i64)segs.size() + nseg > kSegBudget)) break;
+      segBegin.push_back((int)segs.size());
+      rows.push_back(b - a);
+      for (i64 j = 0; j < nseg; ++j) {
+        i64 s0 = a + j * kSegRows, s1 = std::min(b, s0 + kSegRows);
+        segs.push_back({img - chunkImg0, s0, s1});
+      }
+      ++img;
+    }
+    segBegin.push_back((int)segs.size());
+    const i64 nimg = img - chunkImg0;
+    const i64 row1 = h_offsets[img];
+    const i64 nrows = row1 - row0;
+    const i64 nseg = (i64)segs.size();
+
+    T *q = sc.slot[3].get<T>(std::max<i64>(1, nrows) * K);
+    double *llp = sc.slot[4].get<double>(estep_ll_parts(nrows));
+    if (nrows > 0) exact_estep(X + row0 * D, nrows, m, der, q, llp, (flags & 4) != 0, s);
+
+    Segment *dsegs = sc.slot[5].get<Segment>(nseg);
+    int *dbeg = sc.slot[6].get<int>(nimg + 1);
+    i64 *drows = sc.slot[7].get<i64>(nimg);
+    double *pu = sc.slot[8].get<double>(nseg * K * D);
+    double *pv = sc.slot[9].get<double>(nseg * K * D);
+    unsigned long long *pnt = sc.slot[14].get<unsigned long long>(nseg * K);
+    VLB_CUDA(cudaMemcpyAsync(dsegs, segs.data(), sizeof(Segment) * nseg, cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(dbeg, segBegin.data(), sizeof(int) * (nimg + 1), cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(drows, rows.data(), sizeof(i64) * nimg, cudaMemcpyHostToDevice, s));
+    dim3 g((unsigned)nseg, grid1(K, TKC), grid1(D, DB));
+    VLB_LAUNCH("exact_fisher_stats", s,
+               (k_fisher_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
+                   X, q, row0, (int)K, (int)D, dsegs, m.means, der.sis, m.priors, pu, pv, pnt)));
+    VLB_LAUNCH("exact_fisher_finalize", s,
+               k_fisher_finalize<T><<<(unsigned)nimg, kThreads, 0, s>>>(
+                   (int)K, (int)D, dbeg, drows, pu, pv, pnt, m.priors, flags, chunkImg0, enc,
+                   nterms));
+  }
+}
+
+// ------------------------------------------------------ instantiations
+#define VLB_INST(T)                                                                          \
+  template void exact_prepare<T>(const DevModel<T> &, DevDerived<T> &, cudaStream_t);        \
+  template void exact_estep<T>(const T *, i64, const DevModel<T> &, const DevDerived<T> &,   \
+                               T *, double *, bool, cudaStream_t);                           \
+  template void exact_mstep<T>(const T *, i64, const T *, T *, T *, T *, i64, i64,           \
+                               const double *, cudaStream_t);                                \
+  template void column_mass<T>(const T *, i64, i64, double *, cudaStream_t);                 \
+  template void restart_split<T>(T *, const T *, i64, i64, i64, i64, i64, i64, T,           \
+                                 cudaStream_t);                                              \
+  template void apply_bounds<T>(T *, i64, i64, const double *, cudaStream_t);                \
+  template void exact_fisher_batch<T>(const T *, const i64 *, i64, const DevModel<T> &, T *, \
+                                      unsigned long long *, int, cudaStream_t);
+VLB_INST(float)
+VLB_INST(double)
+
+}  // namespace vlb

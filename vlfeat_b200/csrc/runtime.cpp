@@ -1,0 +1,240 @@
+// Runtime services: the vl_* runtime symbols that programs written against
+// VLFeat link (vl/generic.h), plus the library's stream, scratch, launch
+// accounting and event-timing plumbing.
+#include <atomic>
+#include <chrono>
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <map>
+#include <mutex>
+
+#include "common.h"
+
+extern "C" {
+#include "vlb200.h"
+}
+
+// ---------------------------------------------------------------- errors
+namespace {
+thread_local int g_last_error = VL_ERR_OK;
+thread_local char g_last_msg[1024] = "";
+std::atomic<vl_size> g_num_threads{1};
+std::atomic<int> g_simd{1};
+std::atomic<int> g_precision{VLB200_PREC_EXACT};
+printf_func_t g_printf = (printf_func_t)&printf;
+
+int silent_printf(char const *, ...) { return 0; }
+}  // namespace
+
+extern "C" {
+
+int vl_get_last_error(void) { return g_last_error; }
+char const *vl_get_last_error_message(void) { return g_last_msg; }
+
+int vl_set_last_error(int error, char const *errorMessage, ...) {
+  g_last_error = error;
+  if (errorMessage) {
+    va_list ap;
+    va_start(ap, errorMessage);
+    vsnprintf(g_last_msg, sizeof(g_last_msg), errorMessage, ap);
+    va_end(ap);
+  } else {
+    g_last_msg[0] = 0;
+  }
+  return error;
+}
+
+// ------------------------------------------------------------ info/state
+char const *vl_get_version_string(void) { return "0.9.21-b200"; }
+char const *vlb200_version(void) { return "vlfeat-b200 0.1 (sm_100a)"; }
+void vl_set_simd_enabled(vl_bool x) { g_simd = x ? 1 : 0; }
+vl_bool vl_get_simd_enabled(void) { return g_simd.load(); }
+vl_size vl_get_max_threads(void) { return g_num_threads.load(); }
+void vl_set_num_threads(vl_size n) { g_num_threads = n ? n : 1; }
+vl_size vl_get_thread_limit(void) { return 1; }
+
+int vlb200_set_precision(int p) {
+  if (p < VLB200_PREC_EXACT || p > VLB200_PREC_BF16_ROUTER) {
+    return vl_set_last_error(VL_ERR_BAD_ARG, "vlb200_set_precision: unknown mode %d", p);
+  }
+  g_precision = p;
+  return 0;
+}
+int vlb200_get_precision(void) { return g_precision.load(); }
+
+int vlb200_device_ok(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n > 0;
+}
+
+// ---------------------------------------------------------------- memory
+void *vl_malloc(size_t n) { return malloc(n); }
+void *vl_realloc(void *ptr, size_t n) { return realloc(ptr, n); }
+void *vl_calloc(size_t n, size_t size) { return calloc(n, size); }
+void *vl_memalign(size_t n, size_t size) {
+  void *p = nullptr;
+  if (posix_memalign(&p, n < sizeof(void *) ? sizeof(void *) : n, size)) return nullptr;
+  return p;
+}
+void vl_free(void *ptr) { free(ptr); }
+
+// ---------------------------------------------------------------- printf
+void vl_set_printf_func(printf_func_t f) { g_printf = f ? f : (printf_func_t)&silent_printf; }
+printf_func_t vl_get_printf_func(void) { return g_printf; }
+
+// ---------------------------------------------------------------- timing
+static thread_local std::chrono::steady_clock::time_point g_tic;
+void vl_tic(void) { g_tic = std::chrono::steady_clock::now(); }
+double vl_toc(void) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - g_tic).count();
+}
+double vl_get_cpu_time(void) { return (double)clock() / (double)CLOCKS_PER_SEC; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------ plumbing
+namespace vlb {
+
+void throw_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  cudaGetLastError();
+  char buf[512];
+  snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e),
+           what, file, line);
+  throw Error(e == cudaErrorMemoryAllocation ? VL_ERR_ALLOC : VL_ERR_BAD_ARG, buf);
+}
+
+namespace {
+struct StreamHolder {
+  cudaStream_t s = nullptr;
+  ~StreamHolder() {
+    // Streams die with the context at process exit; destroying them from a
+    // thread_local destructor after the runtime has shut down is unsafe.
+  }
+};
+thread_local StreamHolder g_stream;
+thread_local Scratch *g_scratch = nullptr;
+thread_local DevBuf *g_pinned_dummy = nullptr;
+thread_local void *g_pinned = nullptr;
+thread_local size_t g_pinned_cap = 0;
+
+std::atomic<uint64_t> g_launches{0};
+std::atomic<int> g_profile{0};
+
+struct ProfRec {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  double ms = 0;
+  uint64_t launches = 0;
+};
+std::mutex g_prof_mu;
+std::map<std::string, ProfRec> g_prof;
+thread_local cudaEvent_t g_open_event = nullptr;
+}  // namespace
+
+cudaStream_t thread_stream() {
+  if (!g_stream.s) VLB_CUDA(cudaStreamCreateWithFlags(&g_stream.s, cudaStreamNonBlocking));
+  return g_stream.s;
+}
+
+Scratch &thread_scratch() {
+  if (!g_scratch) g_scratch = new Scratch();  // lives until process exit
+  return *g_scratch;
+}
+
+void *pinned_host(size_t bytes) {
+  (void)g_pinned_dummy;
+  if (bytes > g_pinned_cap) {
+    if (g_pinned) cudaFreeHost(g_pinned);
+    g_pinned = nullptr;
+    g_pinned_cap = 0;
+    size_t want = bytes + bytes / 8;
+    VLB_CUDA(cudaMallocHost(&g_pinned, want));
+    g_pinned_cap = want;
+  }
+  return g_pinned;
+}
+
+int default_precision() { return g_precision.load(); }
+
+int resolve_precision(int p, bool is_double) {
+  if (is_double) return VLB200_PREC_EXACT;
+  if (p == VLB200_PREC_DEFAULT) p = g_precision.load();
+  VLB_CHECK(p >= VLB200_PREC_EXACT && p <= VLB200_PREC_BF16_ROUTER, VL_ERR_BAD_ARG,
+            "unknown precision mode");
+  return p;
+}
+
+void launch_begin(const char *name, cudaStream_t s) {
+  (void)name;
+  if (g_profile.load()) {
+    VLB_CUDA(cudaEventCreate(&g_open_event));
+    VLB_CUDA(cudaEventRecord(g_open_event, s));
+  }
+}
+
+void launch_end(const char *name, cudaStream_t s) {
+  g_launches.fetch_add(1);
+  if (g_profile.load() && g_open_event) {
+    cudaEvent_t e1;
+    VLB_CUDA(cudaEventCreate(&e1));
+    VLB_CUDA(cudaEventRecord(e1, s));
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    auto &r = g_prof[name];
+    r.pending.emplace_back(g_open_event, e1);
+    r.launches++;
+    g_open_event = nullptr;
+  }
+}
+
+}  // namespace vlb
+
+extern "C" {
+
+vl_uint64 vlb200_launch_count(void) { return vlb::g_launches.load(); }
+
+void vlb200_profile_enable(int on) { vlb::g_profile = on ? 1 : 0; }
+
+void vlb200_profile_reset(void) {
+  std::lock_guard<std::mutex> lk(vlb::g_prof_mu);
+  for (auto &kv : vlb::g_prof)
+    for (auto &pe : kv.second.pending) {
+      cudaEventDestroy(pe.first);
+      cudaEventDestroy(pe.second);
+    }
+  vlb::g_prof.clear();
+}
+
+int vlb200_profile_read(char *names, vl_size nameStride, double *ms, vl_uint64 *launches,
+                        vl_size maxEntries) {
+  std::lock_guard<std::mutex> lk(vlb::g_prof_mu);
+  vl_size i = 0;
+  for (auto &kv : vlb::g_prof) {
+    auto &r = kv.second;
+    for (auto &pe : r.pending) {
+      float t = 0;
+      if (cudaEventSynchronize(pe.second) == cudaSuccess &&
+          cudaEventElapsedTime(&t, pe.first, pe.second) == cudaSuccess)
+        r.ms += t;
+      cudaEventDestroy(pe.first);
+      cudaEventDestroy(pe.second);
+    }
+    r.pending.clear();
+    if (i < maxEntries) {
+      if (names && nameStride) {
+        strncpy(names + i * nameStride, kv.first.c_str(), nameStride - 1);
+        names[i * nameStride + nameStride - 1] = 0;
+      }
+      if (ms) ms[i] = r.ms;
+      if (launches) launches[i] = r.launches;
+    }
+    ++i;
+  }
+  return (int)i;
+}
+
+}  // extern "C"
