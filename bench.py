@@ -338,6 +338,8 @@ def main():
     from vlfeat_b200 import capi
     capi.lib()
     dev = torch.device("cuda")
+    # All timing uses one explicit stream shared by torch and the library.
+    torch.cuda.set_stream(torch.cuda.Stream())
     wl = make_workload(rank, dev)
     enc = torch.empty((NUM_IMAGES, 2 * K * D), device=dev)
     nt = torch.empty(NUM_IMAGES, dtype=torch.int64, device=dev)

@@ -1,0 +1,120 @@
+"""GPU parity of the tensor-core (tcgen05) paths through the C-ABI.
+
+Reference: the FP64 C restatement (oracle/), itself pinned to VLFeat's own
+double results.  Tolerances (relative L2 error of each Fisher vector):
+FP32 mode (bf16x3 on both contractions) 2e-5; BF16 mode 1e-3 (the metric's
+bound).  Posteriors: max |q - q64| <= 1e-4 in FP32 mode."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from oracle.oracle import FLAG_FAST, FLAG_IMPROVED, FLAG_NORMALIZED, FLAG_SQUARE_ROOT
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp32": 2e-5, "bf16": 1e-3}
+
+
+@pytest.fixture(autouse=True)
+def reset_mode(vl):
+    yield
+    vl.set_precision("exact")
+
+
+def _t(a, dev="cuda"):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+@pytest.mark.parametrize("KD", [(256, 80), (64, 64), (128, 80), (64, 128)])
+def test_fv_single(vl, restatement, mode, KD):
+    from vlfeat_b200 import workloads as W
+    K, D = KD
+    pr, mu, cv = W.fv_gmm(K, D, seed=3)
+    x = W.pca_like(3000, D, seed=4)
+    ref, nref = restatement.fisher(x.astype(np.float64), mu.astype(np.float64), cv.astype(np.float64),
+                                   pr.astype(np.float64), FLAG_IMPROVED)
+    vl.set_precision(mode)
+    enc, nt = vl.fisher_encode(x, mu, cv, pr, FLAG_IMPROVED)
+    assert rel_err(enc, ref) < TOL[mode]
+    assert abs(nt - nref) <= max(2, 1e-3 * nref)
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+@pytest.mark.parametrize("flags", [0, FLAG_SQUARE_ROOT, FLAG_NORMALIZED, FLAG_IMPROVED | FLAG_FAST])
+def test_fv_flags(vl, restatement, mode, flags):
+    from vlfeat_b200 import workloads as W
+    pr, mu, cv = W.fv_gmm(256, 80, seed=7)
+    x = W.pca_like(1000, 80, seed=8)
+    ref, nref = restatement.fisher(x.astype(np.float64), mu.astype(np.float64), cv.astype(np.float64),
+                                   pr.astype(np.float64), flags)
+    vl.set_precision(mode)
+    enc, nt = vl.fisher_encode(x, mu, cv, pr, flags)
+    tol = TOL[mode] * (3 if flags & FLAG_FAST else 1)
+    assert rel_err(enc, ref) < tol
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+def test_batched_uneven(vl, restatement, mode):
+    import torch
+    from vlfeat_b200 import workloads as W
+    K, D = 256, 80
+    pr, mu, cv = W.fv_gmm(K, D, seed=9)
+    counts = np.array([0, 1, 5, 127, 128, 129, 3000, 0, 9000, 17, 20000, 250])
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    x = W.pca_like(int(offs[-1]), D, seed=10)
+    enc = torch.zeros((len(counts), 2 * K * D), device="cuda")
+    nt = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+    vl.fisher_encode_batch_device(enc, _t(mu), _t(cv), _t(pr), _t(x), offs, FLAG_IMPROVED, mode, nt)
+    enc = enc.cpu().numpy()
+    nt = nt.cpu().numpy()
+    for j in range(len(counts)):
+        e, n = restatement.fisher(x[offs[j]:offs[j + 1]].astype(np.float64), mu.astype(np.float64),
+                                  cv.astype(np.float64), pr.astype(np.float64), FLAG_IMPROVED)
+        if counts[j] == 0:
+            assert np.all(enc[j] == 0) and nt[j] == 0
+        else:
+            assert rel_err(enc[j], e) < TOL[mode] * 2, j
+            assert abs(int(nt[j]) - n) <= max(2, 1e-3 * n), j
+
+
+def test_posteriors_fp32(vl, restatement):
+    from vlfeat_b200 import workloads as W
+    pr, mu, cv = W.fv_gmm(256, 80, seed=12)
+    x = W.pca_like(5000, 80, seed=13)
+    q64, ll64 = restatement.posteriors(x.astype(np.float64), pr.astype(np.float64),
+                                       mu.astype(np.float64), cv.astype(np.float64))
+    vl.set_precision("fp32")
+    q, ll = vl.get_gmm_data_posteriors(x, pr, mu, cv)
+    assert np.max(np.abs(q - q64)) < 1e-4
+    assert abs(ll - ll64) < 1e-6 * abs(ll64)
+
+
+def test_em_fp32_estep(vl, restatement):
+    """EM with the tensor-core E-step (config-0 generator, D=64, K=64)."""
+    from vlfeat_b200 import workloads as W
+    c = W.config0(scale=0.3)
+    r = restatement.em(c["data"].astype(np.float64), c["priors"], c["means"], c["covs"],
+                       c["lower_bound"], 5)
+    vl.set_precision("fp32")
+    m = vl.GMM(c["D"], c["K"], np.float32)
+    m.set_initialization("custom")
+    m.set_max_num_iterations(5)
+    m.set_covariance_lower_bound(c["lower_bound"])
+    m.set_means(c["means"])
+    m.set_covariances(c["covs"])
+    m.set_priors(c["priors"])
+    ll = m.cluster(c["data"])
+    assert abs(ll - r["ll"]) <= 2e-5 * abs(r["ll"])
+    assert rel_err(m.means, r["means"]) < 1e-3
+
+
+def test_tc_deterministic(vl):
+    from vlfeat_b200 import workloads as W
+    pr, mu, cv = W.fv_gmm(256, 80, seed=14)
+    x = W.pca_like(7000, 80, seed=15)
+    vl.set_precision("bf16")
+    a, _ = vl.fisher_encode(x, mu, cv, pr)
+    b, _ = vl.fisher_encode(x, mu, cv, pr)
+    assert np.array_equal(a, b)

@@ -342,9 +342,13 @@ def fisher_encode(data, means, covariances, priors, flags=FLAG_IMPROVED):
 
 
 def _stream(stream):
+    """Stream handle for the library.  None -> the library's own per-thread
+    stream; a torch stream whose handle is 0 (the legacy default stream) is
+    passed as cudaStreamLegacy (0x1) so the work stays ordered with it."""
     if stream is None:
         return None
-    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+    h = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+    return C.c_void_p(h if h else 1)
 
 
 def gmm_posteriors_device(post_t, priors_t, means_t, covs_t, data_t, precision="default",

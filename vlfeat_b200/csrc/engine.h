@@ -37,11 +37,11 @@ template <typename T>
 void exact_prepare(const DevModel<T> &m, DevDerived<T> &der, cudaStream_t s);
 
 // E-step over rows [0, N): q (N x K) receives posteriors; per-block LL partials
-// go to ll_part (size >= estep_ll_parts(N)); if fast, q is replaced by the
-// one-hot arg-max (vl/fisher.c:398-417).
+// go to ll_part (capacity estep_ll_parts(N)); returns the number of partials
+// written.  If fast, q is replaced by the one-hot arg-max (vl/fisher.c:398-417).
 i64 estep_ll_parts(i64 N);
 template <typename T>
-void exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,
+i64 exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,
                  double *ll_part, bool fast, cudaStream_t s);
 
 // Deterministic sum of n doubles into *out (device).
@@ -84,8 +84,8 @@ void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const D
 // ------------------------------------------------------- tensor-core path
 // Implemented in k_tc.cu.  Available for float data only.
 bool tc_supported(i64 K, i64 D);
-void tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
-              bool fast, int precision, cudaStream_t s);
+i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
+             bool fast, int precision, cudaStream_t s);
 void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages,
                      const DevModel<float> &m, float *enc, unsigned long long *nterms, int flags,
                      int precision, cudaStream_t s);

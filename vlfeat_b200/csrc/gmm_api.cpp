@@ -81,9 +81,10 @@ double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int pr
   double *llp = sc.slot[15].get<double>(vlb::estep_ll_parts(N));
   double *dll = sc.slot[16].get<double>(1);
   bool done = false;
+  i64 nparts = 0;
   if constexpr (sizeof(T) == 4) {
     if (precision != VLB200_PREC_EXACT && vlb::tc_supported(m.K, m.D)) {
-      vlb::tc_estep(dX, N, m, dq, llp, fast, precision, s);
+      nparts = vlb::tc_estep(dX, N, m, dq, llp, fast, precision, s);
       done = true;
     }
   }
@@ -93,10 +94,10 @@ double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int pr
     der.sis = sc.slot[18].get<T>(m.K * m.D);
     der.cst = sc.slot[19].get<double>(m.K);
     vlb::exact_prepare(m, der, s);
-    vlb::exact_estep(dX, N, m, der, dq, llp, fast, s);
+    nparts = vlb::exact_estep(dX, N, m, der, dq, llp, fast, s);
   }
   if (N <= 0) return 0.0;
-  vlb::sum_doubles(llp, vlb::estep_ll_parts(N), dll, s);
+  vlb::sum_doubles(llp, nparts, dll, s);
   double ll = 0;
   VLB_CUDA(cudaMemcpyAsync(&ll, dll, sizeof(double), cudaMemcpyDeviceToHost, s));
   VLB_CUDA(cudaStreamSynchronize(s));

@@ -481,12 +481,12 @@ void exact_prepare(const DevModel<T> &m, DevDerived<T> &der, cudaStream_t s) {
                                                           der.cst, der.sis));
 }
 
-i64 estep_ll_parts(i64 N) { return (N + 7) / 8 + 1; }
+i64 estep_ll_parts(i64 N) { return (N + 7) / 8 + 1; }  // capacity bound for any E-step kernel
 
 template <typename T>
-void exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,
-                 double *ll_part, bool fast, cudaStream_t s) {
-  if (N <= 0) return;
+i64 exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,
+                double *ll_part, bool fast, cudaStream_t s) {
+  if (N <= 0) return 0;
   constexpr int TM = 32, TK = 64, DC = 32;
   dim3 g(grid1(N, TM), grid1(m.K, TK));
   VLB_LAUNCH("exact_logp", s,
@@ -495,6 +495,7 @@ void exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &d
   VLB_LAUNCH("exact_normalize", s,
              k_normalize<T><<<grid1(N, 8), kThreads, 0, s>>>(q, N, (int)m.K, fast ? 1 : 0,
                                                              ll_part));
+  return (i64)grid1(N, 8);
 }
 
 void sum_doubles(const double *part, i64 n, double *out, cudaStream_t s) {
@@ -635,8 +636,8 @@ void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const D
 // ------------------------------------------------------ instantiations
 #define VLB_INST(T)                                                                          \
   template void exact_prepare<T>(const DevModel<T> &, DevDerived<T> &, cudaStream_t);        \
-  template void exact_estep<T>(const T *, i64, const DevModel<T> &, const DevDerived<T> &,   \
-                               T *, double *, bool, cudaStream_t);                           \
+  template i64 exact_estep<T>(const T *, i64, const DevModel<T> &, const DevDerived<T> &,    \
+                              T *, double *, bool, cudaStream_t);                            \
   template void exact_mstep<T>(const T *, i64, const T *, T *, T *, T *, i64, i64,           \
                                const double *, cudaStream_t);                                \
   template void column_mass<T>(const T *, i64, i64, double *, cudaStream_t);                 \

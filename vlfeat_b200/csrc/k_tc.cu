@@ -1,12 +1,953 @@
-// Tensor-core (tcgen05) path: not built yet; every call routes to the exact kernels.
+// Tensor-core (tcgen05) path for float data.
+//
+// The two contractions of the GMM / Fisher path run on the 5th-generation
+// tensor cores with fp32 accumulators in TMEM:
+//
+//  E-step   S = [x', x'^2] . W^T,  W_k = [mu'_k / sigma2_k, -1 / (2 sigma2_k)] * log2(e)
+//           x' = x - m (m: mean of the component means), so that
+//           log2 p_ik = cst2_k + S_ik with cst2_k the per-component constant of
+//           vl/gmm.c:741-774 in base 2.  The epilogue (4 warps, one row per
+//           thread) turns the TMEM row into posteriors with a log-sum-exp:
+//           max, exp2 + sum (written back to TMEM), normalise, store.
+//  Stats    T = q^T . [x', x'^2, 1]  (per component: sum q x', sum q x'^2, sum q)
+//           accumulated over a work item (a run of rows of one image) in TMEM
+//           and drained to a per-item fp32 partial; a finalize kernel reduces
+//           an image's partials in double and forms the Fisher vector
+//           (vl/fisher.c:419-485) or the M-step update (vl/gmm.c:1169-1205).
+//
+// Precision: both operands are split into bf16 hi + lo parts and each product
+// is formed as hi.hi + hi.lo + lo.hi (bf16x3, ~2^-17 relative per product,
+// fp32 accumulation).  The BF16 mode keeps the split on the E-step (the
+// expanded quadratic cancels) and uses a single bf16 pass for the statistics.
+//
+// Both kernels are persistent and warp-specialised (288 threads):
+//   warps 0-3  producers: load fp32 rows, centre/square, split, and write the
+//              swizzled bf16 operand tiles into a ring of shared-memory stages;
+//   warps 4-7  epilogue: TMEM -> registers -> global;
+//   warp 8     TMEM allocation and, from one lane, tcgen05.mma issue.
+// Operand layouts: E-step A and W are K-major with the 64-byte swizzle (one
+// 32-element k-atom per stage); statistics A (q^T) and B are MN-major with the
+// 128-byte swizzle, which matches the row-major q and x in global memory.
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
 #include "engine.h"
+#include "tc_common.cuh"
+
+extern "C" {
+#include "vlb200.h"
+}
+
 namespace vlb {
-bool tc_supported(i64, i64) { return false; }
-void tc_estep(const float *, i64, const DevModel<float> &, float *, double *, bool, int, cudaStream_t) {
-  throw Error(VL_ERR_BAD_ARG, "tensor-core E-step not available");
+
+namespace {
+
+using namespace tc;
+
+constexpr int kTcThreads = 288;
+constexpr int kSmemLimit = 232448;  // 227 KB opt-in per block
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr double kLn2 = 0.6931471805599453;
+
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    VLB_CUDA(cudaGetDevice(&dev));
+    VLB_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return n;
 }
-void tc_fisher_batch(const float *, const i64 *, i64, const DevModel<float> &, float *,
-                     unsigned long long *, int, int, cudaStream_t) {
-  throw Error(VL_ERR_BAD_ARG, "tensor-core Fisher encoder not available");
+
+__device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
+  return (uint8_t *)(((uintptr_t)p + 1023) & ~(uintptr_t)1023);
 }
+
+// ================================================================ prep
+// Centre m_d = mean over components of mu_kd.
+__global__ void k_tc_center(const float *__restrict__ means, int K, int D, float *__restrict__ ctr) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= D) return;
+  double s = 0;
+  for (int k = 0; k < K; ++k) s += (double)means[(i64)k * D + d];
+  ctr[d] = (float)(s / (double)K);
+}
+
+// W image (hi then lo), K-major 64-byte-swizzled k-atoms of 32 elements:
+// part p, atom c, row k, element e -> p*wbytes + c*Kp*64 + swizzled(k, e).
+__global__ void k_tc_wimg(const float *__restrict__ means, const float *__restrict__ covs,
+                          const float *__restrict__ ctr, int K, int Kp, int D,
+                          __nv_bfloat16 *__restrict__ wimg) {
+  const int KD2 = 2 * D;
+  i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (i64)Kp * KD2) return;
+  const int k = (int)(idx / KD2), e = (int)(idx % KD2);
+  double w = 0;
+  if (k < K) {
+    const int d = e < D ? e : e - D;
+    const double s2 = (double)covs[(i64)k * D + d];
+    const double mup = (double)means[(i64)k * D + d] - (double)ctr[d];
+    w = (e < D ? mup / s2 : -0.5 / s2) * 1.4426950408889634;
+  }
+  __nv_bfloat16 hi, lo;
+  split_bf16((float)w, hi, lo);
+  const size_t wbytes = (size_t)(KD2 / 32) * Kp * 64;
+  const int c = e / 32, ee = e % 32;
+  const size_t off = (size_t)c * Kp * 64 + kmajor_sw64_off(k, ee / 8) + (ee % 8) * 2;
+  char *base = (char *)wimg;
+  *(__nv_bfloat16 *)(base + off) = hi;
+  *(__nv_bfloat16 *)(base + wbytes + off) = lo;
+}
+
+// cst2_k = log2(e) * (log pi_k - D/2 log 2pi - 1/2 sum log s2 - 1/2 sum mu'^2/s2),
+// -inf for padding and for priors below 1e-6 (vl/gmm.c:746-747).
+__global__ void k_tc_cst(const float *__restrict__ priors, const float *__restrict__ means,
+                         const float *__restrict__ covs, const float *__restrict__ ctr, int K,
+                         int Kp, int D, float *__restrict__ cst2) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Kp) return;
+  if (k >= K || (double)priors[k] < 1e-6) {
+    cst2[k] = -INFINITY;
+    return;
+  }
+  double c = log((double)priors[k]) - 0.5 * (double)D * log(2.0 * 3.141592653589793);
+  for (int d = 0; d < D; ++d) {
+    const double s2 = (double)covs[(i64)k * D + d];
+    const double mup = (double)means[(i64)k * D + d] - (double)ctr[d];
+    c -= 0.5 * log(s2) + 0.5 * mup * mup / s2;
+  }
+  cst2[k] = (float)(c * 1.4426950408889634);
+}
+
+// ============================================================ E-step
+struct EParams {
+  const float *X;
+  i64 N;
+  int K, Kp, nst;
+  const uint4 *wimg;
+  const float *cst2;
+  const float *ctr;
+  void *q;
+  int ldq;
+  int fast;
+  unsigned *rowcnt;
+  double *ll_part;
+  int *err;
+  i64 ntiles;
+};
+
+template <int DIM, bool SPLIT3>
+struct ELayout {
+  static constexpr int KD2 = 2 * DIM;
+  static constexpr int NKA = KD2 / 32;
+  static constexpr int NP = SPLIT3 ? 2 : 1;
+  static constexpr int kStage = NP * 8192;
+  __host__ __device__ static size_t wbytes(int Kp) { return (size_t)NKA * Kp * 64; }
+  static size_t fixed(int Kp) { return NP * wbytes(Kp) + 1024 /*cst*/ + 1024 /*ctr*/ + 1024 /*bars*/ + 1024; }
+  static int max_stages(int Kp) { return (int)((kSmemLimit - fixed(Kp)) / kStage); }
+  static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * kStage; }
+};
+
+template <int DIM, bool SPLIT3, bool OUT_BF16>
+__global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
+  using L = ELayout<DIM, SPLIT3>;
+  constexpr int NKA = L::NKA, NP = L::NP;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *base = align1024(smem_raw);
+  const uint32_t wbytes = (uint32_t)L::wbytes(p.Kp);
+  uint8_t *sW = base;
+  uint8_t *sA = sW + NP * wbytes;
+  float *s_cst = (float *)(sA + (size_t)p.nst * L::kStage);
+  float *s_ctr = s_cst + 256;
+  uint64_t *bars = (uint64_t *)(s_ctr + 256);
+  uint64_t *full = bars, *empty = bars + 16, *accf = bars + 32, *acce = bars + 34;
+  uint32_t *s_tmem = (uint32_t *)(bars + 40);
+  volatile int *s_abort = (volatile int *)(s_tmem + 1);
+
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  if (tid == 0) {
+    for (int s = 0; s < p.nst; ++s) {
+      mbar_init(&full[s], 128);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 128);
+    }
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 8) {
+    tmem_alloc(s_tmem, 512);
+    tmem_relinquish();
+  }
+  // Resident W (pre-swizzled image) and per-component constants.
+  {
+    const uint4 *src = p.wimg;
+    uint4 *dst = (uint4 *)sW;
+    const int n16 = (int)(NP * wbytes / 16);
+    for (int i = tid; i < n16; i += kTcThreads) dst[i] = src[i];
+    for (int k = tid; k < 256; k += kTcThreads) s_cst[k] = k < p.Kp ? p.cst2[k] : -INFINITY;
+    for (int d = tid; d < DIM; d += kTcThreads) s_ctr[d] = p.ctr[d];
+    fence_proxy_async_smem();
+  }
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  if (warp < 4) {
+    // ---------------------------------------------------- producers
+    const int r = tid;  // row within the tile
+    int it = 0;
+    bool ok = true;
+    for (i64 tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x) {
+      const i64 row = tile * 128 + r;
+      float xr[DIM];
+      if (row < p.N) {
+        const float4 *src = (const float4 *)(p.X + row * DIM);
+#pragma unroll
+        for (int j = 0; j < DIM / 4; ++j) {
+          float4 v = __ldg(src + j);
+          xr[4 * j + 0] = v.x - s_ctr[4 * j + 0];
+          xr[4 * j + 1] = v.y - s_ctr[4 * j + 1];
+          xr[4 * j + 2] = v.z - s_ctr[4 * j + 2];
+          xr[4 * j + 3] = v.w - s_ctr[4 * j + 3];
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) xr[j] = 0.f;
+      }
+#pragma unroll
+      for (int c = 0; c < NKA; ++c) {
+        const int stage = it % p.nst;
+        if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 1)) {
+          ok = false;
+          break;
+        }
+        const uint32_t a_hi = smem_u32(sA + (size_t)stage * L::kStage);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          uint32_t wh[4], wl[4];
+#pragma unroll
+          for (int j = 0; j < 8; j += 2) {
+            float v0, v1;
+            {
+              const int e = 32 * c + 8 * g + j;
+              v0 = e < DIM ? xr[e < DIM ? e : 0] : xr[e >= DIM ? e - DIM : 0] * xr[e >= DIM ? e - DIM : 0];
+            }
+            {
+              const int e = 32 * c + 8 * g + j + 1;
+              v1 = e < DIM ? xr[e < DIM ? e : 0] : xr[e >= DIM ? e - DIM : 0] * xr[e >= DIM ? e - DIM : 0];
+            }
+            __nv_bfloat16 h0, l0, h1, l1;
+            split_bf16(v0, h0, l0);
+            split_bf16(v1, h1, l1);
+            wh[j / 2] = pack_bf16(h0, h1);
+            wl[j / 2] = pack_bf16(l0, l1);
+          }
+          const uint32_t off = kmajor_sw64_off((uint32_t)r, (uint32_t)g);
+          st_shared_v4(a_hi + off, wh[0], wh[1], wh[2], wh[3]);
+          if (SPLIT3) st_shared_v4(a_hi + 8192 + off, wl[0], wl[1], wl[2], wl[3]);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(&full[stage]);
+        ++it;
+      }
+    }
+  } else if (warp < 8) {
+    // ----------------------------------------------------- epilogue
+    const int ew = warp - 4;
+    const int r = ew * 32 + lane;
+    const int nch = p.Kp / 32;
+    int tt = 0;
+    for (i64 tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++tt) {
+      const int buf = tt & 1;
+      if (!mbar_wait(&accf[buf], (tt >> 1) & 1, s_abort, p.err, 2)) break;
+      tc_fence_after();
+      const uint32_t tb = tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(buf * 256);
+      float m2 = -INFINITY;
+      int am = 0;
+      for (int cc = 0; cc < nch; ++cc) {
+        uint32_t v[32];
+        tmem_ld32(tb + cc * 32, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const float s = __uint_as_float(v[j]) + s_cst[cc * 32 + j];
+          if (s > m2) {
+            m2 = s;
+            am = cc * 32 + j;
+          }
+        }
+      }
+      float sum = 0.f;
+      for (int cc = 0; cc < nch; ++cc) {
+        uint32_t v[32];
+        tmem_ld32(tb + cc * 32, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const float e = ex2_approx(__uint_as_float(v[j]) + s_cst[cc * 32 + j] - m2);
+          sum += e;
+          v[j] = __float_as_uint(e);
+        }
+        tmem_st32(tb + cc * 32, v);
+      }
+      tmem_wait_st();
+      const float inv = 1.f / sum;
+      const i64 row = tile * 128 + r;
+      const bool valid = row < p.N;
+      unsigned cnt = 0;
+      for (int cc = 0; cc < nch; ++cc) {
+        uint32_t v[32];
+        tmem_ld32(tb + cc * 32, v);
+        tmem_wait_ld();
+        if (!valid) continue;
+        float qv[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          float x = p.fast ? (cc * 32 + j == am ? 1.f : 0.f) : __uint_as_float(v[j]) * inv;
+          qv[j] = x;
+          cnt += (x >= 1e-6f) ? 1u : 0u;
+        }
+        const int k0 = cc * 32;
+        if (OUT_BF16) {
+          __nv_bfloat16 *dst = (__nv_bfloat16 *)p.q + row * p.ldq + k0;
+          if (k0 + 32 <= p.K && (p.ldq % 8) == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 8) {
+              uint4 w;
+              w.x = pack_bf16(__float2bfloat16_rn(qv[j]), __float2bfloat16_rn(qv[j + 1]));
+              w.y = pack_bf16(__float2bfloat16_rn(qv[j + 2]), __float2bfloat16_rn(qv[j + 3]));
+              w.z = pack_bf16(__float2bfloat16_rn(qv[j + 4]), __float2bfloat16_rn(qv[j + 5]));
+              w.w = pack_bf16(__float2bfloat16_rn(qv[j + 6]), __float2bfloat16_rn(qv[j + 7]));
+              *(uint4 *)(dst + j) = w;
+            }
+          } else {
+            for (int j = 0; j < 32 && k0 + j < p.K; ++j) dst[j] = __float2bfloat16_rn(qv[j]);
+          }
+        } else {
+          float *dst = (float *)p.q + row * p.ldq + k0;
+          if (k0 + 32 <= p.K && (p.ldq % 4) == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+              *(float4 *)(dst + j) = make_float4(qv[j], qv[j + 1], qv[j + 2], qv[j + 3]);
+          } else {
+            for (int j = 0; j < 32 && k0 + j < p.K; ++j) dst[j] = qv[j];
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[buf]);
+      if (valid && p.rowcnt) p.rowcnt[row] = cnt;
+      // Per-warp log-likelihood partial (fixed shuffle order): 4 per tile.
+      double ll = valid ? ((double)m2 + log2((double)sum)) * kLn2 : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
+      if (lane == 0 && p.ll_part) p.ll_part[tile * 4 + ew] = ll;
+    }
+  } else if (lane == 0) {
+    // ---------------------------------------------------------- MMA
+    const uint32_t idesc = idesc_bf16(128, p.Kp, false, false);
+    const uint32_t w_hi = smem_u32(sW), w_lo = w_hi + wbytes;
+    int it = 0, tt = 0;
+    bool ok = true;
+    for (i64 tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x, ++tt) {
+      const int buf = tt & 1;
+      if (!mbar_wait(&acce[buf], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 3)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + (uint32_t)(buf * 256);
+      for (int c = 0; c < NKA; ++c) {
+        const int stage = it % p.nst;
+        if (!mbar_wait(&full[stage], (it / p.nst) & 1, s_abort, p.err, 4)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t a_hi = smem_u32(sA + (size_t)stage * L::kStage);
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+          const uint64_t ah = sdesc(a_hi + ks * 32, 16, 512, kSw64);
+          const uint64_t bh = sdesc(w_hi + c * p.Kp * 64 + ks * 32, 16, 512, kSw64);
+          mma_bf16(d, ah, bh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+          if (SPLIT3) {
+            const uint64_t bl = sdesc(w_lo + c * p.Kp * 64 + ks * 32, 16, 512, kSw64);
+            const uint64_t al = sdesc(a_hi + 8192 + ks * 32, 16, 512, kSw64);
+            mma_bf16(d, ah, bl, idesc, 1u);
+            mma_bf16(d, al, bh, idesc, 1u);
+          }
+        }
+        mma_commit(&empty[stage]);
+        ++it;
+      }
+      if (ok) mma_commit(&accf[buf]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// ========================================================== statistics
+struct SItem {
+  i64 row0, row1;  // absolute rows of X
+  int slot, pad;
+};
+
+struct SParams {
+  const float *X;
+  const void *q;
+  i64 qbase;  // row of X that q's first row corresponds to
+  int ldq, K, Kp, nst;
+  const float *ctr;
+  float qthr;
+  const SItem *items;
+  const int *order;     // item indices, grouped per CTA
+  const int *cta_beg;   // gridDim.x + 1 offsets into order
+  float *partial;       // [slot][Kp][NST]
+  int *err;
+};
+
+template <int DIM, int MT, bool SPLIT3>
+struct SLayout {
+  static constexpr int NST = 2 * DIM + 16;            // x', x'^2, [1, 0 x 15]
+  static constexpr int NB = (NST + 63) / 64;           // 64-feature MN blocks
+  static constexpr int NCH = (NST + 255) / 256;        // MMA N chunks
+  static constexpr int NP = SPLIT3 ? 2 : 1;
+  static constexpr int A_PART = MT * 2 * 4 * 1024;     // [kgroup 4][mnblk 2MT][1 KB]
+  static constexpr int B_PART = NB * 4 * 1024;         // [kgroup 4][nblk NB][1 KB]
+  static constexpr int kStage = NP * (A_PART + B_PART);
+  static constexpr size_t fixed = 1024 /*ctr*/ + 1024 /*bars*/ + 1024;
+  static int max_stages() { return (int)((kSmemLimit - fixed) / kStage); }
+  static size_t bytes(int nst) { return fixed + (size_t)nst * kStage; }
+  static_assert(MT * NST <= 512, "accumulators exceed TMEM");
+};
+
+template <int DIM, int MT, bool SPLIT3, bool Q_BF16>
+__global__ void __launch_bounds__(kTcThreads, 1) k_tc_stats(const SParams p) {
+  using L = SLayout<DIM, MT, SPLIT3>;
+  constexpr int NST = L::NST, NB = L::NB, NP = L::NP;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *base = align1024(smem_raw);
+  uint8_t *sS = base;
+  float *s_ctr = (float *)(sS + (size_t)p.nst * L::kStage);
+  uint64_t *bars = (uint64_t *)(s_ctr + 256);
+  uint64_t *full = bars, *empty = bars + 16, *accf = bars + 32, *acce = bars + 33;
+  uint32_t *s_tmem = (uint32_t *)(bars + 40);
+  volatile int *s_abort = (volatile int *)(s_tmem + 1);
+
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int comp0 = blockIdx.y * MT * 128;  // first component of this CTA's M tiles
+  if (tid == 0) {
+    for (int s = 0; s < p.nst; ++s) {
+      mbar_init(&full[s], 128);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accf, 1);
+    mbar_init(acce, 128);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 8) {
+    tmem_alloc(s_tmem, 512);
+    tmem_relinquish();
+  }
+  for (int d = tid; d < DIM; d += kTcThreads) s_ctr[d] = p.ctr[d];
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  const int ib = p.cta_beg[blockIdx.x], ie = p.cta_beg[blockIdx.x + 1];
+
+  if (warp < 4) {
+    // ---------------------------------------------------- producers
+    const int r = tid >> 2, qq = tid & 3;  // row of the 32-row stage, quarter
+    const int kr = r & 7, kg = r >> 3;
+    int it = 0;
+    bool ok = true;
+    for (int ii = ib; ii < ie && ok; ++ii) {
+      const SItem item = p.items[p.order[ii]];
+      for (i64 rb = item.row0; rb < item.row1 && ok; rb += 32) {
+        const int stage = it % p.nst;
+        if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 11)) {
+          ok = false;
+          break;
+        }
+        const uint32_t sa = smem_u32(sS + (size_t)stage * L::kStage);
+        const uint32_t sb = sa + NP * L::A_PART;
+        const i64 row = rb + r;
+        const bool valid = row < item.row1;
+        // A = q^T: this thread covers components [qq*MT*32, (qq+1)*MT*32).
+#pragma unroll
+        for (int j = 0; j < MT * 4; ++j) {
+          const int cl = qq * MT * 32 + j * 8;  // local component (0 .. MT*128)
+          const int kc = comp0 + cl;
+          float v[8];
+          if (valid && kc < p.K) {
+            if (Q_BF16) {
+              const uint4 w = *(const uint4 *)((const __nv_bfloat16 *)p.q + (row - p.qbase) * p.ldq + kc);
+              const __nv_bfloat16 *h = (const __nv_bfloat16 *)&w;
+#pragma unroll
+              for (int t = 0; t < 8; ++t) v[t] = __bfloat162float(h[t]);
+            } else {
+              const float4 *src = (const float4 *)((const float *)p.q + (row - p.qbase) * p.ldq + kc);
+              const float4 a = src[0], b = src[1];
+              v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+              v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+            }
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+              if (v[t] < p.qthr || kc + t >= p.K) v[t] = 0.f;
+            }
+          } else {
+#pragma unroll
+            for (int t = 0; t < 8; ++t) v[t] = 0.f;
+          }
+          uint32_t wh[4], wl[4];
+#pragma unroll
+          for (int t = 0; t < 8; t += 2) {
+            __nv_bfloat16 h0, l0, h1, l1;
+            split_bf16(v[t], h0, l0);
+            split_bf16(v[t + 1], h1, l1);
+            wh[t / 2] = pack_bf16(h0, h1);
+            wl[t / 2] = pack_bf16(l0, l1);
+          }
+          const uint32_t off = kg * (MT * 2 * 1024) + (cl >> 6) * 1024 + mnmajor_sw128_off(kr, (cl & 63) >> 3);
+          st_shared_v4(sa + off, wh[0], wh[1], wh[2], wh[3]);
+          if (SPLIT3) st_shared_v4(sa + L::A_PART + off, wl[0], wl[1], wl[2], wl[3]);
+        }
+        // B = [x', x'^2, 1, 0...]: this thread covers feature chunks [qq*NB*2, (qq+1)*NB*2).
+#pragma unroll
+        for (int j = 0; j < NB * 2; ++j) {
+          const int f0 = (qq * NB * 2 + j) * 8;
+          float v[8];
+#pragma unroll
+          for (int t = 0; t < 8; ++t) v[t] = 0.f;
+          if (valid) {
+            if (f0 < 2 * DIM) {
+              const int d0 = f0 < DIM ? f0 : f0 - DIM;
+              const float4 *src = (const float4 *)(p.X + row * DIM + d0);
+              const float4 a = __ldg(src), b = __ldg(src + 1);
+              v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+              v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+#pragma unroll
+              for (int t = 0; t < 8; ++t) {
+                v[t] -= s_ctr[d0 + t];
+                if (f0 >= DIM) v[t] = v[t] * v[t];
+              }
+            } else if (f0 == 2 * DIM) {
+              v[0] = 1.f;
+            }
+          }
+          uint32_t wh[4], wl[4];
+#pragma unroll
+          for (int t = 0; t < 8; t += 2) {
+            __nv_bfloat16 h0, l0, h1, l1;
+            split_bf16(v[t], h0, l0);
+            split_bf16(v[t + 1], h1, l1);
+            wh[t / 2] = pack_bf16(h0, h1);
+            wl[t / 2] = pack_bf16(l0, l1);
+          }
+          const uint32_t off = kg * (NB * 1024) + (f0 >> 6) * 1024 + mnmajor_sw128_off(kr, (f0 & 63) >> 3);
+          st_shared_v4(sb + off, wh[0], wh[1], wh[2], wh[3]);
+          if (SPLIT3) st_shared_v4(sb + L::B_PART + off, wl[0], wl[1], wl[2], wl[3]);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive(&full[stage]);
+        ++it;
+      }
+    }
+  } else if (warp < 8) {
+    // ----------------------------------------------------- epilogue
+    const int ew = warp - 4;
+    int n = 0;
+    for (int ii = ib; ii < ie; ++ii, ++n) {
+      const SItem item = p.items[p.order[ii]];
+      if (!mbar_wait(accf, n & 1, s_abort, p.err, 12)) break;
+      tc_fence_after();
+#pragma unroll 1
+      for (int mt = 0; mt < MT; ++mt) {
+        const int comp = comp0 + mt * 128 + ew * 32 + lane;
+        float *dst = p.partial + ((size_t)item.slot * p.Kp + comp) * NST;
+        const uint32_t tb = tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(mt * NST);
+#pragma unroll 1
+        for (int cc = 0; cc < (NST + 31) / 32; ++cc) {
+          uint32_t v[32];
+          tmem_ld32(tb + cc * 32, v);
+          tmem_wait_ld();
+          if (comp < p.Kp) {
+            if (cc * 32 + 32 <= NST) {
+#pragma unroll
+              for (int j = 0; j < 32; j += 4)
+                *(float4 *)(dst + cc * 32 + j) = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                              __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+            } else {
+#pragma unroll
+              for (int j = 0; j < 32; ++j)
+                if (cc * 32 + j < NST) dst[cc * 32 + j] = __uint_as_float(v[j]);
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acce);
+    }
+  } else if (lane == 0) {
+    // ---------------------------------------------------------- MMA
+    int it = 0, n = 0;
+    bool ok = true;
+    for (int ii = ib; ii < ie && ok; ++ii, ++n) {
+      const SItem item = p.items[p.order[ii]];
+      if (!mbar_wait(acce, (n & 1) ^ 1, s_abort, p.err, 13)) break;
+      tc_fence_after();
+      int chunk = 0;
+      for (i64 rb = item.row0; rb < item.row1; rb += 32, ++chunk) {
+        const int stage = it % p.nst;
+        if (!mbar_wait(&full[stage], (it / p.nst) & 1, s_abort, p.err, 14)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(sS + (size_t)stage * L::kStage);
+        const uint32_t sb = sa + NP * L::A_PART;
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+#pragma unroll
+          for (int mt = 0; mt < MT; ++mt) {
+            const uint32_t a0 = sa + ks * 2 * (MT * 2 * 1024) + mt * 2 * 1024;
+            const uint64_t ah = sdesc(a0, 1024, MT * 2 * 1024, kSw128);
+            const uint64_t al = sdesc(a0 + L::A_PART, 1024, MT * 2 * 1024, kSw128);
+#pragma unroll
+            for (int nc = 0; nc < L::NCH; ++nc) {
+              const int nn = (NST - nc * 256) < 256 ? (NST - nc * 256) : 256;
+              const uint32_t idesc = idesc_bf16(128, nn, true, true);
+              const uint32_t b0 = sb + ks * 2 * (NB * 1024) + nc * 4 * 1024;
+              const uint64_t bh = sdesc(b0, 1024, NB * 1024, kSw128);
+              const uint32_t d = tmem + (uint32_t)(mt * NST + nc * 256);
+              const uint32_t acc = (chunk > 0 || ks > 0) ? 1u : 0u;
+              mma_bf16(d, ah, bh, idesc, acc);
+              if (SPLIT3) {
+                const uint64_t bl = sdesc(b0 + L::B_PART, 1024, NB * 1024, kSw128);
+                mma_bf16(d, ah, bl, idesc, 1u);
+                mma_bf16(d, al, bh, idesc, 1u);
+              }
+            }
+          }
+        }
+        mma_commit(&empty[stage]);
+        ++it;
+      }
+      if (ok) mma_commit(accf);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// ======================================================= finalize (FV)
+// Per image: reduce the item partials in double and form the Fisher vector
+// (vl/fisher.c:419-485) from S0 = sum q, S1 = sum q x', S2 = sum q x'^2:
+//   u = s (S1 - mu' S0),  v = s^2 (S2 - 2 mu' S1 + mu'^2 S0) - S0,
+// scaled by 1/(N sqrt pi) and 1/(N sqrt(2 pi)); signed sqrt; L2.
+__global__ void __launch_bounds__(256) k_tc_fv_finalize(
+    int K, int Kp, int D, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
+    const i64 *__restrict__ imgRow0, const float *__restrict__ means, const float *__restrict__ covs,
+    const float *__restrict__ priors, const float *__restrict__ ctr, const unsigned *__restrict__ rowcnt,
+    i64 rowcntBase, int flags, i64 imgBase, float *__restrict__ enc,
+    unsigned long long *__restrict__ nterms) {
+  __shared__ double sh[256];
+  __shared__ unsigned long long shn[256];
+  const int img = blockIdx.x;
+  const int s0 = imgSlot0[img], s1 = imgSlot0[img + 1];
+  const i64 r0 = imgRow0[img], r1 = imgRow0[img + 1];
+  const i64 n = r1 - r0;
+  const int NST = 2 * D + 16;
+  const i64 KD = (i64)K * D;
+  float *out = enc + (imgBase + img) * 2 * KD;
+  double sq = 0;
+  for (i64 e = threadIdx.x; e < KD; e += 256) {
+    const int k = (int)(e / D), d = (int)(e % D);
+    double S0 = 0, S1 = 0, S2 = 0;
+    for (int s = s0; s < s1; ++s) {
+      const float *pp = partial + ((size_t)s * Kp + k) * NST;
+      S0 += (double)pp[2 * D];
+      S1 += (double)pp[d];
+      S2 += (double)pp[D + d];
+    }
+    const double pk = (double)priors[k];
+    double u = 0, v = 0;
+    if (pk >= 1e-6 && n > 0) {
+      const double s2 = (double)covs[e];
+      const double mup = (double)means[e] - (double)ctr[d];
+      const double isd = 1.0 / sqrt(s2);
+      u = isd * (S1 - mup * S0);
+      v = (S2 - 2.0 * mup * S1 + mup * mup * S0) / s2 - S0;
+      u *= 1.0 / ((double)n * sqrt(pk));
+      v *= 1.0 / ((double)n * sqrt(2.0 * pk));
+    }
+    float uf = (float)u, vf = (float)v;
+    if (flags & 1) {
+      uf = uf >= 0.f ? sqrtf(uf) : -sqrtf(-uf);
+      vf = vf >= 0.f ? sqrtf(vf) : -sqrtf(-vf);
+    }
+    out[e] = uf;
+    out[KD + e] = vf;
+    sq += (double)uf * uf + (double)vf * vf;
+  }
+  unsigned long long nt = 0;
+  if (rowcnt)
+    for (i64 r = r0 + threadIdx.x; r < r1; r += 256) nt += rowcnt[r - rowcntBase];
+  sh[threadIdx.x] = sq;
+  shn[threadIdx.x] = nt;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sh[threadIdx.x] += sh[threadIdx.x + o];
+      shn[threadIdx.x] += shn[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && nterms) nterms[imgBase + img] = shn[0];
+  if (flags & 2) {
+    double nrm = sqrt(sh[0]);
+    if (nrm < 1e-12) nrm = 1e-12;
+    const float nf = (float)nrm;
+    for (i64 e = threadIdx.x; e < 2 * KD; e += 256) out[e] = out[e] / nf;
+  }
+}
+
+// ================================================================ host
+struct TcPrep {
+  int K = 0, Kp = 0, D = 0;
+  float *ctr = nullptr, *cst2 = nullptr;
+  __nv_bfloat16 *wimg = nullptr;
+};
+
+int padK(i64 K) { return (int)((K + 15) / 16 * 16); }
+
+void tc_prepare(const DevModel<float> &m, TcPrep &tp, cudaStream_t s) {
+  Scratch &sc = thread_scratch();
+  tp.K = (int)m.K;
+  tp.Kp = padK(m.K);
+  tp.D = (int)m.D;
+  const int KD2 = 2 * tp.D;
+  tp.ctr = sc.slot[0].get<float>(256);
+  tp.cst2 = sc.slot[1].get<float>(256);
+  tp.wimg = sc.slot[2].get<__nv_bfloat16>((size_t)2 * tp.Kp * KD2);
+  VLB_LAUNCH("tc_center", s, k_tc_center<<<(tp.D + 127) / 128, 128, 0, s>>>(m.means, tp.K, tp.D, tp.ctr));
+  const i64 n = (i64)tp.Kp * KD2;
+  VLB_LAUNCH("tc_wimage", s,
+             k_tc_wimg<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.Kp,
+                                                                  tp.D, tp.wimg));
+  VLB_LAUNCH("tc_constants", s,
+             k_tc_cst<<<(tp.Kp + 127) / 128, 128, 0, s>>>(m.priors, m.means, m.covs, tp.ctr, tp.K,
+                                                          tp.Kp, tp.D, tp.cst2));
+}
+
+template <int DIM, bool SPLIT3, bool OUT_BF16>
+i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
+                 unsigned *rowcnt, double *ll_part, int *err, cudaStream_t s) {
+  using L = ELayout<DIM, SPLIT3>;
+  const i64 ntiles = (N + 127) / 128;
+  if (ntiles == 0) return 0;
+  const int nst = std::min(8, L::max_stages(tp.Kp));
+  VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
+  const size_t smem = L::bytes(tp.Kp, nst);
+  auto kern = k_tc_estep<DIM, SPLIT3, OUT_BF16>;
+  VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EParams p;
+  p.X = X; p.N = N; p.K = tp.K; p.Kp = tp.Kp; p.nst = nst;
+  p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr;
+  p.q = q; p.ldq = ldq; p.fast = fast ? 1 : 0; p.rowcnt = rowcnt; p.ll_part = ll_part;
+  p.err = err; p.ntiles = ntiles;
+  const int grid = (int)std::min<i64>(ntiles, num_sms());
+  VLB_LAUNCH(SPLIT3 ? "tc_estep_bf16x3" : "tc_estep_bf16", s,
+             kern<<<grid, kTcThreads, smem, s>>>(p));
+  return ntiles * 4;  // LL partials written
+}
+
+template <int DIM, int MT, bool SPLIT3, bool Q_BF16>
+void launch_stats(const SParams &p0, int grid_x, int grid_y, cudaStream_t s) {
+  using L = SLayout<DIM, MT, SPLIT3>;
+  SParams p = p0;
+  p.nst = std::min(6, L::max_stages());
+  VLB_CHECK(p.nst >= 2, VL_ERR_BAD_ARG, "tensor-core statistics: operands exceed shared memory");
+  const size_t smem = L::bytes(p.nst);
+  auto kern = k_tc_stats<DIM, MT, SPLIT3, Q_BF16>;
+  VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  VLB_LAUNCH(SPLIT3 ? "tc_stats_bf16x3" : "tc_stats_bf16", s,
+             kern<<<dim3(grid_x, grid_y), kTcThreads, smem, s>>>(p));
+}
+
+// Dimension dispatch: the kernels are instantiated for the descriptor sizes
+// of the benchmarked configurations.
+template <template <int> class F, typename... A>
+auto dispatch_dim(int D, A &&...a) {
+  switch (D) {
+    case 64: return F<64>::run(std::forward<A>(a)...);
+    case 80: return F<80>::run(std::forward<A>(a)...);
+    case 128: return F<128>::run(std::forward<A>(a)...);
+    default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
+  }
+}
+
+template <int DIM>
+struct EstepRun {
+  static i64 run(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast, bool out_bf16,
+                 unsigned *rowcnt, double *ll, int *err, cudaStream_t s) {
+    if (out_bf16) return launch_estep<DIM, true, true>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+    return launch_estep<DIM, true, false>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+  }
+};
+
+template <int DIM>
+struct StatsRun {
+  static constexpr int MT = (2 * (2 * DIM + 16) <= 512) ? 2 : 1;
+  static int mt() { return MT; }
+  static void run(const SParams &p, int grid_x, int Kp, bool split3, bool q_bf16, cudaStream_t s) {
+    const int grid_y = (Kp + MT * 128 - 1) / (MT * 128);
+    if (split3) {
+      if (q_bf16) launch_stats<DIM, MT, true, true>(p, grid_x, grid_y, s);
+      else launch_stats<DIM, MT, true, false>(p, grid_x, grid_y, s);
+    } else {
+      if (q_bf16) launch_stats<DIM, MT, false, true>(p, grid_x, grid_y, s);
+      else launch_stats<DIM, MT, false, false>(p, grid_x, grid_y, s);
+    }
+  }
+};
+
+void check_err(int *derr, cudaStream_t s) {
+  int h = 0;
+  VLB_CUDA(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  if (h) throw Error(VL_ERR_BAD_ARG, "tensor-core kernel gave up waiting (code " + std::to_string(h) + ")");
+}
+
+}  // namespace
+
+bool tc_supported(i64 K, i64 D) {
+  if (!(D == 64 || D == 80 || D == 128)) return false;
+  if (K < 8 || K > 256 || K % 8) return false;
+  // Resident W (hi + lo) plus at least two operand stages must fit.
+  const int Kp = padK(K);
+  const size_t w = (size_t)2 * (2 * D / 32) * Kp * 64;
+  return w + 4096 + 2 * 16384 <= (size_t)kSmemLimit;
+}
+
+i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part, bool fast,
+             int precision, cudaStream_t s) {
+  (void)precision;
+  TcPrep tp;
+  tc_prepare(m, tp, s);
+  int *err = thread_scratch().slot[3].get<int>(1);
+  VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  const i64 n = dispatch_dim<EstepRun>(tp.D, X, N, tp, (void *)q, (int)m.K, fast, false,
+                                       (unsigned *)nullptr, ll_part, err, s);
+  check_err(err, s);
+  return n;
+}
+
+void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const DevModel<float> &m,
+                     float *enc, unsigned long long *nterms, int flags, int precision, cudaStream_t s) {
+  Scratch &sc = thread_scratch();
+  TcPrep tp;
+  tc_prepare(m, tp, s);
+  const bool split_stats = (precision == VLB200_PREC_FP32);
+  const bool q_bf16 = !split_stats;
+  const size_t qsz = q_bf16 ? 2 : 4;
+  const i64 K = m.K, D = m.D;
+  const int NST = (int)(2 * D + 16);
+  int *err = sc.slot[3].get<int>(1);
+  VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  const i64 kRowBudget = std::max<i64>(1 << 16, (i64)(4ull << 30) / (K * (i64)qsz));
+  const i64 kItemRows = 8192;
+  const int nsm = num_sms();
+
+  i64 img = 0;
+  while (img < numImages) {
+    const i64 chunkImg0 = img, row0 = h_offsets[img];
+    while (img < numImages && (img == chunkImg0 || h_offsets[img + 1] - row0 <= kRowBudget)) ++img;
+    const i64 nimg = img - chunkImg0, row1 = h_offsets[img], nrows = row1 - row0;
+    // Work items: runs of at most kItemRows rows of one image; images with no
+    // rows get no item (their statistics are zero).
+    std::vector<SItem> items;
+    std::vector<int> slot0(nimg + 1);
+    std::vector<i64> imgRow0(nimg + 1);
+    for (i64 j = 0; j < nimg; ++j) {
+      const i64 a = h_offsets[chunkImg0 + j], b = h_offsets[chunkImg0 + j + 1];
+      slot0[j] = (int)items.size();
+      imgRow0[j] = a;
+      for (i64 r = a; r < b; r += kItemRows) items.push_back({r, std::min(b, r + kItemRows), (int)items.size(), 0});
+    }
+    slot0[nimg] = (int)items.size();
+    imgRow0[nimg] = row1;
+    const int nitems = (int)items.size();
+    // Longest-processing-time assignment of items to persistent CTAs.
+    const int gx = std::max(1, std::min(nitems, nsm));
+    std::vector<int> idx(nitems);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+      return items[a].row1 - items[a].row0 > items[b].row1 - items[b].row0;
+    });
+    std::vector<std::vector<int>> per(gx);
+    std::vector<i64> load(gx, 0);
+    for (int i : idx) {
+      int best = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      per[best].push_back(i);
+      load[best] += items[i].row1 - items[i].row0;
+    }
+    std::vector<int> order, beg(gx + 1, 0);
+    for (int c = 0; c < gx; ++c) {
+      beg[c] = (int)order.size();
+      order.insert(order.end(), per[c].begin(), per[c].end());
+    }
+    beg[gx] = (int)order.size();
+
+    void *q = sc.slot[4].get<char>((size_t)std::max<i64>(1, nrows) * K * qsz);
+    unsigned *rowcnt = sc.slot[5].get<unsigned>(std::max<i64>(1, nrows));
+    float *partial = sc.slot[6].get<float>((size_t)std::max(1, nitems) * tp.Kp * NST);
+    SItem *ditems = sc.slot[7].get<SItem>(std::max(1, nitems));
+    int *dorder = sc.slot[8].get<int>(std::max(1, nitems));
+    int *dbeg = sc.slot[9].get<int>(gx + 1);
+    int *dslot0 = sc.slot[10].get<int>(nimg + 1);
+    i64 *drow0 = sc.slot[11].get<i64>(nimg + 1);
+    if (nitems) {
+      VLB_CUDA(cudaMemcpyAsync(ditems, items.data(), sizeof(SItem) * nitems, cudaMemcpyHostToDevice, s));
+      VLB_CUDA(cudaMemcpyAsync(dorder, order.data(), sizeof(int) * nitems, cudaMemcpyHostToDevice, s));
+    }
+    VLB_CUDA(cudaMemcpyAsync(dbeg, beg.data(), sizeof(int) * (gx + 1), cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(dslot0, slot0.data(), sizeof(int) * (nimg + 1), cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(drow0, imgRow0.data(), sizeof(i64) * (nimg + 1), cudaMemcpyHostToDevice, s));
+
+    if (nrows > 0) {
+      dispatch_dim<EstepRun>(tp.D, X + row0 * D, nrows, tp, q, (int)K, (flags & 4) != 0, q_bf16,
+                             rowcnt, (double *)nullptr, err, s);
+      SParams sp;
+      sp.X = X; sp.q = q; sp.qbase = row0; sp.ldq = (int)K; sp.K = (int)K; sp.Kp = tp.Kp; sp.nst = 0;
+      sp.ctr = tp.ctr; sp.qthr = 1e-6f; sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg;
+      sp.partial = partial; sp.err = err;
+      switch (tp.D) {
+        case 64: StatsRun<64>::run(sp, gx, tp.Kp, split_stats, q_bf16, s); break;
+        case 80: StatsRun<80>::run(sp, gx, tp.Kp, split_stats, q_bf16, s); break;
+        case 128: StatsRun<128>::run(sp, gx, tp.Kp, split_stats, q_bf16, s); break;
+        default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
+      }
+    }
+    VLB_LAUNCH("tc_fv_finalize", s,
+               k_tc_fv_finalize<<<(unsigned)nimg, 256, 0, s>>>(
+                   (int)K, tp.Kp, (int)D, partial, dslot0, drow0, m.means, m.covs, m.priors, tp.ctr,
+                   nrows > 0 ? rowcnt : nullptr, row0, flags, chunkImg0, enc, nterms));
+  }
+  check_err(err, s);
+}
+
 }  // namespace vlb
