@@ -342,11 +342,12 @@ def fisher_encode(data, means, covariances, priors, flags=FLAG_IMPROVED):
 
 
 def _stream(stream):
-    """Stream handle for the library.  None -> the library's own per-thread
-    stream; a torch stream whose handle is 0 (the legacy default stream) is
-    passed as cudaStreamLegacy (0x1) so the work stays ordered with it."""
+    """Stream handle for the library: the given stream, or torch's current
+    stream when None.  A handle of 0 (the legacy default stream) is passed as
+    cudaStreamLegacy (0x1), since 0 would select the library's own stream."""
     if stream is None:
-        return None
+        import torch  # device calls take torch tensors: order with torch's stream
+        stream = torch.cuda.current_stream()
     h = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
     return C.c_void_p(h if h else 1)
 

@@ -62,8 +62,10 @@ int num_sms() {
   return n;
 }
 
+// Rounds a dynamic shared-memory pointer up to 1 KB by pointer arithmetic,
+// so the compiler keeps treating derived pointers as shared memory.
 __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
-  return (uint8_t *)(((uintptr_t)p + 1023) & ~(uintptr_t)1023);
+  return p + ((1024u - (smem_u32(p) & 1023u)) & 1023u);
 }
 
 // ================================================================ prep
@@ -122,44 +124,72 @@ __global__ void k_tc_cst(const float *__restrict__ priors, const float *__restri
   cst2[k] = (float)(c * 1.4426950408889634);
 }
 
+// Per-dimension power-of-two scale for fp16 statistics operands, chosen from
+// the model so that x'' = x' * scale is O(1) for data the model describes:
+// scale_d = 2^-ceil(log2(max_k |mu'_kd| + 4 sigma_kd)).
+__global__ void k_tc_scale(const float *__restrict__ means, const float *__restrict__ covs,
+                           const float *__restrict__ ctr, int K, int D, float *__restrict__ scale) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= D) return;
+  double b = 0;
+  for (int k = 0; k < K; ++k) {
+    const double v = fabs((double)means[(i64)k * D + d] - (double)ctr[d]) + 4.0 * sqrt((double)covs[(i64)k * D + d]);
+    b = v > b ? v : b;
+  }
+  int e = 0;
+  if (b > 0) frexp(b, &e);
+  scale[d] = (float)ldexp(1.0, -e);
+}
+
 // ============================================================ E-step
+// Output layouts of the posteriors written by the E-step.
+//   kQRow    fp32, row-major q[i * ldq + k] (VLFeat's layout; EM and API).
+//   kQImg16  fp16 operand image of q^T for the statistics GEMM: per 8-row
+//            group g of a 128-row tile, Kq/64 MN-major 128-byte-swizzled
+//            1 KB atoms (64 components x 8 rows), so that a run of 8-row
+//            groups is exactly the MMA's A operand and moves with one bulk
+//            copy per group.
+//   kQImg32  the same image as two bf16 parts (hi, lo) for bf16x3 statistics.
+constexpr int kQRow = 0, kQImg16 = 1, kQImg32 = 2;
+
 struct EParams {
   const float *X;
   i64 N;
-  int K, Kp, nst;
+  int K, Kp, Kq, nst;  // Kq: components in the q image (Kp rounded up to 128)
+  i64 qpart;           // bytes of one part of the q image
   const uint4 *wimg;
   const float *cst2;
   const float *ctr;
   void *q;
   int ldq;
   int fast;
+  float qthr;  // image outputs: posteriors below this are stored as 0 (vl/fisher.c:440)
   unsigned *rowcnt;
   double *ll_part;
   int *err;
   i64 ntiles;
 };
 
-template <int DIM, bool SPLIT3>
+template <int DIM>
 struct ELayout {
   static constexpr int KD2 = 2 * DIM;
   static constexpr int NKA = KD2 / 32;
-  static constexpr int NP = SPLIT3 ? 2 : 1;
-  static constexpr int kStage = NP * 8192;
+  static constexpr int kStage = 2 * 8192;  // hi + lo parts of one 128 x 32 chunk
   __host__ __device__ static size_t wbytes(int Kp) { return (size_t)NKA * Kp * 64; }
-  static size_t fixed(int Kp) { return NP * wbytes(Kp) + 1024 /*cst*/ + 1024 /*ctr*/ + 1024 /*bars*/ + 1024; }
+  static size_t fixed(int Kp) { return 2 * wbytes(Kp) + 1024 /*cst*/ + 1024 /*ctr*/ + 1024 /*bars*/ + 1024; }
   static int max_stages(int Kp) { return (int)((kSmemLimit - fixed(Kp)) / kStage); }
   static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * kStage; }
 };
 
-template <int DIM, bool SPLIT3, bool OUT_BF16>
+template <int DIM, int QF>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
-  using L = ELayout<DIM, SPLIT3>;
-  constexpr int NKA = L::NKA, NP = L::NP;
+  using L = ELayout<DIM>;
+  constexpr int NKA = L::NKA;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *base = align1024(smem_raw);
   const uint32_t wbytes = (uint32_t)L::wbytes(p.Kp);
   uint8_t *sW = base;
-  uint8_t *sA = sW + NP * wbytes;
+  uint8_t *sA = sW + 2 * wbytes;
   float *s_cst = (float *)(sA + (size_t)p.nst * L::kStage);
   float *s_ctr = s_cst + 256;
   uint64_t *bars = (uint64_t *)(s_ctr + 256);
@@ -188,7 +218,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   {
     const uint4 *src = p.wimg;
     uint4 *dst = (uint4 *)sW;
-    const int n16 = (int)(NP * wbytes / 16);
+    const int n16 = (int)(2 * wbytes / 16);
     for (int i = tid; i < n16; i += kTcThreads) dst[i] = src[i];
     for (int k = tid; k < 256; k += kTcThreads) s_cst[k] = k < p.Kp ? p.cst2[k] : -INFINITY;
     for (int d = tid; d < DIM; d += kTcThreads) s_ctr[d] = p.ctr[d];
@@ -200,62 +230,70 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 
   if (warp < 4) {
     // ---------------------------------------------------- producers
-    const int r = tid;  // row within the tile
-    int it = 0;
-    bool ok = true;
-    for (i64 tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x) {
-      const i64 row = tile * 128 + r;
-      float xr[DIM];
-      if (row < p.N) {
-        const float4 *src = (const float4 *)(p.X + row * DIM);
+    // Warp w owns rows [32w, 32w+32) of each tile.  For one 32-element chunk
+    // of the A row [x', x'^2], lane (rg, part) handles rows 32w + 4s + rg,
+    // s = 0..7, and elements [4 part, 4 part + 4): each load instruction reads
+    // 4 rows x 128 contiguous bytes.  The next chunk's rows are prefetched into
+    // registers while the current chunk is converted.
+    const int part = lane & 7, rg = lane >> 3;
+    float4 b0[8], b1[8], b2[8];
+    auto load = [&](float4(&buf)[8], i64 t, int c) {
+      const int e0 = 32 * c + 4 * part;
+      const int d0 = e0 < DIM ? e0 : e0 - DIM;
 #pragma unroll
-        for (int j = 0; j < DIM / 4; ++j) {
-          float4 v = __ldg(src + j);
-          xr[4 * j + 0] = v.x - s_ctr[4 * j + 0];
-          xr[4 * j + 1] = v.y - s_ctr[4 * j + 1];
-          xr[4 * j + 2] = v.z - s_ctr[4 * j + 2];
-          xr[4 * j + 3] = v.w - s_ctr[4 * j + 3];
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) xr[j] = 0.f;
+      for (int s = 0; s < 8; ++s) {
+        const i64 row = t * 128 + 32 * warp + 4 * s + rg;
+        buf[s] = row < p.N ? __ldg((const float4 *)(p.X + row * DIM + d0)) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-#pragma unroll
-      for (int c = 0; c < NKA; ++c) {
-        const int stage = it % p.nst;
-        if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 1)) {
-          ok = false;
-          break;
-        }
-        const uint32_t a_hi = smem_u32(sA + (size_t)stage * L::kStage);
-#pragma unroll
-        for (int g = 0; g < 4; ++g) {
-          uint32_t wh[4], wl[4];
-#pragma unroll
-          for (int j = 0; j < 8; j += 2) {
-            float v0, v1;
-            {
-              const int e = 32 * c + 8 * g + j;
-              v0 = e < DIM ? xr[e < DIM ? e : 0] : xr[e >= DIM ? e - DIM : 0] * xr[e >= DIM ? e - DIM : 0];
-            }
-            {
-              const int e = 32 * c + 8 * g + j + 1;
-              v1 = e < DIM ? xr[e < DIM ? e : 0] : xr[e >= DIM ? e - DIM : 0] * xr[e >= DIM ? e - DIM : 0];
-            }
-            __nv_bfloat16 h0, l0, h1, l1;
-            split_bf16(v0, h0, l0);
-            split_bf16(v1, h1, l1);
-            wh[j / 2] = pack_bf16(h0, h1);
-            wl[j / 2] = pack_bf16(l0, l1);
-          }
-          const uint32_t off = kmajor_sw64_off((uint32_t)r, (uint32_t)g);
-          st_shared_v4(a_hi + off, wh[0], wh[1], wh[2], wh[3]);
-          if (SPLIT3) st_shared_v4(a_hi + 8192 + off, wl[0], wl[1], wl[2], wl[3]);
-        }
-        fence_proxy_async_smem();
-        mbar_arrive(&full[stage]);
-        ++it;
+    };
+    // Positions (tile, chunk) of the chunk being converted and the next two,
+    // whose rows are already in flight (a 3-deep register prefetch ring).
+    i64 t0 = blockIdx.x, t1, t2;
+    int c0 = 0, c1, c2, it = 0;
+    auto adv = [&](i64 t, int c, i64 &tn, int &cn) {
+      tn = t;
+      cn = c + 1;
+      if (cn == NKA) {
+        cn = 0;
+        tn += gridDim.x;
       }
+    };
+    adv(t0, c0, t1, c1);
+    adv(t1, c1, t2, c2);
+    if (t0 < p.ntiles) load(b0, t0, c0);
+    if (t1 < p.ntiles) load(b1, t1, c1);
+    auto step = [&](float4(&cur)[8], float4(&fut)[8]) -> bool {
+      if (t0 >= p.ntiles) return false;
+      if (t2 < p.ntiles) load(fut, t2, c2);
+      const int stage = it % p.nst;
+      if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 1)) return false;
+      const uint32_t a_hi = smem_u32(sA + (size_t)stage * L::kStage);
+      const int e0 = 32 * c0 + 4 * part;
+      const bool sq = e0 >= DIM;
+      const int d0 = sq ? e0 - DIM : e0;
+      const float m0 = s_ctr[d0], m1 = s_ctr[d0 + 1], m2 = s_ctr[d0 + 2], m3 = s_ctr[d0 + 3];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        float v0 = cur[s].x - m0, v1 = cur[s].y - m1, v2 = cur[s].z - m2, v3 = cur[s].w - m3;
+        if (sq) {
+          v0 *= v0; v1 *= v1; v2 *= v2; v3 *= v3;
+        }
+        uint32_t h0, l0, h1, l1;
+        split2<false>(v0, v1, h0, l0);
+        split2<false>(v2, v3, h1, l1);
+        const uint32_t off = kmajor_sw64_off((uint32_t)(32 * warp + 4 * s + rg), (uint32_t)(part >> 1)) + (part & 1) * 8;
+        st_shared_v2(a_hi + off, h0, h1);
+        st_shared_v2(a_hi + 8192 + off, l0, l1);
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(&full[stage]);
+      ++it;
+      t0 = t1; c0 = c1;
+      t1 = t2; c1 = c2;
+      adv(t1, c1, t2, c2);
+      return true;
+    };
+    while (step(b0, b2) && step(b1, b0) && step(b2, b1)) {
     }
   } else if (warp < 8) {
     // ----------------------------------------------------- epilogue
@@ -301,42 +339,53 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       const i64 row = tile * 128 + r;
       const bool valid = row < p.N;
       unsigned cnt = 0;
-      for (int cc = 0; cc < nch; ++cc) {
-        uint32_t v[32];
-        tmem_ld32(tb + cc * 32, v);
-        tmem_wait_ld();
-        if (!valid) continue;
+      // q image: this row's offset inside its tile (8-row group, row in group).
+      uint8_t *ib = (uint8_t *)p.q + (size_t)tile * 128 * p.Kq * 2;
+      const uint32_t rowoff = (uint32_t)((r >> 3) * (p.Kq / 64) * 1024);  // + row-in-group below
+      const int ncw = (QF == kQRow) ? nch : p.Kq / 32;
+      for (int cc = 0; cc < ncw; ++cc) {
         float qv[32];
+        if (cc < nch) {
+          uint32_t v[32];
+          tmem_ld32(tb + cc * 32, v);
+          tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          float x = p.fast ? (cc * 32 + j == am ? 1.f : 0.f) : __uint_as_float(v[j]) * inv;
-          qv[j] = x;
-          cnt += (x >= 1e-6f) ? 1u : 0u;
-        }
-        const int k0 = cc * 32;
-        if (OUT_BF16) {
-          __nv_bfloat16 *dst = (__nv_bfloat16 *)p.q + row * p.ldq + k0;
-          if (k0 + 32 <= p.K && (p.ldq % 8) == 0) {
-#pragma unroll
-            for (int j = 0; j < 32; j += 8) {
-              uint4 w;
-              w.x = pack_bf16(__float2bfloat16_rn(qv[j]), __float2bfloat16_rn(qv[j + 1]));
-              w.y = pack_bf16(__float2bfloat16_rn(qv[j + 2]), __float2bfloat16_rn(qv[j + 3]));
-              w.z = pack_bf16(__float2bfloat16_rn(qv[j + 4]), __float2bfloat16_rn(qv[j + 5]));
-              w.w = pack_bf16(__float2bfloat16_rn(qv[j + 6]), __float2bfloat16_rn(qv[j + 7]));
-              *(uint4 *)(dst + j) = w;
-            }
-          } else {
-            for (int j = 0; j < 32 && k0 + j < p.K; ++j) dst[j] = __float2bfloat16_rn(qv[j]);
+          for (int j = 0; j < 32; ++j) {
+            float x = p.fast ? (cc * 32 + j == am ? 1.f : 0.f) : __uint_as_float(v[j]) * inv;
+            x = valid ? x : 0.f;
+            cnt += (x >= 1e-6f) ? 1u : 0u;
+            if (QF != kQRow && x < p.qthr) x = 0.f;
+            qv[j] = x;
           }
         } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) qv[j] = 0.f;
+        }
+        const int k0 = cc * 32;
+        if (QF == kQRow) {
+          if (!valid) continue;
           float *dst = (float *)p.q + row * p.ldq + k0;
-          if (k0 + 32 <= p.K && (p.ldq % 4) == 0) {
+          if (k0 + 32 <= p.K) {
 #pragma unroll
             for (int j = 0; j < 32; j += 4)
               *(float4 *)(dst + j) = make_float4(qv[j], qv[j + 1], qv[j + 2], qv[j + 3]);
           } else {
-            for (int j = 0; j < 32 && k0 + j < p.K; ++j) dst[j] = qv[j];
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (k0 + j < p.K) dst[j] = qv[j];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int kk = k0 + 8 * j;
+            const uint32_t off = rowoff + (uint32_t)((kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
+            uint4 wh, wl;
+            split2<QF == kQImg16>(qv[8 * j + 0], qv[8 * j + 1], wh.x, wl.x);
+            split2<QF == kQImg16>(qv[8 * j + 2], qv[8 * j + 3], wh.y, wl.y);
+            split2<QF == kQImg16>(qv[8 * j + 4], qv[8 * j + 5], wh.z, wl.z);
+            split2<QF == kQImg16>(qv[8 * j + 6], qv[8 * j + 7], wh.w, wl.w);
+            *(uint4 *)(ib + off) = wh;
+            if (QF == kQImg32) *(uint4 *)(ib + p.qpart + off) = wl;
           }
         }
       }
@@ -371,14 +420,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
           const uint64_t ah = sdesc(a_hi + ks * 32, 16, 512, kSw64);
+          const uint64_t al = sdesc(a_hi + 8192 + ks * 32, 16, 512, kSw64);
           const uint64_t bh = sdesc(w_hi + c * p.Kp * 64 + ks * 32, 16, 512, kSw64);
+          const uint64_t bl = sdesc(w_lo + c * p.Kp * 64 + ks * 32, 16, 512, kSw64);
           mma_bf16(d, ah, bh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-          if (SPLIT3) {
-            const uint64_t bl = sdesc(w_lo + c * p.Kp * 64 + ks * 32, 16, 512, kSw64);
-            const uint64_t al = sdesc(a_hi + 8192 + ks * 32, 16, 512, kSw64);
-            mma_bf16(d, ah, bl, idesc, 1u);
-            mma_bf16(d, al, bh, idesc, 1u);
-          }
+          mma_bf16(d, ah, bl, idesc, 1u);
+          mma_bf16(d, al, bh, idesc, 1u);
         }
         mma_commit(&empty[stage]);
         ++it;
@@ -402,11 +449,12 @@ struct SItem {
 
 struct SParams {
   const float *X;
-  const void *q;
-  i64 qbase;  // row of X that q's first row corresponds to
-  int ldq, K, Kp, nst;
+  const uint8_t *qimg;  // q^T operand image written by the E-step
+  i64 qpart;            // bytes of one image part
+  i64 qbase;            // row of X that the image's first row corresponds to
+  int K, Kp, Kq, nst;
   const float *ctr;
-  float qthr;
+  const float *scale;  // per-dimension scale of x' (fp16 operands), or null
   const SItem *items;
   const int *order;     // item indices, grouped per CTA
   const int *cta_beg;   // gridDim.x + 1 offsets into order
@@ -414,32 +462,47 @@ struct SParams {
   int *err;
 };
 
-template <int DIM, int MT, bool SPLIT3>
+// SPLIT 2: bf16x3 -- q and x both split hi/lo, products hi.hi + hi.lo + lo.hi.
+// SPLIT 1: fp16 operands -- q single fp16, x'' = x' * scale split hi/lo.
+template <int DIM, int MT, int SPLIT>
 struct SLayout {
   static constexpr int NST = 2 * DIM + 16;            // x', x'^2, [1, 0 x 15]
   static constexpr int NB = (NST + 63) / 64;           // 64-feature MN blocks
   static constexpr int NCH = (NST + 255) / 256;        // MMA N chunks
-  static constexpr int NP = SPLIT3 ? 2 : 1;
+  static constexpr int NPA = SPLIT == 2 ? 2 : 1;       // q^T parts
+  static constexpr int NPB = 2;                        // [x'', x''^2, 1] parts
   static constexpr int A_PART = MT * 2 * 4 * 1024;     // [kgroup 4][mnblk 2MT][1 KB]
   static constexpr int B_PART = NB * 4 * 1024;         // [kgroup 4][nblk NB][1 KB]
-  static constexpr int kStage = NP * (A_PART + B_PART);
-  static constexpr size_t fixed = 1024 /*ctr*/ + 1024 /*bars*/ + 1024;
+  static constexpr int XST = (32 * DIM * 4 + 1023) / 1024 * 1024;  // staged x rows
+  static constexpr int kStage = NPA * A_PART + NPB * B_PART + XST;
+  static constexpr size_t fixed = 1024 /*ctr*/ + 1024 /*scale*/ + 1024 /*bars*/ + 1024;
   static int max_stages() { return (int)((kSmemLimit - fixed) / kStage); }
   static size_t bytes(int nst) { return fixed + (size_t)nst * kStage; }
   static_assert(MT * NST <= 512, "accumulators exceed TMEM");
 };
 
-template <int DIM, int MT, bool SPLIT3, bool Q_BF16>
-__global__ void __launch_bounds__(kTcThreads, 1) k_tc_stats(const SParams p) {
-  using L = SLayout<DIM, MT, SPLIT3>;
-  constexpr int NST = L::NST, NB = L::NB, NP = L::NP;
+constexpr int kStatsThreads = 320;  // + one loader warp
+
+// Statistics over work items (runs of rows of one image): for each 32-row
+// chunk, the loader warp bulk-copies the chunk's q^T operand (four 8-row
+// groups of the E-step's image) straight into the operand stage and the
+// chunk's x rows into a staging buffer; converter warps build the x-side
+// operand [x'', x''^2, 1] (zero rows outside the item); one thread issues the
+// MMAs; the epilogue drains the item's accumulators to its partial.
+template <int DIM, int MT, int SPLIT>
+__global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) {
+  using L = SLayout<DIM, MT, SPLIT>;
+  constexpr int NST = L::NST, NB = L::NB, NPA = L::NPA;
+  constexpr bool F16 = (SPLIT == 1);
+  constexpr int NF4 = DIM / 4;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *base = align1024(smem_raw);
   uint8_t *sS = base;
   float *s_ctr = (float *)(sS + (size_t)p.nst * L::kStage);
-  uint64_t *bars = (uint64_t *)(s_ctr + 256);
-  uint64_t *full = bars, *empty = bars + 16, *accf = bars + 32, *acce = bars + 33;
-  uint32_t *s_tmem = (uint32_t *)(bars + 40);
+  float *s_scl = s_ctr + 256;
+  uint64_t *bars = (uint64_t *)(s_scl + 256);
+  uint64_t *full = bars, *empty = bars + 16, *xfull = bars + 32, *accf = bars + 48, *acce = bars + 49;
+  uint32_t *s_tmem = (uint32_t *)(bars + 56);
   volatile int *s_abort = (volatile int *)(s_tmem + 1);
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
@@ -448,6 +511,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_stats(const SParams p) {
     for (int s = 0; s < p.nst; ++s) {
       mbar_init(&full[s], 128);
       mbar_init(&empty[s], 1);
+      mbar_init(&xfull[s], 1);
     }
     mbar_init(accf, 1);
     mbar_init(acce, 128);
@@ -458,104 +522,109 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_stats(const SParams p) {
     tmem_alloc(s_tmem, 512);
     tmem_relinquish();
   }
-  for (int d = tid; d < DIM; d += kTcThreads) s_ctr[d] = p.ctr[d];
+  for (int d = tid; d < DIM; d += kStatsThreads) {
+    s_ctr[d] = p.ctr[d];
+    s_scl[d] = p.scale ? p.scale[d] : 1.f;
+  }
+  // Zero the operand stages once: groups a chunk does not copy keep finite
+  // stale values, and their x-side rows are zero.
+  for (int s = 0; s < p.nst; ++s) {
+    uint4 *st = (uint4 *)(sS + (size_t)s * L::kStage);
+    for (int i = tid; i < (NPA * L::A_PART + L::NPB * L::B_PART) / 16; i += kStatsThreads) st[i] = make_uint4(0, 0, 0, 0);
+  }
+  fence_proxy_async_smem();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
   const int ib = p.cta_beg[blockIdx.x], ie = p.cta_beg[blockIdx.x + 1];
 
-  if (warp < 4) {
-    // ---------------------------------------------------- producers
-    const int r = tid >> 2, qq = tid & 3;  // row of the 32-row stage, quarter
-    const int kr = r & 7, kg = r >> 3;
+  if (warp == 9) {
+    // ------------------------------------------------------- loader
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int ii = ib; ii < ie && ok; ++ii) {
+        const SItem item = p.items[p.order[ii]];
+        for (i64 cb = p.qbase + ((item.row0 - p.qbase) & ~(i64)7); cb < item.row1; cb += 32) {
+          const int stage = it % p.nst;
+          if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 15)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sa = smem_u32(sS + (size_t)stage * L::kStage);
+          const uint32_t sx = sa + NPA * L::A_PART + L::NPB * L::B_PART;
+          const int nkg = (int)min((i64)4, (item.row1 - cb + 7) / 8);
+          const int nx = (int)min((i64)32, item.row1 - cb);
+          const uint32_t gbytes = MT * 2 * 1024;
+          mbar_arrive_expect_tx(&xfull[stage], (uint32_t)(NPA * nkg) * gbytes + (uint32_t)nx * DIM * 4);
+          for (int part = 0; part < NPA; ++part) {
+            for (int kg = 0; kg < nkg; ++kg) {
+              const i64 rel = cb - p.qbase + 8 * kg;  // row of the image
+              const uint8_t *src = p.qimg + part * p.qpart + (size_t)(rel >> 7) * 128 * p.Kq * 2 +
+                                   (size_t)((rel & 127) >> 3) * (p.Kq / 64) * 1024 + (size_t)(comp0 / 64) * 1024;
+              bulk_g2s(sa + part * L::A_PART + kg * gbytes, src, gbytes, &xfull[stage]);
+            }
+          }
+          bulk_g2s(sx, p.X + cb * DIM, (uint32_t)nx * DIM * 4, &xfull[stage]);
+          ++it;
+        }
+      }
+    }
+  } else if (warp < 4) {
+    // ---------------------------------------------------- converters
     int it = 0;
     bool ok = true;
     for (int ii = ib; ii < ie && ok; ++ii) {
       const SItem item = p.items[p.order[ii]];
-      for (i64 rb = item.row0; rb < item.row1 && ok; rb += 32) {
+      for (i64 cb = p.qbase + ((item.row0 - p.qbase) & ~(i64)7); cb < item.row1; cb += 32) {
         const int stage = it % p.nst;
-        if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 11)) {
+        if (!mbar_wait(&xfull[stage], (it / p.nst) & 1, s_abort, p.err, 11)) {
           ok = false;
           break;
         }
         const uint32_t sa = smem_u32(sS + (size_t)stage * L::kStage);
-        const uint32_t sb = sa + NP * L::A_PART;
-        const i64 row = rb + r;
-        const bool valid = row < item.row1;
-        // A = q^T: this thread covers components [qq*MT*32, (qq+1)*MT*32).
+        const uint32_t sb = sa + NPA * L::A_PART;
+        const float *xs = (const float *)(sS + (size_t)stage * L::kStage + NPA * L::A_PART + L::NPB * L::B_PART);
 #pragma unroll
-        for (int j = 0; j < MT * 4; ++j) {
-          const int cl = qq * MT * 32 + j * 8;  // local component (0 .. MT*128)
-          const int kc = comp0 + cl;
-          float v[8];
-          if (valid && kc < p.K) {
-            if (Q_BF16) {
-              const uint4 w = *(const uint4 *)((const __nv_bfloat16 *)p.q + (row - p.qbase) * p.ldq + kc);
-              const __nv_bfloat16 *h = (const __nv_bfloat16 *)&w;
-#pragma unroll
-              for (int t = 0; t < 8; ++t) v[t] = __bfloat162float(h[t]);
-            } else {
-              const float4 *src = (const float4 *)((const float *)p.q + (row - p.qbase) * p.ldq + kc);
-              const float4 a = src[0], b = src[1];
-              v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-              v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-            }
-#pragma unroll
-            for (int t = 0; t < 8; ++t) {
-              if (v[t] < p.qthr || kc + t >= p.K) v[t] = 0.f;
-            }
-          } else {
-#pragma unroll
-            for (int t = 0; t < 8; ++t) v[t] = 0.f;
+        for (int j = 0; j < (32 * NF4 + 127) / 128; ++j) {
+          const int i = tid + 128 * j;
+          if (i >= 32 * NF4) break;
+          const int rs = i / NF4, pp = i % NF4;
+          const i64 row = cb + rs;
+          const bool in = row >= item.row0 && row < item.row1;
+          const int d0 = 4 * pp;
+          float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+          if (in) {
+            const float4 x = *(const float4 *)(xs + rs * DIM + d0);
+            v0 = (x.x - s_ctr[d0]) * s_scl[d0];
+            v1 = (x.y - s_ctr[d0 + 1]) * s_scl[d0 + 1];
+            v2 = (x.z - s_ctr[d0 + 2]) * s_scl[d0 + 2];
+            v3 = (x.w - s_ctr[d0 + 3]) * s_scl[d0 + 3];
           }
-          uint32_t wh[4], wl[4];
-#pragma unroll
-          for (int t = 0; t < 8; t += 2) {
-            __nv_bfloat16 h0, l0, h1, l1;
-            split_bf16(v[t], h0, l0);
-            split_bf16(v[t + 1], h1, l1);
-            wh[t / 2] = pack_bf16(h0, h1);
-            wl[t / 2] = pack_bf16(l0, l1);
+          const int kr = rs & 7, kg = rs >> 3;
+          uint32_t h0, l0, h1, l1;
+          {
+            split2<F16>(v0, v1, h0, l0);
+            split2<F16>(v2, v3, h1, l1);
+            const int f = d0;
+            const uint32_t off = kg * (NB * 1024) + (f >> 6) * 1024 + mnmajor_sw128_off(kr, (f & 63) >> 3) + ((f >> 2) & 1) * 8;
+            st_shared_v2(sb + off, h0, h1);
+            st_shared_v2(sb + L::B_PART + off, l0, l1);
           }
-          const uint32_t off = kg * (MT * 2 * 1024) + (cl >> 6) * 1024 + mnmajor_sw128_off(kr, (cl & 63) >> 3);
-          st_shared_v4(sa + off, wh[0], wh[1], wh[2], wh[3]);
-          if (SPLIT3) st_shared_v4(sa + L::A_PART + off, wl[0], wl[1], wl[2], wl[3]);
-        }
-        // B = [x', x'^2, 1, 0...]: this thread covers feature chunks [qq*NB*2, (qq+1)*NB*2).
-#pragma unroll
-        for (int j = 0; j < NB * 2; ++j) {
-          const int f0 = (qq * NB * 2 + j) * 8;
-          float v[8];
-#pragma unroll
-          for (int t = 0; t < 8; ++t) v[t] = 0.f;
-          if (valid) {
-            if (f0 < 2 * DIM) {
-              const int d0 = f0 < DIM ? f0 : f0 - DIM;
-              const float4 *src = (const float4 *)(p.X + row * DIM + d0);
-              const float4 a = __ldg(src), b = __ldg(src + 1);
-              v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-              v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-#pragma unroll
-              for (int t = 0; t < 8; ++t) {
-                v[t] -= s_ctr[d0 + t];
-                if (f0 >= DIM) v[t] = v[t] * v[t];
-              }
-            } else if (f0 == 2 * DIM) {
-              v[0] = 1.f;
-            }
+          {
+            split2<F16>(v0 * v0, v1 * v1, h0, l0);
+            split2<F16>(v2 * v2, v3 * v3, h1, l1);
+            const int f = DIM + d0;
+            const uint32_t off = kg * (NB * 1024) + (f >> 6) * 1024 + mnmajor_sw128_off(kr, (f & 63) >> 3) + ((f >> 2) & 1) * 8;
+            st_shared_v2(sb + off, h0, h1);
+            st_shared_v2(sb + L::B_PART + off, l0, l1);
           }
-          uint32_t wh[4], wl[4];
-#pragma unroll
-          for (int t = 0; t < 8; t += 2) {
-            __nv_bfloat16 h0, l0, h1, l1;
-            split_bf16(v[t], h0, l0);
-            split_bf16(v[t + 1], h1, l1);
-            wh[t / 2] = pack_bf16(h0, h1);
-            wl[t / 2] = pack_bf16(l0, l1);
+          if (pp == 0) {  // ones column: counts the posterior mass of in-item rows
+            const int f = 2 * DIM;
+            const uint32_t off = kg * (NB * 1024) + (f >> 6) * 1024 + mnmajor_sw128_off(kr, (f & 63) >> 3);
+            const uint16_t one = F16 ? (uint16_t)0x3C00 : (uint16_t)0x3F80;
+            asm volatile("st.shared.u16 [%0], %1;" ::"r"(sb + off), "h"(in ? one : (uint16_t)0) : "memory");
           }
-          const uint32_t off = kg * (NB * 1024) + (f0 >> 6) * 1024 + mnmajor_sw128_off(kr, (f0 & 63) >> 3);
-          st_shared_v4(sb + off, wh[0], wh[1], wh[2], wh[3]);
-          if (SPLIT3) st_shared_v4(sb + L::B_PART + off, wl[0], wl[1], wl[2], wl[3]);
         }
         fence_proxy_async_smem();
         mbar_arrive(&full[stage]);
@@ -597,7 +666,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_stats(const SParams p) {
       tc_fence_before();
       mbar_arrive(acce);
     }
-  } else if (lane == 0) {
+  } else if (warp == 8 && lane == 0) {
     // ---------------------------------------------------------- MMA
     int it = 0, n = 0;
     bool ok = true;
@@ -606,36 +675,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_stats(const SParams p) {
       if (!mbar_wait(acce, (n & 1) ^ 1, s_abort, p.err, 13)) break;
       tc_fence_after();
       int chunk = 0;
-      for (i64 rb = item.row0; rb < item.row1; rb += 32, ++chunk) {
+      for (i64 cb = p.qbase + ((item.row0 - p.qbase) & ~(i64)7); cb < item.row1; cb += 32, ++chunk) {
         const int stage = it % p.nst;
-        if (!mbar_wait(&full[stage], (it / p.nst) & 1, s_abort, p.err, 14)) {
+        if (!mbar_wait(&full[stage], (it / p.nst) & 1, s_abort, p.err, 14) ||
+            !mbar_wait(&xfull[stage], (it / p.nst) & 1, s_abort, p.err, 16)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const uint32_t sa = smem_u32(sS + (size_t)stage * L::kStage);
-        const uint32_t sb = sa + NP * L::A_PART;
+        const uint32_t sb = sa + NPA * L::A_PART;
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
 #pragma unroll
           for (int mt = 0; mt < MT; ++mt) {
             const uint32_t a0 = sa + ks * 2 * (MT * 2 * 1024) + mt * 2 * 1024;
             const uint64_t ah = sdesc(a0, 1024, MT * 2 * 1024, kSw128);
-            const uint64_t al = sdesc(a0 + L::A_PART, 1024, MT * 2 * 1024, kSw128);
 #pragma unroll
             for (int nc = 0; nc < L::NCH; ++nc) {
               const int nn = (NST - nc * 256) < 256 ? (NST - nc * 256) : 256;
-              const uint32_t idesc = idesc_bf16(128, nn, true, true);
+              const uint32_t idesc = F16 ? idesc_f16(128, nn, true, true) : idesc_bf16(128, nn, true, true);
               const uint32_t b0 = sb + ks * 2 * (NB * 1024) + nc * 4 * 1024;
               const uint64_t bh = sdesc(b0, 1024, NB * 1024, kSw128);
+              const uint64_t bl = sdesc(b0 + L::B_PART, 1024, NB * 1024, kSw128);
               const uint32_t d = tmem + (uint32_t)(mt * NST + nc * 256);
-              const uint32_t acc = (chunk > 0 || ks > 0) ? 1u : 0u;
-              mma_bf16(d, ah, bh, idesc, acc);
-              if (SPLIT3) {
-                const uint64_t bl = sdesc(b0 + L::B_PART, 1024, NB * 1024, kSw128);
-                mma_bf16(d, ah, bl, idesc, 1u);
-                mma_bf16(d, al, bh, idesc, 1u);
-              }
+              mma_bf16(d, ah, bh, idesc, (chunk > 0 || ks > 0) ? 1u : 0u);
+              mma_bf16(d, ah, bl, idesc, 1u);
+              if (NPA == 2) mma_bf16(d, sdesc(a0 + L::A_PART, 1024, MT * 2 * 1024, kSw128), bh, idesc, 1u);
             }
           }
         }
@@ -661,9 +727,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_stats(const SParams p) {
 __global__ void __launch_bounds__(256) k_tc_fv_finalize(
     int K, int Kp, int D, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
     const i64 *__restrict__ imgRow0, const float *__restrict__ means, const float *__restrict__ covs,
-    const float *__restrict__ priors, const float *__restrict__ ctr, const unsigned *__restrict__ rowcnt,
-    i64 rowcntBase, int flags, i64 imgBase, float *__restrict__ enc,
-    unsigned long long *__restrict__ nterms) {
+    const float *__restrict__ priors, const float *__restrict__ ctr, const float *__restrict__ scale,
+    const unsigned *__restrict__ rowcnt, i64 rowcntBase, int flags, i64 imgBase,
+    float *__restrict__ enc, unsigned long long *__restrict__ nterms) {
   __shared__ double sh[256];
   __shared__ unsigned long long shn[256];
   const int img = blockIdx.x;
@@ -682,6 +748,11 @@ __global__ void __launch_bounds__(256) k_tc_fv_finalize(
       S0 += (double)pp[2 * D];
       S1 += (double)pp[d];
       S2 += (double)pp[D + d];
+    }
+    if (scale) {  // statistics were taken on x'' = x' * scale
+      const double is = 1.0 / (double)scale[d];
+      S1 *= is;
+      S2 *= is * is;
     }
     const double pk = (double)priors[k];
     double u = 0, v = 0;
@@ -728,13 +799,13 @@ __global__ void __launch_bounds__(256) k_tc_fv_finalize(
 // ================================================================ host
 struct TcPrep {
   int K = 0, Kp = 0, D = 0;
-  float *ctr = nullptr, *cst2 = nullptr;
+  float *ctr = nullptr, *cst2 = nullptr, *scale = nullptr;
   __nv_bfloat16 *wimg = nullptr;
 };
 
 int padK(i64 K) { return (int)((K + 15) / 16 * 16); }
 
-void tc_prepare(const DevModel<float> &m, TcPrep &tp, cudaStream_t s) {
+void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, cudaStream_t s) {
   Scratch &sc = thread_scratch();
   tp.K = (int)m.K;
   tp.Kp = padK(m.K);
@@ -751,85 +822,121 @@ void tc_prepare(const DevModel<float> &m, TcPrep &tp, cudaStream_t s) {
   VLB_LAUNCH("tc_constants", s,
              k_tc_cst<<<(tp.Kp + 127) / 128, 128, 0, s>>>(m.priors, m.means, m.covs, tp.ctr, tp.K,
                                                           tp.Kp, tp.D, tp.cst2));
+  if (want_scale) {
+    tp.scale = sc.slot[12].get<float>(256);
+    VLB_LAUNCH("tc_scale", s,
+               k_tc_scale<<<(tp.D + 127) / 128, 128, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.D, tp.scale));
+  }
 }
 
-template <int DIM, bool SPLIT3, bool OUT_BF16>
+int padQ(int Kp) { return (Kp + 127) / 128 * 128; }
+
+template <int DIM, int QF>
 i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
                  unsigned *rowcnt, double *ll_part, int *err, cudaStream_t s) {
-  using L = ELayout<DIM, SPLIT3>;
+  using L = ELayout<DIM>;
   const i64 ntiles = (N + 127) / 128;
   if (ntiles == 0) return 0;
   const int nst = std::min(8, L::max_stages(tp.Kp));
   VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
   const size_t smem = L::bytes(tp.Kp, nst);
-  auto kern = k_tc_estep<DIM, SPLIT3, OUT_BF16>;
+  auto kern = k_tc_estep<DIM, QF>;
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   EParams p;
-  p.X = X; p.N = N; p.K = tp.K; p.Kp = tp.Kp; p.nst = nst;
+  p.X = X; p.N = N; p.K = tp.K; p.Kp = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
+  p.qpart = ntiles * 128 * (i64)p.Kq * 2;
   p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr;
-  p.q = q; p.ldq = ldq; p.fast = fast ? 1 : 0; p.rowcnt = rowcnt; p.ll_part = ll_part;
+  p.q = q; p.ldq = ldq; p.fast = fast ? 1 : 0; p.qthr = 1e-6f; p.rowcnt = rowcnt; p.ll_part = ll_part;
   p.err = err; p.ntiles = ntiles;
   const int grid = (int)std::min<i64>(ntiles, num_sms());
-  VLB_LAUNCH(SPLIT3 ? "tc_estep_bf16x3" : "tc_estep_bf16", s,
-             kern<<<grid, kTcThreads, smem, s>>>(p));
+  VLB_LAUNCH("tc_estep_bf16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
   return ntiles * 4;  // LL partials written
 }
 
-template <int DIM, int MT, bool SPLIT3, bool Q_BF16>
+template <int DIM, int MT, int SPLIT>
 void launch_stats(const SParams &p0, int grid_x, int grid_y, cudaStream_t s) {
-  using L = SLayout<DIM, MT, SPLIT3>;
+  using L = SLayout<DIM, MT, SPLIT>;
   SParams p = p0;
-  p.nst = std::min(6, L::max_stages());
+  p.nst = std::min(8, L::max_stages());
   VLB_CHECK(p.nst >= 2, VL_ERR_BAD_ARG, "tensor-core statistics: operands exceed shared memory");
   const size_t smem = L::bytes(p.nst);
-  auto kern = k_tc_stats<DIM, MT, SPLIT3, Q_BF16>;
+  auto kern = k_tc_stats<DIM, MT, SPLIT>;
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  VLB_LAUNCH(SPLIT3 ? "tc_stats_bf16x3" : "tc_stats_bf16", s,
-             kern<<<dim3(grid_x, grid_y), kTcThreads, smem, s>>>(p));
+  VLB_LAUNCH(SPLIT == 2 ? "tc_stats_bf16x3" : "tc_stats_f16x2", s,
+             kern<<<dim3(grid_x, grid_y), kStatsThreads, smem, s>>>(p));
 }
 
-// Dimension dispatch: the kernels are instantiated for the descriptor sizes
-// of the benchmarked configurations.
-template <template <int> class F, typename... A>
-auto dispatch_dim(int D, A &&...a) {
+template <int DIM>
+struct Tc {
+  static constexpr bool kTwo = 2 * (2 * DIM + 16) <= 512;  // two M tiles fit in TMEM
+  static i64 estep(int qf, const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
+                   unsigned *rowcnt, double *ll, int *err, cudaStream_t s) {
+    if (qf == kQImg16) return launch_estep<DIM, kQImg16>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+    if (qf == kQImg32) return launch_estep<DIM, kQImg32>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+    return launch_estep<DIM, kQRow>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+  }
+  // split 2: bf16x3 statistics (q image in two bf16 parts); split 1: fp16.
+  static void stats(int split, const SParams &p, int grid_x, cudaStream_t s) {
+    const int mtiles = p.Kq / 128;
+    if (kTwo && mtiles % 2 == 0) {
+      if (split == 1) launch_stats<DIM, (kTwo ? 2 : 1), 1>(p, grid_x, mtiles / 2, s);
+      else launch_stats<DIM, (kTwo ? 2 : 1), 2>(p, grid_x, mtiles / 2, s);
+    } else {
+      if (split == 1) launch_stats<DIM, 1, 1>(p, grid_x, mtiles, s);
+      else launch_stats<DIM, 1, 2>(p, grid_x, mtiles, s);
+    }
+  }
+};
+
+i64 estep_dispatch(int D, int qf, const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
+                   unsigned *rowcnt, double *ll, int *err, cudaStream_t s) {
   switch (D) {
-    case 64: return F<64>::run(std::forward<A>(a)...);
-    case 80: return F<80>::run(std::forward<A>(a)...);
-    case 128: return F<128>::run(std::forward<A>(a)...);
+    case 64: return Tc<64>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+    case 80: return Tc<80>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+    case 128: return Tc<128>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
     default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
   }
 }
 
-template <int DIM>
-struct EstepRun {
-  static i64 run(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast, bool out_bf16,
-                 unsigned *rowcnt, double *ll, int *err, cudaStream_t s) {
-    if (out_bf16) return launch_estep<DIM, true, true>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
-    return launch_estep<DIM, true, false>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+void stats_dispatch(int D, int split, const SParams &p, int grid_x, cudaStream_t s) {
+  switch (D) {
+    case 64: Tc<64>::stats(split, p, grid_x, s); break;
+    case 80: Tc<80>::stats(split, p, grid_x, s); break;
+    case 128: Tc<128>::stats(split, p, grid_x, s); break;
+    default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
   }
-};
-
-template <int DIM>
-struct StatsRun {
-  static constexpr int MT = (2 * (2 * DIM + 16) <= 512) ? 2 : 1;
-  static int mt() { return MT; }
-  static void run(const SParams &p, int grid_x, int Kp, bool split3, bool q_bf16, cudaStream_t s) {
-    const int grid_y = (Kp + MT * 128 - 1) / (MT * 128);
-    if (split3) {
-      if (q_bf16) launch_stats<DIM, MT, true, true>(p, grid_x, grid_y, s);
-      else launch_stats<DIM, MT, true, false>(p, grid_x, grid_y, s);
-    } else {
-      if (q_bf16) launch_stats<DIM, MT, false, true>(p, grid_x, grid_y, s);
-      else launch_stats<DIM, MT, false, false>(p, grid_x, grid_y, s);
-    }
-  }
-};
+}
 
 void check_err(int *derr, cudaStream_t s) {
   int h = 0;
   VLB_CUDA(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
   VLB_CUDA(cudaStreamSynchronize(s));
   if (h) throw Error(VL_ERR_BAD_ARG, "tensor-core kernel gave up waiting (code " + std::to_string(h) + ")");
+}
+
+// Longest-processing-time assignment of work items to persistent CTAs:
+// returns per-CTA item lists as (order, begin offsets).
+void lpt_assign(const std::vector<SItem> &items, int gx, std::vector<int> &order, std::vector<int> &beg) {
+  const int nitems = (int)items.size();
+  std::vector<int> idx(nitems);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+    return items[a].row1 - items[a].row0 > items[b].row1 - items[b].row0;
+  });
+  std::vector<std::vector<int>> per(gx);
+  std::vector<i64> load(gx, 0);
+  for (int i : idx) {
+    const int best = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    per[best].push_back(i);
+    load[best] += items[i].row1 - items[i].row0;
+  }
+  order.clear();
+  beg.assign(gx + 1, 0);
+  for (int c = 0; c < gx; ++c) {
+    beg[c] = (int)order.size();
+    order.insert(order.end(), per[c].begin(), per[c].end());
+  }
+  beg[gx] = (int)order.size();
 }
 
 }  // namespace
@@ -847,11 +954,10 @@ i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *
              int precision, cudaStream_t s) {
   (void)precision;
   TcPrep tp;
-  tc_prepare(m, tp, s);
+  tc_prepare(m, tp, false, s);
   int *err = thread_scratch().slot[3].get<int>(1);
   VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  const i64 n = dispatch_dim<EstepRun>(tp.D, X, N, tp, (void *)q, (int)m.K, fast, false,
-                                       (unsigned *)nullptr, ll_part, err, s);
+  const i64 n = estep_dispatch(tp.D, kQRow, X, N, tp, (void *)q, (int)m.K, fast, nullptr, ll_part, err, s);
   check_err(err, s);
   return n;
 }
@@ -859,16 +965,18 @@ i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *
 void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const DevModel<float> &m,
                      float *enc, unsigned long long *nterms, int flags, int precision, cudaStream_t s) {
   Scratch &sc = thread_scratch();
+  const bool fp32 = (precision == VLB200_PREC_FP32);
   TcPrep tp;
-  tc_prepare(m, tp, s);
-  const bool split_stats = (precision == VLB200_PREC_FP32);
-  const bool q_bf16 = !split_stats;
-  const size_t qsz = q_bf16 ? 2 : 4;
+  tc_prepare(m, tp, !fp32, s);
+  const int qf = fp32 ? kQImg32 : kQImg16;
+  const int split = fp32 ? 2 : 1;
+  const size_t qsz = fp32 ? 4 : 2;  // bytes per q element over the image parts
+  const int Kq = padQ(tp.Kp);
   const i64 K = m.K, D = m.D;
   const int NST = (int)(2 * D + 16);
   int *err = sc.slot[3].get<int>(1);
   VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  const i64 kRowBudget = std::max<i64>(1 << 16, (i64)(4ull << 30) / (K * (i64)qsz));
+  const i64 kRowBudget = std::max<i64>(1 << 16, (i64)(4ull << 30) / (tp.Kp * (i64)qsz));
   const i64 kItemRows = 8192;
   const int nsm = num_sms();
 
@@ -891,28 +999,12 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const 
     slot0[nimg] = (int)items.size();
     imgRow0[nimg] = row1;
     const int nitems = (int)items.size();
-    // Longest-processing-time assignment of items to persistent CTAs.
     const int gx = std::max(1, std::min(nitems, nsm));
-    std::vector<int> idx(nitems);
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
-      return items[a].row1 - items[a].row0 > items[b].row1 - items[b].row0;
-    });
-    std::vector<std::vector<int>> per(gx);
-    std::vector<i64> load(gx, 0);
-    for (int i : idx) {
-      int best = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-      per[best].push_back(i);
-      load[best] += items[i].row1 - items[i].row0;
-    }
-    std::vector<int> order, beg(gx + 1, 0);
-    for (int c = 0; c < gx; ++c) {
-      beg[c] = (int)order.size();
-      order.insert(order.end(), per[c].begin(), per[c].end());
-    }
-    beg[gx] = (int)order.size();
+    std::vector<int> order, beg;
+    lpt_assign(items, gx, order, beg);
 
-    void *q = sc.slot[4].get<char>((size_t)std::max<i64>(1, nrows) * K * qsz);
+    const i64 ntiles = (nrows + 127) / 128;
+    void *q = sc.slot[4].get<char>((size_t)std::max<i64>(1, ntiles) * 128 * Kq * qsz);
     unsigned *rowcnt = sc.slot[5].get<unsigned>(std::max<i64>(1, nrows));
     float *partial = sc.slot[6].get<float>((size_t)std::max(1, nitems) * tp.Kp * NST);
     SItem *ditems = sc.slot[7].get<SItem>(std::max(1, nitems));
@@ -929,23 +1021,19 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const 
     VLB_CUDA(cudaMemcpyAsync(drow0, imgRow0.data(), sizeof(i64) * (nimg + 1), cudaMemcpyHostToDevice, s));
 
     if (nrows > 0) {
-      dispatch_dim<EstepRun>(tp.D, X + row0 * D, nrows, tp, q, (int)K, (flags & 4) != 0, q_bf16,
-                             rowcnt, (double *)nullptr, err, s);
+      estep_dispatch(tp.D, qf, X + row0 * D, nrows, tp, q, (int)K, (flags & 4) != 0, rowcnt, nullptr, err, s);
       SParams sp;
-      sp.X = X; sp.q = q; sp.qbase = row0; sp.ldq = (int)K; sp.K = (int)K; sp.Kp = tp.Kp; sp.nst = 0;
-      sp.ctr = tp.ctr; sp.qthr = 1e-6f; sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg;
-      sp.partial = partial; sp.err = err;
-      switch (tp.D) {
-        case 64: StatsRun<64>::run(sp, gx, tp.Kp, split_stats, q_bf16, s); break;
-        case 80: StatsRun<80>::run(sp, gx, tp.Kp, split_stats, q_bf16, s); break;
-        case 128: StatsRun<128>::run(sp, gx, tp.Kp, split_stats, q_bf16, s); break;
-        default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
-      }
+      sp.X = X; sp.qimg = (const uint8_t *)q; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = row0;
+      sp.K = (int)K; sp.Kp = tp.Kp; sp.Kq = Kq; sp.nst = 0;
+      sp.ctr = tp.ctr; sp.scale = fp32 ? nullptr : tp.scale;
+      sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg; sp.partial = partial; sp.err = err;
+      stats_dispatch(tp.D, split, sp, gx, s);
     }
     VLB_LAUNCH("tc_fv_finalize", s,
                k_tc_fv_finalize<<<(unsigned)nimg, 256, 0, s>>>(
                    (int)K, tp.Kp, (int)D, partial, dslot0, drow0, m.means, m.covs, m.priors, tp.ctr,
-                   nrows > 0 ? rowcnt : nullptr, row0, flags, chunkImg0, enc, nterms));
+                   fp32 ? nullptr : tp.scale, nrows > 0 ? rowcnt : nullptr, row0, flags, chunkImg0,
+                   enc, nterms));
   }
   check_err(err, s);
 }
