@@ -90,12 +90,13 @@ struct DevBuf {
   }
 };
 
-// Per-thread scratch arena: named slots reused across calls on one thread.
+// Per-thread scratch arenas of device buffers reused across calls on one
+// thread.  Each module owns an arena so slot numbers never collide.
 struct Scratch {
   DevBuf slot[32];
-  DevBuf host_pinned_unused;
 };
-Scratch &thread_scratch();
+enum ScratchArena { kArenaApi = 0, kArenaExact = 1, kArenaTc = 2, kArenaRouter = 3, kNumArenas = 4 };
+Scratch &thread_scratch(int arena = kArenaApi);
 
 // Pinned host staging buffer (per thread), for host-pointer API calls.
 void *pinned_host(size_t bytes);

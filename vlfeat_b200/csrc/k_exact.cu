@@ -518,7 +518,7 @@ void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i6
   constexpr int TKC = 32, RC = 32, JMAX = sizeof(T) == 8 ? 8 : 16, DB = 8 * JMAX;
   const i64 rps = pick_slab_rows(N > 0 ? N : 1);
   const int nslab = (int)((N + rps - 1) / rps > 0 ? (N + rps - 1) / rps : 1);
-  Scratch &sc = thread_scratch();
+  Scratch &sc = thread_scratch(kArenaExact);
   double *pmass = sc.slot[10].get<double>((size_t)nslab * K);
   double *ps1 = sc.slot[11].get<double>((size_t)nslab * K * D);
   double *ps2 = sc.slot[12].get<double>((size_t)nslab * K * D);
@@ -542,7 +542,7 @@ template <typename T>
 void column_mass(const T *q, i64 N, i64 K, double *mass, cudaStream_t s) {
   const i64 rps = pick_slab_rows(N > 0 ? N : 1);
   const int nslab = (int)((N + rps - 1) / rps > 0 ? (N + rps - 1) / rps : 1);
-  double *part = thread_scratch().slot[13].get<double>((size_t)nslab * K);
+  double *part = thread_scratch(kArenaExact).slot[13].get<double>((size_t)nslab * K);
   if (N > 0) {
     VLB_LAUNCH("column_mass", s, k_colmass<T><<<nslab, kThreads, 0, s>>>(q, N, (int)K, rps, part));
   } else {
@@ -577,7 +577,7 @@ void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const D
   constexpr i64 kSegRows = 2048;
   const i64 kRowBudget = std::max<i64>(4096, (i64)(1u << 30) / (K * (i64)sizeof(T)));
   const i64 kSegBudget = std::max<i64>(64, (i64)(256u << 20) / (2 * K * D * 8));
-  Scratch &sc = thread_scratch();
+  Scratch &sc = thread_scratch(kArenaExact);
   DevDerived<T> der;
   der.inv = sc.slot[0].get<T>(K * D);
   der.sis = sc.slot[1].get<T>(K * D);

@@ -47,7 +47,7 @@ namespace {
 
 using namespace tc;
 
-constexpr int kTcThreads = 288;
+constexpr int kTcThreads = 416;  // E-step: 4 producer, 8 epilogue, 1 MMA warp
 constexpr int kSmemLimit = 232448;  // 227 KB opt-in per block
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr double kLn2 = 0.6931471805599453;
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 8) {
+  if (warp == 12) {
     tmem_alloc(s_tmem, 512);
     tmem_relinquish();
   }
@@ -295,75 +295,96 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     };
     while (step(b0, b2) && step(b1, b0) && step(b2, b1)) {
     }
-  } else if (warp < 8) {
+  } else if (warp < 12) {
     // ----------------------------------------------------- epilogue
-    const int ew = warp - 4;
+    // Two warpgroups: group g drains the tiles whose accumulator is TMEM
+    // buffer g (alternate tiles), so one tile's log-sum-exp overlaps the next.
+    // Warp w reads TMEM lanes 32 (w % 4) .. +31, i.e. rows of the tile.
+    const int eg = (warp - 4) >> 2, ew = warp & 3;
     const int r = ew * 32 + lane;
     const int nch = p.Kp / 32;
     int tt = 0;
     for (i64 tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++tt) {
       const int buf = tt & 1;
+      if (buf != eg) continue;
       if (!mbar_wait(&accf[buf], (tt >> 1) & 1, s_abort, p.err, 2)) break;
       tc_fence_after();
       const uint32_t tb = tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(buf * 256);
-      float m2 = -INFINITY;
+      // Pass A: online log-sum-exp over 64-column groups.  e = 2^(s - m_g)
+      // is written back to TMEM with the running maximum m_g of its group.
+      float m = -INFINITY, sum = 0.f, mg[4];
       int am = 0;
-      for (int cc = 0; cc < nch; ++cc) {
-        uint32_t v[32];
-        tmem_ld32(tb + cc * 32, v);
+#pragma unroll 1
+      for (int pc = 0; pc < nch; pc += 2) {
+        const bool two = pc + 1 < nch;
+        uint32_t va[32], vb[32];
+        tmem_ld32(tb + pc * 32, va);
+        if (two) tmem_ld32(tb + pc * 32 + 32, vb);
         tmem_wait_ld();
+        float cm = -INFINITY;
+        int cam = 0;
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-          const float s = __uint_as_float(v[j]) + s_cst[cc * 32 + j];
-          if (s > m2) {
-            m2 = s;
-            am = cc * 32 + j;
+          const float x = __uint_as_float(va[j]) + s_cst[pc * 32 + j];
+          va[j] = __float_as_uint(x);
+          if (x > cm) { cm = x; cam = pc * 32 + j; }
+        }
+        if (two) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const float x = __uint_as_float(vb[j]) + s_cst[pc * 32 + 32 + j];
+            vb[j] = __float_as_uint(x);
+            if (x > cm) { cm = x; cam = pc * 32 + 32 + j; }
           }
         }
-      }
-      float sum = 0.f;
-      for (int cc = 0; cc < nch; ++cc) {
-        uint32_t v[32];
-        tmem_ld32(tb + cc * 32, v);
-        tmem_wait_ld();
+        if (cm > m) {
+          sum = (m == -INFINITY) ? 0.f : sum * ex2_approx(m - cm);
+          m = cm;
+          am = cam;
+        }
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-          const float e = ex2_approx(__uint_as_float(v[j]) + s_cst[cc * 32 + j] - m2);
+          const float e = ex2_approx(__uint_as_float(va[j]) - m);
           sum += e;
-          v[j] = __float_as_uint(e);
+          va[j] = __float_as_uint(e);
         }
-        tmem_st32(tb + cc * 32, v);
+        tmem_st32(tb + pc * 32, va);
+        if (two) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const float e = ex2_approx(__uint_as_float(vb[j]) - m);
+            sum += e;
+            vb[j] = __float_as_uint(e);
+          }
+          tmem_st32(tb + pc * 32 + 32, vb);
+        }
+        mg[pc >> 1] = m;
       }
       tmem_wait_st();
       const float inv = 1.f / sum;
       const i64 row = tile * 128 + r;
       const bool valid = row < p.N;
       unsigned cnt = 0;
-      // q image: this row's offset inside its tile (8-row group, row in group).
+      // q image: this row's 8-row group inside its tile.
       uint8_t *ib = (uint8_t *)p.q + (size_t)tile * 128 * p.Kq * 2;
-      const uint32_t rowoff = (uint32_t)((r >> 3) * (p.Kq / 64) * 1024);  // + row-in-group below
+      const uint32_t rowoff = (uint32_t)((r >> 3) * (p.Kq / 64) * 1024);
       const int ncw = (QF == kQRow) ? nch : p.Kq / 32;
-      for (int cc = 0; cc < ncw; ++cc) {
+      // Pass B: q = e * 2^(m_g - m) / sum, thresholded and stored, one
+      // 32-column chunk at a time.
+      auto emit = [&](const uint32_t(&v)[32], int cc, bool have, float sc) {
         float qv[32];
-        if (cc < nch) {
-          uint32_t v[32];
-          tmem_ld32(tb + cc * 32, v);
-          tmem_wait_ld();
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            float x = p.fast ? (cc * 32 + j == am ? 1.f : 0.f) : __uint_as_float(v[j]) * inv;
-            x = valid ? x : 0.f;
-            cnt += (x >= 1e-6f) ? 1u : 0u;
-            if (QF != kQRow && x < p.qthr) x = 0.f;
-            qv[j] = x;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) qv[j] = 0.f;
+        for (int j = 0; j < 32; ++j) {
+          float x = have ? __uint_as_float(v[j]) * sc : 0.f;
+          if (p.fast) x = (have && cc * 32 + j == am) ? 1.f : 0.f;
+          x = valid ? x : 0.f;
+          cnt += (x >= 1e-6f) ? 1u : 0u;
+          if (QF != kQRow && x < p.qthr) x = 0.f;
+          qv[j] = x;
         }
         const int k0 = cc * 32;
         if (QF == kQRow) {
-          if (!valid) continue;
+          if (!valid || !have) return;
           float *dst = (float *)p.q + row * p.ldq + k0;
           if (k0 + 32 <= p.K) {
 #pragma unroll
@@ -380,25 +401,43 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
             const int kk = k0 + 8 * j;
             const uint32_t off = rowoff + (uint32_t)((kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
             uint4 wh, wl;
-            split2<QF == kQImg16>(qv[8 * j + 0], qv[8 * j + 1], wh.x, wl.x);
-            split2<QF == kQImg16>(qv[8 * j + 2], qv[8 * j + 3], wh.y, wl.y);
-            split2<QF == kQImg16>(qv[8 * j + 4], qv[8 * j + 5], wh.z, wl.z);
-            split2<QF == kQImg16>(qv[8 * j + 6], qv[8 * j + 7], wh.w, wl.w);
+            if (QF == kQImg16) {
+              wh.x = pack2<true>(qv[8 * j + 0], qv[8 * j + 1]);
+              wh.y = pack2<true>(qv[8 * j + 2], qv[8 * j + 3]);
+              wh.z = pack2<true>(qv[8 * j + 4], qv[8 * j + 5]);
+              wh.w = pack2<true>(qv[8 * j + 6], qv[8 * j + 7]);
+            } else {
+              split2<false>(qv[8 * j + 0], qv[8 * j + 1], wh.x, wl.x);
+              split2<false>(qv[8 * j + 2], qv[8 * j + 3], wh.y, wl.y);
+              split2<false>(qv[8 * j + 4], qv[8 * j + 5], wh.z, wl.z);
+              split2<false>(qv[8 * j + 6], qv[8 * j + 7], wh.w, wl.w);
+            }
             *(uint4 *)(ib + off) = wh;
             if (QF == kQImg32) *(uint4 *)(ib + p.qpart + off) = wl;
           }
         }
+      };
+#pragma unroll 1
+      for (int cc = 0; cc < ncw; ++cc) {
+        uint32_t va[32];
+        const bool ha = cc < nch;
+        if (ha) {
+          tmem_ld32(tb + cc * 32, va);
+          tmem_wait_ld();
+        }
+        const float sc = ha ? ex2_approx(mg[cc >> 1] - m) * inv : 0.f;
+        emit(va, cc, ha, sc);
       }
       tc_fence_before();
       mbar_arrive(&acce[buf]);
       if (valid && p.rowcnt) p.rowcnt[row] = cnt;
       // Per-warp log-likelihood partial (fixed shuffle order): 4 per tile.
-      double ll = valid ? ((double)m2 + log2((double)sum)) * kLn2 : 0.0;
+      double ll = valid ? ((double)m + log2((double)sum)) * kLn2 : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
       if (lane == 0 && p.ll_part) p.ll_part[tile * 4 + ew] = ll;
     }
-  } else if (lane == 0) {
+  } else if (warp == 12 && lane == 0) {
     // ---------------------------------------------------------- MMA
     const uint32_t idesc = idesc_bf16(128, p.Kp, false, false);
     const uint32_t w_hi = smem_u32(sW), w_lo = w_hi + wbytes;
@@ -435,7 +474,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 8) {
+  if (warp == 12) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
   }
@@ -720,22 +759,46 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) 
 }
 
 // ======================================================= finalize (FV)
+// Per-component constants of the Fisher finalisation, computed once per call:
+// mu' = mu - m, 1/sigma2, 1/sigma (K x D) and the prefactors 1/sqrt(pi),
+// 1/sqrt(2 pi) (0 for components skipped by vl/fisher.c:436).
+__global__ void k_tc_fv_consts(const float *__restrict__ means, const float *__restrict__ covs,
+                               const float *__restrict__ priors, const float *__restrict__ ctr, int K,
+                               int D, double *__restrict__ cmu, double *__restrict__ cis2,
+                               double *__restrict__ cisd, double *__restrict__ cup,
+                               double *__restrict__ cvp) {
+  const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < (i64)K * D) {
+    const int d = (int)(e % D);
+    const double s2 = (double)covs[e];
+    cmu[e] = (double)means[e] - (double)ctr[d];
+    cis2[e] = 1.0 / s2;
+    cisd[e] = 1.0 / sqrt(s2);
+  }
+  if (e < K) {
+    const double pk = (double)priors[e];
+    cup[e] = pk >= 1e-6 ? 1.0 / sqrt(pk) : 0.0;
+    cvp[e] = pk >= 1e-6 ? 1.0 / sqrt(2.0 * pk) : 0.0;
+  }
+}
+
 // Per image: reduce the item partials in double and form the Fisher vector
 // (vl/fisher.c:419-485) from S0 = sum q, S1 = sum q x', S2 = sum q x'^2:
-//   u = s (S1 - mu' S0),  v = s^2 (S2 - 2 mu' S1 + mu'^2 S0) - S0,
+//   u = (S1 - mu' S0) / sigma,  v = (S2 - 2 mu' S1 + mu'^2 S0) / sigma2 - S0,
 // scaled by 1/(N sqrt pi) and 1/(N sqrt(2 pi)); signed sqrt; L2.
 __global__ void __launch_bounds__(256) k_tc_fv_finalize(
     int K, int Kp, int D, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
-    const i64 *__restrict__ imgRow0, const float *__restrict__ means, const float *__restrict__ covs,
-    const float *__restrict__ priors, const float *__restrict__ ctr, const float *__restrict__ scale,
-    const unsigned *__restrict__ rowcnt, i64 rowcntBase, int flags, i64 imgBase,
-    float *__restrict__ enc, unsigned long long *__restrict__ nterms) {
+    const i64 *__restrict__ imgRow0, const double *__restrict__ cmu, const double *__restrict__ cis2,
+    const double *__restrict__ cisd, const double *__restrict__ cup, const double *__restrict__ cvp,
+    const float *__restrict__ scale, const unsigned *__restrict__ rowcnt, i64 rowcntBase, int flags,
+    i64 imgBase, float *__restrict__ enc, unsigned long long *__restrict__ nterms) {
   __shared__ double sh[256];
   __shared__ unsigned long long shn[256];
   const int img = blockIdx.x;
   const int s0 = imgSlot0[img], s1 = imgSlot0[img + 1];
   const i64 r0 = imgRow0[img], r1 = imgRow0[img + 1];
   const i64 n = r1 - r0;
+  const double in = n > 0 ? 1.0 / (double)n : 0.0;
   const int NST = 2 * D + 16;
   const i64 KD = (i64)K * D;
   float *out = enc + (imgBase + img) * 2 * KD;
@@ -754,17 +817,9 @@ __global__ void __launch_bounds__(256) k_tc_fv_finalize(
       S1 *= is;
       S2 *= is * is;
     }
-    const double pk = (double)priors[k];
-    double u = 0, v = 0;
-    if (pk >= 1e-6 && n > 0) {
-      const double s2 = (double)covs[e];
-      const double mup = (double)means[e] - (double)ctr[d];
-      const double isd = 1.0 / sqrt(s2);
-      u = isd * (S1 - mup * S0);
-      v = (S2 - 2.0 * mup * S1 + mup * mup * S0) / s2 - S0;
-      u *= 1.0 / ((double)n * sqrt(pk));
-      v *= 1.0 / ((double)n * sqrt(2.0 * pk));
-    }
+    const double mup = cmu[e];
+    const double u = cisd[e] * (S1 - mup * S0) * (cup[k] * in);
+    const double v = ((S2 - 2.0 * mup * S1 + mup * mup * S0) * cis2[e] - S0) * (cvp[k] * in);
     float uf = (float)u, vf = (float)v;
     if (flags & 1) {
       uf = uf >= 0.f ? sqrtf(uf) : -sqrtf(-uf);
@@ -803,10 +858,10 @@ struct TcPrep {
   __nv_bfloat16 *wimg = nullptr;
 };
 
-int padK(i64 K) { return (int)((K + 15) / 16 * 16); }
+int padK(i64 K) { return (int)((K + 31) / 32 * 32); }
 
 void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, cudaStream_t s) {
-  Scratch &sc = thread_scratch();
+  Scratch &sc = thread_scratch(kArenaTc);
   tp.K = (int)m.K;
   tp.Kp = padK(m.K);
   tp.D = (int)m.D;
@@ -955,7 +1010,7 @@ i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *
   (void)precision;
   TcPrep tp;
   tc_prepare(m, tp, false, s);
-  int *err = thread_scratch().slot[3].get<int>(1);
+  int *err = thread_scratch(kArenaTc).slot[3].get<int>(1);
   VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
   const i64 n = estep_dispatch(tp.D, kQRow, X, N, tp, (void *)q, (int)m.K, fast, nullptr, ll_part, err, s);
   check_err(err, s);
@@ -964,7 +1019,7 @@ i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *
 
 void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const DevModel<float> &m,
                      float *enc, unsigned long long *nterms, int flags, int precision, cudaStream_t s) {
-  Scratch &sc = thread_scratch();
+  Scratch &sc = thread_scratch(kArenaTc);
   const bool fp32 = (precision == VLB200_PREC_FP32);
   TcPrep tp;
   tc_prepare(m, tp, !fp32, s);
@@ -979,6 +1034,12 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const 
   const i64 kRowBudget = std::max<i64>(1 << 16, (i64)(4ull << 30) / (tp.Kp * (i64)qsz));
   const i64 kItemRows = 8192;
   const int nsm = num_sms();
+  double *cmu = sc.slot[13].get<double>(K * D), *cis2 = sc.slot[14].get<double>(K * D);
+  double *cisd = sc.slot[15].get<double>(K * D), *cup = sc.slot[16].get<double>(K);
+  double *cvp = sc.slot[17].get<double>(K);
+  VLB_LAUNCH("tc_fv_consts", s,
+             k_tc_fv_consts<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
+                 m.means, m.covs, m.priors, tp.ctr, (int)K, (int)D, cmu, cis2, cisd, cup, cvp));
 
   i64 img = 0;
   while (img < numImages) {
@@ -1031,7 +1092,7 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const 
     }
     VLB_LAUNCH("tc_fv_finalize", s,
                k_tc_fv_finalize<<<(unsigned)nimg, 256, 0, s>>>(
-                   (int)K, tp.Kp, (int)D, partial, dslot0, drow0, m.means, m.covs, m.priors, tp.ctr,
+                   (int)K, tp.Kp, (int)D, partial, dslot0, drow0, cmu, cis2, cisd, cup, cvp,
                    fp32 ? nullptr : tp.scale, nrows > 0 ? rowcnt : nullptr, row0, flags, chunkImg0,
                    enc, nterms));
   }

@@ -118,7 +118,7 @@ struct StreamHolder {
   }
 };
 thread_local StreamHolder g_stream;
-thread_local Scratch *g_scratch = nullptr;
+thread_local Scratch *g_scratch[kNumArenas] = {nullptr, nullptr, nullptr, nullptr};
 thread_local DevBuf *g_pinned_dummy = nullptr;
 thread_local void *g_pinned = nullptr;
 thread_local size_t g_pinned_cap = 0;
@@ -141,9 +141,10 @@ cudaStream_t thread_stream() {
   return g_stream.s;
 }
 
-Scratch &thread_scratch() {
-  if (!g_scratch) g_scratch = new Scratch();  // lives until process exit
-  return *g_scratch;
+Scratch &thread_scratch(int arena) {
+  if (arena < 0 || arena >= kNumArenas) arena = kArenaApi;
+  if (!g_scratch[arena]) g_scratch[arena] = new Scratch();  // lives until process exit
+  return *g_scratch[arena];
 }
 
 void *pinned_host(size_t bytes) {

@@ -197,21 +197,36 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool a_mn_major, 
 }
 
 // Two 16-bit values (bf16 or fp16 by F16) of a float pair, hi parts and lo
-// parts packed into one 32-bit word each.
+// parts packed into one 32-bit word each.  Paired conversions (one
+// instruction per two values) and an exact widening of the hi part keep the
+// split off the conversion unit that MUFU.EX2 also uses.
 template <bool F16>
 __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo) {
   if (F16) {
-    const __half ha = __float2half_rn(a), hb = __float2half_rn(b);
-    const __half la = __float2half_rn(a - __half2float(ha)), lb = __float2half_rn(b - __half2float(hb));
-    hi = (uint32_t)__half_as_ushort(ha) | ((uint32_t)__half_as_ushort(hb) << 16);
-    lo = (uint32_t)__half_as_ushort(la) | ((uint32_t)__half_as_ushort(lb) << 16);
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+    hi = *(const uint32_t *)&h;
+    lo = *(const uint32_t *)&l;
   } else {
-    __nv_bfloat16 ha, la, hb, lb;
-    split_bf16(a, ha, la);
-    split_bf16(b, hb, lb);
-    hi = pack_bf16(ha, hb);
-    lo = pack_bf16(la, lb);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    const uint32_t hu = *(const uint32_t *)&h;
+    const float ha = __uint_as_float(hu << 16), hb = __uint_as_float(hu & 0xFFFF0000u);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(a - ha, b - hb);
+    hi = hu;
+    lo = *(const uint32_t *)&l;
   }
+}
+
+// Two values rounded to one 16-bit pair (hi part only).
+template <bool F16>
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+  if (F16) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *(const uint32_t *)&h;
+  }
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *(const uint32_t *)&h;
 }
 
 // Arm `bar` for `bytes` of incoming bulk-copy data (one arrival).
