@@ -93,4 +93,25 @@ VL_EXPORT int vlb200_fisher_encode_batch_device(float *enc, float const *means, 
                                                 int flags, int precision, vl_uint64 *numTerms,
                                                 void *stream);
 
+/* Fisher encoding of one image that allocates nothing.  No counterpart in
+ * the reference: it exists for callers that cannot allocate device memory on
+ * the call path (work being recorded into a CUDA graph by stream capture,
+ * services that forbid allocation after start-up, hosts with a fixed memory
+ * budget).  The caller passes inputs and outputs as device pointers, as for
+ * vlb200_fisher_encode_device; the scratch is a fixed 8 MiB device array
+ * inside the library, held by every GPU that loads it until the process
+ * exits.  Limits: numData <= 4096, numClusters <= 256, dimension <= 128;
+ * larger requests fail with VL_ERR_BAD_ARG.  Arithmetic: the exact fp32
+ * path (VLB200_PREC_EXACT).  numTerms: one uint64 in device memory, or NULL.
+ * stream: a cudaStream_t; NULL is the legacy default stream.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (on different streams, or from
+ * different threads) race and must be serialised by the caller. */
+VL_EXPORT int vlb200_fisher_encode_noalloc(float *enc, float const *means, vl_size dimension,
+                                           vl_size numClusters, float const *covariances,
+                                           float const *priors, float const *data,
+                                           vl_size numData, int flags, vl_uint64 *numTerms,
+                                           void *stream);
+
 #endif /* VLB200_H */

@@ -53,6 +53,16 @@ void launch_end(const char *name, cudaStream_t s);
     ::vlb::launch_end((name), (stream));        \
   } while (0)
 
+// Launch without the optional event timing (which creates CUDA events): used
+// by the entry point that must not allocate.  The launch is still counted.
+void count_launch();
+#define VLB_LAUNCH_PLAIN(stream, ...)  \
+  do {                                 \
+    __VA_ARGS__;                       \
+    VLB_CUDA(cudaGetLastError());      \
+    ::vlb::count_launch();             \
+  } while (0)
+
 // Grow-only device buffer.  Contents are not preserved across growth.
 struct DevBuf {
   void *p = nullptr;

@@ -81,6 +81,22 @@ template <typename T>
 void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const DevModel<T> &m,
                         T *enc, unsigned long long *nterms, int flags, cudaStream_t s);
 
+// Single-image exact Fisher encoding on caller-provided scratch (no
+// allocation, no host-to-device copies, no event timing).  Every scratch
+// element the kernels read is written earlier in the same call.
+struct ExactFvScratch {
+  float *inv, *sis, *q;
+  double *cst, *llp, *pu, *pv;
+  Segment *segs;
+  int *segBegin;
+  i64 *rows;
+  unsigned long long *pnt;
+};
+i64 exact_fv_segments(i64 N);  // segments one image of N rows is cut into
+void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, float *enc,
+                               unsigned long long *nterms, int flags, const ExactFvScratch &sc,
+                               cudaStream_t s);
+
 // ------------------------------------------------------- tensor-core path
 // Implemented in k_tc.cu.  Available for float data only.
 bool tc_supported(i64 K, i64 D);

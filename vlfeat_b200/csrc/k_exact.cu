@@ -633,6 +633,52 @@ void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const D
   }
 }
 
+namespace {
+constexpr i64 kFixedSegRows = 2048;
+
+// Segment tables of one image, written on the device so a call needs no
+// host-to-device copy.
+__global__ void k_single_segments(i64 N, i64 nseg, Segment *segs, int *segBegin, i64 *rows) {
+  for (i64 j = threadIdx.x; j < nseg; j += blockDim.x) {
+    const i64 a = j * kFixedSegRows;
+    segs[j] = Segment{0, a, a + kFixedSegRows < N ? a + kFixedSegRows : N};
+  }
+  if (threadIdx.x == 0) {
+    segBegin[0] = 0;
+    segBegin[1] = (int)nseg;
+    rows[0] = N;
+  }
+}
+}  // namespace
+
+i64 exact_fv_segments(i64 N) { return N > 0 ? (N + kFixedSegRows - 1) / kFixedSegRows : 1; }
+
+void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, float *enc,
+                               unsigned long long *nterms, int flags, const ExactFvScratch &sc,
+                               cudaStream_t s) {
+  constexpr int TKC = 32, RC = 32, JMAX = 10, DB = 8 * JMAX;
+  constexpr int TM = 32, TK = 64, DC = 32;
+  const i64 K = m.K, D = m.D, nseg = exact_fv_segments(N);
+  VLB_LAUNCH_PLAIN(s, k_single_segments<<<1, 32, 0, s>>>(N, nseg, sc.segs, sc.segBegin, sc.rows));
+  VLB_LAUNCH_PLAIN(s, k_prepare<float><<<grid1(K, 128), 128, 0, s>>>(
+                          m.priors, m.covs, (int)K, (int)D, half_dim_log_2pi<float>(D), sc.inv,
+                          sc.cst, sc.sis));
+  if (N > 0) {
+    dim3 g(grid1(N, TM), grid1(K, TK));
+    VLB_LAUNCH_PLAIN(s, (k_logp<float, TM, TK, DC><<<g, kThreads, 0, s>>>(X, N, (int)D, (int)K, m.means,
+                                                                         sc.inv, sc.cst, sc.q)));
+    VLB_LAUNCH_PLAIN(s, k_normalize<float><<<grid1(N, 8), kThreads, 0, s>>>(sc.q, N, (int)K,
+                                                                         (flags & 4) ? 1 : 0, sc.llp));
+  }
+  dim3 g2((unsigned)nseg, grid1(K, TKC), grid1(D, DB));
+  VLB_LAUNCH_PLAIN(s, (k_fisher_stats<float, TKC, RC, JMAX><<<g2, kThreads, 0, s>>>(
+                          X, sc.q, 0, (int)K, (int)D, sc.segs, m.means, sc.sis, m.priors, sc.pu,
+                          sc.pv, sc.pnt)));
+  VLB_LAUNCH_PLAIN(s, k_fisher_finalize<float><<<1, kThreads, 0, s>>>(
+                          (int)K, (int)D, sc.segBegin, sc.rows, sc.pu, sc.pv, sc.pnt, m.priors,
+                          flags, 0, enc, nterms));
+}
+
 // ------------------------------------------------------ instantiations
 #define VLB_INST(T)                                                                          \
   template void exact_prepare<T>(const DevModel<T> &, DevDerived<T> &, cudaStream_t);        \
