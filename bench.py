@@ -122,6 +122,27 @@ def make_workload(rank, device):
                 np_gmm=(pr, mu, cv))
 
 
+def train_router(capi, wl, n_train=200_000, m=16, threshold=0.99):
+    """Router for the BF16+router path: trained (untimed) on the full-E-step
+    posteriors of the first n_train descriptors of the workload."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    from vlfeat_b200.router import Router, targets
+    x = wl["x"][:n_train].contiguous()
+    q = torch.zeros((n_train, K), device="cuda")
+    capi.gmm_posteriors_device(q, wl["priors"], wl["means"], wl["covs"], x, "exact")
+    tidx = torch.zeros((n_train, 8), dtype=torch.int32, device="cuda")
+    tw = torch.zeros((n_train, 8), dtype=torch.float32, device="cuda")
+    targets(q, tidx, tw)
+    r = Router(D, K, hidden=(128,), seed=7)
+    r.set_input_transform(np.zeros(D, np.float32),
+                          (1.0 / np.sqrt(W.pca_lambdas(D))).astype(np.float32))
+    r.train(x, tidx, tw, epochs=4, batch=1024, lr=2e-3)
+    r.set_default(m=m, threshold=threshold)
+    del q, tidx, tw
+    return r
+
+
 def encode(capi, wl, enc, nt, prec, stream):
     capi.fisher_encode_batch_device(enc, wl["means"], wl["covs"], wl["priors"], wl["x"], wl["offs"],
                                     FLAGS, prec, nt, stream)
@@ -345,6 +366,7 @@ def main():
     nt = torch.empty(NUM_IMAGES, dtype=torch.int64, device=dev)
 
     ref = fp64_reference(capi, wl) if rank == 0 else None
+    router = train_router(capi, wl) if "bf16_router" in args.paths else None  # noqa: F841
     results = {}
     launches_of = {}
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:

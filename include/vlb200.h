@@ -93,6 +93,51 @@ VL_EXPORT int vlb200_fisher_encode_batch_device(float *enc, float const *means, 
                                                 int flags, int precision, vl_uint64 *numTerms,
                                                 void *stream);
 
+/* ----------------------------------------------------------------- router
+ * Learned candidate router for the E-step (no reference counterpart; the
+ * reference always evaluates every component, vl/gmm.c:758-791).  An MLP
+ * D -> hidden... -> K (ReLU, bf16 weights, fp32 accumulation) predicts each
+ * descriptor's top-m components; the exact posterior is computed on those
+ * only, and the full E-step is used for descriptors whose predicted candidate
+ * mass is below a threshold.  Trained on the GPU by the library's own
+ * forward / backward / Adam kernels against the top-8 posteriors of the full
+ * E-step.  All pointers to data are device pointers unless stated. */
+typedef struct _VlB200Router VlB200Router;
+VL_EXPORT VlB200Router *vlb200_router_new(vl_size dimension, vl_size numClusters,
+                                          vl_size const *hidden, vl_size numHidden,
+                                          vl_uint32 seed);
+VL_EXPORT void vlb200_router_delete(VlB200Router *router);
+VL_EXPORT vl_size vlb200_router_num_params(VlB200Router const *router);
+/* Host vector: per layer W (out x in, row-major) then b. */
+VL_EXPORT int vlb200_router_get_params(VlB200Router const *router, float *params);
+VL_EXPORT int vlb200_router_set_params(VlB200Router *router, float const *params);
+/* Input features z = (x - centre) * scale; host arrays of D. */
+VL_EXPORT int vlb200_router_set_input_transform(VlB200Router *router, float const *centre,
+                                                float const *scale);
+/* Top-8 targets (N x 8 indices and renormalised weights) of posteriors. */
+VL_EXPORT int vlb200_router_targets(float const *posteriors, vl_size numData,
+                                    vl_size numClusters, int *targetIdx, float *targetWeight);
+/* Mean top-8 cross-entropy of a batch and, if grads (host) is non-NULL, its
+ * gradient in the get_params layout. */
+VL_EXPORT int vlb200_router_loss_grad(VlB200Router *router, float const *data, vl_size batch,
+                                      int const *targetIdx, float const *targetWeight,
+                                      double *loss, float *grads);
+VL_EXPORT int vlb200_router_train(VlB200Router *router, float const *data, vl_size numData,
+                                  int const *targetIdx, float const *targetWeight, vl_size epochs,
+                                  vl_size batch, float learningRate, double *lastEpochLoss);
+/* Posteriors (N x K, zero off the candidates) from the top-m candidates;
+ * fallbackRows (host, may be NULL) counts rows that used the full E-step. */
+VL_EXPORT int vlb200_router_posteriors(VlB200Router *router, float *posteriors,
+                                       float const *priors, float const *means,
+                                       float const *covariances, float const *data,
+                                       vl_size numData, vl_size m, float threshold,
+                                       vl_uint64 *fallbackRows, void *stream);
+VL_EXPORT int vlb200_router_missed_mass(float const *fullPosteriors,
+                                        float const *candidatePosteriors, vl_size numData,
+                                        vl_size numClusters, double *meanMissedMass);
+/* Router used by VLB200_PREC_BF16_ROUTER calls (not owned; NULL clears). */
+VL_EXPORT int vlb200_router_set_default(VlB200Router *router, vl_size m, float threshold);
+
 /* Fisher encoding of one image that allocates nothing.  No counterpart in
  * the reference: it exists for callers that cannot allocate device memory on
  * the call path (work being recorded into a CUDA graph by stream capture,

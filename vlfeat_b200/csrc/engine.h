@@ -79,7 +79,8 @@ struct Segment {
 // array.  enc: numImages x 2KD (device).  nterms: numImages (device) or null.
 template <typename T>
 void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const DevModel<T> &m,
-                        T *enc, unsigned long long *nterms, int flags, cudaStream_t s);
+                        T *enc, unsigned long long *nterms, int flags, cudaStream_t s,
+                        bool use_router = false);
 
 // Single-image exact Fisher encoding on caller-provided scratch (no
 // allocation, no host-to-device copies, no event timing).  Every scratch
@@ -95,6 +96,11 @@ struct ExactFvScratch {
 i64 exact_fv_segments(i64 N);  // segments one image of N rows is cut into
 void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, float *enc,
                                unsigned long long *nterms, int flags, const ExactFvScratch &sc,
+                               cudaStream_t s);
+
+// Posteriors (N x K, row-major) from the process-wide default router
+// (vlb200_router_set_default); implemented in k_router.cu.
+void router_default_posteriors(const float *X, i64 N, const DevModel<float> &m, float *q,
                                cudaStream_t s);
 
 // ------------------------------------------------------- tensor-core path

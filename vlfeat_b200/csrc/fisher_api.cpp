@@ -37,7 +37,8 @@ void encode_batch(T *enc, const vlb::DevModel<T> &m, const T *X, const i64 *h_of
       return;
     }
   }
-  vlb::exact_fisher_batch<T>(X, h_offsets, numImages, m, enc, nterms, flags, s);
+  vlb::exact_fisher_batch<T>(X, h_offsets, numImages, m, enc, nterms, flags, s,
+                             sizeof(T) == 4 && precision == VLB200_PREC_BF16_ROUTER);
 }
 
 template <typename T>

@@ -162,6 +162,26 @@ __global__ void __launch_bounds__(kThreads) k_normalize(T *__restrict__ q, i64 N
   }
 }
 
+// One-hot of each row's first arg-max (vl/fisher.c:398-417), one warp per row.
+__global__ void __launch_bounds__(kThreads) k_onehot(float *__restrict__ q, i64 N, int K) {
+  const i64 i = (i64)blockIdx.x * (kThreads / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (i >= N) return;
+  float *row = q + i * K;
+  float bv = -INFINITY;
+  int bi = 0x7fffffff;
+  for (int k = lane; k < K; k += 32)
+    if (row[k] > bv) { bv = row[k]; bi = k; }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+  }
+  if (bi == 0x7fffffff) bi = 0;
+  __syncwarp();
+  for (int k = lane; k < K; k += 32) row[k] = (float)(k == bi);
+}
+
 __global__ void k_sum_doubles(const double *__restrict__ part, i64 n, double *__restrict__ out) {
   __shared__ double sh[kThreads];
   double s = 0;
@@ -571,7 +591,8 @@ void apply_bounds(T *covs, i64 K, i64 D, const double *lb, cudaStream_t s) {
 // kSegRows rows so long images still spread over many blocks.
 template <typename T>
 void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const DevModel<T> &m,
-                        T *enc, unsigned long long *nterms, int flags, cudaStream_t s) {
+                        T *enc, unsigned long long *nterms, int flags, cudaStream_t s,
+                        bool use_router) {
   const i64 K = m.K, D = m.D;
   constexpr int TKC = 32, RC = 32, JMAX = sizeof(T) == 8 ? 5 : 10, DB = 8 * JMAX;
   constexpr i64 kSegRows = 2048;
@@ -611,7 +632,21 @@ void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const D
 
     T *q = sc.slot[3].get<T>(std::max<i64>(1, nrows) * K);
     double *llp = sc.slot[4].get<double>(estep_ll_parts(nrows));
-    if (nrows > 0) exact_estep(X + row0 * D, nrows, m, der, q, llp, (flags & 4) != 0, s);
+    if (nrows > 0) {
+      if constexpr (sizeof(T) == 4) {
+        if (use_router) {
+          router_default_posteriors(X + row0 * D, nrows, m, q, s);
+          if (flags & 4) {  // FAST: one-hot of each row's arg-max
+            VLB_LAUNCH("exact_onehot", s,
+                       k_onehot<<<grid1(nrows, 8), kThreads, 0, s>>>(q, nrows, (int)K));
+          }
+        } else {
+          exact_estep(X + row0 * D, nrows, m, der, q, llp, (flags & 4) != 0, s);
+        }
+      } else {
+        exact_estep(X + row0 * D, nrows, m, der, q, llp, (flags & 4) != 0, s);
+      }
+    }
 
     Segment *dsegs = sc.slot[5].get<Segment>(nseg);
     int *dbeg = sc.slot[6].get<int>(nimg + 1);
@@ -691,7 +726,7 @@ void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, 
                                  cudaStream_t);                                              \
   template void apply_bounds<T>(T *, i64, i64, const double *, cudaStream_t);                \
   template void exact_fisher_batch<T>(const T *, const i64 *, i64, const DevModel<T> &, T *, \
-                                      unsigned long long *, int, cudaStream_t);
+                                      unsigned long long *, int, cudaStream_t, bool);
 VLB_INST(float)
 VLB_INST(double)
 

@@ -1,0 +1,670 @@
+// Learned candidate router for the E-step.
+//
+// A small MLP  x -> [Linear, ReLU]* -> Linear -> K logits  predicts, for each
+// descriptor, which mixture components carry its posterior mass.  Inference
+// keeps the top-m components, evaluates the exact posterior on those only
+// (the reference's arithmetic, vl/gmm.c:762-790, restricted to the
+// candidates), and falls back to the full E-step for descriptors whose
+// predicted candidate mass (router softmax summed over the top-m) is below a
+// threshold (0.99 by default).  The router is trained here, on the GPU, by
+// the kernels of this file: forward, backward (data and weight gradients),
+// top-8 cross-entropy against posteriors produced by the full E-step, and
+// Adam.  Weights are held in fp32 and used in the forward and backward passes
+// rounded to bf16 (BF16 weights, fp32 accumulation).
+//
+// All reductions run in a fixed order, so training and inference are
+// bitwise reproducible for a given seed.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <vector>
+
+#include "engine.h"
+
+extern "C" {
+#include "vlb200.h"
+}
+
+using vlb::i64;
+
+namespace vlb {
+namespace {
+
+constexpr int kT = 256;
+inline unsigned gridn(i64 n, int b) { return (unsigned)((n + b - 1) / b); }
+
+__device__ __forceinline__ float bf16_round(float x) {
+  return __bfloat162float(__float2bfloat16_rn(x));
+}
+
+// C(m, n) = sum_k A(m, k) B(n, k) (+ bias[n]) (ReLU), with A(m,k) = A[m*sam + k*sak],
+// B(n,k) = B[n*sbn + k*sbk].  64 x 64 tiles, 16-deep k slices, 4 x 4 outputs
+// per thread, fp32 accumulation; every output is summed over k in order.
+template <bool RELU, bool BIAS>
+__global__ void __launch_bounds__(kT) k_gemm(const float *__restrict__ A, i64 sam, i64 sak,
+                                            const float *__restrict__ B, i64 sbn, i64 sbk,
+                                            const float *__restrict__ bias, float *__restrict__ C,
+                                            i64 ldc, int M, int N, int Kd) {
+  __shared__ float sa[16][64 + 4];
+  __shared__ float sb[16][64 + 4];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+  float acc[4][4] = {};
+  for (int k0 = 0; k0 < Kd; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += kT) {
+      const int kk = e / 64, mm = e % 64;
+      const int m = m0 + mm, k = k0 + kk;
+      sa[kk][mm] = (m < M && k < Kd) ? A[(i64)m * sam + (i64)k * sak] : 0.f;
+      const int n = n0 + mm;
+      sb[kk][mm] = (n < N && k < Kd) ? B[(i64)n * sbn + (i64)k * sbk] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a[i] = sa[kk][ty * 4 + i];
+        b[i] = sb[kk][tx * 4 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int m = m0 + ty * 4 + i;
+    if (m >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int n = n0 + tx * 4 + j;
+      if (n >= N) continue;
+      float v = acc[i][j] + (BIAS ? bias[n] : 0.f);
+      if (RELU) v = v > 0.f ? v : 0.f;
+      C[(i64)m * ldc + n] = v;
+    }
+  }
+}
+
+// Input features: z = (x - centre) * scale.
+__global__ void k_features(const float *__restrict__ X, i64 n, int D, const float *__restrict__ ctr,
+                           const float *__restrict__ scl, float *__restrict__ Z) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * D) return;
+  const int d = (int)(i % D);
+  Z[i] = (X[i] - ctr[d]) * scl[d];
+}
+
+__global__ void k_round_bf16(const float *__restrict__ w, float *__restrict__ wq, i64 n) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) wq[i] = bf16_round(w[i]);
+}
+
+// dH *= (H > 0): ReLU derivative applied to an upstream gradient.
+__global__ void k_relu_mask(float *__restrict__ g, const float *__restrict__ h, i64 n) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !(h[i] > 0.f)) g[i] = 0.f;
+}
+
+// Column sums db[n] = sum_m G[m, n] (fixed order over m).
+__global__ void k_colsum(const float *__restrict__ G, int M, int N, float *__restrict__ db) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  float s = 0.f;
+  for (int m = 0; m < M; ++m) s += G[(i64)m * N + n];
+  db[n] = s;
+}
+
+// Top-T targets of each row of the posteriors: indices and weights
+// renormalised over the T entries.  One warp per row, T rounds of arg-max.
+template <int T>
+__global__ void k_topk_targets(const float *__restrict__ q, i64 n, int K, int *__restrict__ idx,
+                               float *__restrict__ w) {
+  const i64 row = (i64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (row >= n) return;
+  const float *r = q + row * K;
+  int taken[T];
+  float tv[T];
+  float tot = 0.f;
+  for (int t = 0; t < T; ++t) {
+    float bv = -1.f;
+    int bi = 0x7fffffff;
+    for (int k = lane; k < K; k += 32) {
+      bool used = false;
+      for (int u = 0; u < t; ++u) used |= (taken[u] == k);
+      const float v = r[k];
+      if (!used && (v > bv || (v == bv && k < bi))) { bv = v; bi = k; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    taken[t] = bi;
+    tv[t] = bv > 0.f ? bv : 0.f;
+    tot += tv[t];
+  }
+  if (lane < T) {
+    idx[row * T + lane] = taken[lane];
+    w[row * T + lane] = tot > 0.f ? tv[lane] / tot : 1.f / T;
+  }
+}
+
+// Softmax cross-entropy against sparse top-T target distributions:
+// loss_row = -sum_t w_t log softmax(z)_{idx_t};  dZ = (softmax(z) - target) / B.
+template <int T>
+__global__ void k_xent(const float *__restrict__ Zl, int B, int K, const int *__restrict__ idx,
+                       const float *__restrict__ w, float *__restrict__ dZ,
+                       double *__restrict__ rowloss) {
+  const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (row >= B) return;
+  const float *z = Zl + (i64)row * K;
+  float mx = -INFINITY;
+  for (int k = lane; k < K; k += 32) mx = fmaxf(mx, z[k]);
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  float s = 0.f;
+  for (int k = lane; k < K; k += 32) s += expf(z[k] - mx);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  const float lse = mx + logf(s);
+  const float invB = 1.f / (float)B;
+  for (int k = lane; k < K; k += 32) {
+    float t = 0.f;
+#pragma unroll
+    for (int u = 0; u < T; ++u)
+      if (idx[(i64)row * T + u] == k) t += w[(i64)row * T + u];
+    dZ[(i64)row * K + k] = (expf(z[k] - lse) - t) * invB;
+  }
+  if (lane == 0) {
+    double l = 0;
+    for (int u = 0; u < T; ++u) l -= (double)w[(i64)row * T + u] * ((double)z[idx[(i64)row * T + u]] - lse);
+    rowloss[row] = l;
+  }
+}
+
+__global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, i64 n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Candidates: top-m logits of each row and the router's softmax mass on them.
+template <int MM>
+__global__ void k_select(const float *__restrict__ Zl, i64 n, int K, int m, int *__restrict__ cand,
+                         float *__restrict__ cmass) {
+  const i64 row = (i64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (row >= n) return;
+  const float *z = Zl + row * K;
+  float mx = -INFINITY;
+  for (int k = lane; k < K; k += 32) mx = fmaxf(mx, z[k]);
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  float s = 0.f;
+  for (int k = lane; k < K; k += 32) s += expf(z[k] - mx);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  int taken[MM];
+  float sel = 0.f;
+  for (int t = 0; t < m; ++t) {
+    float bv = -INFINITY;
+    int bi = 0x7fffffff;
+    for (int k = lane; k < K; k += 32) {
+      bool used = false;
+      for (int u = 0; u < t; ++u) used |= (taken[u] == k);
+      const float v = z[k];
+      if (!used && (v > bv || (v == bv && k < bi))) { bv = v; bi = k; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    taken[t] = bi;
+    sel += expf(bv - mx);
+  }
+  if (lane < m) cand[row * m + lane] = taken[lane];
+  if (lane == 0) cmass[row] = sel / s;
+}
+
+// Exact posteriors on the candidates (vl/gmm.c:762-790 restricted to them),
+// or on all K components for fallback rows.  One warp per row; the dimension
+// is spread over the lanes.  Writes a dense row of q (zeros off the
+// candidates), the row's log-likelihood share and whether it fell back.
+__global__ void k_candidate_estep(const float *__restrict__ X, i64 n, int D, int K,
+                                  const float *__restrict__ means, const float *__restrict__ inv,
+                                  const double *__restrict__ cst, const int *__restrict__ cand,
+                                  const float *__restrict__ cmass, int m, float thr,
+                                  float *__restrict__ q, unsigned char *__restrict__ fell) {
+  const i64 row = (i64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (row >= n) return;
+  const float *x = X + row * D;
+  float *qr = q + row * K;
+  const bool fb = cmass[row] < thr;
+  const int nc = fb ? K : m;
+  for (int k = lane; k < K; k += 32) qr[k] = 0.f;
+  __syncwarp();
+  // Pass 1: log-densities (stored temporarily in q) and their maximum.
+  float mx = -INFINITY;
+  for (int c = 0; c < nc; ++c) {
+    const int k = fb ? c : cand[row * m + c];
+    const float *mu = means + (i64)k * D, *iv = inv + (i64)k * D;
+    float acc = 0.f;
+    for (int d = lane; d < D; d += 32) {
+      const float df = x[d] - mu[d];
+      acc += df * df * iv[d];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    const float p = (float)(cst[k] - 0.5 * (double)acc);
+    if (lane == 0) qr[k] = p;
+    mx = fmaxf(mx, p);
+  }
+  __syncwarp();
+  float s = 0.f;
+  for (int c = lane; c < nc; c += 32) {
+    const int k = fb ? c : cand[row * m + c];
+    s += expf(qr[k] - mx);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __syncwarp();
+  for (int c = lane; c < nc; c += 32) {
+    const int k = fb ? c : cand[row * m + c];
+    qr[k] = expf(qr[k] - mx) / s;
+  }
+  if (lane == 0) fell[row] = fb ? 1 : 0;
+}
+
+// Missed posterior mass of each row: sum of the full-E-step posteriors that
+// the candidate rows set to zero.
+__global__ void k_missed(const float *__restrict__ qfull, const float *__restrict__ qc, i64 n, int K,
+                         double *__restrict__ out) {
+  const i64 row = (i64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (row >= n) return;
+  float s = 0.f;
+  for (int k = lane; k < K; k += 32)
+    if (qc[row * K + k] == 0.f) s += qfull[row * K + k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[row] = s;
+}
+
+}  // namespace
+}  // namespace vlb
+
+// ====================================================================== host
+struct _VlB200Router {
+  int D = 0, K = 0;
+  std::vector<int> sizes;  // D, hidden..., K
+  // Parameters (device): per layer W (out x in), b (out); Adam moments.
+  std::vector<vlb::DevBuf *> W, b, Wq, mW, vW, mb, vb, gW, gb;
+  vlb::DevBuf ctr, scl;
+  long step = 0;
+  ~_VlB200Router() {
+    for (auto *v : {&W, &b, &Wq, &mW, &vW, &mb, &vb, &gW, &gb})
+      for (auto *p : *v) delete p;
+  }
+};
+
+namespace {
+
+using vlb::DevBuf;
+
+template <typename F>
+int guarded(F &&f) {
+  try {
+    f();
+    return 0;
+  } catch (const vlb::Error &e) {
+    return vl_set_last_error(e.code, "%s", e.what());
+  } catch (const std::exception &e) {
+    return vl_set_last_error(VL_ERR_BAD_ARG, "%s", e.what());
+  }
+}
+
+int nlayers(const VlB200Router *r) { return (int)r->sizes.size() - 1; }
+
+void gemm(bool relu, bool bias, const float *A, i64 sam, i64 sak, const float *B, i64 sbn, i64 sbk,
+          const float *bvec, float *C, i64 ldc, int M, int N, int Kd, cudaStream_t s) {
+  dim3 g(vlb::gridn(N, 64), vlb::gridn(M, 64));
+  if (relu && bias)
+    VLB_LAUNCH("router_gemm", s, (vlb::k_gemm<true, true><<<g, vlb::kT, 0, s>>>(A, sam, sak, B, sbn, sbk, bvec, C, ldc, M, N, Kd)));
+  else if (bias)
+    VLB_LAUNCH("router_gemm", s, (vlb::k_gemm<false, true><<<g, vlb::kT, 0, s>>>(A, sam, sak, B, sbn, sbk, bvec, C, ldc, M, N, Kd)));
+  else
+    VLB_LAUNCH("router_gemm", s, (vlb::k_gemm<false, false><<<g, vlb::kT, 0, s>>>(A, sam, sak, B, sbn, sbk, bvec, C, ldc, M, N, Kd)));
+}
+
+void refresh_bf16(VlB200Router *r, cudaStream_t s) {
+  for (int l = 0; l < nlayers(r); ++l) {
+    const i64 n = (i64)r->sizes[l + 1] * r->sizes[l];
+    VLB_LAUNCH("router_round", s,
+               vlb::k_round_bf16<<<vlb::gridn(n, 256), 256, 0, s>>>((float *)r->W[l]->p, (float *)r->Wq[l]->p, n));
+  }
+}
+
+// Activations of a batch: act[0] = features, act[l+1] = layer l output.
+void forward(VlB200Router *r, const float *X, i64 B, std::vector<float *> &act, cudaStream_t s) {
+  const int L = nlayers(r);
+  VLB_LAUNCH("router_features", s,
+             vlb::k_features<<<vlb::gridn(B * r->D, 256), 256, 0, s>>>(X, B, r->D, (float *)r->ctr.p,
+                                                                     (float *)r->scl.p, act[0]));
+  for (int l = 0; l < L; ++l) {
+    const int in = r->sizes[l], out = r->sizes[l + 1];
+    gemm(l + 1 < L, true, act[l], in, 1, (float *)r->Wq[l]->p, in, 1, (float *)r->b[l]->p, act[l + 1],
+         out, (int)B, out, in, s);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+VlB200Router *vlb200_router_new(vl_size dimension, vl_size numClusters, vl_size const *hidden,
+                                vl_size numHidden, vl_uint32 seed) {
+  VlB200Router *r = nullptr;
+  int rc = guarded([&] {
+    VLB_CHECK(dimension >= 1 && numClusters >= 2, VL_ERR_BAD_ARG, "router: bad sizes");
+    r = new VlB200Router();
+    r->D = (int)dimension;
+    r->K = (int)numClusters;
+    r->sizes.push_back((int)dimension);
+    for (vl_size i = 0; i < numHidden; ++i) r->sizes.push_back((int)hidden[i]);
+    r->sizes.push_back((int)numClusters);
+    std::mt19937_64 gen(seed);
+    cudaStream_t s = vlb::thread_stream();
+    for (int l = 0; l < nlayers(r); ++l) {
+      const int in = r->sizes[l], out = r->sizes[l + 1];
+      std::vector<float> w((size_t)in * out), bb(out, 0.f);
+      std::normal_distribution<float> nd(0.f, std::sqrt(2.f / (float)in));  // He initialisation
+      for (auto &v : w) v = nd(gen);
+      for (auto *vec : {&r->W, &r->Wq, &r->mW, &r->vW, &r->gW}) vec->push_back(new DevBuf());
+      for (auto *vec : {&r->b, &r->mb, &r->vb, &r->gb}) vec->push_back(new DevBuf());
+      float *dW = r->W[l]->get<float>(w.size());
+      r->Wq[l]->get<float>(w.size());
+      r->gW[l]->get<float>(w.size());
+      VLB_CUDA(cudaMemsetAsync(r->mW[l]->get<float>(w.size()), 0, w.size() * 4, s));
+      VLB_CUDA(cudaMemsetAsync(r->vW[l]->get<float>(w.size()), 0, w.size() * 4, s));
+      VLB_CUDA(cudaMemsetAsync(r->mb[l]->get<float>(out), 0, out * 4, s));
+      VLB_CUDA(cudaMemsetAsync(r->vb[l]->get<float>(out), 0, out * 4, s));
+      r->gb[l]->get<float>(out);
+      VLB_CUDA(cudaMemcpyAsync(dW, w.data(), w.size() * 4, cudaMemcpyHostToDevice, s));
+      VLB_CUDA(cudaMemcpyAsync(r->b[l]->get<float>(out), bb.data(), out * 4, cudaMemcpyHostToDevice, s));
+    }
+    std::vector<float> one((size_t)dimension, 1.f), zero((size_t)dimension, 0.f);
+    VLB_CUDA(cudaMemcpyAsync(r->ctr.get<float>(dimension), zero.data(), dimension * 4, cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(r->scl.get<float>(dimension), one.data(), dimension * 4, cudaMemcpyHostToDevice, s));
+    refresh_bf16(r, s);
+    VLB_CUDA(cudaStreamSynchronize(s));
+  });
+  if (rc) {
+    delete r;
+    return nullptr;
+  }
+  return r;
+}
+
+void vlb200_router_delete(VlB200Router *r) { delete r; }
+
+vl_size vlb200_router_num_params(VlB200Router const *r) {
+  vl_size n = 0;
+  for (size_t l = 0; l + 1 < r->sizes.size(); ++l) n += (vl_size)r->sizes[l + 1] * (r->sizes[l] + 1);
+  return n;
+}
+
+// Parameters as one host vector: for each layer W (out x in, row-major) then b.
+int vlb200_router_get_params(VlB200Router const *r, float *out) {
+  return guarded([&] {
+    cudaStream_t s = vlb::thread_stream();
+    size_t o = 0;
+    for (int l = 0; l < nlayers(r); ++l) {
+      const size_t nw = (size_t)r->sizes[l + 1] * r->sizes[l], nb = r->sizes[l + 1];
+      VLB_CUDA(cudaMemcpyAsync(out + o, r->W[l]->p, nw * 4, cudaMemcpyDeviceToHost, s));
+      o += nw;
+      VLB_CUDA(cudaMemcpyAsync(out + o, r->b[l]->p, nb * 4, cudaMemcpyDeviceToHost, s));
+      o += nb;
+    }
+    VLB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int vlb200_router_set_params(VlB200Router *r, float const *in) {
+  return guarded([&] {
+    cudaStream_t s = vlb::thread_stream();
+    size_t o = 0;
+    for (int l = 0; l < nlayers(r); ++l) {
+      const size_t nw = (size_t)r->sizes[l + 1] * r->sizes[l], nb = r->sizes[l + 1];
+      VLB_CUDA(cudaMemcpyAsync(r->W[l]->p, in + o, nw * 4, cudaMemcpyHostToDevice, s));
+      o += nw;
+      VLB_CUDA(cudaMemcpyAsync(r->b[l]->p, in + o, nb * 4, cudaMemcpyHostToDevice, s));
+      o += nb;
+    }
+    refresh_bf16(r, s);
+    VLB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+// Feature normalisation z = (x - centre) * scale (host arrays of D).
+int vlb200_router_set_input_transform(VlB200Router *r, float const *centre, float const *scale) {
+  return guarded([&] {
+    cudaStream_t s = vlb::thread_stream();
+    VLB_CUDA(cudaMemcpyAsync(r->ctr.p, centre, r->D * 4, cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(r->scl.p, scale, r->D * 4, cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+// Loss and gradients of one batch against top-8 targets (device arrays
+// tidx, tw: B x 8).  grads: host vector in the get_params layout, or NULL.
+// Used by training and by the gradient check against the CPU oracle.
+int vlb200_router_loss_grad(VlB200Router *r, float const *X, vl_size B, int const *tidx,
+                            float const *tw, double *loss, float *grads) {
+  return guarded([&] {
+    cudaStream_t s = vlb::thread_stream();
+    vlb::Scratch &sc = vlb::thread_scratch(vlb::kArenaRouter);
+    const int L = nlayers(r);
+    std::vector<float *> act(L + 1), gact(L + 1);
+    for (int l = 0; l <= L; ++l) act[l] = sc.slot[l].get<float>((size_t)B * r->sizes[l]);
+    for (int l = 1; l <= L; ++l) gact[l] = sc.slot[10 + l].get<float>((size_t)B * r->sizes[l]);
+    double *rl = sc.slot[20].get<double>(B);
+    double *tot = sc.slot[21].get<double>(1);
+    forward(r, X, (i64)B, act, s);
+    VLB_LAUNCH("router_xent", s,
+               vlb::k_xent<8><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], (int)B, r->K, tidx, tw, gact[L], rl));
+    for (int l = L - 1; l >= 0; --l) {
+      const int in = r->sizes[l], out = r->sizes[l + 1];
+      // dW = dY^T X  (out x in), summed over the batch in order.
+      gemm(false, false, gact[l + 1], 1, out, act[l], 1, in, nullptr, (float *)r->gW[l]->p, in, out, in,
+           (int)B, s);
+      VLB_LAUNCH("router_colsum", s,
+                 vlb::k_colsum<<<vlb::gridn(out, 256), 256, 0, s>>>(gact[l + 1], (int)B, out, (float *)r->gb[l]->p));
+      if (l > 0) {
+        // dX = dY W (B x in), then the ReLU mask of layer l's output.
+        gemm(false, false, gact[l + 1], out, 1, (float *)r->Wq[l]->p, 1, in, nullptr, gact[l], in, (int)B,
+             in, out, s);
+        VLB_LAUNCH("router_relu_mask", s,
+                   vlb::k_relu_mask<<<vlb::gridn((i64)B * in, 256), 256, 0, s>>>(gact[l], act[l], (i64)B * in));
+      }
+    }
+    vlb::sum_doubles(rl, (i64)B, tot, s);
+    double h = 0;
+    VLB_CUDA(cudaMemcpyAsync(&h, tot, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (grads) {
+      size_t o = 0;
+      for (int l = 0; l < L; ++l) {
+        const size_t nw = (size_t)r->sizes[l + 1] * r->sizes[l], nb = r->sizes[l + 1];
+        VLB_CUDA(cudaMemcpyAsync(grads + o, r->gW[l]->p, nw * 4, cudaMemcpyDeviceToHost, s));
+        o += nw;
+        VLB_CUDA(cudaMemcpyAsync(grads + o, r->gb[l]->p, nb * 4, cudaMemcpyDeviceToHost, s));
+        o += nb;
+      }
+    }
+    VLB_CUDA(cudaStreamSynchronize(s));
+    if (loss) *loss = h / (double)B;
+  });
+}
+
+// Top-8 targets (indices, renormalised weights) of N posterior rows (device).
+int vlb200_router_targets(float const *posteriors, vl_size N, vl_size K, int *tidx, float *tw) {
+  return guarded([&] {
+    cudaStream_t s = vlb::thread_stream();
+    VLB_LAUNCH("router_targets", s,
+               vlb::k_topk_targets<8><<<vlb::gridn(N, 8), 256, 0, s>>>(posteriors, (i64)N, (int)K, tidx, tw));
+    VLB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+// Trains the router with Adam on descriptors X (device, N x D) and top-8
+// targets (device, N x 8) for `epochs` passes in batches of `batch` rows (in
+// order; the caller shuffles).  *loss: mean loss of the last epoch.
+int vlb200_router_train(VlB200Router *r, float const *X, vl_size N, int const *tidx, float const *tw,
+                        vl_size epochs, vl_size batch, float lr, double *loss) {
+  return guarded([&] {
+    cudaStream_t s = vlb::thread_stream();
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    double last = 0;
+    for (vl_size ep = 0; ep < epochs; ++ep) {
+      double acc = 0;
+      vl_size nb = 0;
+      for (vl_size i0 = 0; i0 + batch <= N; i0 += batch, ++nb) {
+        double l = 0;
+        if (vlb200_router_loss_grad(r, X + i0 * r->D, batch, tidx + i0 * 8, tw + i0 * 8, &l, nullptr))
+          throw vlb::Error(vl_get_last_error(), vl_get_last_error_message());
+        acc += l;
+        r->step++;
+        const float c1 = 1.f - std::pow(b1, (float)r->step), c2 = 1.f - std::pow(b2, (float)r->step);
+        for (int l2 = 0; l2 < nlayers(r); ++l2) {
+          const i64 nw = (i64)r->sizes[l2 + 1] * r->sizes[l2], nbb = r->sizes[l2 + 1];
+          VLB_LAUNCH("router_adam", s,
+                     vlb::k_adam<<<vlb::gridn(nw, 256), 256, 0, s>>>((float *)r->W[l2]->p, (float *)r->gW[l2]->p,
+                                                                    (float *)r->mW[l2]->p, (float *)r->vW[l2]->p,
+                                                                    nw, lr, b1, b2, eps, c1, c2));
+          VLB_LAUNCH("router_adam", s,
+                     vlb::k_adam<<<vlb::gridn(nbb, 256), 256, 0, s>>>((float *)r->b[l2]->p, (float *)r->gb[l2]->p,
+                                                                     (float *)r->mb[l2]->p, (float *)r->vb[l2]->p,
+                                                                     nbb, lr, b1, b2, eps, c1, c2));
+        }
+        refresh_bf16(r, s);
+      }
+      last = nb ? acc / (double)nb : 0.0;
+    }
+    VLB_CUDA(cudaStreamSynchronize(s));
+    if (loss) *loss = last;
+  });
+}
+
+// Router E-step: posteriors (device, N x K, dense with zeros off the
+// candidates) from the exact evaluation of the top-m candidates, with the
+// full E-step for rows whose predicted candidate mass is below `threshold`.
+// fallbackRows (host, may be NULL) receives the number of fallback rows.
+int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *priors,
+                             float const *means, float const *covariances, float const *X,
+                             vl_size N, vl_size m, float threshold, vl_uint64 *fallbackRows,
+                             void *stream) {
+  return guarded([&] {
+    VLB_CHECK(m >= 1 && m <= 32 && (int)m <= r->K, VL_ERR_BAD_ARG, "router: m must be in [1, 32]");
+    cudaStream_t s = vlb::pick_stream(stream);
+    vlb::Scratch &sc = vlb::thread_scratch(vlb::kArenaRouter);
+    const int L = nlayers(r), K = r->K, D = r->D;
+    vlb::DevModel<float> md;
+    md.means = means; md.covs = covariances; md.priors = priors; md.K = K; md.D = D;
+    vlb::DevDerived<float> der;
+    der.inv = sc.slot[22].get<float>((size_t)K * D);
+    der.sis = sc.slot[23].get<float>((size_t)K * D);
+    der.cst = sc.slot[24].get<double>(K);
+    vlb::exact_prepare(md, der, s);
+    const i64 chunk = 1 << 17;
+    unsigned long long nfb = 0;
+    for (i64 i0 = 0; i0 < (i64)N; i0 += chunk) {
+      const i64 B = std::min<i64>(chunk, (i64)N - i0);
+      std::vector<float *> act(L + 1);
+      for (int l = 0; l <= L; ++l) act[l] = sc.slot[l].get<float>((size_t)chunk * r->sizes[l]);
+      int *cand = sc.slot[25].get<int>((size_t)chunk * m);
+      float *cm = sc.slot[26].get<float>(chunk);
+      unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
+      forward(r, X + i0 * D, B, act, s);
+      VLB_LAUNCH("router_select", s,
+                 vlb::k_select<32><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+      VLB_LAUNCH("router_candidate_estep", s,
+                 vlb::k_candidate_estep<<<vlb::gridn(B, 8), 256, 0, s>>>(
+                     X + i0 * D, B, D, K, means, der.inv, der.cst, cand, cm, (int)m, threshold,
+                     posteriors + i0 * K, fell));
+      if (fallbackRows) {
+        std::vector<unsigned char> h(B);
+        VLB_CUDA(cudaMemcpyAsync(h.data(), fell, B, cudaMemcpyDeviceToHost, s));
+        VLB_CUDA(cudaStreamSynchronize(s));
+        for (auto v : h) nfb += v;
+      }
+    }
+    if (fallbackRows) *fallbackRows = nfb;
+  });
+}
+
+// Mean missed posterior mass of candidate posteriors qc against the full
+// E-step posteriors qfull (both device, N x K).
+int vlb200_router_missed_mass(float const *qfull, float const *qc, vl_size N, vl_size K, double *mean) {
+  return guarded([&] {
+    cudaStream_t s = vlb::thread_stream();
+    vlb::Scratch &sc = vlb::thread_scratch(vlb::kArenaRouter);
+    double *rows = sc.slot[28].get<double>(N), *tot = sc.slot[29].get<double>(1);
+    VLB_LAUNCH("router_missed", s,
+               vlb::k_missed<<<vlb::gridn(N, 8), 256, 0, s>>>(qfull, qc, (i64)N, (int)K, rows));
+    vlb::sum_doubles(rows, (i64)N, tot, s);
+    double h = 0;
+    VLB_CUDA(cudaMemcpyAsync(&h, tot, sizeof(double), cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+    *mean = N ? h / (double)N : 0.0;
+  });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------ default router
+namespace {
+std::mutex g_default_mu;
+VlB200Router *g_default = nullptr;
+vl_size g_default_m = 8;
+float g_default_thr = 0.99f;
+}  // namespace
+
+extern "C" int vlb200_router_set_default(VlB200Router *router, vl_size m, float threshold) {
+  if (router && (m < 1 || m > 32))
+    return vl_set_last_error(VL_ERR_BAD_ARG, "vlb200_router_set_default: m must be in [1, 32]");
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  g_default = router;
+  g_default_m = m;
+  g_default_thr = threshold;
+  return 0;
+}
+
+namespace vlb {
+void router_default_posteriors(const float *X, i64 N, const DevModel<float> &m, float *q,
+                               cudaStream_t s) {
+  VlB200Router *r;
+  vl_size mm;
+  float thr;
+  {
+    std::lock_guard<std::mutex> lk(g_default_mu);
+    r = g_default;
+    mm = g_default_m;
+    thr = g_default_thr;
+  }
+  VLB_CHECK(r != nullptr, VL_ERR_BAD_ARG,
+            "VLB200_PREC_BF16_ROUTER: no router set (vlb200_router_set_default)");
+  VLB_CHECK(r->K == m.K && r->D == m.D, VL_ERR_BAD_ARG, "router does not match the model's K and D");
+  if (vlb200_router_posteriors(r, q, m.priors, m.means, m.covs, X, (vl_size)N, mm, thr, nullptr, s))
+    throw Error(vl_get_last_error(), vl_get_last_error_message());
+}
+}  // namespace vlb

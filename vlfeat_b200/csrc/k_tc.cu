@@ -851,6 +851,58 @@ __global__ void __launch_bounds__(256) k_tc_fv_finalize(
   }
 }
 
+// Row-major fp32 posteriors -> fp16 q^T operand image (the layout the
+// E-step writes), with VLFeat's q < 1e-6 skip, the optional FAST one-hot of
+// the row's arg-max (vl/fisher.c:398-417) and per-row term counts.  One warp
+// per row; rows past n (tile padding) are written as zeros.
+__global__ void k_rows_to_image16(const float *__restrict__ q, i64 n, int K, int Kq, float thr,
+                                  __half *__restrict__ img, unsigned *__restrict__ rowcnt,
+                                  i64 rowsPad, bool fast) {
+  const i64 row = (i64)blockIdx.x * 8 + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (row >= rowsPad) return;
+  const bool valid = row < n;
+  int am = 0;
+  if (fast && valid) {
+    float bv = -1.f;
+    int bi = 0x7fffffff;
+    for (int k = lane; k < K; k += 32) {
+      const float v = q[row * K + k];
+      if (v > bv || (v == bv && k < bi)) { bv = v; bi = k; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    am = bi;
+  }
+  uint8_t *tb = (uint8_t *)img + (size_t)(row >> 7) * 128 * Kq * 2;
+  const int r = (int)(row & 127);
+  unsigned cnt = 0;
+  for (int g = lane; g < Kq / 8; g += 32) {
+    float v[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int k = g * 8 + t;
+      float x = (valid && k < K) ? q[row * K + k] : 0.f;
+      if (fast) x = (valid && k == am) ? 1.f : 0.f;
+      cnt += (x >= 1e-6f) ? 1u : 0u;
+      v[t] = x < thr ? 0.f : x;
+    }
+    uint4 w;
+    w.x = pack2<true>(v[0], v[1]);
+    w.y = pack2<true>(v[2], v[3]);
+    w.z = pack2<true>(v[4], v[5]);
+    w.w = pack2<true>(v[6], v[7]);
+    const int kk = g * 8;
+    const uint32_t off = (uint32_t)((r >> 3) * (Kq / 64) * 1024 + (kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
+    *(uint4 *)(tb + off) = w;
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0 && valid && rowcnt) rowcnt[row] = cnt;
+}
+
 // ================================================================ host
 struct TcPrep {
   int K = 0, Kp = 0, D = 0;
@@ -1082,7 +1134,17 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const 
     VLB_CUDA(cudaMemcpyAsync(drow0, imgRow0.data(), sizeof(i64) * (nimg + 1), cudaMemcpyHostToDevice, s));
 
     if (nrows > 0) {
-      estep_dispatch(tp.D, qf, X + row0 * D, nrows, tp, q, (int)K, (flags & 4) != 0, rowcnt, nullptr, err, s);
+      if (precision == VLB200_PREC_BF16_ROUTER) {
+        // Router posteriors (row-major) -> fp16 operand image + row counts.
+        float *qrows = sc.slot[18].get<float>((size_t)nrows * K);
+        router_default_posteriors(X + row0 * D, nrows, m, qrows, s);
+        const i64 rowsPad = ntiles * 128;
+        VLB_LAUNCH("tc_rows_to_image", s,
+                   k_rows_to_image16<<<(unsigned)((rowsPad + 7) / 8), 256, 0, s>>>(
+                       qrows, nrows, (int)K, Kq, 1e-6f, (__half *)q, rowcnt, rowsPad, (flags & 4) != 0));
+      } else {
+        estep_dispatch(tp.D, qf, X + row0 * D, nrows, tp, q, (int)K, (flags & 4) != 0, rowcnt, nullptr, err, s);
+      }
       SParams sp;
       sp.X = X; sp.qimg = (const uint8_t *)q; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = row0;
       sp.K = (int)K; sp.Kp = tp.Kp; sp.Kq = Kq; sp.nst = 0;
