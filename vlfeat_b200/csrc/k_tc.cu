@@ -181,7 +181,7 @@ struct ELayout {
   static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * kStage; }
 };
 
-template <int DIM, int QF>
+template <int DIM, int QF, bool FAST>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   using L = ELayout<DIM>;
   constexpr int NKA = L::NKA;
@@ -300,9 +300,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     // Two warpgroups: group g drains the tiles whose accumulator is TMEM
     // buffer g (alternate tiles), so one tile's log-sum-exp overlaps the next.
     // Warp w reads TMEM lanes 32 (w % 4) .. +31, i.e. rows of the tile.
+    // Arithmetic on pairs of columns uses packed f32x2 instructions.
     const int eg = (warp - 4) >> 2, ew = warp & 3;
     const int r = ew * 32 + lane;
     const int nch = p.Kp / 32;
+    const unsigned long long* cst2v = (const unsigned long long*)s_cst;
     int tt = 0;
     for (i64 tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++tt) {
       const int buf = tt & 1;
@@ -324,40 +326,61 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         float cm = -INFINITY;
         int cam = 0;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const float x = __uint_as_float(va[j]) + s_cst[pc * 32 + j];
-          va[j] = __float_as_uint(x);
-          if (x > cm) { cm = x; cam = pc * 32 + j; }
+        for (int j = 0; j < 16; ++j) {
+          const unsigned long long s = add2(f2u(__uint_as_float(va[2 * j]), __uint_as_float(va[2 * j + 1])),
+                                            cst2v[pc * 16 + j]);
+          va[2 * j] = __float_as_uint(lo32(s));
+          va[2 * j + 1] = __float_as_uint(hi32(s));
+          if (FAST) {
+            if (lo32(s) > cm) { cm = lo32(s); cam = pc * 32 + 2 * j; }
+            if (hi32(s) > cm) { cm = hi32(s); cam = pc * 32 + 2 * j + 1; }
+          } else {
+            cm = fmaxf(cm, fmaxf(lo32(s), hi32(s)));
+          }
         }
         if (two) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const float x = __uint_as_float(vb[j]) + s_cst[pc * 32 + 32 + j];
-            vb[j] = __float_as_uint(x);
-            if (x > cm) { cm = x; cam = pc * 32 + 32 + j; }
+          for (int j = 0; j < 16; ++j) {
+            const unsigned long long s = add2(f2u(__uint_as_float(vb[2 * j]), __uint_as_float(vb[2 * j + 1])),
+                                              cst2v[pc * 16 + 16 + j]);
+            vb[2 * j] = __float_as_uint(lo32(s));
+            vb[2 * j + 1] = __float_as_uint(hi32(s));
+            if (FAST) {
+              if (lo32(s) > cm) { cm = lo32(s); cam = pc * 32 + 32 + 2 * j; }
+              if (hi32(s) > cm) { cm = hi32(s); cam = pc * 32 + 32 + 2 * j + 1; }
+            } else {
+              cm = fmaxf(cm, fmaxf(lo32(s), hi32(s)));
+            }
           }
         }
         if (cm > m) {
           sum = (m == -INFINITY) ? 0.f : sum * ex2_approx(m - cm);
           m = cm;
-          am = cam;
+          if (FAST) am = cam;
         }
+        const unsigned long long nm = f2u(-m, -m);
+        unsigned long long acc = 0ull;  // two partial sums (+0.0f, +0.0f)
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const float e = ex2_approx(__uint_as_float(va[j]) - m);
-          sum += e;
-          va[j] = __float_as_uint(e);
+        for (int j = 0; j < 16; ++j) {
+          const unsigned long long d = add2(f2u(__uint_as_float(va[2 * j]), __uint_as_float(va[2 * j + 1])), nm);
+          const float e0 = ex2_approx(lo32(d)), e1 = ex2_approx(hi32(d));
+          acc = add2(acc, f2u(e0, e1));
+          va[2 * j] = __float_as_uint(e0);
+          va[2 * j + 1] = __float_as_uint(e1);
         }
         tmem_st32(tb + pc * 32, va);
         if (two) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const float e = ex2_approx(__uint_as_float(vb[j]) - m);
-            sum += e;
-            vb[j] = __float_as_uint(e);
+          for (int j = 0; j < 16; ++j) {
+            const unsigned long long d = add2(f2u(__uint_as_float(vb[2 * j]), __uint_as_float(vb[2 * j + 1])), nm);
+            const float e0 = ex2_approx(lo32(d)), e1 = ex2_approx(hi32(d));
+            acc = add2(acc, f2u(e0, e1));
+            vb[2 * j] = __float_as_uint(e0);
+            vb[2 * j + 1] = __float_as_uint(e1);
           }
           tmem_st32(tb + pc * 32 + 32, vb);
         }
+        sum += lo32(acc) + hi32(acc);
         mg[pc >> 1] = m;
       }
       tmem_wait_st();
@@ -370,21 +393,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       const uint32_t rowoff = (uint32_t)((r >> 3) * (p.Kq / 64) * 1024);
       const int ncw = (QF == kQRow) ? nch : p.Kq / 32;
       // Pass B: q = e * 2^(m_g - m) / sum, thresholded and stored, one
-      // 32-column chunk at a time.
+      // 32-column chunk at a time.  Rows past N (tile padding) store zeros.
       auto emit = [&](const uint32_t(&v)[32], int cc, bool have, float sc) {
         float qv[32];
+        const unsigned long long sc2 = f2u(sc, sc);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          float x = have ? __uint_as_float(v[j]) * sc : 0.f;
-          if (p.fast) x = (have && cc * 32 + j == am) ? 1.f : 0.f;
-          x = valid ? x : 0.f;
-          cnt += (x >= 1e-6f) ? 1u : 0u;
-          if (QF != kQRow && x < p.qthr) x = 0.f;
-          qv[j] = x;
+        for (int j = 0; j < 16; ++j) {
+          float x0, x1;
+          if (FAST) {
+            x0 = (have && cc * 32 + 2 * j == am) ? 1.f : 0.f;
+            x1 = (have && cc * 32 + 2 * j + 1 == am) ? 1.f : 0.f;
+          } else {
+            const unsigned long long q2 = mul2(f2u(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1])), sc2);
+            x0 = lo32(q2);
+            x1 = hi32(q2);
+          }
+          const bool k0 = x0 >= 1e-6f, k1 = x1 >= 1e-6f;
+          cnt += (unsigned)k0 + (unsigned)k1;
+          if (QF != kQRow) {
+            x0 = x0 < p.qthr ? 0.f : x0;
+            x1 = x1 < p.qthr ? 0.f : x1;
+          }
+          qv[2 * j] = x0;
+          qv[2 * j + 1] = x1;
         }
         const int k0 = cc * 32;
         if (QF == kQRow) {
-          if (!valid || !have) return;
+          if (!have) return;
           float *dst = (float *)p.q + row * p.ldq + k0;
           if (k0 + 32 <= p.K) {
 #pragma unroll
@@ -417,6 +452,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
           }
         }
       };
+      // TMEM loads stay warp-uniform; only the stores depend on the row.
 #pragma unroll 1
       for (int cc = 0; cc < ncw; ++cc) {
         uint32_t va[32];
@@ -424,9 +460,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         if (ha) {
           tmem_ld32(tb + cc * 32, va);
           tmem_wait_ld();
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) va[j] = 0u;
         }
-        const float sc = ha ? ex2_approx(mg[cc >> 1] - m) * inv : 0.f;
-        emit(va, cc, ha, sc);
+        if (valid) {
+          const float sc = ha ? ex2_approx(mg[cc >> 1] - m) * inv : 0.f;
+          emit(va, cc, ha, sc);
+        } else if (QF != kQRow) {
+          // Padding row of the last tile: its q image entries are zero.
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int kk = cc * 32 + 8 * j;
+            const uint32_t off = rowoff + (uint32_t)((kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
+            *(uint4 *)(ib + off) = make_uint4(0, 0, 0, 0);
+            if (QF == kQImg32) *(uint4 *)(ib + p.qpart + off) = make_uint4(0, 0, 0, 0);
+          }
+        }
       }
       tc_fence_before();
       mbar_arrive(&acce[buf]);
@@ -947,7 +997,7 @@ i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool
   const int nst = std::min(8, L::max_stages(tp.Kp));
   VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
   const size_t smem = L::bytes(tp.Kp, nst);
-  auto kern = k_tc_estep<DIM, QF>;
+  auto kern = fast ? k_tc_estep<DIM, QF, true> : k_tc_estep<DIM, QF, false>;
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   EParams p;
   p.X = X; p.N = N; p.K = tp.K; p.Kp = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
