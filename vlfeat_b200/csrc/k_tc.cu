@@ -87,17 +87,20 @@ __global__ void k_tc_wimg(const float *__restrict__ means, const float *__restri
   i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (i64)Kp * KD2) return;
   const int k = (int)(idx / KD2), e = (int)(idx % KD2);
+  // K order of the product: chunk c (32 elements) holds x'_d for
+  // d = 16c .. 16c+15, then x'_d^2 for the same d, so that the E-step's
+  // producers read each element of x once.
+  const int c = e / 32, ee = e % 32;
   double w = 0;
   if (k < K) {
-    const int d = e < D ? e : e - D;
+    const int d = 16 * c + (ee & 15);
     const double s2 = (double)covs[(i64)k * D + d];
     const double mup = (double)means[(i64)k * D + d] - (double)ctr[d];
-    w = (e < D ? mup / s2 : -0.5 / s2) * 1.4426950408889634;
+    w = (ee < 16 ? mup / s2 : -0.5 / s2) * 1.4426950408889634;
   }
   __nv_bfloat16 hi, lo;
   split_bf16((float)w, hi, lo);
   const size_t wbytes = (size_t)(KD2 / 32) * Kp * 64;
-  const int c = e / 32, ee = e % 32;
   const size_t off = (size_t)c * Kp * 64 + kmajor_sw64_off(k, ee / 8) + (ee % 8) * 2;
   char *base = (char *)wimg;
   *(__nv_bfloat16 *)(base + off) = hi;
@@ -175,8 +178,13 @@ struct ELayout {
   static constexpr int KD2 = 2 * DIM;
   static constexpr int NKA = KD2 / 32;
   static constexpr int kStage = 2 * 8192;  // hi + lo parts of one 128 x 32 chunk
+  // Epilogue staging: each of the 8 epilogue warps transposes its 32 rows x
+  // 32 components (64 B per row) of q through 2 KB before the global stores.
+  static constexpr int kStaging = 8 * 2048;
   __host__ __device__ static size_t wbytes(int Kp) { return (size_t)NKA * Kp * 64; }
-  static size_t fixed(int Kp) { return 2 * wbytes(Kp) + 1024 /*cst*/ + 1024 /*ctr*/ + 1024 /*bars*/ + 1024; }
+  static size_t fixed(int Kp) {
+    return 2 * wbytes(Kp) + 1024 /*cst*/ + 1024 /*ctr, bars*/ + kStaging + 1024 /*alignment*/;
+  }
   static int max_stages(int Kp) { return (int)((kSmemLimit - fixed(Kp)) / kStage); }
   static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * kStage; }
 };
@@ -191,11 +199,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   uint8_t *sW = base;
   uint8_t *sA = sW + 2 * wbytes;
   float *s_cst = (float *)(sA + (size_t)p.nst * L::kStage);
-  float *s_ctr = s_cst + 256;
-  uint64_t *bars = (uint64_t *)(s_ctr + 256);
+  float *s_ctr = s_cst + 256;                     // DIM <= 128 floats
+  uint64_t *bars = (uint64_t *)(s_ctr + 128);     // 36 barriers, then TMEM base and abort flag
   uint64_t *full = bars, *empty = bars + 16, *accf = bars + 32, *acce = bars + 34;
-  uint32_t *s_tmem = (uint32_t *)(bars + 40);
+  uint32_t *s_tmem = (uint32_t *)(bars + 36);
   volatile int *s_abort = (volatile int *)(s_tmem + 1);
+  uint8_t *s_stage = (uint8_t *)(s_cst + 512);   // 8 x 2 KB epilogue staging
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   if (tid == 0) {
@@ -230,19 +239,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 
   if (warp < 4) {
     // ---------------------------------------------------- producers
-    // Warp w owns rows [32w, 32w+32) of each tile.  For one 32-element chunk
-    // of the A row [x', x'^2], lane (rg, part) handles rows 32w + 4s + rg,
-    // s = 0..7, and elements [4 part, 4 part + 4): each load instruction reads
-    // 4 rows x 128 contiguous bytes.  The next chunk's rows are prefetched into
-    // registers while the current chunk is converted.
-    const int part = lane & 7, rg = lane >> 3;
-    float4 b0[8], b1[8], b2[8];
-    auto load = [&](float4(&buf)[8], i64 t, int c) {
-      const int e0 = 32 * c + 4 * part;
-      const int d0 = e0 < DIM ? e0 : e0 - DIM;
+    // Warp w owns rows [32w, 32w+32) of each tile.  Chunk c of the A row is
+    // [x'_d, x'_d^2] for d = 16c .. 16c+15 (the K order of the W image), so
+    // lane (rg, part) reads dimensions 16c + 4 part .. +3 of rows
+    // 32w + 8s + rr, s = 0..3, once and writes both the x' and the x'^2
+    // elements: each load instruction reads 8 rows x 64 contiguous bytes.
+    // rr permutes rg so that the 16 lanes of each half-warp store to 16
+    // distinct bank groups of the 64-byte-swizzled stage.  The next chunks'
+    // rows are prefetched into registers while the current chunk is converted.
+    const int part = lane & 3, rg = lane >> 2;
+    const int rr = (rg & 1) | ((rg & 2) << 1) | ((rg & 4) >> 1);
+    float4 b0[4], b1[4], b2[4];
+    auto load = [&](float4(&buf)[4], i64 t, int c) {
+      const int d0 = 16 * c + 4 * part;
 #pragma unroll
-      for (int s = 0; s < 8; ++s) {
-        const i64 row = t * 128 + 32 * warp + 4 * s + rg;
+      for (int s = 0; s < 4; ++s) {
+        const i64 row = t * 128 + 32 * warp + 8 * s + rr;
         buf[s] = row < p.N ? __ldg((const float4 *)(p.X + row * DIM + d0)) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     };
@@ -262,28 +274,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     adv(t1, c1, t2, c2);
     if (t0 < p.ntiles) load(b0, t0, c0);
     if (t1 < p.ntiles) load(b1, t1, c1);
-    auto step = [&](float4(&cur)[8], float4(&fut)[8]) -> bool {
+    auto step = [&](float4(&cur)[4], float4(&fut)[4]) -> bool {
       if (t0 >= p.ntiles) return false;
       if (t2 < p.ntiles) load(fut, t2, c2);
       const int stage = it % p.nst;
       if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 1)) return false;
       const uint32_t a_hi = smem_u32(sA + (size_t)stage * L::kStage);
-      const int e0 = 32 * c0 + 4 * part;
-      const bool sq = e0 >= DIM;
-      const int d0 = sq ? e0 - DIM : e0;
+      const int d0 = 16 * c0 + 4 * part;
       const float m0 = s_ctr[d0], m1 = s_ctr[d0 + 1], m2 = s_ctr[d0 + 2], m3 = s_ctr[d0 + 3];
 #pragma unroll
-      for (int s = 0; s < 8; ++s) {
-        float v0 = cur[s].x - m0, v1 = cur[s].y - m1, v2 = cur[s].z - m2, v3 = cur[s].w - m3;
-        if (sq) {
-          v0 *= v0; v1 *= v1; v2 *= v2; v3 *= v3;
-        }
-        uint32_t h0, l0, h1, l1;
+      for (int s = 0; s < 4; ++s) {
+        const float v0 = cur[s].x - m0, v1 = cur[s].y - m1, v2 = cur[s].z - m2, v3 = cur[s].w - m3;
+        uint32_t h0, l0, h1, l1, h2, l2, h3, l3;
         split2<false>(v0, v1, h0, l0);
         split2<false>(v2, v3, h1, l1);
-        const uint32_t off = kmajor_sw64_off((uint32_t)(32 * warp + 4 * s + rg), (uint32_t)(part >> 1)) + (part & 1) * 8;
-        st_shared_v2(a_hi + off, h0, h1);
-        st_shared_v2(a_hi + 8192 + off, l0, l1);
+        split2<false>(v0 * v0, v1 * v1, h2, l2);
+        split2<false>(v2 * v2, v3 * v3, h3, l3);
+        const uint32_t row = (uint32_t)(32 * warp + 8 * s + rr);
+        const uint32_t o1 = kmajor_sw64_off(row, (uint32_t)(part >> 1)) + (part & 1) * 8;
+        const uint32_t o2 = kmajor_sw64_off(row, (uint32_t)(2 + (part >> 1))) + (part & 1) * 8;
+        st_shared_v2(a_hi + o1, h0, h1);
+        st_shared_v2(a_hi + 8192 + o1, l0, l1);
+        st_shared_v2(a_hi + o2, h2, h3);
+        st_shared_v2(a_hi + 8192 + o2, l2, l3);
       }
       fence_proxy_async_smem();
       mbar_arrive(&full[stage]);
@@ -298,13 +311,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   } else if (warp < 12) {
     // ----------------------------------------------------- epilogue
     // Two warpgroups: group g drains the tiles whose accumulator is TMEM
-    // buffer g (alternate tiles), so one tile's log-sum-exp overlaps the next.
+    // buffer g (alternate tiles), so one tile's log-sum-exp overlaps the
+    // next tile's stores and the two groups keep different pipes busy.
     // Warp w reads TMEM lanes 32 (w % 4) .. +31, i.e. rows of the tile.
     // Arithmetic on pairs of columns uses packed f32x2 instructions.
     const int eg = (warp - 4) >> 2, ew = warp & 3;
     const int r = ew * 32 + lane;
     const int nch = p.Kp / 32;
-    const unsigned long long* cst2v = (const unsigned long long*)s_cst;
+    const int ncw = (QF == kQRow) ? nch : p.Kq / 32;
+    const unsigned long long *cst2v = (const unsigned long long *)s_cst;
+    uint8_t *stg = s_stage + (warp - 4) * 2048;
     int tt = 0;
     for (i64 tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++tt) {
       const int buf = tt & 1;
@@ -335,7 +351,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
             if (lo32(s) > cm) { cm = lo32(s); cam = pc * 32 + 2 * j; }
             if (hi32(s) > cm) { cm = hi32(s); cam = pc * 32 + 2 * j + 1; }
           } else {
-            cm = fmaxf(cm, fmaxf(lo32(s), hi32(s)));
+            cm = max3f(cm, lo32(s), hi32(s));
           }
         }
         if (two) {
@@ -349,7 +365,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
               if (lo32(s) > cm) { cm = lo32(s); cam = pc * 32 + 32 + 2 * j; }
               if (hi32(s) > cm) { cm = hi32(s); cam = pc * 32 + 32 + 2 * j + 1; }
             } else {
-              cm = fmaxf(cm, fmaxf(lo32(s), hi32(s)));
+              cm = max3f(cm, lo32(s), hi32(s));
             }
           }
         }
@@ -384,105 +400,117 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         mg[pc >> 1] = m;
       }
       tmem_wait_st();
-      const float inv = 1.f / sum;
+      const float mt = m, st = sum;
+      const float inv = 1.f / st;
       const i64 row = tile * 128 + r;
       const bool valid = row < p.N;
-      unsigned cnt = 0;
-      // q image: this row's 8-row group inside its tile.
+      unsigned long long cnt2 = 0ull;  // (+0.0f, +0.0f): per-row term counts, exact below 2^24
+      // -prev(qthr) * 2^64, prev(qthr) the largest float below qthr (> 0).
+      const float nthr = -__uint_as_float(__float_as_uint(p.qthr) - 1u) * 0x1p64f;
+      // q image of this tile; this warp's rows are its 8-row groups 4 ew .. 4 ew + 3.
       uint8_t *ib = (uint8_t *)p.q + (size_t)tile * 128 * p.Kq * 2;
-      const uint32_t rowoff = (uint32_t)((r >> 3) * (p.Kq / 64) * 1024);
-      const int ncw = (QF == kQRow) ? nch : p.Kq / 32;
-      // Pass B: q = e * 2^(m_g - m) / sum, thresholded and stored, one
-      // 32-column chunk at a time.  Rows past N (tile padding) store zeros.
-      auto emit = [&](const uint32_t(&v)[32], int cc, bool have, float sc) {
-        float qv[32];
-        const unsigned long long sc2 = f2u(sc, sc);
+      // Image stores go through this warp's staging (32 rows x 64 B, 16-byte
+      // chunks swizzled by row so that both sides are free of bank conflicts):
+      // lane = row on the way in; on the way out lane (a, b) moves chunk b of
+      // row 8i + a, so one store instruction writes 8 rows x 64 contiguous
+      // bytes of the image instead of 32 scattered 16-byte pieces.
+      auto stage_out = [&](const uint4(&w)[4], int cc, size_t part_off) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          float x0, x1;
-          if (FAST) {
-            x0 = (have && cc * 32 + 2 * j == am) ? 1.f : 0.f;
-            x1 = (have && cc * 32 + 2 * j + 1 == am) ? 1.f : 0.f;
-          } else {
-            const unsigned long long q2 = mul2(f2u(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1])), sc2);
-            x0 = lo32(q2);
-            x1 = hi32(q2);
-          }
-          const bool k0 = x0 >= 1e-6f, k1 = x1 >= 1e-6f;
-          cnt += (unsigned)k0 + (unsigned)k1;
-          if (QF != kQRow) {
-            x0 = x0 < p.qthr ? 0.f : x0;
-            x1 = x1 < p.qthr ? 0.f : x1;
-          }
-          qv[2 * j] = x0;
-          qv[2 * j + 1] = x1;
+        for (int j = 0; j < 4; ++j) *(uint4 *)(stg + lane * 64 + ((j ^ ((lane >> 1) & 3)) << 4)) = w[j];
+        __syncwarp();
+        const int a = lane >> 2, b = lane & 3;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const uint4 v = *(const uint4 *)(stg + (8 * i + a) * 64 + ((b ^ ((a >> 1) & 3)) << 4));
+          const size_t off = (size_t)(4 * ew + i) * (p.Kq / 64) * 1024 + (size_t)(cc >> 1) * 1024 +
+                             mnmajor_sw128_off((uint32_t)a, (uint32_t)((cc & 1) * 4 + b));
+          *(uint4 *)(ib + part_off + off) = v;
         }
-        const int k0 = cc * 32;
-        if (QF == kQRow) {
-          if (!have) return;
-          float *dst = (float *)p.q + row * p.ldq + k0;
-          if (k0 + 32 <= p.K) {
-#pragma unroll
-            for (int j = 0; j < 32; j += 4)
-              *(float4 *)(dst + j) = make_float4(qv[j], qv[j + 1], qv[j + 2], qv[j + 3]);
-          } else {
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (k0 + j < p.K) dst[j] = qv[j];
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int kk = k0 + 8 * j;
-            const uint32_t off = rowoff + (uint32_t)((kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
-            uint4 wh, wl;
-            if (QF == kQImg16) {
-              wh.x = pack2<true>(qv[8 * j + 0], qv[8 * j + 1]);
-              wh.y = pack2<true>(qv[8 * j + 2], qv[8 * j + 3]);
-              wh.z = pack2<true>(qv[8 * j + 4], qv[8 * j + 5]);
-              wh.w = pack2<true>(qv[8 * j + 6], qv[8 * j + 7]);
-            } else {
-              split2<false>(qv[8 * j + 0], qv[8 * j + 1], wh.x, wl.x);
-              split2<false>(qv[8 * j + 2], qv[8 * j + 3], wh.y, wl.y);
-              split2<false>(qv[8 * j + 4], qv[8 * j + 5], wh.z, wl.z);
-              split2<false>(qv[8 * j + 6], qv[8 * j + 7], wh.w, wl.w);
-            }
-            *(uint4 *)(ib + off) = wh;
-            if (QF == kQImg32) *(uint4 *)(ib + p.qpart + off) = wl;
-          }
-        }
+        __syncwarp();
       };
-      // TMEM loads stay warp-uniform; only the stores depend on the row.
+      // Pass B: q = e * 2^(m_g - m) / sum, thresholded, one 32-column chunk at
+      // a time.  TMEM loads and staging stay warp-uniform; rows past N (tile
+      // padding) and image columns past Kp are zeros.
 #pragma unroll 1
       for (int cc = 0; cc < ncw; ++cc) {
-        uint32_t va[32];
+        float qv[32];
         const bool ha = cc < nch;
+        const bool live = valid && ha;
         if (ha) {
+          uint32_t va[32];
           tmem_ld32(tb + cc * 32, va);
           tmem_wait_ld();
+          const float sc = live ? ex2_approx(mg[cc >> 1] - mt) * inv : 0.f;
+          const unsigned long long sc2 = f2u(sc, sc);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            float x0, x1;
+            if (FAST) {
+              x0 = (live && cc * 32 + 2 * j == am) ? 1.f : 0.f;
+              x1 = (live && cc * 32 + 2 * j + 1 == am) ? 1.f : 0.f;
+            } else {
+              const unsigned long long q2 = mul2(f2u(__uint_as_float(va[2 * j]), __uint_as_float(va[2 * j + 1])), sc2);
+              x0 = lo32(q2);
+              x1 = hi32(q2);
+            }
+            // Keep flags (1.0 / 0.0) for q >= qthr, counted in packed float
+            // pairs and, for the image, applied by a packed multiply.  The
+            // flag is sat((q - prev(qthr)) 2^64), exact in one fma: the
+            // difference is either <= 0 or at least one ulp of qthr.
+            const unsigned long long kk = f2u(__saturatef(fmaf(x0, 0x1p64f, nthr)),
+                                              __saturatef(fmaf(x1, 0x1p64f, nthr)));
+            cnt2 = add2(cnt2, kk);
+            if (QF != kQRow) {
+              const unsigned long long xk = mul2(f2u(x0, x1), kk);
+              x0 = lo32(xk);
+              x1 = hi32(xk);
+            }
+            qv[2 * j] = x0;
+            qv[2 * j + 1] = x1;
+          }
         } else {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) va[j] = 0u;
+          for (int j = 0; j < 32; ++j) qv[j] = 0.f;
         }
-        if (valid) {
-          const float sc = ha ? ex2_approx(mg[cc >> 1] - m) * inv : 0.f;
-          emit(va, cc, ha, sc);
-        } else if (QF != kQRow) {
-          // Padding row of the last tile: its q image entries are zero.
+        if (QF == kQRow) {
+          if (live) {
+            const int k0 = cc * 32;
+            float *dst = (float *)p.q + row * p.ldq + k0;
+            if (k0 + 32 <= p.K) {
+#pragma unroll
+              for (int j = 0; j < 32; j += 4)
+                *(float4 *)(dst + j) = make_float4(qv[j], qv[j + 1], qv[j + 2], qv[j + 3]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < 32; ++j)
+                if (k0 + j < p.K) dst[j] = qv[j];
+            }
+          }
+        } else {
+          uint4 wh[4], wl[4];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            const int kk = cc * 32 + 8 * j;
-            const uint32_t off = rowoff + (uint32_t)((kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
-            *(uint4 *)(ib + off) = make_uint4(0, 0, 0, 0);
-            if (QF == kQImg32) *(uint4 *)(ib + p.qpart + off) = make_uint4(0, 0, 0, 0);
+            if (QF == kQImg16) {
+              wh[j].x = pack2<true>(qv[8 * j + 0], qv[8 * j + 1]);
+              wh[j].y = pack2<true>(qv[8 * j + 2], qv[8 * j + 3]);
+              wh[j].z = pack2<true>(qv[8 * j + 4], qv[8 * j + 5]);
+              wh[j].w = pack2<true>(qv[8 * j + 6], qv[8 * j + 7]);
+            } else {
+              split2<false>(qv[8 * j + 0], qv[8 * j + 1], wh[j].x, wl[j].x);
+              split2<false>(qv[8 * j + 2], qv[8 * j + 3], wh[j].y, wl[j].y);
+              split2<false>(qv[8 * j + 4], qv[8 * j + 5], wh[j].z, wl[j].z);
+              split2<false>(qv[8 * j + 6], qv[8 * j + 7], wh[j].w, wl[j].w);
+            }
           }
+          stage_out(wh, cc, 0);
+          if (QF == kQImg32) stage_out(wl, cc, (size_t)p.qpart);
         }
       }
       tc_fence_before();
       mbar_arrive(&acce[buf]);
-      if (valid && p.rowcnt) p.rowcnt[row] = cnt;
+      if (valid && p.rowcnt) p.rowcnt[row] = (unsigned)(lo32(cnt2) + hi32(cnt2));
       // Per-warp log-likelihood partial (fixed shuffle order): 4 per tile.
-      double ll = valid ? ((double)m + log2((double)sum)) * kLn2 : 0.0;
+      double ll = valid ? ((double)mt + log2((double)st)) * kLn2 : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
       if (lane == 0 && p.ll_part) p.ll_part[tile * 4 + ew] = ll;
@@ -836,37 +864,41 @@ __global__ void k_tc_fv_consts(const float *__restrict__ means, const float *__r
 // (vl/fisher.c:419-485) from S0 = sum q, S1 = sum q x', S2 = sum q x'^2:
 //   u = (S1 - mu' S0) / sigma,  v = (S2 - 2 mu' S1 + mu'^2 S0) / sigma2 - S0,
 // scaled by 1/(N sqrt pi) and 1/(N sqrt(2 pi)); signed sqrt; L2.
+template <int DIM>
 __global__ void __launch_bounds__(256) k_tc_fv_finalize(
-    int K, int Kp, int D, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
+    int K, int Kp, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
     const i64 *__restrict__ imgRow0, const double *__restrict__ cmu, const double *__restrict__ cis2,
     const double *__restrict__ cisd, const double *__restrict__ cup, const double *__restrict__ cvp,
     const float *__restrict__ scale, const unsigned *__restrict__ rowcnt, i64 rowcntBase, int flags,
     i64 imgBase, float *__restrict__ enc, unsigned long long *__restrict__ nterms) {
+  constexpr int NST = 2 * DIM + 16;
   __shared__ double sh[256];
   __shared__ unsigned long long shn[256];
+  __shared__ double s_is[DIM];  // 1 / scale_d (exact: scale_d is a power of two)
   const int img = blockIdx.x;
   const int s0 = imgSlot0[img], s1 = imgSlot0[img + 1];
   const i64 r0 = imgRow0[img], r1 = imgRow0[img + 1];
   const i64 n = r1 - r0;
   const double in = n > 0 ? 1.0 / (double)n : 0.0;
-  const int NST = 2 * D + 16;
-  const i64 KD = (i64)K * D;
-  float *out = enc + (imgBase + img) * 2 * KD;
+  const int KD = K * DIM;
+  const size_t slotStride = (size_t)Kp * NST;
+  float *out = enc + (imgBase + img) * 2 * (i64)KD;
+  for (int d = threadIdx.x; d < DIM; d += 256) s_is[d] = scale ? 1.0 / (double)scale[d] : 1.0;
+  __syncthreads();
   double sq = 0;
-  for (i64 e = threadIdx.x; e < KD; e += 256) {
-    const int k = (int)(e / D), d = (int)(e % D);
+  for (int e = threadIdx.x; e < KD; e += 256) {
+    const int k = e / DIM, d = e - k * DIM;
     double S0 = 0, S1 = 0, S2 = 0;
-    for (int s = s0; s < s1; ++s) {
-      const float *pp = partial + ((size_t)s * Kp + k) * NST;
-      S0 += (double)pp[2 * D];
+    const float *pp = partial + ((size_t)s0 * Kp + k) * NST;
+    for (int s = s0; s < s1; ++s, pp += slotStride) {
+      S0 += (double)pp[2 * DIM];
       S1 += (double)pp[d];
-      S2 += (double)pp[D + d];
+      S2 += (double)pp[DIM + d];
     }
-    if (scale) {  // statistics were taken on x'' = x' * scale
-      const double is = 1.0 / (double)scale[d];
-      S1 *= is;
-      S2 *= is * is;
-    }
+    // Statistics were taken on x'' = x' * scale (s_is = 1 without scaling).
+    const double is = s_is[d];
+    S1 *= is;
+    S2 *= is * is;
     const double mup = cmu[e];
     const double u = cisd[e] * (S1 - mup * S0) * (cup[k] * in);
     const double v = ((S2 - 2.0 * mup * S1 + mup * mup * S0) * cis2[e] - S0) * (cvp[k] * in);
@@ -897,7 +929,7 @@ __global__ void __launch_bounds__(256) k_tc_fv_finalize(
     double nrm = sqrt(sh[0]);
     if (nrm < 1e-12) nrm = 1e-12;
     const float nf = (float)nrm;
-    for (i64 e = threadIdx.x; e < 2 * KD; e += 256) out[e] = out[e] / nf;
+    for (int e = threadIdx.x; e < 2 * KD; e += 256) out[e] = out[e] / nf;
   }
 }
 
@@ -1101,10 +1133,11 @@ void lpt_assign(const std::vector<SItem> &items, int gx, std::vector<int> &order
 bool tc_supported(i64 K, i64 D) {
   if (!(D == 64 || D == 80 || D == 128)) return false;
   if (K < 8 || K > 256 || K % 8) return false;
-  // Resident W (hi + lo) plus at least two operand stages must fit.
+  // Resident W (hi + lo), constants, epilogue staging and at least two
+  // operand stages must fit (the E-step's shared-memory layout).
   const int Kp = padK(K);
   const size_t w = (size_t)2 * (2 * D / 32) * Kp * 64;
-  return w + 4096 + 2 * 16384 <= (size_t)kSmemLimit;
+  return w + 2048 + 8 * 2048 + 1024 + 2 * 16384 <= (size_t)kSmemLimit;
 }
 
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part, bool fast,
@@ -1202,9 +1235,10 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const 
       sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg; sp.partial = partial; sp.err = err;
       stats_dispatch(tp.D, split, sp, gx, s);
     }
+    auto fin = D == 64 ? k_tc_fv_finalize<64> : D == 80 ? k_tc_fv_finalize<80> : k_tc_fv_finalize<128>;
     VLB_LAUNCH("tc_fv_finalize", s,
-               k_tc_fv_finalize<<<(unsigned)nimg, 256, 0, s>>>(
-                   (int)K, tp.Kp, (int)D, partial, dslot0, drow0, cmu, cis2, cisd, cup, cvp,
+               fin<<<(unsigned)nimg, 256, 0, s>>>(
+                   (int)K, tp.Kp, partial, dslot0, drow0, cmu, cis2, cisd, cup, cvp,
                    fp32 ? nullptr : tp.scale, nrows > 0 ? rowcnt : nullptr, row0, flags, chunkImg0,
                    enc, nterms));
   }

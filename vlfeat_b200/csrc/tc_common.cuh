@@ -277,6 +277,12 @@ __device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigne
   return r;
 }
 
+// Three-input maximum (sm_100 and later).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
 __device__ __forceinline__ float ex2_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
