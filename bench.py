@@ -10,7 +10,11 @@ of 40,960 floats per image.  One step = one batched encode of all images.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Each path (exact CUDA-core fp32, tensor-core FP32 = bf16x3, BF16, BF16 +
-router) is timed with CUDA events on the launching stream; the headline
+router) is timed with CUDA events on the launching stream.  The tensor-core
+FP32 and BF16 paths run through a batched-encode plan (vlb200_fisher_plan_*):
+its tile shapes are autotuned on the workload and one whole encode is
+captured in a CUDA graph before the timed region, and each step replays the
+graph; the other paths call vlb200_fisher_encode_batch_device.  The headline
 `value` is the fastest path whose Fisher vectors stay within rel err 1e-3 of
 the FP64 GPU path.  `e2e` times the same metric through the public API with
 host buffers (pinned host -> device copy of the step's descriptors, encode,
@@ -148,11 +152,44 @@ def encode(capi, wl, enc, nt, prec, stream):
                                     FLAGS, prec, nt, stream)
 
 
-def time_path(capi, wl, enc, nt, prec, steps, warmup, dist):
+PLAN_PATHS = ("fp32", "bf16")  # tensor-core paths: autotuned plan replayed as a CUDA graph
+
+
+def make_encoder(capi, wl, x, enc, nt, prec, stream, config=None):
+    """One encode of the workload on `stream`: returns (replay, eager, info).
+    Tensor-core paths use a batched-encode plan bound to (x, enc, nt): tile
+    shapes autotuned on the workload (or `config`), one encode captured as a
+    CUDA graph, `replay` launches the graph and `eager` runs the plan's
+    launches directly.  Other paths call the batched API."""
+    if prec not in PLAN_PATHS:
+        def run():
+            encode(capi, dict(wl, x=x), enc, nt, prec, stream)
+        return run, run, {"api": "vlb200_fisher_encode_batch_device", "cuda_graph": False}
+    plan = capi.FisherPlan(D, K, wl["offs"], FLAGS, prec)
+    plan.set_gmm(wl["means"], wl["covs"], wl["priors"])
+    tuned = None
+    if config is None:
+        tuned = plan.autotune(enc, x, nt, stream=stream)
+    else:
+        plan.set_config(stream=stream, **config)
+    plan.capture(enc, x, nt, stream=stream)
+    info = {"api": "vlb200_fisher_plan (autotuned, CUDA graph)", "cuda_graph": True,
+            "plan_config": plan.get_config(), "autotune_best_ms": tuned}
+
+    def replay():
+        plan.launch(stream=stream)
+
+    def eager():
+        plan.execute(enc, x, nt, stream=stream)
+    replay.plan = plan  # keep the plan alive with its closures
+    return replay, eager, info
+
+
+def time_path(capi, run, steps, warmup, dist):
     import torch
     s = torch.cuda.current_stream()
     for _ in range(warmup):
-        encode(capi, wl, enc, nt, prec, s)
+        run()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -161,7 +198,7 @@ def time_path(capi, wl, enc, nt, prec, steps, warmup, dist):
     l0 = capi.launch_count()
     e0.record(s)
     for _ in range(steps):
-        encode(capi, wl, enc, nt, prec, s)
+        run()
     e1.record(s)
     torch.cuda.synchronize()
     launches = capi.launch_count() - l0
@@ -222,9 +259,10 @@ def cpu_baseline(wl, budget_s=12.0, kind_pref="reference"):
 
 
 # ------------------------------------------------------------- roofline
-def roofline(capi, wl, enc, nt, prec):
+def roofline(capi, wl, run, prec):
     """Dominant kernel's achieved rate from live CUDA-event timing of every
-    launch (library profiling), against the measured peak."""
+    launch (library profiling) of `run` (one eager encode), against the
+    measured peak."""
     import torch
     peaks = {}
     try:
@@ -236,9 +274,8 @@ def roofline(capi, wl, enc, nt, prec):
     bf16 = peaks.get("bf16_tflops", 1590.0)
     capi.profile_reset()
     capi.profile_enable(True)
-    s = torch.cuda.current_stream()
     for _ in range(2):
-        encode(capi, wl, enc, nt, prec, s)
+        run()
     torch.cuda.synchronize()
     prof = capi.profile_read()
     capi.profile_enable(False)
@@ -287,23 +324,28 @@ def roofline(capi, wl, enc, nt, prec):
 
 
 # -------------------------------------------------------------- e2e
-def e2e(capi, wl, prec, steps=3):
-    """Same metric through the public API from pinned host buffers."""
+def e2e(capi, wl, prec, config, steps=3):
+    """Same metric through the public API from pinned host buffers: each step
+    copies the descriptors host -> device, encodes them (the path's plan with
+    the tuned configuration, bound to these device buffers and replayed as a
+    CUDA graph; or the batched API) and copies the encodings device -> host."""
     import torch
     x_host = wl["x"].cpu().pin_memory()
     total = wl["total"]
     enc_host = torch.empty((NUM_IMAGES, 2 * K * D), dtype=torch.float32).pin_memory()
     x_dev = torch.empty_like(wl["x"])
+    x_dev.copy_(wl["x"])
     enc = torch.empty((NUM_IMAGES, 2 * K * D), device="cuda")
+    nt = torch.empty(NUM_IMAGES, dtype=torch.int64, device="cuda")
     s = torch.cuda.current_stream()
-    w2 = dict(wl)
-    w2["x"] = x_dev
+    run, _, _ = make_encoder(capi, wl, x_dev, enc, nt, prec, s, config=config)
+    run()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(s)
     for _ in range(steps):
         x_dev.copy_(x_host, non_blocking=True)
-        encode(capi, w2, enc, None, prec, s)
+        run()
         enc_host.copy_(enc, non_blocking=True)
     e1.record(s)
     torch.cuda.synchronize()
@@ -396,18 +438,25 @@ def main():
     router = train_router(capi, wl) if "bf16_router" in args.paths else None  # noqa: F841
     results = {}
     launches_of = {}
+    eager_of = {}
+    s = torch.cuda.current_stream()
+    encoders = {}
+    for p in args.paths.split(","):  # plans: autotuned and captured before the timed regions
+        encoders[p] = make_encoder(capi, wl, wl["x"], enc, nt, p, s)
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for p in args.paths.split(","):
-            ms, launches = time_path(capi, wl, enc, nt, p, args.steps, args.warmup, dist)
+            run, eager, info = encoders[p]
+            ms, launches = time_path(capi, run, args.steps, args.warmup, dist)
             err = rel_errs(enc.cpu().numpy(), ref) if rank == 0 else None
             results[p] = {"value": wl["total"] * world / (ms / 1e3), "ms_per_step": ms,
-                          "rel_err_vs_fp64": err}
+                          "rel_err_vs_fp64": err, **info}
             launches_of[p] = launches
+            eager_of[p] = eager
     ok = [p for p in results if results[p]["rel_err_vs_fp64"] is not None
           and results[p]["rel_err_vs_fp64"] <= 1e-3]
     head = max(ok or list(results), key=lambda p: results[p]["value"])
     if rank == 0:
-        roof, shares = roofline(capi, wl, enc, nt, head)
+        roof, shares = roofline(capi, wl, eager_of[head], head)
         out = {"metric": METRIC, "value": results[head]["value"], "unit": "descriptors/s",
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": results[head]["ms_per_step"], "higher_is_better": True,
@@ -417,7 +466,7 @@ def main():
                "paths": results, "roofline": roof, "kernel_time_share": shares,
                "gpu_launches": launches_of[head], "clocks": clk.summary()}
         if not args.no_e2e:
-            out["e2e"] = e2e(capi, wl, head)
+            out["e2e"] = e2e(capi, wl, head, results[head].get("plan_config"))
         if not args.no_cpu and world == 1:
             out["cpu_baseline"] = cpu_baseline(wl)
         print(json.dumps(out), flush=True)

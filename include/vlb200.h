@@ -93,6 +93,54 @@ VL_EXPORT int vlb200_fisher_encode_batch_device(float *enc, float const *means, 
                                                 int flags, int precision, vl_uint64 *numTerms,
                                                 void *stream);
 
+/* ------------------------------------------------------ batched encode plan
+ * A plan binds the tensor-core batched encoder to one batch layout (offsets,
+ * numImages), dimension, numClusters, flags and precision (FP32, BF16 or
+ * BF16_ROUTER; DEFAULT resolves as elsewhere).  It owns every table and
+ * scratch buffer of the encode, so that execute only launches kernels: after
+ * its first call it allocates nothing, copies nothing from the host and does
+ * not synchronise, and a whole encode can be captured in a CUDA graph and
+ * replayed.  Results equal numImages calls of vl_fisher_encode
+ * (vl/fisher.c:548-579) computed in the chosen precision; no reference
+ * counterpart.  Functions returning int return 0 or a VL_ERR_* code (also
+ * recorded as the last error); vlb200_fisher_plan_new returns NULL on error.
+ *
+ * Tile configuration (vlb200_fisher_plan_get/set_config), five int64:
+ *   [0] rows per statistics work item (multiple of 128, default 8192)
+ *   [1] 128-component M tiles per statistics CTA (0: two when they fit; 1; 2)
+ *   [2] operand stages of the statistics kernel (0: as many as fit)
+ *   [3] operand stages of the E-step (0: as many as fit)
+ *   [4] rows per E-step launch (0: a 4 GB posterior image)
+ * vlb200_fisher_plan_autotune times a set of candidates on the given data
+ * (CUDA events, median of three runs each) and keeps the fastest; bestMs
+ * (may be NULL) receives its time per encode. */
+typedef struct _VlB200FisherPlan VlB200FisherPlan;
+VL_EXPORT VlB200FisherPlan *vlb200_fisher_plan_new(vl_size dimension, vl_size numClusters,
+                                                   vl_int64 const *offsets, vl_size numImages,
+                                                   int flags, int precision);
+VL_EXPORT void vlb200_fisher_plan_delete(VlB200FisherPlan *plan);
+/* Binds the GMM by device pointers (means, covariances: K x D; priors: K).
+ * Every execute reads their current contents. */
+VL_EXPORT int vlb200_fisher_plan_set_gmm(VlB200FisherPlan *plan, float const *means,
+                                         float const *covariances, float const *priors);
+VL_EXPORT int vlb200_fisher_plan_execute(VlB200FisherPlan *plan, float *enc, float const *data,
+                                         vl_uint64 *numTerms, void *stream);
+VL_EXPORT int vlb200_fisher_plan_autotune(VlB200FisherPlan *plan, float *enc, float const *data,
+                                          vl_uint64 *numTerms, void *stream, double *bestMs);
+VL_EXPORT int vlb200_fisher_plan_get_config(VlB200FisherPlan const *plan, vl_int64 config[5]);
+VL_EXPORT int vlb200_fisher_plan_set_config(VlB200FisherPlan *plan, vl_int64 const config[5],
+                                            void *stream);
+/* Runs one encode outside capture, then captures one into a CUDA graph bound
+ * to these buffers and this stream (a created stream, not the default one).
+ * vlb200_fisher_plan_launch replays it.  set_gmm, set_config and autotune
+ * drop the graph. */
+VL_EXPORT int vlb200_fisher_plan_capture(VlB200FisherPlan *plan, float *enc, float const *data,
+                                         vl_uint64 *numTerms, void *stream);
+VL_EXPORT int vlb200_fisher_plan_launch(VlB200FisherPlan *plan, void *stream);
+/* Synchronises the stream and returns the kernels' error word: 0, or the
+ * code of a bounded wait that gave up. */
+VL_EXPORT int vlb200_fisher_plan_status(VlB200FisherPlan *plan, void *stream);
+
 /* ----------------------------------------------------------------- router
  * Learned candidate router for the E-step (no reference counterpart; the
  * reference always evaluates every component, vl/gmm.c:758-791).  An MLP

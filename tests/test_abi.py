@@ -89,3 +89,21 @@ def test_without_gpu_reports_error(libpath):
     with pytest.raises(capi.VLError):
         capi.fisher_encode(np.zeros((3, 2), np.float32), np.zeros((1, 2), np.float32),
                            np.ones((1, 2), np.float32), np.ones(1, np.float32))
+
+
+def test_fisher_plan_argument_checks(libpath):
+    """The plan's argument checks run on the host before any device call:
+    precision EXACT (the plan is the tensor-core encoder), an unsupported
+    dimension and decreasing offsets return NULL with VL_ERR_BAD_ARG."""
+    import numpy as np
+    from vlfeat_b200 import capi
+    L = capi.lib()
+    offs = np.array([0, 10, 25], np.int64)
+    assert not L.vlb200_fisher_plan_new(80, 256, capi._np_ptr(offs), 2, 0, 1)  # EXACT
+    assert L.vl_get_last_error() == 3
+    assert not L.vlb200_fisher_plan_new(96, 256, capi._np_ptr(offs), 2, 0, 3)  # D = 96
+    assert L.vl_get_last_error() == 3
+    bad = np.array([0, 10, 5], np.int64)
+    assert not L.vlb200_fisher_plan_new(80, 256, capi._np_ptr(bad), 2, 0, 3)
+    assert L.vl_get_last_error() == 3
+    assert L.vlb200_fisher_plan_launch(None, None) == 3

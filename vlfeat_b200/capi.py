@@ -97,6 +97,16 @@ def _decl(L):
       C.c_int, C.POINTER(C.c_uint64), _vp)
     f("vlb200_fisher_encode_batch_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _sz,
       C.c_int, C.c_int, _vp, _vp)
+    f("vlb200_fisher_plan_new", _vp, _sz, _sz, _vp, _sz, C.c_int, C.c_int)
+    f("vlb200_fisher_plan_delete", None, _vp)
+    f("vlb200_fisher_plan_set_gmm", C.c_int, _vp, _vp, _vp, _vp)
+    f("vlb200_fisher_plan_execute", C.c_int, _vp, _vp, _vp, _vp, _vp)
+    f("vlb200_fisher_plan_autotune", C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_double))
+    f("vlb200_fisher_plan_get_config", C.c_int, _vp, _vp)
+    f("vlb200_fisher_plan_set_config", C.c_int, _vp, _vp, _vp)
+    f("vlb200_fisher_plan_capture", C.c_int, _vp, _vp, _vp, _vp, _vp)
+    f("vlb200_fisher_plan_launch", C.c_int, _vp, _vp)
+    f("vlb200_fisher_plan_status", C.c_int, _vp, _vp)
 
 
 def lib(path: str = LIB_PATH):
@@ -396,3 +406,84 @@ def fisher_encode_batch_device(enc_t, means_t, covs_t, priors_t, data_t, offsets
         nterms_t.data_ptr() if nterms_t is not None else None, _stream(stream))
     if rc:
         _raise_last("vlb200_fisher_encode_batch_device")
+
+
+class FisherPlan:
+    """vlb200_fisher_plan_*: the batched tensor-core encoder bound to one batch
+    layout, with autotuned tile shapes and CUDA-graph replay.  The GMM and the
+    data/output buffers are torch CUDA tensors that must outlive their use."""
+
+    CONFIG_KEYS = ("item_rows", "stats_mt", "stats_stages", "estep_stages", "row_budget")
+
+    def __init__(self, D, K, offsets, flags=FLAG_IMPROVED, precision="bf16"):
+        self.offsets = np.ascontiguousarray(offsets, np.int64)
+        _clear()
+        h = lib().vlb200_fisher_plan_new(D, K, _np_ptr(self.offsets), len(self.offsets) - 1,
+                                         int(flags), _prec(precision))
+        if not h:
+            _raise_last("vlb200_fisher_plan_new")
+        self._h = h
+        self._keep = ()
+
+    def close(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.vlb200_fisher_plan_delete(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc:
+            _raise_last(what)
+
+    def set_gmm(self, means_t, covs_t, priors_t):
+        self._gmm = (means_t, covs_t, priors_t)
+        _clear()
+        self._check(lib().vlb200_fisher_plan_set_gmm(self._h, means_t.data_ptr(), covs_t.data_ptr(),
+                                                     priors_t.data_ptr()), "vlb200_fisher_plan_set_gmm")
+
+    def execute(self, enc_t, data_t, nterms_t=None, stream=None):
+        _clear()
+        self._check(lib().vlb200_fisher_plan_execute(
+            self._h, enc_t.data_ptr(), data_t.data_ptr(),
+            nterms_t.data_ptr() if nterms_t is not None else None, _stream(stream)),
+            "vlb200_fisher_plan_execute")
+
+    def autotune(self, enc_t, data_t, nterms_t=None, stream=None) -> float:
+        ms = C.c_double(0)
+        _clear()
+        self._check(lib().vlb200_fisher_plan_autotune(
+            self._h, enc_t.data_ptr(), data_t.data_ptr(),
+            nterms_t.data_ptr() if nterms_t is not None else None, _stream(stream), C.byref(ms)),
+            "vlb200_fisher_plan_autotune")
+        return ms.value
+
+    def get_config(self) -> dict:
+        c = np.zeros(5, np.int64)
+        self._check(lib().vlb200_fisher_plan_get_config(self._h, _np_ptr(c)),
+                    "vlb200_fisher_plan_get_config")
+        return dict(zip(self.CONFIG_KEYS, (int(v) for v in c)))
+
+    def set_config(self, stream=None, **kw):
+        cur = self.get_config()
+        cur.update(kw)
+        c = np.array([cur[k] for k in self.CONFIG_KEYS], np.int64)
+        _clear()
+        self._check(lib().vlb200_fisher_plan_set_config(self._h, _np_ptr(c), _stream(stream)),
+                    "vlb200_fisher_plan_set_config")
+
+    def capture(self, enc_t, data_t, nterms_t=None, stream=None):
+        self._keep = (enc_t, data_t, nterms_t)
+        _clear()
+        self._check(lib().vlb200_fisher_plan_capture(
+            self._h, enc_t.data_ptr(), data_t.data_ptr(),
+            nterms_t.data_ptr() if nterms_t is not None else None, _stream(stream)),
+            "vlb200_fisher_plan_capture")
+
+    def launch(self, stream=None):
+        self._check(lib().vlb200_fisher_plan_launch(self._h, _stream(stream)),
+                    "vlb200_fisher_plan_launch")
+
+    def status(self, stream=None) -> int:
+        return int(lib().vlb200_fisher_plan_status(self._h, _stream(stream)))

@@ -56,6 +56,10 @@ void launch_end(const char *name, cudaStream_t s);
 // Launch without the optional event timing (which creates CUDA events): used
 // by the entry point that must not allocate.  The launch is still counted.
 void count_launch();
+// Adds n launches (the kernels of a replayed CUDA graph) to the count.
+void count_launches(unsigned long long n);
+// Sets the per-launch event timing on or off; returns the previous setting.
+bool profile_swap(bool on);
 #define VLB_LAUNCH_PLAIN(stream, ...)  \
   do {                                 \
     __VA_ARGS__;                       \

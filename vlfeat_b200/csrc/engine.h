@@ -112,4 +112,29 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages,
                      const DevModel<float> &m, float *enc, unsigned long long *nterms, int flags,
                      int precision, cudaStream_t s);
 
+// Tunable shapes of the batched Fisher encoder (0: the built-in choice).
+struct TcFvConfig {
+  i64 itemRows = 8192;  // rows per statistics work item (multiple of 128)
+  int statsMT = 0;      // 128-component M tiles per statistics CTA: 0 (two when they fit), 1, 2
+  int statsStages = 0;  // operand stages of the statistics kernel (0: as many as fit)
+  int estepStages = 0;  // operand stages of the E-step (0: as many as fit, at most 8)
+  i64 rowBudget = 0;    // rows per E-step launch (0: a 4 GB q image)
+};
+
+// A batched encoder bound to one batch layout (image offsets), flags and
+// precision.  It owns its tables and scratch, so that tc_fv_plan_run only
+// launches kernels: no allocation after the first run, no host copies and no
+// synchronisation, which makes it capturable in a CUDA graph.
+struct TcFvPlan;
+TcFvPlan *tc_fv_plan_new(i64 D, i64 K, const i64 *offsets, i64 numImages, int flags, int precision,
+                         cudaStream_t s);
+void tc_fv_plan_delete(TcFvPlan *p);
+TcFvConfig tc_fv_plan_config(const TcFvPlan *p);
+void tc_fv_plan_set_config(TcFvPlan *p, const TcFvConfig &c, cudaStream_t s);
+void tc_fv_plan_run(TcFvPlan *p, const DevModel<float> &m, const float *X, float *enc,
+                    unsigned long long *nterms, cudaStream_t s);
+int tc_fv_plan_error(TcFvPlan *p, cudaStream_t s);  // the kernels' error word (synchronises)
+TcFvConfig tc_fv_plan_autotune(TcFvPlan *p, const DevModel<float> &m, const float *X, float *enc,
+                               unsigned long long *nterms, cudaStream_t s, double *best_ms);
+
 }  // namespace vlb

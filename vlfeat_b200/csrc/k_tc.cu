@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <memory>
 #include <numeric>
 #include <vector>
 
@@ -994,8 +995,7 @@ struct TcPrep {
 
 int padK(i64 K) { return (int)((K + 31) / 32 * 32); }
 
-void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, cudaStream_t s) {
-  Scratch &sc = thread_scratch(kArenaTc);
+void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &sc, cudaStream_t s) {
   tp.K = (int)m.K;
   tp.Kp = padK(m.K);
   tp.D = (int)m.D;
@@ -1022,11 +1022,11 @@ int padQ(int Kp) { return (Kp + 127) / 128 * 128; }
 
 template <int DIM, int QF>
 i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                 unsigned *rowcnt, double *ll_part, int *err, cudaStream_t s) {
+                 unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s) {
   using L = ELayout<DIM>;
   const i64 ntiles = (N + 127) / 128;
   if (ntiles == 0) return 0;
-  const int nst = std::min(8, L::max_stages(tp.Kp));
+  const int nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(tp.Kp));
   VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
   const size_t smem = L::bytes(tp.Kp, nst);
   auto kern = fast ? k_tc_estep<DIM, QF, true> : k_tc_estep<DIM, QF, false>;
@@ -1043,10 +1043,10 @@ i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool
 }
 
 template <int DIM, int MT, int SPLIT>
-void launch_stats(const SParams &p0, int grid_x, int grid_y, cudaStream_t s) {
+void launch_stats(const SParams &p0, int grid_x, int grid_y, int nst_req, cudaStream_t s) {
   using L = SLayout<DIM, MT, SPLIT>;
   SParams p = p0;
-  p.nst = std::min(8, L::max_stages());
+  p.nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages());
   VLB_CHECK(p.nst >= 2, VL_ERR_BAD_ARG, "tensor-core statistics: operands exceed shared memory");
   const size_t smem = L::bytes(p.nst);
   auto kern = k_tc_stats<DIM, MT, SPLIT>;
@@ -1059,39 +1059,40 @@ template <int DIM>
 struct Tc {
   static constexpr bool kTwo = 2 * (2 * DIM + 16) <= 512;  // two M tiles fit in TMEM
   static i64 estep(int qf, const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                   unsigned *rowcnt, double *ll, int *err, cudaStream_t s) {
-    if (qf == kQImg16) return launch_estep<DIM, kQImg16>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
-    if (qf == kQImg32) return launch_estep<DIM, kQImg32>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
-    return launch_estep<DIM, kQRow>(X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+                   unsigned *rowcnt, double *ll, int *err, int nst, cudaStream_t s) {
+    if (qf == kQImg16) return launch_estep<DIM, kQImg16>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
+    if (qf == kQImg32) return launch_estep<DIM, kQImg32>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
+    return launch_estep<DIM, kQRow>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
   }
   // split 2: bf16x3 statistics (q image in two bf16 parts); split 1: fp16.
-  static void stats(int split, const SParams &p, int grid_x, cudaStream_t s) {
+  // mt: 128-component M tiles per CTA (0: two when they fit in TMEM).
+  static void stats(int split, const SParams &p, int grid_x, int mt, int nst, cudaStream_t s) {
     const int mtiles = p.Kq / 128;
-    if (kTwo && mtiles % 2 == 0) {
-      if (split == 1) launch_stats<DIM, (kTwo ? 2 : 1), 1>(p, grid_x, mtiles / 2, s);
-      else launch_stats<DIM, (kTwo ? 2 : 1), 2>(p, grid_x, mtiles / 2, s);
+    if (kTwo && mtiles % 2 == 0 && mt != 1) {
+      if (split == 1) launch_stats<DIM, (kTwo ? 2 : 1), 1>(p, grid_x, mtiles / 2, nst, s);
+      else launch_stats<DIM, (kTwo ? 2 : 1), 2>(p, grid_x, mtiles / 2, nst, s);
     } else {
-      if (split == 1) launch_stats<DIM, 1, 1>(p, grid_x, mtiles, s);
-      else launch_stats<DIM, 1, 2>(p, grid_x, mtiles, s);
+      if (split == 1) launch_stats<DIM, 1, 1>(p, grid_x, mtiles, nst, s);
+      else launch_stats<DIM, 1, 2>(p, grid_x, mtiles, nst, s);
     }
   }
 };
 
 i64 estep_dispatch(int D, int qf, const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                   unsigned *rowcnt, double *ll, int *err, cudaStream_t s) {
+                   unsigned *rowcnt, double *ll, int *err, int nst, cudaStream_t s) {
   switch (D) {
-    case 64: return Tc<64>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
-    case 80: return Tc<80>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
-    case 128: return Tc<128>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, s);
+    case 64: return Tc<64>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
+    case 80: return Tc<80>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
+    case 128: return Tc<128>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
     default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
   }
 }
 
-void stats_dispatch(int D, int split, const SParams &p, int grid_x, cudaStream_t s) {
+void stats_dispatch(int D, int split, const SParams &p, int grid_x, int mt, int nst, cudaStream_t s) {
   switch (D) {
-    case 64: Tc<64>::stats(split, p, grid_x, s); break;
-    case 80: Tc<80>::stats(split, p, grid_x, s); break;
-    case 128: Tc<128>::stats(split, p, grid_x, s); break;
+    case 64: Tc<64>::stats(split, p, grid_x, mt, nst, s); break;
+    case 80: Tc<80>::stats(split, p, grid_x, mt, nst, s); break;
+    case 128: Tc<128>::stats(split, p, grid_x, mt, nst, s); break;
     default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
   }
 }
@@ -1143,106 +1144,296 @@ bool tc_supported(i64 K, i64 D) {
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part, bool fast,
              int precision, cudaStream_t s) {
   (void)precision;
+  Scratch &sc = thread_scratch(kArenaTc);
   TcPrep tp;
-  tc_prepare(m, tp, false, s);
-  int *err = thread_scratch(kArenaTc).slot[3].get<int>(1);
+  tc_prepare(m, tp, false, sc, s);
+  int *err = sc.slot[3].get<int>(1);
   VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  const i64 n = estep_dispatch(tp.D, kQRow, X, N, tp, (void *)q, (int)m.K, fast, nullptr, ll_part, err, s);
+  const i64 n = estep_dispatch(tp.D, kQRow, X, N, tp, (void *)q, (int)m.K, fast, nullptr, ll_part, err, 0, s);
   check_err(err, s);
   return n;
 }
 
-void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const DevModel<float> &m,
-                     float *enc, unsigned long long *nterms, int flags, int precision, cudaStream_t s) {
-  Scratch &sc = thread_scratch(kArenaTc);
+// ------------------------------------------------- batched Fisher encoding
+namespace {
+
+// Host-side layout of one batch of images: chunks of whole images (one
+// E-step launch each, at most rowBudget rows unless one image is larger),
+// work items (runs of at most itemRows rows of one image; images without rows
+// get none and encode to zeros) assigned to the persistent statistics CTAs by
+// LPT, and the per-image slot and row tables of the finalize kernel.  The
+// tables of all chunks are concatenated; each chunk records its offsets.
+struct FvChunk {
+  i64 img0 = 0, nimg = 0, row0 = 0, nrows = 0;
+  int nitems = 0, gx = 1;
+  size_t items = 0, beg = 0, img = 0;  // offsets into items/order, beg, slot0/row0
+};
+
+struct FvLayout {
+  std::vector<FvChunk> chunks;
+  std::vector<SItem> items;
+  std::vector<int> order, beg, slot0;
+  std::vector<i64> row0;
+  i64 maxRows = 0, maxTiles = 0;
+  int maxItems = 0;
+};
+
+i64 default_row_budget(int Kp, bool fp32) {
+  const i64 qsz = fp32 ? 4 : 2;  // bytes per q element over the image parts
+  return std::max<i64>(1 << 16, (i64)(4ull << 30) / (Kp * qsz));
+}
+
+void fv_layout(const i64 *off, i64 numImages, i64 rowBudget, i64 itemRows, int nsm, FvLayout &L) {
+  L = FvLayout();
+  i64 img = 0;
+  while (img < numImages) {
+    FvChunk c;
+    c.img0 = img;
+    c.row0 = off[img];
+    while (img < numImages && (img == c.img0 || off[img + 1] - c.row0 <= rowBudget)) ++img;
+    c.nimg = img - c.img0;
+    c.nrows = off[img] - c.row0;
+    c.items = L.items.size();
+    c.img = L.slot0.size();
+    std::vector<SItem> items;
+    for (i64 j = 0; j < c.nimg; ++j) {
+      const i64 a = off[c.img0 + j], b = off[c.img0 + j + 1];
+      L.slot0.push_back((int)items.size());
+      L.row0.push_back(a);
+      for (i64 r = a; r < b; r += itemRows) items.push_back({r, std::min(b, r + itemRows), (int)items.size(), 0});
+    }
+    L.slot0.push_back((int)items.size());
+    L.row0.push_back(off[img]);
+    c.nitems = (int)items.size();
+    c.gx = std::max(1, std::min(c.nitems, nsm));
+    std::vector<int> order, beg;
+    lpt_assign(items, c.gx, order, beg);
+    c.beg = L.beg.size();
+    L.items.insert(L.items.end(), items.begin(), items.end());
+    L.order.insert(L.order.end(), order.begin(), order.end());
+    L.beg.insert(L.beg.end(), beg.begin(), beg.end());
+    L.maxRows = std::max(L.maxRows, c.nrows);
+    L.maxTiles = std::max(L.maxTiles, (c.nrows + 127) / 128);
+    L.maxItems = std::max(L.maxItems, c.nitems);
+    L.chunks.push_back(c);
+  }
+}
+
+// Scratch slots of the batched encoder (each encoder owns its arena):
+// 0-2, 12 model prep; 3 error word; 4 q image; 5 row counts; 6 item
+// partials; 7-11 layout tables; 13-17 Fisher constants; 18 router posteriors.
+template <typename T>
+T *upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s) {
+  T *d = b.get<T>(std::max<size_t>(1, v.size()));
+  if (!v.empty()) VLB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+void fv_upload(const FvLayout &L, int Kp, int Kq, int NST, bool fp32, Scratch &sc, cudaStream_t s) {
+  const size_t qsz = fp32 ? 4 : 2;
+  sc.slot[4].get<char>((size_t)std::max<i64>(1, L.maxTiles) * 128 * Kq * qsz);
+  sc.slot[5].get<unsigned>(std::max<i64>(1, L.maxRows));
+  sc.slot[6].get<float>((size_t)std::max(1, L.maxItems) * Kp * NST);
+  upload(sc.slot[7], L.items, s);
+  upload(sc.slot[8], L.order, s);
+  upload(sc.slot[9], L.beg, s);
+  upload(sc.slot[10], L.slot0, s);
+  upload(sc.slot[11], L.row0, s);
+}
+
+// All launches of one batched encode; no host copies, no synchronisation and,
+// once the scratch is sized by fv_upload and one earlier run, no allocation.
+void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float> &m, float *enc,
+            unsigned long long *nterms, int flags, int precision, const TcFvConfig &cfg, cudaStream_t s) {
   const bool fp32 = (precision == VLB200_PREC_FP32);
   TcPrep tp;
-  tc_prepare(m, tp, !fp32, s);
+  tc_prepare(m, tp, !fp32, sc, s);
   const int qf = fp32 ? kQImg32 : kQImg16;
   const int split = fp32 ? 2 : 1;
-  const size_t qsz = fp32 ? 4 : 2;  // bytes per q element over the image parts
   const int Kq = padQ(tp.Kp);
   const i64 K = m.K, D = m.D;
-  const int NST = (int)(2 * D + 16);
   int *err = sc.slot[3].get<int>(1);
   VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  const i64 kRowBudget = std::max<i64>(1 << 16, (i64)(4ull << 30) / (tp.Kp * (i64)qsz));
-  const i64 kItemRows = 8192;
-  const int nsm = num_sms();
   double *cmu = sc.slot[13].get<double>(K * D), *cis2 = sc.slot[14].get<double>(K * D);
   double *cisd = sc.slot[15].get<double>(K * D), *cup = sc.slot[16].get<double>(K);
   double *cvp = sc.slot[17].get<double>(K);
   VLB_LAUNCH("tc_fv_consts", s,
              k_tc_fv_consts<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
                  m.means, m.covs, m.priors, tp.ctr, (int)K, (int)D, cmu, cis2, cisd, cup, cvp));
-
-  i64 img = 0;
-  while (img < numImages) {
-    const i64 chunkImg0 = img, row0 = h_offsets[img];
-    while (img < numImages && (img == chunkImg0 || h_offsets[img + 1] - row0 <= kRowBudget)) ++img;
-    const i64 nimg = img - chunkImg0, row1 = h_offsets[img], nrows = row1 - row0;
-    // Work items: runs of at most kItemRows rows of one image; images with no
-    // rows get no item (their statistics are zero).
-    std::vector<SItem> items;
-    std::vector<int> slot0(nimg + 1);
-    std::vector<i64> imgRow0(nimg + 1);
-    for (i64 j = 0; j < nimg; ++j) {
-      const i64 a = h_offsets[chunkImg0 + j], b = h_offsets[chunkImg0 + j + 1];
-      slot0[j] = (int)items.size();
-      imgRow0[j] = a;
-      for (i64 r = a; r < b; r += kItemRows) items.push_back({r, std::min(b, r + kItemRows), (int)items.size(), 0});
-    }
-    slot0[nimg] = (int)items.size();
-    imgRow0[nimg] = row1;
-    const int nitems = (int)items.size();
-    const int gx = std::max(1, std::min(nitems, nsm));
-    std::vector<int> order, beg;
-    lpt_assign(items, gx, order, beg);
-
-    const i64 ntiles = (nrows + 127) / 128;
-    void *q = sc.slot[4].get<char>((size_t)std::max<i64>(1, ntiles) * 128 * Kq * qsz);
-    unsigned *rowcnt = sc.slot[5].get<unsigned>(std::max<i64>(1, nrows));
-    float *partial = sc.slot[6].get<float>((size_t)std::max(1, nitems) * tp.Kp * NST);
-    SItem *ditems = sc.slot[7].get<SItem>(std::max(1, nitems));
-    int *dorder = sc.slot[8].get<int>(std::max(1, nitems));
-    int *dbeg = sc.slot[9].get<int>(gx + 1);
-    int *dslot0 = sc.slot[10].get<int>(nimg + 1);
-    i64 *drow0 = sc.slot[11].get<i64>(nimg + 1);
-    if (nitems) {
-      VLB_CUDA(cudaMemcpyAsync(ditems, items.data(), sizeof(SItem) * nitems, cudaMemcpyHostToDevice, s));
-      VLB_CUDA(cudaMemcpyAsync(dorder, order.data(), sizeof(int) * nitems, cudaMemcpyHostToDevice, s));
-    }
-    VLB_CUDA(cudaMemcpyAsync(dbeg, beg.data(), sizeof(int) * (gx + 1), cudaMemcpyHostToDevice, s));
-    VLB_CUDA(cudaMemcpyAsync(dslot0, slot0.data(), sizeof(int) * (nimg + 1), cudaMemcpyHostToDevice, s));
-    VLB_CUDA(cudaMemcpyAsync(drow0, imgRow0.data(), sizeof(i64) * (nimg + 1), cudaMemcpyHostToDevice, s));
-
-    if (nrows > 0) {
+  void *q = sc.slot[4].p;
+  unsigned *rowcnt = (unsigned *)sc.slot[5].p;
+  float *partial = (float *)sc.slot[6].p;
+  const SItem *ditems = (const SItem *)sc.slot[7].p;
+  const int *dorder = (const int *)sc.slot[8].p, *dbeg = (const int *)sc.slot[9].p;
+  const int *dslot0 = (const int *)sc.slot[10].p;
+  const i64 *drow0 = (const i64 *)sc.slot[11].p;
+  auto fin = D == 64 ? k_tc_fv_finalize<64> : D == 80 ? k_tc_fv_finalize<80> : k_tc_fv_finalize<128>;
+  for (const FvChunk &c : L.chunks) {
+    const i64 ntiles = (c.nrows + 127) / 128;
+    if (c.nrows > 0) {
       if (precision == VLB200_PREC_BF16_ROUTER) {
         // Router posteriors (row-major) -> fp16 operand image + row counts.
-        float *qrows = sc.slot[18].get<float>((size_t)nrows * K);
-        router_default_posteriors(X + row0 * D, nrows, m, qrows, s);
+        float *qrows = sc.slot[18].get<float>((size_t)L.maxRows * K);
+        router_default_posteriors(X + c.row0 * D, c.nrows, m, qrows, s);
         const i64 rowsPad = ntiles * 128;
         VLB_LAUNCH("tc_rows_to_image", s,
                    k_rows_to_image16<<<(unsigned)((rowsPad + 7) / 8), 256, 0, s>>>(
-                       qrows, nrows, (int)K, Kq, 1e-6f, (__half *)q, rowcnt, rowsPad, (flags & 4) != 0));
+                       qrows, c.nrows, (int)K, Kq, 1e-6f, (__half *)q, rowcnt, rowsPad, (flags & 4) != 0));
       } else {
-        estep_dispatch(tp.D, qf, X + row0 * D, nrows, tp, q, (int)K, (flags & 4) != 0, rowcnt, nullptr, err, s);
+        estep_dispatch(tp.D, qf, X + c.row0 * D, c.nrows, tp, q, (int)K, (flags & 4) != 0, rowcnt, nullptr,
+                       err, cfg.estepStages, s);
       }
       SParams sp;
-      sp.X = X; sp.qimg = (const uint8_t *)q; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = row0;
+      sp.X = X; sp.qimg = (const uint8_t *)q; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = c.row0;
       sp.K = (int)K; sp.Kp = tp.Kp; sp.Kq = Kq; sp.nst = 0;
       sp.ctr = tp.ctr; sp.scale = fp32 ? nullptr : tp.scale;
-      sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg; sp.partial = partial; sp.err = err;
-      stats_dispatch(tp.D, split, sp, gx, s);
+      sp.items = ditems + c.items; sp.order = dorder + c.items; sp.cta_beg = dbeg + c.beg;
+      sp.partial = partial; sp.err = err;
+      stats_dispatch(tp.D, split, sp, c.gx, cfg.statsMT, cfg.statsStages, s);
     }
-    auto fin = D == 64 ? k_tc_fv_finalize<64> : D == 80 ? k_tc_fv_finalize<80> : k_tc_fv_finalize<128>;
     VLB_LAUNCH("tc_fv_finalize", s,
-               fin<<<(unsigned)nimg, 256, 0, s>>>(
-                   (int)K, tp.Kp, partial, dslot0, drow0, cmu, cis2, cisd, cup, cvp,
-                   fp32 ? nullptr : tp.scale, nrows > 0 ? rowcnt : nullptr, row0, flags, chunkImg0,
-                   enc, nterms));
+               fin<<<(unsigned)c.nimg, 256, 0, s>>>(
+                   (int)K, tp.Kp, partial, dslot0 + c.img, drow0 + c.img, cmu, cis2, cisd, cup, cvp,
+                   fp32 ? nullptr : tp.scale, c.nrows > 0 ? rowcnt : nullptr, c.row0, flags, c.img0, enc,
+                   nterms));
   }
-  check_err(err, s);
+}
+
+}  // namespace
+
+void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const DevModel<float> &m,
+                     float *enc, unsigned long long *nterms, int flags, int precision, cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaTc);
+  const bool fp32 = (precision == VLB200_PREC_FP32);
+  const int Kp = padK(m.K);
+  TcFvConfig cfg;
+  FvLayout L;
+  fv_layout(h_offsets, numImages, default_row_budget(Kp, fp32), cfg.itemRows, num_sms(), L);
+  fv_upload(L, Kp, padQ(Kp), (int)(2 * m.D + 16), fp32, sc, s);
+  fv_run(L, sc, X, m, enc, nterms, flags, precision, cfg, s);
+  check_err((int *)sc.slot[3].p, s);
+}
+
+// A batch encoder bound to one batch layout: it owns its scratch arena and
+// device tables, so that run() only launches kernels and can be captured.
+struct TcFvPlan {
+  i64 D = 0, K = 0, numImages = 0;
+  int flags = 0, precision = 0, Kp = 0;
+  std::vector<i64> offsets;
+  TcFvConfig cfg;
+  FvLayout layout;
+  Scratch sc;
+};
+
+namespace {
+void plan_build(TcFvPlan &p, cudaStream_t s) {
+  const bool fp32 = (p.precision == VLB200_PREC_FP32);
+  const i64 budget = p.cfg.rowBudget > 0 ? p.cfg.rowBudget : default_row_budget(p.Kp, fp32);
+  fv_layout(p.offsets.data(), p.numImages, budget, p.cfg.itemRows, num_sms(), p.layout);
+  fv_upload(p.layout, p.Kp, padQ(p.Kp), (int)(2 * p.D + 16), fp32, p.sc, s);
+  VLB_CUDA(cudaStreamSynchronize(s));
+}
+}  // namespace
+
+TcFvPlan *tc_fv_plan_new(i64 D, i64 K, const i64 *offsets, i64 numImages, int flags, int precision,
+                         cudaStream_t s) {
+  VLB_CHECK(tc_supported(K, D), VL_ERR_BAD_ARG, "batched Fisher plan: unsupported (numClusters, dimension)");
+  VLB_CHECK(precision == VLB200_PREC_FP32 || precision == VLB200_PREC_BF16 ||
+                precision == VLB200_PREC_BF16_ROUTER,
+            VL_ERR_BAD_ARG, "batched Fisher plan: precision must be FP32, BF16 or BF16_ROUTER");
+  VLB_CHECK(numImages >= 0 && offsets != nullptr, VL_ERR_BAD_ARG, "batched Fisher plan: bad offsets");
+  for (i64 j = 0; j < numImages; ++j)
+    VLB_CHECK(offsets[j + 1] >= offsets[j], VL_ERR_BAD_ARG, "batched Fisher plan: offsets must not decrease");
+  auto p = std::make_unique<TcFvPlan>();
+  p->D = D; p->K = K; p->numImages = numImages; p->flags = flags; p->precision = precision;
+  p->Kp = padK(K);
+  p->offsets.assign(offsets, offsets + numImages + 1);
+  plan_build(*p, s);
+  return p.release();
+}
+
+void tc_fv_plan_delete(TcFvPlan *p) { delete p; }
+
+TcFvConfig tc_fv_plan_config(const TcFvPlan *p) { return p->cfg; }
+
+void tc_fv_plan_set_config(TcFvPlan *p, const TcFvConfig &c, cudaStream_t s) {
+  VLB_CHECK(c.itemRows >= 128 && c.itemRows % 128 == 0, VL_ERR_BAD_ARG, "plan config: itemRows must be a positive multiple of 128");
+  VLB_CHECK(c.statsMT >= 0 && c.statsMT <= 2, VL_ERR_BAD_ARG, "plan config: statsMT must be 0, 1 or 2");
+  VLB_CHECK(c.statsStages >= 0 && c.estepStages >= 0 && c.rowBudget >= 0, VL_ERR_BAD_ARG, "plan config: negative value");
+  VLB_CHECK(c.statsStages != 1 && c.estepStages != 1, VL_ERR_BAD_ARG, "plan config: at least two operand stages");
+  VLB_CUDA(cudaStreamSynchronize(s));  // earlier runs may still read the tables
+  p->cfg = c;
+  plan_build(*p, s);
+}
+
+void tc_fv_plan_run(TcFvPlan *p, const DevModel<float> &m, const float *X, float *enc,
+                    unsigned long long *nterms, cudaStream_t s) {
+  VLB_CHECK(m.K == p->K && m.D == p->D, VL_ERR_BAD_ARG, "batched Fisher plan: model shape differs from the plan");
+  fv_run(p->layout, p->sc, X, m, enc, nterms, p->flags, p->precision, p->cfg, s);
+}
+
+int tc_fv_plan_error(TcFvPlan *p, cudaStream_t s) {
+  int h = 0;
+  VLB_CUDA(cudaMemcpyAsync(&h, p->sc.slot[3].p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+// Times each candidate configuration on the plan's own batch (one warm-up
+// run, then the median of three runs timed with CUDA events on the stream)
+// and keeps the fastest.  Candidates: statistics item rows, statistics
+// M tiles per CTA, operand stages of both kernels and the chunk row budget.
+TcFvConfig tc_fv_plan_autotune(TcFvPlan *p, const DevModel<float> &m, const float *X, float *enc,
+                               unsigned long long *nterms, cudaStream_t s, double *best_ms) {
+  const bool fp32 = (p->precision == VLB200_PREC_FP32);
+  const i64 total = p->offsets.back() - p->offsets.front();
+  std::vector<TcFvConfig> cands;
+  const i64 whole = std::max<i64>(total, 1);
+  const i64 qsz = fp32 ? 4 : 2;
+  // A single chunk when its q image fits in 16 GB; else the default budget.
+  const i64 big = std::min<i64>(whole, (i64)(16ull << 30) / (p->Kp * qsz));
+  for (int itemRows : {4096, 8192, 16384})
+    for (int mt : {0, 1})
+      for (int est : {0, 2})
+        for (i64 budget : {(i64)0, big}) {
+          TcFvConfig c;
+          c.itemRows = itemRows; c.statsMT = mt; c.estepStages = est; c.rowBudget = budget;
+          cands.push_back(c);
+        }
+  cudaEvent_t e0, e1;
+  VLB_CUDA(cudaEventCreate(&e0));
+  VLB_CUDA(cudaEventCreate(&e1));
+  TcFvConfig best = p->cfg;
+  double bms = 1e300;
+  try {
+    for (const TcFvConfig &c : cands) {
+      tc_fv_plan_set_config(p, c, s);
+      tc_fv_plan_run(p, m, X, enc, nterms, s);  // warm-up (sizes every buffer)
+      float t[3];
+      for (float &ti : t) {
+        VLB_CUDA(cudaEventRecord(e0, s));
+        tc_fv_plan_run(p, m, X, enc, nterms, s);
+        VLB_CUDA(cudaEventRecord(e1, s));
+        VLB_CUDA(cudaEventSynchronize(e1));
+        VLB_CUDA(cudaEventElapsedTime(&ti, e0, e1));
+      }
+      std::sort(t, t + 3);
+      VLB_CHECK(tc_fv_plan_error(p, s) == 0, VL_ERR_BAD_ARG, "autotune: a candidate kernel gave up waiting");
+      if (t[1] < bms) {
+        bms = t[1];
+        best = c;
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  tc_fv_plan_set_config(p, best, s);
+  if (best_ms) *best_ms = bms;
+  return best;
 }
 
 }  // namespace vlb

@@ -179,6 +179,8 @@ void launch_begin(const char *name, cudaStream_t s) {
 }
 
 void count_launch() { g_launches.fetch_add(1); }
+void count_launches(unsigned long long n) { g_launches.fetch_add(n); }
+bool profile_swap(bool on) { return g_profile.exchange(on ? 1 : 0) != 0; }
 
 void launch_end(const char *name, cudaStream_t s) {
   g_launches.fetch_add(1);
