@@ -125,6 +125,15 @@ VL_EXPORT int vlb200_fisher_plan_set_gmm(VlB200FisherPlan *plan, float const *me
                                          float const *covariances, float const *priors);
 VL_EXPORT int vlb200_fisher_plan_execute(VlB200FisherPlan *plan, float *enc, float const *data,
                                          vl_uint64 *numTerms, void *stream);
+/* The same encode from HOST buffers (data: the batch's rows, enc: numImages x
+ * 2DK, numTerms: numImages or NULL), like vl_fisher_encode: the batch is cut
+ * into about 16 chunks of whole images whose host -> device copies, encodes
+ * and device -> host copies overlap on three streams.  Returns when the
+ * results are on the host.  Page-locked buffers (cudaHostAlloc,
+ * cudaHostRegister) are needed for the copies to overlap. */
+VL_EXPORT int vlb200_fisher_plan_execute_host(VlB200FisherPlan *plan, float *enc,
+                                              float const *data, vl_uint64 *numTerms,
+                                              void *stream);
 VL_EXPORT int vlb200_fisher_plan_autotune(VlB200FisherPlan *plan, float *enc, float const *data,
                                           vl_uint64 *numTerms, void *stream, double *bestMs);
 VL_EXPORT int vlb200_fisher_plan_get_config(VlB200FisherPlan const *plan, vl_int64 config[5]);

@@ -172,3 +172,35 @@ def test_plan_rejects(vl, batch):
         p.set_config(item_rows=100)  # not a multiple of 128
     with pytest.raises(vl.VLError):
         p.launch()  # nothing captured
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_plan_execute_host(vl, batch, refs, pinned):
+    """Host buffers in and out, copies overlapped chunk by chunk.  The
+    host-buffer layout cuts the batch into more E-step chunks than the device
+    execute; the statistics kernel groups rows into MMA k-steps by their
+    position in the chunk's posterior image, so the fp32 accumulation order,
+    not the arithmetic, changes: results agree to 1e-6 relative, term counts
+    exactly."""
+    import torch
+    pr, mu, cv, offs, x = batch
+    p, g = _plan(vl, batch, "bf16")
+    xh = torch.from_numpy(x.copy())
+    enc_h = torch.zeros((len(COUNTS), 2 * K * D))
+    nt_h = torch.zeros(len(COUNTS), dtype=torch.int64)
+    if pinned:
+        xh, enc_h, nt_h = xh.pin_memory(), enc_h.pin_memory(), nt_h.pin_memory()
+    p.execute_host(enc_h, xh, nt_h)
+    enc, nt = _out(len(COUNTS))
+    p.execute(enc, _t(x), nt)
+    torch.cuda.synchronize()
+    dev = enc.cpu().numpy()
+    for j in range(len(COUNTS)):
+        assert rel_err(enc_h.numpy()[j], dev[j]) <= 1e-6, j
+    assert np.array_equal(nt_h.numpy(), nt.cpu().numpy())
+    # numpy buffers, no term counts, a second call reusing the plan's buffers:
+    # the same layout as the first call, so the same bits.
+    enc_np = np.zeros((len(COUNTS), 2 * K * D), np.float32)
+    p.execute_host(enc_np, np.ascontiguousarray(x))
+    assert np.array_equal(enc_np, enc_h.numpy())
+    _check(torch.from_numpy(enc_np), nt, refs, "bf16")

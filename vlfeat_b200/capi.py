@@ -101,6 +101,7 @@ def _decl(L):
     f("vlb200_fisher_plan_delete", None, _vp)
     f("vlb200_fisher_plan_set_gmm", C.c_int, _vp, _vp, _vp, _vp)
     f("vlb200_fisher_plan_execute", C.c_int, _vp, _vp, _vp, _vp, _vp)
+    f("vlb200_fisher_plan_execute_host", C.c_int, _vp, _vp, _vp, _vp, _vp)
     f("vlb200_fisher_plan_autotune", C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_double))
     f("vlb200_fisher_plan_get_config", C.c_int, _vp, _vp)
     f("vlb200_fisher_plan_set_config", C.c_int, _vp, _vp, _vp)
@@ -449,6 +450,18 @@ class FisherPlan:
             self._h, enc_t.data_ptr(), data_t.data_ptr(),
             nterms_t.data_ptr() if nterms_t is not None else None, _stream(stream)),
             "vlb200_fisher_plan_execute")
+
+    def execute_host(self, enc, data, nterms=None, stream=None):
+        """Host buffers (numpy arrays or CPU torch tensors; page-locked ones let
+        the copies overlap the encode).  Returns when the results are written."""
+        def ptr(a):
+            if a is None:
+                return None
+            return a.data_ptr() if hasattr(a, "data_ptr") else _np_ptr(a)
+        _clear()
+        self._check(lib().vlb200_fisher_plan_execute_host(self._h, ptr(enc), ptr(data), ptr(nterms),
+                                                          _stream(stream)),
+                    "vlb200_fisher_plan_execute_host")
 
     def autotune(self, enc_t, data_t, nterms_t=None, stream=None) -> float:
         ms = C.c_double(0)

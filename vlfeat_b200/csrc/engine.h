@@ -134,6 +134,10 @@ void tc_fv_plan_set_config(TcFvPlan *p, const TcFvConfig &c, cudaStream_t s);
 void tc_fv_plan_run(TcFvPlan *p, const DevModel<float> &m, const float *X, float *enc,
                     unsigned long long *nterms, cudaStream_t s);
 int tc_fv_plan_error(TcFvPlan *p, cudaStream_t s);  // the kernels' error word (synchronises)
+// Host buffers in and out, copies overlapped with the encode chunk by chunk;
+// returns when the encodings are on the host.
+void tc_fv_plan_run_host(TcFvPlan *p, const DevModel<float> &m, const float *Xh, float *ench,
+                         unsigned long long *nth, cudaStream_t s);
 TcFvConfig tc_fv_plan_autotune(TcFvPlan *p, const DevModel<float> &m, const float *X, float *enc,
                                unsigned long long *nterms, cudaStream_t s, double *best_ms);
 

@@ -115,6 +115,16 @@ int vlb200_fisher_plan_execute(VlB200FisherPlan *plan, float *enc, float const *
   });
 }
 
+int vlb200_fisher_plan_execute_host(VlB200FisherPlan *plan, float *enc, float const *data,
+                                    vl_uint64 *numTerms, void *stream) {
+  return guarded([&] {
+    need_model(plan);
+    VLB_CHECK(enc != nullptr && data != nullptr, VL_ERR_BAD_ARG, "NULL argument");
+    vlb::tc_fv_plan_run_host(plan->plan, plan->model, data, enc, (unsigned long long *)numTerms,
+                             vlb::pick_stream(stream));
+  });
+}
+
 int vlb200_fisher_plan_autotune(VlB200FisherPlan *plan, float *enc, float const *data,
                                 vl_uint64 *numTerms, void *stream, double *bestMs) {
   return guarded([&] {

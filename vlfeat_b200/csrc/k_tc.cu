@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <functional>
 #include <memory>
 #include <numeric>
 #include <vector>
@@ -1241,10 +1242,14 @@ void fv_upload(const FvLayout &L, int Kp, int Kq, int NST, bool fp32, Scratch &s
   upload(sc.slot[11], L.row0, s);
 }
 
+// Called with a chunk's index before its launches and after its finalize.
+using ChunkHook = std::function<void(size_t)>;
+
 // All launches of one batched encode; no host copies, no synchronisation and,
 // once the scratch is sized by fv_upload and one earlier run, no allocation.
 void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float> &m, float *enc,
-            unsigned long long *nterms, int flags, int precision, const TcFvConfig &cfg, cudaStream_t s) {
+            unsigned long long *nterms, int flags, int precision, const TcFvConfig &cfg, cudaStream_t s,
+            const ChunkHook &before = nullptr, const ChunkHook &after = nullptr) {
   const bool fp32 = (precision == VLB200_PREC_FP32);
   TcPrep tp;
   tc_prepare(m, tp, !fp32, sc, s);
@@ -1268,7 +1273,9 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
   const int *dslot0 = (const int *)sc.slot[10].p;
   const i64 *drow0 = (const i64 *)sc.slot[11].p;
   auto fin = D == 64 ? k_tc_fv_finalize<64> : D == 80 ? k_tc_fv_finalize<80> : k_tc_fv_finalize<128>;
-  for (const FvChunk &c : L.chunks) {
+  for (size_t ci = 0; ci < L.chunks.size(); ++ci) {
+    const FvChunk &c = L.chunks[ci];
+    if (before) before(ci);
     const i64 ntiles = (c.nrows + 127) / 128;
     if (c.nrows > 0) {
       if (precision == VLB200_PREC_BF16_ROUTER) {
@@ -1296,6 +1303,7 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
                    (int)K, tp.Kp, partial, dslot0 + c.img, drow0 + c.img, cmu, cis2, cisd, cup, cvp,
                    fp32 ? nullptr : tp.scale, c.nrows > 0 ? rowcnt : nullptr, c.row0, flags, c.img0, enc,
                    nterms));
+    if (after) after(ci);
   }
 }
 
@@ -1323,6 +1331,32 @@ struct TcFvPlan {
   TcFvConfig cfg;
   FvLayout layout;
   Scratch sc;
+  // Host-buffer execution: a layout of about kPipeChunks chunks whose
+  // host -> device copies, encodes and device -> host copies overlap.
+  static constexpr int kPipeChunks = 16;
+  bool pipeBuilt = false;
+  FvLayout pipe;
+  Scratch scPipe;
+  DevBuf xdev, encdev, ntdev;
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t evStart = nullptr, evEnd = nullptr;
+  std::vector<cudaEvent_t> evIn, evOut;
+
+  void drop_pipe() {
+    for (cudaEvent_t e : evIn) cudaEventDestroy(e);
+    for (cudaEvent_t e : evOut) cudaEventDestroy(e);
+    evIn.clear();
+    evOut.clear();
+    pipeBuilt = false;
+  }
+  ~TcFvPlan() {
+    cudaDeviceSynchronize();
+    drop_pipe();
+    if (evStart) cudaEventDestroy(evStart);
+    if (evEnd) cudaEventDestroy(evEnd);
+    if (h2d) cudaStreamDestroy(h2d);
+    if (d2h) cudaStreamDestroy(d2h);
+  }
 };
 
 namespace {
@@ -1363,6 +1397,7 @@ void tc_fv_plan_set_config(TcFvPlan *p, const TcFvConfig &c, cudaStream_t s) {
   VLB_CHECK(c.statsStages != 1 && c.estepStages != 1, VL_ERR_BAD_ARG, "plan config: at least two operand stages");
   VLB_CUDA(cudaStreamSynchronize(s));  // earlier runs may still read the tables
   p->cfg = c;
+  p->drop_pipe();
   plan_build(*p, s);
 }
 
@@ -1372,11 +1407,73 @@ void tc_fv_plan_run(TcFvPlan *p, const DevModel<float> &m, const float *X, float
   fv_run(p->layout, p->sc, X, m, enc, nterms, p->flags, p->precision, p->cfg, s);
 }
 
-int tc_fv_plan_error(TcFvPlan *p, cudaStream_t s) {
-  int h = 0;
-  VLB_CUDA(cudaMemcpyAsync(&h, p->sc.slot[3].p, sizeof(int), cudaMemcpyDeviceToHost, s));
+// Host buffers in and out: the chunks' host -> device copies (stream h2d),
+// encodes (stream s) and device -> host copies (stream d2h) overlap, ordered
+// by per-chunk events.  Overlap needs page-locked host buffers; the call
+// returns when the encodings are on the host.
+void tc_fv_plan_run_host(TcFvPlan *p, const DevModel<float> &m, const float *Xh, float *ench,
+                         unsigned long long *nth, cudaStream_t s) {
+  VLB_CHECK(m.K == p->K && m.D == p->D, VL_ERR_BAD_ARG, "batched Fisher plan: model shape differs from the plan");
+  const bool fp32 = (p->precision == VLB200_PREC_FP32);
+  const i64 row0 = p->offsets.front(), total = p->offsets.back() - row0;
+  const i64 D = p->D, FV = 2 * p->K * p->D;
+  if (!p->pipeBuilt) {
+    const i64 budget = std::max<i64>(1, (total + TcFvPlan::kPipeChunks - 1) / TcFvPlan::kPipeChunks);
+    fv_layout(p->offsets.data(), p->numImages, budget, p->cfg.itemRows, num_sms(), p->pipe);
+    fv_upload(p->pipe, p->Kp, padQ(p->Kp), (int)(2 * p->D + 16), fp32, p->scPipe, s);
+    if (!p->h2d) VLB_CUDA(cudaStreamCreateWithFlags(&p->h2d, cudaStreamNonBlocking));
+    if (!p->d2h) VLB_CUDA(cudaStreamCreateWithFlags(&p->d2h, cudaStreamNonBlocking));
+    if (!p->evStart) VLB_CUDA(cudaEventCreateWithFlags(&p->evStart, cudaEventDisableTiming));
+    if (!p->evEnd) VLB_CUDA(cudaEventCreateWithFlags(&p->evEnd, cudaEventDisableTiming));
+    p->evIn.resize(p->pipe.chunks.size(), nullptr);
+    p->evOut.resize(p->pipe.chunks.size(), nullptr);
+    for (auto *v : {&p->evIn, &p->evOut})
+      for (cudaEvent_t &e : *v) VLB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    VLB_CUDA(cudaStreamSynchronize(s));
+    p->pipeBuilt = true;
+  }
+  // Device images of the batch: rows row0.. of X, all images of enc.
+  float *Xd = p->xdev.get<float>((size_t)std::max<i64>(1, total) * D) - row0 * D;
+  float *encd = p->encdev.get<float>((size_t)std::max<i64>(1, p->numImages) * FV);
+  unsigned long long *ntd = p->ntdev.get<unsigned long long>(std::max<i64>(1, p->numImages));
+  // This call's copies start after the work already queued on s (an earlier
+  // call's encode still reading these device buffers).
+  VLB_CUDA(cudaEventRecord(p->evStart, s));
+  VLB_CUDA(cudaStreamWaitEvent(p->h2d, p->evStart, 0));
+  VLB_CUDA(cudaStreamWaitEvent(p->d2h, p->evStart, 0));
+  const std::vector<FvChunk> &ch = p->pipe.chunks;
+  for (size_t ci = 0; ci < ch.size(); ++ci) {
+    if (ch[ci].nrows > 0)
+      VLB_CUDA(cudaMemcpyAsync(Xd + ch[ci].row0 * D, Xh + (ch[ci].row0 - row0) * D,
+                               sizeof(float) * ch[ci].nrows * D, cudaMemcpyHostToDevice, p->h2d));
+    VLB_CUDA(cudaEventRecord(p->evIn[ci], p->h2d));
+  }
+  fv_run(p->pipe, p->scPipe, Xd, m, encd, ntd, p->flags, p->precision, p->cfg, s,
+         [&](size_t ci) { VLB_CUDA(cudaStreamWaitEvent(s, p->evIn[ci], 0)); },
+         [&](size_t ci) {
+           const FvChunk &c = ch[ci];
+           VLB_CUDA(cudaEventRecord(p->evOut[ci], s));
+           VLB_CUDA(cudaStreamWaitEvent(p->d2h, p->evOut[ci], 0));
+           VLB_CUDA(cudaMemcpyAsync(ench + c.img0 * FV, encd + c.img0 * FV, sizeof(float) * c.nimg * FV,
+                                    cudaMemcpyDeviceToHost, p->d2h));
+           if (nth)
+             VLB_CUDA(cudaMemcpyAsync(nth + c.img0, ntd + c.img0, sizeof(unsigned long long) * c.nimg,
+                                      cudaMemcpyDeviceToHost, p->d2h));
+         });
+  VLB_CUDA(cudaEventRecord(p->evEnd, p->d2h));
+  VLB_CUDA(cudaStreamWaitEvent(s, p->evEnd, 0));
   VLB_CUDA(cudaStreamSynchronize(s));
-  return h;
+  VLB_CHECK(tc_fv_plan_error(p, s) == 0, VL_ERR_BAD_ARG, "tensor-core kernel gave up waiting");
+}
+
+int tc_fv_plan_error(TcFvPlan *p, cudaStream_t s) {
+  int h[2] = {0, 0};
+  if (p->sc.slot[3].p)
+    VLB_CUDA(cudaMemcpyAsync(&h[0], p->sc.slot[3].p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (p->scPipe.slot[3].p)
+    VLB_CUDA(cudaMemcpyAsync(&h[1], p->scPipe.slot[3].p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  return h[0] ? h[0] : h[1];
 }
 
 // Times each candidate configuration on the plan's own batch (one warm-up
