@@ -421,6 +421,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--images", type=int, default=4096,
                     help="encode only the first IMAGES images of the workload (small profiling cases)")
+    ap.add_argument("--plan", default=None,
+                    help="fixed plan configuration instead of autotuning, e.g. "
+                         "item_rows=4096,row_budget=0 (keys of FisherPlan.get_config)")
     args = ap.parse_args()
     global NUM_IMAGES
     NUM_IMAGES = args.images
@@ -457,8 +460,11 @@ def main():
     eager_of = {}
     s = torch.cuda.current_stream()
     encoders = {}
+    fixed = None
+    if args.plan:
+        fixed = {k: int(v) for k, v in (kv.split("=") for kv in args.plan.split(","))}
     for p in args.paths.split(","):  # plans: autotuned and captured before the timed regions
-        encoders[p] = make_encoder(capi, wl, wl["x"], enc, nt, p, s)
+        encoders[p] = make_encoder(capi, wl, wl["x"], enc, nt, p, s, config=fixed)
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for p in args.paths.split(","):
             run, eager, info = encoders[p]

@@ -36,6 +36,8 @@
 #include <numeric>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "engine.h"
 #include "tc_common.cuh"
 
@@ -48,6 +50,7 @@ namespace vlb {
 namespace {
 
 using namespace tc;
+namespace cg = cooperative_groups;
 
 constexpr int kTcThreads = 416;  // E-step: 4 producer, 8 epilogue, 1 MMA warp
 constexpr int kSmemLimit = 232448;  // 227 KB opt-in per block
@@ -71,13 +74,21 @@ __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
 }
 
 // ================================================================ prep
-// Centre m_d = mean over components of mu_kd.
+// Sum over the 32 lanes in a fixed butterfly order (the same bits every run).
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Centre m_d = mean over components of mu_kd.  One warp per dimension.
 __global__ void k_tc_center(const float *__restrict__ means, int K, int D, float *__restrict__ ctr) {
-  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  const int d = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x % 32;
   if (d >= D) return;
   double s = 0;
-  for (int k = 0; k < K; ++k) s += (double)means[(i64)k * D + d];
-  ctr[d] = (float)(s / (double)K);
+  for (int k = lane; k < K; k += 32) s += (double)means[(i64)k * D + d];
+  s = warp_sum(s);
+  if (lane == 0) ctr[d] = (float)(s / (double)K);
 }
 
 // W image (hi then lo), K-major 64-byte-swizzled k-atoms of 32 elements:
@@ -114,19 +125,21 @@ __global__ void k_tc_wimg(const float *__restrict__ means, const float *__restri
 __global__ void k_tc_cst(const float *__restrict__ priors, const float *__restrict__ means,
                          const float *__restrict__ covs, const float *__restrict__ ctr, int K,
                          int Kp, int D, float *__restrict__ cst2) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // One warp per component; lanes take dimensions d = lane, lane + 32, ...
+  const int k = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x % 32;
   if (k >= Kp) return;
   if (k >= K || (double)priors[k] < 1e-6) {
-    cst2[k] = -INFINITY;
+    if (lane == 0) cst2[k] = -INFINITY;
     return;
   }
-  double c = log((double)priors[k]) - 0.5 * (double)D * log(2.0 * 3.141592653589793);
-  for (int d = 0; d < D; ++d) {
+  double c = 0;
+  for (int d = lane; d < D; d += 32) {
     const double s2 = (double)covs[(i64)k * D + d];
     const double mup = (double)means[(i64)k * D + d] - (double)ctr[d];
-    c -= 0.5 * log(s2) + 0.5 * mup * mup / s2;
+    c += 0.5 * log(s2) + 0.5 * mup * mup / s2;
   }
-  cst2[k] = (float)(c * 1.4426950408889634);
+  c = log((double)priors[k]) - 0.5 * (double)D * log(2.0 * 3.141592653589793) - warp_sum(c);
+  if (lane == 0) cst2[k] = (float)(c * 1.4426950408889634);
 }
 
 // Per-dimension power-of-two scale for fp16 statistics operands, chosen from
@@ -134,13 +147,17 @@ __global__ void k_tc_cst(const float *__restrict__ priors, const float *__restri
 // scale_d = 2^-ceil(log2(max_k |mu'_kd| + 4 sigma_kd)).
 __global__ void k_tc_scale(const float *__restrict__ means, const float *__restrict__ covs,
                            const float *__restrict__ ctr, int K, int D, float *__restrict__ scale) {
-  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  // One warp per dimension; the maximum does not depend on the order.
+  const int d = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x % 32;
   if (d >= D) return;
   double b = 0;
-  for (int k = 0; k < K; ++k) {
+  for (int k = lane; k < K; k += 32) {
     const double v = fabs((double)means[(i64)k * D + d] - (double)ctr[d]) + 4.0 * sqrt((double)covs[(i64)k * D + d]);
     b = v > b ? v : b;
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+  if (lane != 0) return;
   int e = 0;
   if (b > 0) frexp(b, &e);
   scale[d] = (float)ldexp(1.0, -e);
@@ -866,30 +883,45 @@ __global__ void k_tc_fv_consts(const float *__restrict__ means, const float *__r
 // (vl/fisher.c:419-485) from S0 = sum q, S1 = sum q x', S2 = sum q x'^2:
 //   u = (S1 - mu' S0) / sigma,  v = (S2 - 2 mu' S1 + mu'^2 S0) / sigma2 - S0,
 // scaled by 1/(N sqrt pi) and 1/(N sqrt(2 pi)); signed sqrt; L2.
+// One cluster of kFinCluster CTAs per image: CTA r forms the outputs of
+// components [r K/C, (r+1) K/C) in shared memory (2 (K/C) DIM floats), the
+// CTAs exchange their partial L2 norms and term counts through distributed
+// shared memory (summed in rank order on every CTA, so every CTA scales by
+// the same bits), and each writes its normalised part once, coalesced.
+constexpr int kFinThreads = 256;
+constexpr int kFinCluster = 4;  // divides K (a multiple of 8 on this path)
+
 template <int DIM>
-__global__ void __launch_bounds__(256) k_tc_fv_finalize(
+__global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThreads) k_tc_fv_finalize(
     int K, int Kp, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
     const i64 *__restrict__ imgRow0, const double *__restrict__ cmu, const double *__restrict__ cis2,
     const double *__restrict__ cisd, const double *__restrict__ cup, const double *__restrict__ cvp,
     const float *__restrict__ scale, const unsigned *__restrict__ rowcnt, i64 rowcntBase, int flags,
     i64 imgBase, float *__restrict__ enc, unsigned long long *__restrict__ nterms) {
   constexpr int NST = 2 * DIM + 16;
-  __shared__ double sh[256];
-  __shared__ unsigned long long shn[256];
+  constexpr int NW = kFinThreads / 32;
+  extern __shared__ float s_fv[];  // 2 E: this CTA's u values, then its v values
+  __shared__ double s_sq[NW];
+  __shared__ unsigned long long s_nt[NW];
   __shared__ double s_is[DIM];  // 1 / scale_d (exact: scale_d is a power of two)
-  const int img = blockIdx.x;
+  __shared__ double s_part, s_tot;
+  __shared__ unsigned long long s_partn;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int img = blockIdx.x / kFinCluster;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int Kc = K / kFinCluster, k0 = rank * Kc;
+  const int E = Kc * DIM, KD = K * DIM, eBase = k0 * DIM;
   const int s0 = imgSlot0[img], s1 = imgSlot0[img + 1];
   const i64 r0 = imgRow0[img], r1 = imgRow0[img + 1];
   const i64 n = r1 - r0;
   const double in = n > 0 ? 1.0 / (double)n : 0.0;
-  const int KD = K * DIM;
   const size_t slotStride = (size_t)Kp * NST;
-  float *out = enc + (imgBase + img) * 2 * (i64)KD;
-  for (int d = threadIdx.x; d < DIM; d += 256) s_is[d] = scale ? 1.0 / (double)scale[d] : 1.0;
+  for (int d = tid; d < DIM; d += kFinThreads) s_is[d] = scale ? 1.0 / (double)scale[d] : 1.0;
   __syncthreads();
   double sq = 0;
-  for (int e = threadIdx.x; e < KD; e += 256) {
-    const int k = e / DIM, d = e - k * DIM;
+  for (int el = tid; el < E; el += kFinThreads) {
+    const int kl = el / DIM, d = el - kl * DIM, k = k0 + kl, e = eBase + el;
     double S0 = 0, S1 = 0, S2 = 0;
     const float *pp = partial + ((size_t)s0 * Kp + k) * NST;
     for (int s = s0; s < s1; ++s, pp += slotStride) {
@@ -909,30 +941,61 @@ __global__ void __launch_bounds__(256) k_tc_fv_finalize(
       uf = uf >= 0.f ? sqrtf(uf) : -sqrtf(-uf);
       vf = vf >= 0.f ? sqrtf(vf) : -sqrtf(-vf);
     }
-    out[e] = uf;
-    out[KD + e] = vf;
+    s_fv[el] = uf;
+    s_fv[E + el] = vf;
     sq += (double)uf * uf + (double)vf * vf;
   }
+  // Term counts: the image's rows are split over the cluster's CTAs.
   unsigned long long nt = 0;
   if (rowcnt)
-    for (i64 r = r0 + threadIdx.x; r < r1; r += 256) nt += rowcnt[r - rowcntBase];
-  sh[threadIdx.x] = sq;
-  shn[threadIdx.x] = nt;
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) {
-      sh[threadIdx.x] += sh[threadIdx.x + o];
-      shn[threadIdx.x] += shn[threadIdx.x + o];
-    }
-    __syncthreads();
+    for (i64 r = r0 + rank * kFinThreads + tid; r < r1; r += kFinThreads * kFinCluster)
+      nt += rowcnt[r - rowcntBase];
+  sq = warp_sum(sq);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nt += __shfl_xor_sync(0xffffffffu, nt, o);
+  if (lane == 0) {
+    s_sq[warp] = sq;
+    s_nt[warp] = nt;
   }
-  if (threadIdx.x == 0 && nterms) nterms[imgBase + img] = shn[0];
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0;
+    unsigned long long c = 0;
+    for (int w = 0; w < NW; ++w) {
+      t += s_sq[w];
+      c += s_nt[w];
+    }
+    s_part = t;
+    s_partn = c;
+  }
+  cluster.sync();  // every CTA's partials are written
+  if (tid == 0) {
+    double t = 0;
+    unsigned long long c = 0;
+    for (int q = 0; q < kFinCluster; ++q) {
+      t += *cluster.map_shared_rank(&s_part, q);
+      c += *cluster.map_shared_rank(&s_partn, q);
+    }
+    s_tot = t;
+    if (rank == 0 && nterms) nterms[imgBase + img] = c;
+  }
+  __syncthreads();
+  float *out = enc + (imgBase + img) * 2 * (i64)KD + eBase;
   if (flags & 2) {
-    double nrm = sqrt(sh[0]);
+    double nrm = sqrt(s_tot);
     if (nrm < 1e-12) nrm = 1e-12;
     const float nf = (float)nrm;
-    for (int e = threadIdx.x; e < 2 * KD; e += 256) out[e] = out[e] / nf;
+    for (int el = tid; el < E; el += kFinThreads) {
+      out[el] = s_fv[el] / nf;
+      out[KD + el] = s_fv[E + el] / nf;
+    }
+  } else {
+    for (int el = tid; el < E; el += kFinThreads) {
+      out[el] = s_fv[el];
+      out[KD + el] = s_fv[E + el];
+    }
   }
+  cluster.sync();  // the partials stay readable until every CTA has read them
 }
 
 // Row-major fp32 posteriors -> fp16 q^T operand image (the layout the
@@ -1004,18 +1067,18 @@ void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &
   tp.ctr = sc.slot[0].get<float>(256);
   tp.cst2 = sc.slot[1].get<float>(256);
   tp.wimg = sc.slot[2].get<__nv_bfloat16>((size_t)2 * tp.Kp * KD2);
-  VLB_LAUNCH("tc_center", s, k_tc_center<<<(tp.D + 127) / 128, 128, 0, s>>>(m.means, tp.K, tp.D, tp.ctr));
+  VLB_LAUNCH("tc_center", s, k_tc_center<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, tp.K, tp.D, tp.ctr));
   const i64 n = (i64)tp.Kp * KD2;
   VLB_LAUNCH("tc_wimage", s,
              k_tc_wimg<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.Kp,
                                                                   tp.D, tp.wimg));
   VLB_LAUNCH("tc_constants", s,
-             k_tc_cst<<<(tp.Kp + 127) / 128, 128, 0, s>>>(m.priors, m.means, m.covs, tp.ctr, tp.K,
+             k_tc_cst<<<(tp.Kp + 7) / 8, 256, 0, s>>>(m.priors, m.means, m.covs, tp.ctr, tp.K,
                                                           tp.Kp, tp.D, tp.cst2));
   if (want_scale) {
     tp.scale = sc.slot[12].get<float>(256);
     VLB_LAUNCH("tc_scale", s,
-               k_tc_scale<<<(tp.D + 127) / 128, 128, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.D, tp.scale));
+               k_tc_scale<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.D, tp.scale));
   }
 }
 
@@ -1273,6 +1336,8 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
   const int *dslot0 = (const int *)sc.slot[10].p;
   const i64 *drow0 = (const i64 *)sc.slot[11].p;
   auto fin = D == 64 ? k_tc_fv_finalize<64> : D == 80 ? k_tc_fv_finalize<80> : k_tc_fv_finalize<128>;
+  const size_t finSmem = sizeof(float) * 2 * (K / kFinCluster) * D;
+  VLB_CUDA(cudaFuncSetAttribute(fin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)finSmem));
   for (size_t ci = 0; ci < L.chunks.size(); ++ci) {
     const FvChunk &c = L.chunks[ci];
     if (before) before(ci);
@@ -1299,7 +1364,7 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
       stats_dispatch(tp.D, split, sp, c.gx, cfg.statsMT, cfg.statsStages, s);
     }
     VLB_LAUNCH("tc_fv_finalize", s,
-               fin<<<(unsigned)c.nimg, 256, 0, s>>>(
+               fin<<<(unsigned)(c.nimg * kFinCluster), kFinThreads, finSmem, s>>>(
                    (int)K, tp.Kp, partial, dslot0 + c.img, drow0 + c.img, cmu, cis2, cisd, cup, cvp,
                    fp32 ? nullptr : tp.scale, c.nrows > 0 ? rowcnt : nullptr, c.row0, flags, c.img0, enc,
                    nterms));
