@@ -371,6 +371,68 @@ def e2e(capi, wl, prec, config, steps=3):
             "d2h_bytes_per_step": int(NUM_IMAGES * (2 * K * D * 4 + 8)), "ms_per_step": ms}
 
 
+def em_throughput(capi, iters=5, cpu=True):
+    """EM iterations/s (a north-star throughput besides the Fisher metric).
+
+    Config 1 (N=1,000,000 SIFT-like descriptors, D=128, K=256, custom init,
+    variance floor 1e-4 x max global variance) and config 0 (N=50,000, D=64,
+    K=64) run EM on device-resident data through vlb200_gmm_em_device in the
+    EXACT (CUDA-core) and FP32 (tensor-core E-step) modes.  An iteration is one
+    E-step plus one M-step (T iterations run T+1 E-steps, as vl/gmm.c:1220-1308).
+    Timing: wall clock around the blocking call, after one untimed run.  The
+    reference arm is VLFeat's OpenMP EM (oracle/_ref) on all host cores on a
+    100,000-row sample of config 1."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    out = {"timing": "wall clock around vlb200_gmm_em_device (blocking), after one untimed run"}
+    cfgs = [("config1_sift_n1m_d128_k256", W.config1(N=1_000_000, K=256, iters=iters), iters),
+            ("config0_n50k_d64_k64", W.config0(), 10)]
+    for name, c, T in cfgs:
+        x = torch.from_numpy(np.ascontiguousarray(c["data"])).cuda()
+        N = int(x.shape[0])
+        res = {"N": N, "D": c["D"], "K": c["K"], "max_iterations": T}
+        for prec in ("exact", "fp32"):
+            def run():
+                g = capi.GMM(c["D"], c["K"], np.float32)
+                g.set_initialization("custom")
+                g.set_max_num_iterations(T)
+                g.set_covariance_lower_bound(c["lower_bound"])
+                g.set_means(c["means"])
+                g.set_covariances(c["covs"])
+                g.set_priors(c["priors"])
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                ll = g.em_device(x, prec)
+                torch.cuda.synchronize()
+                return g, ll, time.perf_counter() - t0
+            run()
+            g, ll, dt = run()
+            its = max(1, len(g.ll_trace) - 1)
+            res[prec] = {"iterations": its, "ms_per_iteration": 1e3 * dt / its,
+                         "iterations_per_s": its / dt, "descriptor_iterations_per_s": N * its / dt,
+                         "log_likelihood": ll, "restarts": g.num_restarts,
+                         "estep": "tensor-core bf16x3" if prec == "fp32" else "CUDA-core fp32"}
+        out[name] = res
+        del x
+    if cpu:
+        from oracle import oracle as O
+        c = cfgs[0][1]
+        n = 100_000
+        try:
+            impl, kind = O.Reference(threads=os.cpu_count() or 1), "reference"
+        except (FileNotFoundError, OSError):
+            impl, kind = O.Restatement(), "port"
+        t0 = time.perf_counter()
+        impl.em(np.ascontiguousarray(c["data"][:n]), c["priors"], c["means"], c["covs"],
+                c["lower_bound"], 2)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"kind": kind, "cores": os.cpu_count() or 1,
+                               "sample": f"config 1, first {n} descriptors, 2 iterations of vl_gmm_cluster",
+                               "descriptor_iterations_per_s": n * 2 / dt,
+                               "ms_per_iteration": 1e3 * dt / 2}
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: VLFeat's own CPU code on the host cores."""
     if rank != 0:
@@ -419,6 +481,7 @@ def main():
     ap.add_argument("--paths", default=",".join(PATHS))
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-em", action="store_true", help="skip the EM iterations/s measurement")
     ap.add_argument("--images", type=int, default=4096,
                     help="encode only the first IMAGES images of the workload (small profiling cases)")
     ap.add_argument("--plan", default=None,
@@ -491,6 +554,10 @@ def main():
             out["e2e"] = e2e(capi, wl, head, results[head].get("plan_config"))
         if not args.no_cpu and world == 1:
             out["cpu_baseline"] = cpu_baseline(wl)
+        if not args.no_em and world == 1:
+            del encoders, eager_of
+            torch.cuda.empty_cache()
+            out["em"] = em_throughput(capi, cpu=not args.no_cpu)
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

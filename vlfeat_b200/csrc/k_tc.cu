@@ -192,7 +192,11 @@ struct EParams {
   i64 ntiles;
 };
 
-template <int DIM>
+// Shared-memory layout of the E-step.  With W resident (SW false) the W
+// image (hi + lo) is copied in once; with W streamed (SW true: W does not fit,
+// e.g. D=128 at K=256) each operand stage also holds the k-atom of W its
+// MMAs read, bulk-copied from global memory (L2) when the stage is filled.
+template <int DIM, bool SW = false>
 struct ELayout {
   static constexpr int KD2 = 2 * DIM;
   static constexpr int NKA = KD2 / 32;
@@ -201,23 +205,29 @@ struct ELayout {
   // 32 components (64 B per row) of q through 2 KB before the global stores.
   static constexpr int kStaging = 8 * 2048;
   __host__ __device__ static size_t wbytes(int Kp) { return (size_t)NKA * Kp * 64; }
+  __host__ __device__ static size_t wstage(int Kp) { return SW ? (size_t)2 * Kp * 64 : 0; }
+  __host__ __device__ static size_t stage(int Kp) { return kStage + wstage(Kp); }
   static size_t fixed(int Kp) {
-    return 2 * wbytes(Kp) + 1024 /*cst*/ + 1024 /*ctr, bars*/ + kStaging + 1024 /*alignment*/;
+    return (SW ? 0 : 2 * wbytes(Kp)) + 1024 /*cst*/ + 1024 /*ctr, bars*/ + kStaging + 1024 /*alignment*/;
   }
-  static int max_stages(int Kp) { return (int)((kSmemLimit - fixed(Kp)) / kStage); }
-  static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * kStage; }
+  static int max_stages(int Kp) {
+    return fixed(Kp) >= (size_t)kSmemLimit ? 0 : (int)((kSmemLimit - fixed(Kp)) / stage(Kp));
+  }
+  static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * stage(Kp); }
 };
 
-template <int DIM, int QF, bool FAST>
+template <int DIM, int QF, bool FAST, bool SW = false>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
-  using L = ELayout<DIM>;
+  using L = ELayout<DIM, SW>;
   constexpr int NKA = L::NKA;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *base = align1024(smem_raw);
   const uint32_t wbytes = (uint32_t)L::wbytes(p.Kp);
+  const uint32_t stageBytes = (uint32_t)L::stage(p.Kp);
+  const uint32_t wpart = (uint32_t)p.Kp * 64;  // one k-atom of one W part
   uint8_t *sW = base;
-  uint8_t *sA = sW + 2 * wbytes;
-  float *s_cst = (float *)(sA + (size_t)p.nst * L::kStage);
+  uint8_t *sA = sW + (SW ? 0 : 2 * wbytes);
+  float *s_cst = (float *)(sA + (size_t)p.nst * stageBytes);
   float *s_ctr = s_cst + 256;                     // DIM <= 128 floats
   uint64_t *bars = (uint64_t *)(s_ctr + 128);     // 36 barriers, then TMEM base and abort flag
   uint64_t *full = bars, *empty = bars + 16, *accf = bars + 32, *acce = bars + 34;
@@ -228,7 +238,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   if (tid == 0) {
     for (int s = 0; s < p.nst; ++s) {
-      mbar_init(&full[s], 128);
+      mbar_init(&full[s], SW ? 129 : 128);  // + the W copy's expect-tx arrival
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -246,7 +256,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   {
     const uint4 *src = p.wimg;
     uint4 *dst = (uint4 *)sW;
-    const int n16 = (int)(2 * wbytes / 16);
+    const int n16 = SW ? 0 : (int)(2 * wbytes / 16);
     for (int i = tid; i < n16; i += kTcThreads) dst[i] = src[i];
     for (int k = tid; k < 256; k += kTcThreads) s_cst[k] = k < p.Kp ? p.cst2[k] : -INFINITY;
     for (int d = tid; d < DIM; d += kTcThreads) s_ctr[d] = p.ctr[d];
@@ -298,7 +308,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       if (t2 < p.ntiles) load(fut, t2, c2);
       const int stage = it % p.nst;
       if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 1)) return false;
-      const uint32_t a_hi = smem_u32(sA + (size_t)stage * L::kStage);
+      const uint32_t a_hi = smem_u32(sA + (size_t)stage * stageBytes);
+      if (SW && warp == 0 && lane == 0) {
+        // This stage's k-atom of W: its hi and lo parts, complete on full[stage].
+        const uint8_t *w = (const uint8_t *)p.wimg + (size_t)c0 * wpart;
+        mbar_arrive_expect_tx(&full[stage], 2 * wpart);
+        bulk_g2s(a_hi + L::kStage, w, wpart, &full[stage]);
+        bulk_g2s(a_hi + L::kStage + wpart, w + wbytes, wpart, &full[stage]);
+      }
       const int d0 = 16 * c0 + 4 * part;
       const float m0 = s_ctr[d0], m1 = s_ctr[d0 + 1], m2 = s_ctr[d0 + 2], m3 = s_ctr[d0 + 3];
 #pragma unroll
@@ -552,13 +569,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
           break;
         }
         tc_fence_after();
-        const uint32_t a_hi = smem_u32(sA + (size_t)stage * L::kStage);
+        const uint32_t a_hi = smem_u32(sA + (size_t)stage * stageBytes);
+        const uint32_t b_hi = SW ? a_hi + L::kStage : w_hi + c * wpart;
+        const uint32_t b_lo = SW ? a_hi + L::kStage + wpart : w_lo + c * wpart;
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
           const uint64_t ah = sdesc(a_hi + ks * 32, 16, 512, kSw64);
           const uint64_t al = sdesc(a_hi + 8192 + ks * 32, 16, 512, kSw64);
-          const uint64_t bh = sdesc(w_hi + c * p.Kp * 64 + ks * 32, 16, 512, kSw64);
-          const uint64_t bl = sdesc(w_lo + c * p.Kp * 64 + ks * 32, 16, 512, kSw64);
+          const uint64_t bh = sdesc(b_hi + ks * 32, 16, 512, kSw64);
+          const uint64_t bl = sdesc(b_lo + ks * 32, 16, 512, kSw64);
           mma_bf16(d, ah, bh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
           mma_bf16(d, ah, bl, idesc, 1u);
           mma_bf16(d, al, bh, idesc, 1u);
@@ -1084,16 +1103,16 @@ void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &
 
 int padQ(int Kp) { return (Kp + 127) / 128 * 128; }
 
-template <int DIM, int QF>
-i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                 unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s) {
-  using L = ELayout<DIM>;
+template <int DIM, int QF, bool SW>
+i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
+                      unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s) {
+  using L = ELayout<DIM, SW>;
   const i64 ntiles = (N + 127) / 128;
   if (ntiles == 0) return 0;
   const int nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(tp.Kp));
   VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
   const size_t smem = L::bytes(tp.Kp, nst);
-  auto kern = fast ? k_tc_estep<DIM, QF, true> : k_tc_estep<DIM, QF, false>;
+  auto kern = fast ? k_tc_estep<DIM, QF, true, SW> : k_tc_estep<DIM, QF, false, SW>;
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   EParams p;
   p.X = X; p.N = N; p.K = tp.K; p.Kp = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
@@ -1104,6 +1123,19 @@ i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool
   const int grid = (int)std::min<i64>(ntiles, num_sms());
   VLB_LAUNCH("tc_estep_bf16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
   return ntiles * 4;  // LL partials written
+}
+
+// W resident in shared memory when two operand stages fit beside it, else
+// streamed through the stages (built for D=128, the only supported dimension
+// whose W can exceed shared memory at K <= 256).
+template <int DIM, int QF>
+i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
+                 unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s) {
+  if constexpr (DIM == 128) {
+    if (ELayout<DIM, false>::max_stages(tp.Kp) < 2)
+      return launch_estep_impl<DIM, QF, true>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s);
+  }
+  return launch_estep_impl<DIM, QF, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s);
 }
 
 template <int DIM, int MT, int SPLIT>
@@ -1198,11 +1230,11 @@ void lpt_assign(const std::vector<SItem> &items, int gx, std::vector<int> &order
 bool tc_supported(i64 K, i64 D) {
   if (!(D == 64 || D == 80 || D == 128)) return false;
   if (K < 8 || K > 256 || K % 8) return false;
-  // Resident W (hi + lo), constants, epilogue staging and at least two
-  // operand stages must fit (the E-step's shared-memory layout).
+  // W resident beside two operand stages, or (D=128) streamed through them;
+  // TMEM holds two K_pad-column accumulators.
   const int Kp = padK(K);
-  const size_t w = (size_t)2 * (2 * D / 32) * Kp * 64;
-  return w + 2048 + 8 * 2048 + 1024 + 2 * 16384 <= (size_t)kSmemLimit;
+  if (D == 128) return ELayout<128, true>::max_stages(Kp) >= 2;
+  return D == 64 ? ELayout<64, false>::max_stages(Kp) >= 2 : ELayout<80, false>::max_stages(Kp) >= 2;
 }
 
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part, bool fast,
