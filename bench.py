@@ -377,7 +377,8 @@ def em_throughput(capi, iters=5, cpu=True):
     Config 1 (N=1,000,000 SIFT-like descriptors, D=128, K=256, custom init,
     variance floor 1e-4 x max global variance) and config 0 (N=50,000, D=64,
     K=64) run EM on device-resident data through vlb200_gmm_em_device in the
-    EXACT (CUDA-core) and FP32 (tensor-core E-step) modes.  An iteration is one
+    EXACT (CUDA cores) and the FP32 and BF16 modes (E-step GEMM and M-step
+    statistics GEMM on the tensor cores).  An iteration is one
     E-step plus one M-step (T iterations run T+1 E-steps, as vl/gmm.c:1220-1308).
     Timing: wall clock around the blocking call, after one untimed run.  The
     reference arm is VLFeat's OpenMP EM (oracle/_ref) on all host cores on a
@@ -391,7 +392,7 @@ def em_throughput(capi, iters=5, cpu=True):
         x = torch.from_numpy(np.ascontiguousarray(c["data"])).cuda()
         N = int(x.shape[0])
         res = {"N": N, "D": c["D"], "K": c["K"], "max_iterations": T}
-        for prec in ("exact", "fp32"):
+        for prec in ("exact", "fp32", "bf16"):
             def run():
                 g = capi.GMM(c["D"], c["K"], np.float32)
                 g.set_initialization("custom")
@@ -411,7 +412,9 @@ def em_throughput(capi, iters=5, cpu=True):
             res[prec] = {"iterations": its, "ms_per_iteration": 1e3 * dt / its,
                          "iterations_per_s": its / dt, "descriptor_iterations_per_s": N * its / dt,
                          "log_likelihood": ll, "restarts": g.num_restarts,
-                         "estep": "tensor-core bf16x3" if prec == "fp32" else "CUDA-core fp32"}
+                         "kernels": {"exact": "CUDA-core fp32 E-step and M-step",
+                                     "fp32": "tcgen05 bf16x3 E-step, bf16x3 M-step statistics",
+                                     "bf16": "tcgen05 bf16x3 E-step, fp16 M-step statistics"}[prec]}
         out[name] = res
         del x
     if cpu:

@@ -54,6 +54,10 @@ template <typename T>
 void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i64 K, i64 D,
                  const double *lb, cudaStream_t s);
 
+// priors /= max(sum priors, 1e-12) on the device (vl/gmm.c:1196-1211).
+template <typename T>
+void normalize_priors(T *priors, i64 K, cudaStream_t s);
+
 // Un-thresholded posterior mass per component (vl/gmm.c:835-844), K doubles.
 template <typename T>
 void column_mass(const T *q, i64 N, i64 K, double *mass, cudaStream_t s);
@@ -108,6 +112,15 @@ void router_default_posteriors(const float *X, i64 N, const DevModel<float> &m, 
 bool tc_supported(i64 K, i64 D);
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
              bool fast, int precision, cudaStream_t s);
+// EM with the tensor-core M-step.  tc_estep_em is the E-step of tc_estep that
+// also writes the posteriors as the statistics operand image, thresholded at
+// the M-step's skip (vl/gmm.c:1099); tc_mstep then runs the M-step
+// (vl/gmm.c:1036-1213) from that image and the centre of that E-step's model,
+// on the same thread, in place on means/covs/priors (device, fp32).
+i64 tc_estep_em(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
+                int precision, cudaStream_t s);
+void tc_mstep(const float *X, i64 N, float *means, float *covs, float *priors, i64 K, i64 D,
+              const double *lb, int precision, cudaStream_t s);
 void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages,
                      const DevModel<float> &m, float *enc, unsigned long long *nterms, int flags,
                      int precision, cudaStream_t s);

@@ -74,9 +74,11 @@ void sync_posteriors(VlGMM *self) {
   self->postOnDevice = false;
 }
 
+// em_image: also write the posteriors as the tensor-core M-step's operand
+// image (EM with the tensor-core path; see vlb::tc_estep_em).
 template <typename T>
 double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int precision,
-                    bool fast, cudaStream_t s) {
+                    bool fast, cudaStream_t s, bool em_image = false) {
   vlb::Scratch &sc = vlb::thread_scratch();
   double *llp = sc.slot[15].get<double>(vlb::estep_ll_parts(N));
   double *dll = sc.slot[16].get<double>(1);
@@ -84,7 +86,8 @@ double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int pr
   i64 nparts = 0;
   if constexpr (sizeof(T) == 4) {
     if (precision != VLB200_PREC_EXACT && vlb::tc_supported(m.K, m.D)) {
-      nparts = vlb::tc_estep(dX, N, m, dq, llp, fast, precision, s);
+      nparts = em_image ? vlb::tc_estep_em(dX, N, m, dq, llp, precision, s)
+                        : vlb::tc_estep(dX, N, m, dq, llp, fast, precision, s);
       done = true;
     }
   }
@@ -196,9 +199,13 @@ double em_device(VlGMM *self, const T *dX, i64 N, int precision) {
   m.D = D;
 
   vlb::apply_bounds<T>(dcovs, K, D, dlb, s);  // vl/gmm.c:1233
+  // Tensor-core modes run the M-step's statistics on the tensor cores from
+  // the E-step's posterior image; EXACT and double stay on the CUDA cores.
+  bool tcm = false;
+  if constexpr (sizeof(T) == 4) tcm = precision != VLB200_PREC_EXACT && vlb::tc_supported(K, D);
   double prevLL = -INFINITY, LL = -INFINITY;
   for (vl_size it = 0;; ++it) {
-    LL = device_estep<T>(dX, N, m, dq, precision, false, s);
+    LL = device_estep<T>(dX, N, m, dq, precision, false, s, tcm);
     self->llTrace.push_back(LL);
     if (self->verbosity)
       VLB_PRINTF("gmm: em: iteration %d: loglikelihood = %f (variation = %f)\n", (int)it, LL,
@@ -217,13 +224,23 @@ double em_device(VlGMM *self, const T *dX, i64 N, int precision) {
       break;
     }
     prevLL = LL;
+    vl_size r = 0;
     if (it > 1) {
-      vl_size r = restart_empty_modes<T>(self, dX, N, dq, dmeans, dcovs, dpriors, dlb, s);
+      r = restart_empty_modes<T>(self, dX, N, dq, dmeans, dcovs, dpriors, dlb, s);
       self->numRestarts += r;
       if (r > 0 && self->verbosity)
         VLB_PRINTF("gmm: em: %d Gaussian modes restarted because they had become empty.\n", (int)r);
     }
-    vlb::exact_mstep<T>(dX, N, dq, dmeans, dcovs, dpriors, K, D, dlb, s);
+    // A restart rewrites posteriors (vl/gmm.c:969-989), so the image is stale:
+    // that iteration's M-step reads the rows.
+    bool done = false;
+    if constexpr (sizeof(T) == 4) {
+      if (tcm && r == 0) {
+        vlb::tc_mstep(dX, N, dmeans, dcovs, dpriors, K, D, dlb, precision, s);
+        done = true;
+      }
+    }
+    if (!done) vlb::exact_mstep<T>(dX, N, dq, dmeans, dcovs, dpriors, K, D, dlb, s);
   }
   VLB_CUDA(cudaMemcpyAsync(self->means, dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
   VLB_CUDA(cudaMemcpyAsync(self->covariances, dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));

@@ -559,6 +559,11 @@ void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i6
 }
 
 template <typename T>
+void normalize_priors(T *priors, i64 K, cudaStream_t s) {
+  VLB_LAUNCH("normalize_priors", s, k_normalize_priors<T><<<1, kThreads, 0, s>>>(priors, (int)K));
+}
+
+template <typename T>
 void column_mass(const T *q, i64 N, i64 K, double *mass, cudaStream_t s) {
   const i64 rps = pick_slab_rows(N > 0 ? N : 1);
   const int nslab = (int)((N + rps - 1) / rps > 0 ? (N + rps - 1) / rps : 1);
@@ -722,6 +727,7 @@ void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, 
   template void exact_mstep<T>(const T *, i64, const T *, T *, T *, T *, i64, i64,           \
                                const double *, cudaStream_t);                                \
   template void column_mass<T>(const T *, i64, i64, double *, cudaStream_t);                 \
+  template void normalize_priors<T>(T *, i64, cudaStream_t);                                 \
   template void restart_split<T>(T *, const T *, i64, i64, i64, i64, i64, i64, T,           \
                                  cudaStream_t);                                              \
   template void apply_bounds<T>(T *, i64, i64, const double *, cudaStream_t);                \

@@ -172,7 +172,12 @@ __global__ void k_tc_scale(const float *__restrict__ means, const float *__restr
 //            groups is exactly the MMA's A operand and moves with one bulk
 //            copy per group.
 //   kQImg32  the same image as two bf16 parts (hi, lo) for bf16x3 statistics.
-constexpr int kQRow = 0, kQImg16 = 1, kQImg32 = 2;
+//   kQRowImg16, kQRowImg32  both: the row-major posteriors (unthresholded)
+//            and the image (thresholded), for EM with the tensor-core M-step.
+constexpr int kQRow = 0, kQImg16 = 1, kQImg32 = 2, kQRowImg16 = 3, kQRowImg32 = 4;
+__host__ __device__ constexpr bool q_rows(int qf) { return qf == kQRow || qf == kQRowImg16 || qf == kQRowImg32; }
+__host__ __device__ constexpr bool q_image(int qf) { return qf != kQRow; }
+__host__ __device__ constexpr bool q_image32(int qf) { return qf == kQImg32 || qf == kQRowImg32; }
 
 struct EParams {
   const float *X;
@@ -182,7 +187,8 @@ struct EParams {
   const uint4 *wimg;
   const float *cst2;
   const float *ctr;
-  void *q;
+  void *q;     // row-major posteriors (kQRow*) or the image (kQImg*)
+  void *qimg;  // the image of the combined formats
   int ldq;
   int fast;
   float qthr;  // image outputs: posteriors below this are stored as 0 (vl/fisher.c:440)
@@ -354,7 +360,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     const int eg = (warp - 4) >> 2, ew = warp & 3;
     const int r = ew * 32 + lane;
     const int nch = p.Kp / 32;
-    const int ncw = (QF == kQRow) ? nch : p.Kq / 32;
+    const int ncw = q_image(QF) ? p.Kq / 32 : nch;
     const unsigned long long *cst2v = (const unsigned long long *)s_cst;
     uint8_t *stg = s_stage + (warp - 4) * 2048;
     int tt = 0;
@@ -444,7 +450,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       // -prev(qthr) * 2^64, prev(qthr) the largest float below qthr (> 0).
       const float nthr = -__uint_as_float(__float_as_uint(p.qthr) - 1u) * 0x1p64f;
       // q image of this tile; this warp's rows are its 8-row groups 4 ew .. 4 ew + 3.
-      uint8_t *ib = (uint8_t *)p.q + (size_t)tile * 128 * p.Kq * 2;
+      uint8_t *ib = (uint8_t *)(q_rows(QF) ? p.qimg : p.q) + (size_t)tile * 128 * p.Kq * 2;
       // Image stores go through this warp's staging (32 rows x 64 B, 16-byte
       // chunks swizzled by row so that both sides are free of bank conflicts):
       // lane = row on the way in; on the way out lane (a, b) moves chunk b of
@@ -496,7 +502,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
             const unsigned long long kk = f2u(__saturatef(fmaf(x0, 0x1p64f, nthr)),
                                               __saturatef(fmaf(x1, 0x1p64f, nthr)));
             cnt2 = add2(cnt2, kk);
-            if (QF != kQRow) {
+            if (QF == kQImg16 || QF == kQImg32) {
               const unsigned long long xk = mul2(f2u(x0, x1), kk);
               x0 = lo32(xk);
               x1 = hi32(xk);
@@ -508,7 +514,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 #pragma unroll
           for (int j = 0; j < 32; ++j) qv[j] = 0.f;
         }
-        if (QF == kQRow) {
+        if (q_rows(QF)) {
           if (live) {
             const int k0 = cc * 32;
             float *dst = (float *)p.q + row * p.ldq + k0;
@@ -522,11 +528,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
                 if (k0 + j < p.K) dst[j] = qv[j];
             }
           }
-        } else {
+        }
+        if (q_image(QF)) {
+          if (q_rows(QF)) {
+            // Combined formats: the rows above keep every posterior; the image
+            // keeps those >= qthr (the same flag as in the loop above).
+#pragma unroll
+            for (int j = 0; j < 32; ++j) qv[j] *= __saturatef(fmaf(qv[j], 0x1p64f, nthr));
+          }
           uint4 wh[4], wl[4];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            if (QF == kQImg16) {
+            if (!q_image32(QF)) {
               wh[j].x = pack2<true>(qv[8 * j + 0], qv[8 * j + 1]);
               wh[j].y = pack2<true>(qv[8 * j + 2], qv[8 * j + 3]);
               wh[j].z = pack2<true>(qv[8 * j + 4], qv[8 * j + 5]);
@@ -539,7 +552,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
             }
           }
           stage_out(wh, cc, 0);
-          if (QF == kQImg32) stage_out(wl, cc, (size_t)p.qpart);
+          if (q_image32(QF)) stage_out(wl, cc, (size_t)p.qpart);
         }
       }
       tc_fence_before();
@@ -1017,6 +1030,49 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
   cluster.sync();  // the partials stay readable until every CTA has read them
 }
 
+// ============================================================ M-step
+// M-step (vl/gmm.c:1169-1194) from the statistics of the tensor-core kernel:
+// per item S0 = sum q, S1 = sum q x'', S2 = sum q x''^2 with x'' = (x - c)
+// scale over the rows whose posterior passed the skip q >= 1e-2/K
+// (vl/gmm.c:1099).  Items are summed in f64 in index order; the reference's
+// sums follow exactly: sum q x = S1 + c S0, sum q (x - mu_old)^2 =
+// S2 - 2 a S1 + a^2 S0 with a = mu_old - c.  Then the reference's update:
+// mean, variance about the new mean, the variance floor, and the mass as
+// the unnormalised prior.
+__global__ void k_tc_mstep_finalize(int nitems, int K, int Kp, int D, const float *__restrict__ partial,
+                                    const float *__restrict__ ctr, const float *__restrict__ scale,
+                                    const double *__restrict__ lb, float *__restrict__ means,
+                                    float *__restrict__ covs, float *__restrict__ priors) {
+  const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (i64)K * D) return;
+  const int k = (int)(idx / D), d = (int)(idx % D);
+  const int NST = 2 * D + 16;
+  double S0 = 0, S1 = 0, S2 = 0;
+  for (int it = 0; it < nitems; ++it) {
+    const float *pp = partial + ((size_t)it * Kp + k) * NST;
+    S0 += (double)pp[2 * D];
+    S1 += (double)pp[d];
+    S2 += (double)pp[D + d];
+  }
+  const double is = scale ? 1.0 / (double)scale[d] : 1.0;
+  S1 *= is;
+  S2 *= is * is;
+  const double c = (double)ctr[d], oldmu = (double)means[idx], a = oldmu - c;
+  const double mass = S0;
+  double mu = S1 + c * S0, v = S2 - 2.0 * a * S1 + a * a * S0;
+  if (mass >= 1e-6 / (double)K) {
+    mu /= mass;
+    v /= mass;
+    const double df = mu - oldmu;
+    v -= df * df;
+  }
+  float vt = (float)v;
+  if ((double)vt < lb[d]) vt = (float)lb[d];
+  means[idx] = (float)mu;
+  covs[idx] = vt;
+  if (d == 0) priors[k] = (float)mass;
+}
+
 // Row-major fp32 posteriors -> fp16 q^T operand image (the layout the
 // E-step writes), with VLFeat's q < 1e-6 skip, the optional FAST one-hot of
 // the row's arg-max (vl/fisher.c:398-417) and per-row term counts.  One warp
@@ -1103,22 +1159,43 @@ void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &
 
 int padQ(int Kp) { return (Kp + 127) / 128 * 128; }
 
+// Smallest float >= t: the kernels keep q >= qthr (float compare), which then
+// equals the reference's "skip p < t" with t a double constant.
+float float_at_least(double t) {
+  float f = (float)t;
+  if ((double)f < t) f = std::nextafter(f, INFINITY);
+  return f;
+}
+
+// Extra outputs of the combined formats: the image and its threshold.
+struct EOut {
+  void *qimg = nullptr;
+  double qthr = 1e-6;  // vl/fisher.c:440 (the Fisher skip)
+};
+
 template <int DIM, int QF, bool SW>
 i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                      unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s) {
+                      unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s,
+                      const EOut &eo) {
   using L = ELayout<DIM, SW>;
   const i64 ntiles = (N + 127) / 128;
   if (ntiles == 0) return 0;
   const int nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(tp.Kp));
   VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
   const size_t smem = L::bytes(tp.Kp, nst);
-  auto kern = fast ? k_tc_estep<DIM, QF, true, SW> : k_tc_estep<DIM, QF, false, SW>;
+  auto kern = k_tc_estep<DIM, QF, false, SW>;
+  if constexpr (!q_rows(QF) || QF == kQRow) {
+    if (fast) kern = k_tc_estep<DIM, QF, true, SW>;
+  } else {
+    VLB_CHECK(!fast, VL_ERR_BAD_ARG, "tensor-core E-step: the combined formats have no FAST variant");
+  }
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   EParams p;
   p.X = X; p.N = N; p.K = tp.K; p.Kp = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
   p.qpart = ntiles * 128 * (i64)p.Kq * 2;
   p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr;
-  p.q = q; p.ldq = ldq; p.fast = fast ? 1 : 0; p.qthr = 1e-6f; p.rowcnt = rowcnt; p.ll_part = ll_part;
+  p.q = q; p.qimg = eo.qimg; p.ldq = ldq; p.fast = fast ? 1 : 0; p.qthr = float_at_least(eo.qthr);
+  p.rowcnt = rowcnt; p.ll_part = ll_part;
   p.err = err; p.ntiles = ntiles;
   const int grid = (int)std::min<i64>(ntiles, num_sms());
   VLB_LAUNCH("tc_estep_bf16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
@@ -1130,12 +1207,13 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
 // whose W can exceed shared memory at K <= 256).
 template <int DIM, int QF>
 i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                 unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s) {
+                 unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s,
+                 const EOut &eo) {
   if constexpr (DIM == 128) {
     if (ELayout<DIM, false>::max_stages(tp.Kp) < 2)
-      return launch_estep_impl<DIM, QF, true>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s);
+      return launch_estep_impl<DIM, QF, true>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
   }
-  return launch_estep_impl<DIM, QF, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s);
+  return launch_estep_impl<DIM, QF, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
 }
 
 template <int DIM, int MT, int SPLIT>
@@ -1155,10 +1233,14 @@ template <int DIM>
 struct Tc {
   static constexpr bool kTwo = 2 * (2 * DIM + 16) <= 512;  // two M tiles fit in TMEM
   static i64 estep(int qf, const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                   unsigned *rowcnt, double *ll, int *err, int nst, cudaStream_t s) {
-    if (qf == kQImg16) return launch_estep<DIM, kQImg16>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
-    if (qf == kQImg32) return launch_estep<DIM, kQImg32>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
-    return launch_estep<DIM, kQRow>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
+                   unsigned *rowcnt, double *ll, int *err, int nst, cudaStream_t s, const EOut &eo) {
+    switch (qf) {
+      case kQImg16: return launch_estep<DIM, kQImg16>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
+      case kQImg32: return launch_estep<DIM, kQImg32>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
+      case kQRowImg16: return launch_estep<DIM, kQRowImg16>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
+      case kQRowImg32: return launch_estep<DIM, kQRowImg32>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
+      default: return launch_estep<DIM, kQRow>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
+    }
   }
   // split 2: bf16x3 statistics (q image in two bf16 parts); split 1: fp16.
   // mt: 128-component M tiles per CTA (0: two when they fit in TMEM).
@@ -1175,11 +1257,12 @@ struct Tc {
 };
 
 i64 estep_dispatch(int D, int qf, const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
-                   unsigned *rowcnt, double *ll, int *err, int nst, cudaStream_t s) {
+                   unsigned *rowcnt, double *ll, int *err, int nst, cudaStream_t s,
+                   const EOut &eo = EOut()) {
   switch (D) {
-    case 64: return Tc<64>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
-    case 80: return Tc<80>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
-    case 128: return Tc<128>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s);
+    case 64: return Tc<64>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
+    case 80: return Tc<80>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
+    case 128: return Tc<128>::estep(qf, X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
     default: throw Error(VL_ERR_BAD_ARG, "tensor-core path: unsupported dimension");
   }
 }
@@ -1250,6 +1333,69 @@ i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *
   return n;
 }
 
+// ------------------------------------------------- EM, tensor-core M-step
+// Host table -> a scratch buffer (stream-ordered; the host copy is staged).
+template <typename T>
+T *upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s) {
+  T *d = b.get<T>(std::max<size_t>(1, v.size()));
+  if (!v.empty()) VLB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+i64 tc_estep_em(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
+                int precision, cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaTc);
+  const bool fp32 = (precision == VLB200_PREC_FP32);
+  TcPrep tp;
+  tc_prepare(m, tp, !fp32, sc, s);
+  const int Kq = padQ(tp.Kp);
+  const i64 ntiles = (N + 127) / 128;
+  EOut eo;
+  eo.qimg = sc.slot[4].get<char>((size_t)std::max<i64>(1, ntiles) * 128 * Kq * (fp32 ? 4 : 2));
+  eo.qthr = 1e-2 / (double)m.K;  // vl/gmm.c:1099
+  int *err = sc.slot[3].get<int>(1);
+  VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  const i64 n = estep_dispatch(tp.D, fp32 ? kQRowImg32 : kQRowImg16, X, N, tp, (void *)q, (int)m.K, false,
+                               nullptr, ll_part, err, 0, s, eo);
+  check_err(err, s);
+  return n;
+}
+
+void tc_mstep(const float *X, i64 N, float *means, float *covs, float *priors, i64 K, i64 D,
+              const double *lb, int precision, cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaTc);
+  const bool fp32 = (precision == VLB200_PREC_FP32);
+  const int Kp = padK(K), Kq = padQ(Kp), NST = (int)(2 * D + 16);
+  const i64 ntiles = (N + 127) / 128;
+  constexpr i64 kItemRows = 8192;
+  std::vector<SItem> items;
+  for (i64 r = 0; r < N; r += kItemRows) items.push_back({r, std::min(N, r + kItemRows), (int)items.size(), 0});
+  const int nitems = (int)items.size();
+  const int gx = std::max(1, std::min(nitems, num_sms()));
+  std::vector<int> order, beg;
+  lpt_assign(items, gx, order, beg);
+  SItem *ditems = upload(sc.slot[7], items, s);
+  int *dorder = upload(sc.slot[8], order, s);
+  int *dbeg = upload(sc.slot[9], beg, s);
+  float *partial = sc.slot[6].get<float>((size_t)std::max(1, nitems) * Kp * NST);
+  int *err = sc.slot[3].get<int>(1);
+  VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  if (nitems > 0) {
+    SParams sp;
+    sp.X = X; sp.qimg = (const uint8_t *)sc.slot[4].p; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = 0;
+    sp.K = (int)K; sp.Kp = Kp; sp.Kq = Kq; sp.nst = 0;
+    sp.ctr = (const float *)sc.slot[0].p; sp.scale = fp32 ? nullptr : (const float *)sc.slot[12].p;
+    sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg; sp.partial = partial; sp.err = err;
+    stats_dispatch((int)D, fp32 ? 2 : 1, sp, gx, 0, 0, s);
+  }
+  VLB_LAUNCH("tc_mstep_finalize", s,
+             k_tc_mstep_finalize<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
+                 nitems, (int)K, Kp, (int)D, partial, (const float *)sc.slot[0].p,
+                 fp32 ? nullptr : (const float *)sc.slot[12].p, lb, means, covs, priors));
+  normalize_priors<float>(priors, K, s);
+  check_err(err, s);
+}
+
 // ------------------------------------------------- batched Fisher encoding
 namespace {
 
@@ -1318,12 +1464,6 @@ void fv_layout(const i64 *off, i64 numImages, i64 rowBudget, i64 itemRows, int n
 // Scratch slots of the batched encoder (each encoder owns its arena):
 // 0-2, 12 model prep; 3 error word; 4 q image; 5 row counts; 6 item
 // partials; 7-11 layout tables; 13-17 Fisher constants; 18 router posteriors.
-template <typename T>
-T *upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s) {
-  T *d = b.get<T>(std::max<size_t>(1, v.size()));
-  if (!v.empty()) VLB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
-  return d;
-}
 
 void fv_upload(const FvLayout &L, int Kp, int Kq, int NST, bool fp32, Scratch &sc, cudaStream_t s) {
   const size_t qsz = fp32 ? 4 : 2;
