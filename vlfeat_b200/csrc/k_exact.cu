@@ -331,6 +331,52 @@ __global__ void k_colmass(const T *__restrict__ q, i64 N, int K, i64 rowsPerSlab
   }
 }
 
+// The same sums for fp32 posteriors with K a multiple of 4 (K <= 1024):
+// each thread reads four columns as a float4, the block covers
+// 1024 / K rows per pass (coalesced 16-byte loads), four rows per thread are
+// in flight, and the row groups are summed in index order at the end.
+__global__ void __launch_bounds__(kThreads) k_colmass4(const float *__restrict__ q, i64 N, int K,
+                                                       i64 rowsPerSlab, double *__restrict__ part) {
+  __shared__ double sh[4 * kThreads];  // [row group][column]
+  const int tpr = K / 4, rpb = kThreads / tpr;
+  const int rg = threadIdx.x / tpr, c4 = threadIdx.x % tpr;
+  const i64 r0 = (i64)blockIdx.x * rowsPerSlab, r1 = min(N, r0 + rowsPerSlab);
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  if (rg < rpb) {
+    i64 i = r0 + rg;
+    for (; i + 3 * rpb < r1; i += 4 * rpb) {
+      float4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = __ldg((const float4 *)(q + (i + u * rpb) * K) + c4);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        s0 += (double)v[u].x;
+        s1 += (double)v[u].y;
+        s2 += (double)v[u].z;
+        s3 += (double)v[u].w;
+      }
+    }
+    for (; i < r1; i += rpb) {
+      const float4 v = __ldg((const float4 *)(q + i * K) + c4);
+      s0 += (double)v.x;
+      s1 += (double)v.y;
+      s2 += (double)v.z;
+      s3 += (double)v.w;
+    }
+    double *row = sh + rg * K + 4 * c4;
+    row[0] = s0;
+    row[1] = s1;
+    row[2] = s2;
+    row[3] = s3;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < K; k += kThreads) {
+    double t = 0;
+    for (int g = 0; g < rpb; ++g) t += sh[g * K + k];
+    part[(i64)blockIdx.x * K + k] = t;
+  }
+}
+
 __global__ void k_sum_slabs(const double *__restrict__ part, int nslab, int K,
                             double *__restrict__ out) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -569,7 +615,14 @@ void column_mass(const T *q, i64 N, i64 K, double *mass, cudaStream_t s) {
   const int nslab = (int)((N + rps - 1) / rps > 0 ? (N + rps - 1) / rps : 1);
   double *part = thread_scratch(kArenaExact).slot[13].get<double>((size_t)nslab * K);
   if (N > 0) {
-    VLB_LAUNCH("column_mass", s, k_colmass<T><<<nslab, kThreads, 0, s>>>(q, N, (int)K, rps, part));
+    bool done = false;
+    if constexpr (sizeof(T) == 4) {
+      if (K % 4 == 0 && K <= 4 * kThreads) {
+        VLB_LAUNCH("column_mass", s, k_colmass4<<<nslab, kThreads, 0, s>>>((const float *)q, N, (int)K, rps, part));
+        done = true;
+      }
+    }
+    if (!done) VLB_LAUNCH("column_mass", s, k_colmass<T><<<nslab, kThreads, 0, s>>>(q, N, (int)K, rps, part));
   } else {
     VLB_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * nslab * K, s));
   }
