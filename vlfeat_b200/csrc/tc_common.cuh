@@ -38,14 +38,18 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
       : "memory");
 }
 
+// The waiting thread is suspended until the phase completes or up to
+// kSuspendNs, so idle roles do not take issue slots from working warps.
+constexpr uint32_t kSuspendNs = 1000000;
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
