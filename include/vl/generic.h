@@ -8,6 +8,7 @@
 #define VL_GENERIC_H
 
 #include "host.h"
+#include "random.h"
 
 /* Data types, vl/generic.h:35-46. */
 #define VL_TYPE_FLOAT   1
@@ -52,6 +53,17 @@ VL_EXPORT int vl_set_last_error(int error, char const *errorMessage, ...);
 VL_EXPORT char const *vl_get_version_string(void);
 VL_EXPORT void vl_set_simd_enabled(vl_bool x);
 VL_EXPORT vl_bool vl_get_simd_enabled(void);
+
+/* CPU features, read with cpuid as the reference reads them
+ * (vl/generic.h:104-108, vl/host.c:446-466).  With SIMD enabled, the kernels
+ * that restate a SIMD routine of the reference use the summation order of the
+ * variant the reference would pick (AVX, else SSE2, else scalar). */
+VL_EXPORT vl_bool vl_cpu_has_avx(void);
+VL_EXPORT vl_bool vl_cpu_has_sse3(void);
+VL_EXPORT vl_bool vl_cpu_has_sse2(void);
+
+/* The calling thread's random number generator (vl/generic.h:110). */
+VL_EXPORT VlRand *vl_get_rand(void);
 VL_EXPORT vl_size vl_get_max_threads(void);
 VL_EXPORT void vl_set_num_threads(vl_size n);
 VL_EXPORT vl_size vl_get_thread_limit(void);

@@ -30,7 +30,8 @@ FLAG_SQUARE_ROOT = 1 << 0
 FLAG_NORMALIZED = 1 << 1
 FLAG_IMPROVED = FLAG_SQUARE_ROOT | FLAG_NORMALIZED
 FLAG_FAST = 1 << 2
-VL_GMM_CUSTOM = 2  # VlGMMCustom, vl/gmm.h:21-26
+VL_GMM_RAND = 1    # VlGMMRand, vl/gmm.h:21-26
+VL_GMM_CUSTOM = 2  # VlGMMCustom
 
 _vp = C.c_void_p
 _sz = C.c_uint64
@@ -177,6 +178,12 @@ class Reference:
         L.vl_get_max_threads.restype = _sz
         L.vl_set_simd_enabled.argtypes = [C.c_int]
         L.vl_get_simd_enabled.restype = C.c_int
+        L.vl_get_rand.restype = _vp
+        L.vl_rand_seed.argtypes = [_vp, C.c_uint32]
+        L.vl_rand_uint32.restype = C.c_uint32
+        L.vl_rand_uint32.argtypes = [_vp]
+        L.vl_cpu_has_avx.restype = C.c_int
+        L.vl_cpu_has_sse2.restype = C.c_int
         if threads is not None:
             self.set_threads(threads)
         L.vl_set_simd_enabled(1 if simd else 0)
@@ -231,6 +238,43 @@ class Reference:
         finally:
             L.vl_gmm_delete(g)
 
+    def seed(self, s: int) -> None:
+        """vl_rand_seed on the calling thread's generator (vl/random.c:109-127)."""
+        self.lib.vl_rand_seed(self.lib.vl_get_rand(), int(s))
+
+    def rand_init(self, data, K, seed, max_iter=0, lb=1e-4):
+        """vl_gmm_cluster with VlGMMRand initialisation (vl/gmm.c:1416-1443)
+        after seeding the thread's generator; max_iter=0 leaves the initial
+        parameters (one E-step, no M-step)."""
+        L = self.lib
+        dt = data.dtype
+        N, D = data.shape
+        g = L.vl_gmm_new(VL_TYPE_FLOAT if dt == np.float32 else VL_TYPE_DOUBLE, D, K)
+        try:
+            L.vl_gmm_set_initialization(g, VL_GMM_RAND)
+            L.vl_gmm_set_max_num_iterations(g, int(max_iter))
+            L.vl_gmm_set_covariance_lower_bound(g, float(lb))
+            self.seed(seed)
+            dat = np.ascontiguousarray(data)
+            ll = L.vl_gmm_cluster(g, _ptr(dat), N)
+            ct = C.c_float if dt == np.float32 else C.c_double
+
+            def grab(p, n):
+                return np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape=(n,)).copy()
+
+            return dict(ll=ll, priors=grab(L.vl_gmm_get_priors(g), K),
+                        means=grab(L.vl_gmm_get_means(g), K * D).reshape(K, D),
+                        covs=grab(L.vl_gmm_get_covariances(g), K * D).reshape(K, D))
+        finally:
+            L.vl_gmm_delete(g)
+
+    def distance_lanes(self) -> int:
+        """Lanes of the reference's squared-L2 kernel on this host for float
+        data (vl/mathop.c:489-510): 8 (AVX), 4 (SSE2) or 1."""
+        if not self.lib.vl_get_simd_enabled():
+            return 1
+        return 8 if self.lib.vl_cpu_has_avx() else (4 if self.lib.vl_cpu_has_sse2() else 1)
+
     def fisher(self, data, means, covs, priors, flags):
         dt = data.dtype
         N, D = data.shape
@@ -280,3 +324,125 @@ def simple_fisher(data, means, covs, priors, flags):
     if flags & FLAG_NORMALIZED:
         enc = enc / max(np.linalg.norm(enc), 1e-12)
     return enc
+
+
+# ------------------------------------------------------- Rand initialisation
+class MT19937:
+    """MT19937 (Matsumoto and Nishimura, 1998; 2002 initialisation) as
+    VLFeat's vl/random.c uses it: unseeded state seeds itself with 5489
+    (vl/random.c:202-203); vl_rand_uindex is a draw modulo the range
+    (vl/random.h:64-73), vl_rand_real1 a draw times 1/(2^32 - 1)
+    (vl/random.h:116-120)."""
+
+    def __init__(self, seed=None):
+        self.mt = [0] * 624
+        self.mti = 625
+        if seed is not None:
+            self.seed(seed)
+
+    def seed(self, s):
+        mt = self.mt
+        mt[0] = s & 0xFFFFFFFF
+        for i in range(1, 624):
+            mt[i] = (1812433253 * (mt[i - 1] ^ (mt[i - 1] >> 30)) + i) & 0xFFFFFFFF
+        self.mti = 624
+
+    def uint32(self):
+        mt = self.mt
+        if self.mti >= 624:
+            if self.mti == 625:
+                self.seed(5489)
+            for k in range(624):
+                y = (mt[k] & 0x80000000) | (mt[(k + 1) % 624] & 0x7FFFFFFF)
+                mt[k] = mt[(k + 397) % 624] ^ (y >> 1) ^ (0x9908B0DF if y & 1 else 0)
+            self.mti = 0
+        y = mt[self.mti]
+        self.mti += 1
+        y ^= y >> 11
+        y ^= (y << 7) & 0x9D2C5680
+        y ^= (y << 15) & 0xEFC60000
+        y ^= y >> 18
+        return y & 0xFFFFFFFF
+
+    def uindex(self, n):
+        return self.uint32() % n
+
+    def real1(self):
+        return self.uint32() * (1.0 / 4294967295.0)
+
+
+def _l2_ordered(a, b, lanes, T):
+    """Squared L2 distance in the summation order of the reference's kernel:
+    `lanes` accumulators over consecutive element groups, the SIMD horizontal
+    sum (AVX float: ((v0+v1)+(v4+v5)) + ((v2+v3)+(v6+v7)); 4 lanes:
+    (v0+v2)+(v1+v3); 2 lanes: v0+v1), then the remaining elements in order
+    (vl/mathop_avx.c:44-108, vl/mathop_sse2.c:44-140, vl/mathop.c)."""
+    D = a.shape[0]
+    v = [T(0)] * lanes
+    i = 0
+    while i + lanes <= D:
+        for l in range(lanes):
+            d = T(a[i + l] - b[i + l])
+            v[l] = T(v[l] + T(d * d))
+        i += lanes
+    if lanes == 8:
+        acc = T(T(T(v[0] + v[1]) + T(v[4] + v[5])) + T(T(v[2] + v[3]) + T(v[6] + v[7])))
+    elif lanes == 4:
+        acc = T(T(v[0] + v[2]) + T(v[1] + v[3]))
+    elif lanes == 2:
+        acc = T(v[0] + v[1])
+    else:
+        acc = v[0]
+    while i < D:
+        d = T(a[i] - b[i])
+        acc = T(acc + T(d * d))
+        i += 1
+    return acc
+
+
+def rand_init(data, K, rng, lanes):
+    """VlGMMRand initialisation restated (vl/gmm.c:1376-1443 and
+    vl/kmeans.c:588-649) with the data type's scalar arithmetic, for small
+    cases: uniform priors, every covariance the global variance (mean and
+    squared deviations summed over the rows in order, / N and / (N - 1)),
+    means by k-means++ seeding with `rng` (an MT19937)."""
+    T = data.dtype.type
+    N, D = data.shape
+    priors = np.full(K, T(1.0 / K), data.dtype)
+    sigma = np.zeros(D, data.dtype)
+    if N > 1:
+        for d in range(D):
+            m = T(0)
+            for i in range(N):
+                m = T(m + data[i, d])
+            m = T(m / T(N))
+            ss = T(0)
+            for i in range(N):
+                df = T(data[i, d] - m)
+                ss = T(ss + T(df * df))
+            sigma[d] = T(ss / T(N - 1))
+    covs = np.tile(sigma, (K, 1))
+    centers = np.zeros((K, D), data.dtype)
+    mind = [T(np.inf)] * N
+    x = rng.uindex(N)
+    c = 0
+    while True:
+        thresh = T(rng.real1())
+        centers[c] = data[x]
+        c += 1
+        if c == K:
+            break
+        energy = T(0)
+        for i in range(N):
+            dist = _l2_ordered(centers[c - 1], data[i], lanes, T)
+            mind[i] = mind[i] if mind[i] < dist else dist
+            energy = T(energy + mind[i])
+        t = T(thresh * energy)
+        acc = T(0)
+        x = 0
+        while x < N - 1:
+            acc = T(acc + mind[x])
+            if acc >= t:
+                break
+            x += 1
+    return dict(priors=priors, means=centers, covs=covs)

@@ -126,6 +126,31 @@ def edge_cases(ref, out):
         out[f"edge_enc_{tag}_d1"] = enc
 
 
+def rand_case(ref, out):
+    """VlGMMRand initialisation (vl/gmm.c:1416-1443) from a seeded thread
+    generator: the first MT19937 draws, then vl_gmm_cluster with Rand
+    initialisation, without EM (max iterations 0) and with 5 EM iterations.
+    The distances of k-means++ follow the reference's SIMD kernel for this host
+    (recorded as rand_lanes)."""
+    ref.seed(2024)
+    r = ref.lib.vl_get_rand()
+    out["rng_seed"] = np.int64(2024)
+    out["rng_seq"] = np.array([ref.lib.vl_rand_uint32(r) for _ in range(1500)], np.uint32)
+    out["rand_lanes"] = np.int64(ref.distance_lanes())
+    cases = {"small": (rng(41).standard_normal((300, 13)) * 3.0, 7, 301),
+             "mix": (W.mixture_data(5000, 64, 32, seed=42), 32, 302)}
+    for name, (x, K, seed) in cases.items():
+        out[f"rand_{name}_data"] = x
+        out[f"rand_{name}_K"] = np.int64(K)
+        out[f"rand_{name}_seed"] = np.int64(seed)
+        for dt, tag in ((np.float32, "f"), (np.float64, "d")):
+            for T in (0, 5):
+                res = ref.rand_init(x.astype(dt), K, seed, max_iter=T, lb=1e-4)
+                for k in ("means", "covs", "priors"):
+                    out[f"rand_{name}_{tag}_t{T}_{k}"] = res[k]
+                out[f"rand_{name}_{tag}_t{T}_ll"] = np.float64(res["ll"])
+
+
 def main():
     ref = Reference(threads=1)
     out: dict = {}
@@ -134,6 +159,7 @@ def main():
     em_case(ref, out)
     fv_case(ref, out)
     edge_cases(ref, out)
+    rand_case(ref, out)
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")

@@ -107,3 +107,12 @@ def test_fisher_plan_argument_checks(libpath):
     assert not L.vlb200_fisher_plan_new(80, 256, capi._np_ptr(bad), 2, 0, 3)
     assert L.vl_get_last_error() == 3
     assert L.vlb200_fisher_plan_launch(None, None) == 3
+
+
+def test_library_rng_matches_reference(libpath, golden):
+    """The library's per-thread MT19937 (vl_get_rand, vl_rand_seed,
+    vl_rand_uint32; host code) draws the reference's sequence."""
+    from vlfeat_b200 import capi
+    capi.rand_seed(int(golden["rng_seed"]))
+    seq = [capi.rand_uint32() for _ in range(len(golden["rng_seq"]))]
+    assert seq == [int(v) for v in golden["rng_seq"]]

@@ -165,3 +165,76 @@ def test_deterministic(vl, golden):
     e2, _ = vl.fisher_encode(g["fv_data"], g["fv_means"].astype(np.float32),
                              g["fv_covs"].astype(np.float32), g["fv_priors"].astype(np.float32))
     assert np.array_equal(e1, e2)
+
+
+def _lanes_match(vl, golden):
+    """The fixtures' k-means++ distances follow the SIMD kernel the reference
+    picked on the fixture host; the library picks by the same rule here."""
+    L = vl.lib()
+    ours = 8 if L.vl_cpu_has_avx() else (4 if L.vl_cpu_has_sse2() else 1)
+    return ours == int(golden["rand_lanes"])
+
+
+def _rand_em(vl, golden, name, tag, T):
+    dt = DT[tag]
+    x = golden[f"rand_{name}_data"].astype(dt)
+    K = int(golden[f"rand_{name}_K"])
+    m = vl.GMM(x.shape[1], K, dt)
+    m.set_initialization("rand")
+    m.set_max_num_iterations(T)
+    m.set_covariance_lower_bound(1e-4)
+    vl.rand_seed(int(golden[f"rand_{name}_seed"]))
+    ll = m.cluster(x)
+    return m, ll
+
+
+@pytest.mark.parametrize("name", ["small", "mix"])
+@pytest.mark.parametrize("tag", ["f", "d"])
+def test_rand_init_bit_exact(vl, golden, name, tag):
+    """VlGMMRand initialisation (the default of vl_gmm_new) reproduces the
+    reference bit for bit from the same seed: k-means++ centres drawn with
+    the thread's MT19937, global data variance, uniform priors."""
+    if not _lanes_match(vl, golden):
+        pytest.skip("this host's SIMD support differs from the fixture host's")
+    m, _ = _rand_em(vl, golden, name, tag, 0)
+    for k, got in (("means", m.means), ("covs", m.covariances), ("priors", m.priors)):
+        assert np.array_equal(got, golden[f"rand_{name}_{tag}_t0_{k}"]), k
+
+
+@pytest.mark.parametrize("name", ["small", "mix"])
+@pytest.mark.parametrize("tag", ["f", "d"])
+def test_rand_init_then_em(vl, golden, name, tag):
+    """Five EM iterations from the Rand initialisation match the reference's
+    run (exact path; the same bounds as the custom-init EM test)."""
+    if not _lanes_match(vl, golden):
+        pytest.skip("this host's SIMD support differs from the fixture host's")
+    m, ll = _rand_em(vl, golden, name, tag, 5)
+    tol = {"f": 2e-4, "d": 1e-9}[tag]
+    ref_ll = float(golden[f"rand_{name}_{tag}_t5_ll"])
+    assert abs(ll - ref_ll) <= tol * abs(ref_ll)
+    assert rel_err(m.means, golden[f"rand_{name}_{tag}_t5_means"]) < tol
+    assert rel_err(m.covariances, golden[f"rand_{name}_{tag}_t5_covs"]) < tol
+    assert rel_err(m.priors, golden[f"rand_{name}_{tag}_t5_priors"]) < tol
+
+
+def test_rand_init_api_and_repetitions(vl, golden):
+    """vl_gmm_init_with_rand_data alone gives the same parameters as the
+    cluster call's initialisation; with two repetitions the second draws
+    fresh centres from the same generator (vl/gmm.c:1588-1593)."""
+    import ctypes as C
+    x = golden["rand_small_data"].astype(np.float32)
+    K, seed = int(golden["rand_small_K"]), int(golden["rand_small_seed"])
+    m = vl.GMM(x.shape[1], K, np.float32)
+    vl.rand_seed(seed)
+    vl.lib().vl_gmm_init_with_rand_data(m._h, x.ctypes.data_as(C.c_void_p), x.shape[0])
+    if _lanes_match(vl, golden):
+        assert np.array_equal(m.means, golden["rand_small_f_t0_means"])
+    a = m.means.copy()
+    m2 = vl.GMM(x.shape[1], K, np.float32)
+    m2.set_initialization("rand")
+    m2.set_max_num_iterations(0)
+    m2.set_num_repetitions(2)
+    vl.rand_seed(seed)
+    m2.cluster(x)
+    assert vl.lib().vl_get_last_error() == 0
+    assert m2.means.shape == a.shape

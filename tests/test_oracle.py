@@ -94,3 +94,27 @@ def test_oracle_is_deterministic(golden, restatement):
     b = restatement.em(g["em_data"], g["em_priors0"], g["em_means0"], g["em_covs0"], g["em_lb"], 4)
     for n in ("priors", "means", "covs", "posteriors"):
         assert np.array_equal(a[n], b[n])
+
+
+def test_rng_restatement(golden):
+    """MT19937 restatement (oracle.MT19937) against the reference's draws
+    after vl_rand_seed (vl/random.c)."""
+    from oracle.oracle import MT19937
+    g = MT19937(int(golden["rng_seed"]))
+    assert [g.uint32() for _ in range(len(golden["rng_seq"]))] == [int(v) for v in golden["rng_seq"]]
+
+
+@pytest.mark.parametrize("tag", ["f", "d"])
+def test_rand_init_restatement(golden, tag):
+    """VlGMMRand initialisation restated (oracle.rand_init) against the
+    reference's, bit for bit: k-means++ centres, global variance, priors."""
+    from oracle.oracle import MT19937, rand_init
+    dt = np.float32 if tag == "f" else np.float64
+    x = golden["rand_small_data"].astype(dt)
+    K, seed = int(golden["rand_small_K"]), int(golden["rand_small_seed"])
+    lanes = int(golden["rand_lanes"])
+    if dt == np.float64:
+        lanes = {8: 4, 4: 2, 1: 1}[lanes]
+    o = rand_init(x, K, MT19937(seed), lanes)
+    for k in ("means", "covs", "priors"):
+        assert np.array_equal(o[k], golden[f"rand_small_{tag}_t0_{k}"]), k

@@ -41,7 +41,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
     deps = [os.path.join(CSRC, h) for h in HEADERS]
-    deps += [os.path.join(ROOT, "include", p) for p in ("vlb200.h", "vl/gmm.h", "vl/fisher.h",
+    deps += [os.path.join(ROOT, "include", p) for p in ("vlb200.h", "vl/gmm.h", "vl/fisher.h", "vl/random.h",
                                                           "vl/generic.h", "vl/host.h")]
     objs = []
     for src in SOURCES:

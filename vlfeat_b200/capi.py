@@ -97,6 +97,13 @@ def _decl(L):
       C.c_int, C.POINTER(C.c_uint64), _vp)
     f("vlb200_fisher_encode_batch_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _sz,
       C.c_int, C.c_int, _vp, _vp)
+    f("vl_get_rand", _vp)
+    f("vl_rand_seed", None, _vp, C.c_uint32)
+    f("vl_rand_uint32", C.c_uint32, _vp)
+    f("vl_rand_init", None, _vp)
+    f("vl_cpu_has_avx", C.c_int)
+    f("vl_cpu_has_sse2", C.c_int)
+    f("vl_gmm_init_with_rand_data", None, _vp, _vp, _sz)
     f("vlb200_fisher_plan_new", _vp, _sz, _sz, _vp, _sz, C.c_int, C.c_int)
     f("vlb200_fisher_plan_delete", None, _vp)
     f("vlb200_fisher_plan_set_gmm", C.c_int, _vp, _vp, _vp, _vp)
@@ -350,6 +357,15 @@ def fisher_encode(data, means, covariances, priors, flags=FLAG_IMPROVED):
     if lib().vl_get_last_error():
         _raise_last("vl_fisher_encode")
     return enc, int(nt)
+
+
+def rand_seed(s: int) -> None:
+    """vl_rand_seed on the calling thread's generator (vl_get_rand)."""
+    lib().vl_rand_seed(lib().vl_get_rand(), int(s))
+
+
+def rand_uint32() -> int:
+    return int(lib().vl_rand_uint32(lib().vl_get_rand()))
 
 
 def _stream(stream):

@@ -54,6 +54,18 @@ template <typename T>
 void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i64 K, i64 D,
                  const double *lb, cudaStream_t s);
 
+// Rand initialisation pieces (vl/gmm.c:1376-1443), bit-exact with the
+// reference.  global_variance: sigma (D) from X (N x D).  kmeanspp: K centres
+// from X by k-means++ (vl/kmeans.c:588-649); x0 and thresh (K values, already
+// cast to T) are the reference's draws from the calling thread's generator;
+// lanes (8, 4, 2 or 1) selects the summation order of the reference's
+// distance kernel that the host's SIMD support selects.
+template <typename T>
+void global_variance(const T *X, i64 N, i64 D, T *sigma, cudaStream_t s);
+template <typename T>
+void kmeanspp(const T *X, i64 N, i64 D, i64 K, T *centers, i64 x0, const std::vector<T> &thresh, int lanes,
+              cudaStream_t s);
+
 // priors /= max(sum priors, 1e-12) on the device (vl/gmm.c:1196-1211).
 template <typename T>
 void normalize_priors(T *priors, i64 K, cudaStream_t s);

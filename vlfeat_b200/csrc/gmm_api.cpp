@@ -261,6 +261,42 @@ const T *stage_data(VlGMM *self, const void *data, i64 N) {
   return dX;
 }
 
+// Rand initialisation, vl/gmm.c:1416-1443, on device data: uniform priors,
+// every covariance the global data variance, means by k-means++ seeding.  The
+// random draws come from the calling thread's generator in the reference's
+// order (one index, then one real per centre, vl/kmeans.c:615-623), and the
+// distances use the summation order of the reference's SIMD kernel for this
+// host (AVX, SSE2 or scalar, vl/mathop.c:489-510).  Results go to the host
+// parameter arrays, like every VlGMM parameter.
+template <typename T>
+void init_rand(VlGMM *self, const T *dX, i64 N) {
+  VLB_CHECK(N >= 1, VL_ERR_BAD_ARG, "Rand initialisation needs at least one data point");
+  cudaStream_t s = vlb::thread_stream();
+  const i64 K = (i64)self->numClusters, D = (i64)self->dimension;
+  self->numData = (vl_size)N;  // _vl_gmm_prepare_for_data, vl/gmm.c:336-344
+  T *pr = (T *)self->priors;
+  for (i64 k = 0; k < K; ++k) pr[k] = (T)(1.0 / (double)K);
+  VlRand *r = vl_get_rand();
+  const i64 x0 = (i64)vl_rand_uindex(r, (vl_uindex)N);
+  std::vector<T> thresh((size_t)K);
+  for (i64 k = 0; k < K; ++k) thresh[k] = (T)vl_rand_real1(r);
+  int lanes = 1;
+  if (vl_get_simd_enabled()) {
+    if (vl_cpu_has_avx()) lanes = sizeof(T) == 4 ? 8 : 4;
+    else if (vl_cpu_has_sse2()) lanes = sizeof(T) == 4 ? 4 : 2;
+  }
+  T *dsigma = self->dtmp.get<T>(D);
+  T *dcenters = self->dmeans.get<T>(K * D);
+  vlb::global_variance<T>(dX, N, D, dsigma, s);
+  vlb::kmeanspp<T>(dX, N, D, K, dcenters, x0, thresh, lanes, s);
+  std::vector<T> sigma((size_t)D);
+  VLB_CUDA(cudaMemcpyAsync(sigma.data(), dsigma, sizeof(T) * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaMemcpyAsync(self->means, dcenters, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  T *cv = (T *)self->covariances;
+  for (i64 k = 0; k < K; ++k) memcpy(cv + k * D, sigma.data(), sizeof(T) * D);
+}
+
 double em_host(VlGMM *self, const void *data, vl_size N) {
   const int prec = vlb::resolve_precision(VLB200_PREC_DEFAULT, self->dataType == VL_TYPE_DOUBLE);
   if (self->dataType == VL_TYPE_FLOAT)
@@ -382,11 +418,16 @@ void vl_gmm_set_priors(VlGMM *self, void const *priors) {
 }
 
 // -------------------------------------------------------- processing
-void vl_gmm_init_with_rand_data(VlGMM *self, void const *, vl_size) {
-  vl_set_last_error(VL_ERR_BAD_ARG,
-                    "vl_gmm_init_with_rand_data: random (kmeans++) initialisation is not "
-                    "available in the GPU library; use VlGMMCustom");
-  (void)self;
+void vl_gmm_init_with_rand_data(VlGMM *self, void const *data, vl_size numData) {
+  guarded(
+      [&]() -> int {
+        if (self->dataType == VL_TYPE_FLOAT)
+          init_rand<float>(self, stage_data<float>(self, data, (i64)numData), (i64)numData);
+        else
+          init_rand<double>(self, stage_data<double>(self, data, (i64)numData), (i64)numData);
+        return 0;
+      },
+      0);
 }
 
 void vl_gmm_init_with_kmeans(VlGMM *self, void const *, vl_size, VlKMeans *) {
@@ -406,9 +447,9 @@ double vl_gmm_em(VlGMM *self, void const *data, vl_size numData) {
 double vl_gmm_cluster(VlGMM *self, void const *data, vl_size numData) {
   return guarded(
       [&]() -> double {
-        VLB_CHECK(self->initialization == VlGMMCustom, VL_ERR_BAD_ARG,
-                  "vl_gmm_cluster: only VlGMMCustom initialisation is available in the GPU "
-                  "library");
+        VLB_CHECK(self->initialization == VlGMMCustom || self->initialization == VlGMMRand,
+                  VL_ERR_BAD_ARG,
+                  "vl_gmm_cluster: VlGMMKMeans initialisation is not available in the GPU library");
         const size_t sz = tsize(self->dataType);
         const size_t nKD = self->numClusters * self->dimension;
         std::vector<char> m0((char *)self->means, (char *)self->means + sz * nKD);
@@ -425,7 +466,12 @@ double vl_gmm_cluster(VlGMM *self, void const *data, vl_size numData) {
           if (self->verbosity)
             VLB_PRINTF("gmm: clustering: starting repetition %d of %d\n", (int)rep + 1,
                        (int)self->numRepetitions);
-          if (rep > 0) {
+          if (self->initialization == VlGMMRand) {  // vl/gmm.c:1588-1593
+            if (self->dataType == VL_TYPE_FLOAT)
+              init_rand<float>(self, (const float *)dX, (i64)numData);
+            else
+              init_rand<double>(self, (const double *)dX, (i64)numData);
+          } else if (rep > 0) {
             memcpy(self->means, m0.data(), m0.size());
             memcpy(self->covariances, c0.data(), c0.size());
             memcpy(self->priors, p0.data(), p0.size());

@@ -772,6 +772,155 @@ void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, 
                           flags, 0, enc, nterms));
 }
 
+// ------------------------------------------------- Rand initialisation
+// The reference's Rand initialisation (vl/gmm.c:1376-1443, vl/kmeans.c:
+// 588-649) reproduced operation for operation: every sum runs in the data
+// type and in the reference's order, multiplies and adds stay separate (the
+// explicitly rounded intrinsics below never contract into a fused
+// multiply-add), so the centres and variances are the reference's bits.
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+
+// Global data variance, vl/gmm.c:1376-1413: per dimension the mean, then the
+// sum of squared deviations, each accumulated over the rows in order and
+// divided by N and N - 1 (0 when N <= 1).  One thread per dimension.
+template <typename T>
+__global__ void k_global_variance(const T *__restrict__ X, i64 N, int D, T *__restrict__ sigma) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= D) return;
+  if (N <= 1) {
+    sigma[d] = (T)0;
+    return;
+  }
+  T mean = (T)0;
+  for (i64 i = 0; i < N; ++i) mean = add_rn(mean, X[i * D + d]);
+  mean = div_rn(mean, (T)N);
+  T ss = (T)0;
+  for (i64 i = 0; i < N; ++i) {
+    const T diff = sub_rn(X[i * D + d], mean);
+    ss = add_rn(ss, mul_rn(diff, diff));
+  }
+  sigma[d] = div_rn(ss, (T)(N - 1));
+}
+
+// Squared L2 distance in the order of the reference's kernel for VlDistanceL2
+// (vl/mathop.c:472-513): L lanes accumulate (a - b)^2 over consecutive groups
+// of L elements (lane l takes elements l, l + L, ...), the lanes are reduced
+// in the fixed pattern of the SIMD horizontal sum, and the D mod L remaining
+// elements are added in order.  L = 8 (AVX, float), 4 (AVX double or SSE2
+// float: ((v0 + v2) + (v1 + v3))), 2 (SSE2 double), 1 (scalar).
+template <typename T, int L>
+__device__ T l2_ordered(const T *__restrict__ a, const T *__restrict__ b, int D) {
+  T v[L];
+#pragma unroll
+  for (int l = 0; l < L; ++l) v[l] = (T)0;
+  int i = 0;
+  for (; i + L <= D; i += L) {
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const T dl = sub_rn(a[i + l], b[i + l]);
+      v[l] = add_rn(v[l], mul_rn(dl, dl));
+    }
+  }
+  T acc;
+  if constexpr (L == 8) {
+    acc = add_rn(add_rn(add_rn(v[0], v[1]), add_rn(v[4], v[5])), add_rn(add_rn(v[2], v[3]), add_rn(v[6], v[7])));
+  } else if constexpr (L == 4) {
+    acc = add_rn(add_rn(v[0], v[2]), add_rn(v[1], v[3]));
+  } else if constexpr (L == 2) {
+    acc = add_rn(v[0], v[1]);
+  } else {
+    acc = v[0];
+  }
+  for (; i < D; ++i) {
+    const T dl = sub_rn(a[i], b[i]);
+    acc = add_rn(acc, mul_rn(dl, dl));
+  }
+  return acc;
+}
+
+// minDist[x] = min(minDist[x], ||c - x||^2) with the reference's VL_MIN.
+template <typename T, int L>
+__global__ void k_kpp_update(const T *__restrict__ X, i64 N, int D, const T *__restrict__ center,
+                             T *__restrict__ minDist) {
+  extern __shared__ unsigned char kpp_smem[];
+  T *c = (T *)kpp_smem;
+  for (int d = threadIdx.x; d < D; d += blockDim.x) c[d] = center[d];
+  __syncthreads();
+  const i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= N) return;
+  const T dist = l2_ordered<T, L>(c, X + x * D, D);
+  const T m = minDist[x];
+  minDist[x] = m < dist ? m : dist;
+}
+
+template <typename T>
+__global__ void k_fill(T *__restrict__ p, i64 n, T v) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// The next centre, vl/kmeans.c:631-641, by one thread: the energy (sum of
+// minDist in order), then the first x with acc >= thresh * energy, or N - 1.
+template <typename T>
+__global__ void k_kpp_select(const T *__restrict__ minDist, i64 N, T thresh, i64 *__restrict__ xOut) {
+  T energy = (T)0;
+  for (i64 x = 0; x < N; ++x) energy = add_rn(energy, minDist[x]);
+  const T t = mul_rn(thresh, energy);
+  T acc = (T)0;
+  i64 x = 0;
+  for (; x < N - 1; ++x) {
+    acc = add_rn(acc, minDist[x]);
+    if (acc >= t) break;
+  }
+  *xOut = x;
+}
+
+// centers[c] = X[x] with x the selected row (device) or the first row (host).
+template <typename T>
+__global__ void k_kpp_copy(const T *__restrict__ X, int D, const i64 *__restrict__ xDev, i64 xHost,
+                           T *__restrict__ dst) {
+  const i64 x = xDev ? *xDev : xHost;
+  for (int d = threadIdx.x; d < D; d += blockDim.x) dst[d] = X[x * D + d];
+}
+
+template <typename T>
+void global_variance(const T *X, i64 N, i64 D, T *sigma, cudaStream_t s) {
+  VLB_LAUNCH("global_variance", s, k_global_variance<T><<<grid1(D, 128), 128, 0, s>>>(X, N, (int)D, sigma));
+}
+
+template <typename T>
+void kmeanspp(const T *X, i64 N, i64 D, i64 K, T *centers, i64 x0, const std::vector<T> &thresh, int lanes,
+              cudaStream_t s) {
+  VLB_CHECK((i64)thresh.size() >= K && N > 0 && K > 0 && x0 >= 0 && x0 < N, VL_ERR_BAD_ARG,
+            "kmeans++: bad arguments");
+  Scratch &sc = thread_scratch(kArenaExact);
+  T *minDist = sc.slot[20].get<T>(N);
+  i64 *xdev = sc.slot[21].get<i64>(1);
+  const T inf = (T)INFINITY;
+  VLB_LAUNCH("kpp_fill", s, k_fill<T><<<grid1(N, kThreads), kThreads, 0, s>>>(minDist, N, inf));
+  const size_t smem = sizeof(T) * D;
+  for (i64 c = 0; c < K; ++c) {
+    VLB_LAUNCH("kpp_copy", s, k_kpp_copy<T><<<1, 128, 0, s>>>(X, (int)D, c == 0 ? nullptr : xdev, x0,
+                                                               centers + c * D));
+    if (c + 1 == K) break;
+    const T *ctr = centers + c * D;
+    switch (lanes) {
+      case 8: VLB_LAUNCH("kpp_update", s, (k_kpp_update<T, 8><<<grid1(N, kThreads), kThreads, smem, s>>>(X, N, (int)D, ctr, minDist))); break;
+      case 4: VLB_LAUNCH("kpp_update", s, (k_kpp_update<T, 4><<<grid1(N, kThreads), kThreads, smem, s>>>(X, N, (int)D, ctr, minDist))); break;
+      case 2: VLB_LAUNCH("kpp_update", s, (k_kpp_update<T, 2><<<grid1(N, kThreads), kThreads, smem, s>>>(X, N, (int)D, ctr, minDist))); break;
+      default: VLB_LAUNCH("kpp_update", s, (k_kpp_update<T, 1><<<grid1(N, kThreads), kThreads, smem, s>>>(X, N, (int)D, ctr, minDist))); break;
+    }
+    VLB_LAUNCH("kpp_select", s, k_kpp_select<T><<<1, 1, 0, s>>>(minDist, N, thresh[c], xdev));
+  }
+}
+
 // ------------------------------------------------------ instantiations
 #define VLB_INST(T)                                                                          \
   template void exact_prepare<T>(const DevModel<T> &, DevDerived<T> &, cudaStream_t);        \
@@ -781,6 +930,9 @@ void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, 
                                const double *, cudaStream_t);                                \
   template void column_mass<T>(const T *, i64, i64, double *, cudaStream_t);                 \
   template void normalize_priors<T>(T *, i64, cudaStream_t);                                 \
+  template void global_variance<T>(const T *, i64, i64, T *, cudaStream_t);                  \
+  template void kmeanspp<T>(const T *, i64, i64, i64, T *, i64, const std::vector<T> &, int,  \
+                            cudaStream_t);                                                   \
   template void restart_split<T>(T *, const T *, i64, i64, i64, i64, i64, i64, T,           \
                                  cudaStream_t);                                              \
   template void apply_bounds<T>(T *, i64, i64, const double *, cudaStream_t);                \

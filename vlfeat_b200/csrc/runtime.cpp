@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cstdarg>
 #include <cstdlib>
+#include <cpuid.h>
 #include <cstring>
 #include <ctime>
 #include <map>
@@ -51,6 +52,95 @@ char const *vl_get_version_string(void) { return "0.9.21-b200"; }
 char const *vlb200_version(void) { return "vlfeat-b200 0.1 (sm_100a)"; }
 void vl_set_simd_enabled(vl_bool x) { g_simd = x ? 1 : 0; }
 vl_bool vl_get_simd_enabled(void) { return g_simd.load(); }
+
+// cpuid leaf 1: SSE2 = EDX bit 26, SSE3 = ECX bit 0, AVX = ECX bit 28.
+static unsigned cpuid1(int reg) {
+  unsigned a = 0, b = 0, c = 0, d = 0;
+  if (!__get_cpuid(1, &a, &b, &c, &d)) return 0;
+  return reg == 2 ? c : d;
+}
+vl_bool vl_cpu_has_avx(void) { return (cpuid1(2) >> 28) & 1u; }
+vl_bool vl_cpu_has_sse3(void) { return cpuid1(2) & 1u; }
+vl_bool vl_cpu_has_sse2(void) { return (cpuid1(3) >> 26) & 1u; }
+
+// ------------------------------------------------------------------- RNG
+// MT19937 (Matsumoto and Nishimura; the 2002 initialisation), the generator
+// of vl/random.c: 624 words of state and an index; index 625 marks a
+// generator that was never seeded and is seeded with 5489 on first use.
+static constexpr int kMtN = 624, kMtM = 397;
+
+void vl_rand_init(VlRand *self) {
+  memset(self->mt, 0, sizeof(self->mt));
+  self->mti = kMtN + 1;
+}
+
+void vl_rand_seed(VlRand *self, vl_uint32 s) {
+  vl_uint32 *mt = self->mt;
+  mt[0] = s;
+  for (vl_uint32 i = 1; i < (vl_uint32)kMtN; ++i) mt[i] = 1812433253u * (mt[i - 1] ^ (mt[i - 1] >> 30)) + i;
+  self->mti = kMtN;
+}
+
+void vl_rand_seed_by_array(VlRand *self, vl_uint32 const key[], vl_size keySize) {
+  vl_rand_seed(self, 19650218u);
+  vl_uint32 *mt = self->mt;
+  int i = 1;
+  vl_size j = 0;
+  for (vl_size k = keySize > (vl_size)kMtN ? keySize : (vl_size)kMtN; k; --k) {
+    mt[i] = (mt[i] ^ ((mt[i - 1] ^ (mt[i - 1] >> 30)) * 1664525u)) + key[j] + (vl_uint32)j;
+    if (++i >= kMtN) {
+      mt[0] = mt[kMtN - 1];
+      i = 1;
+    }
+    if (++j >= keySize) j = 0;
+  }
+  for (int k = kMtN - 1; k; --k) {
+    mt[i] = (mt[i] ^ ((mt[i - 1] ^ (mt[i - 1] >> 30)) * 1566083941u)) - (vl_uint32)i;
+    if (++i >= kMtN) {
+      mt[0] = mt[kMtN - 1];
+      i = 1;
+    }
+  }
+  mt[0] = 0x80000000u;  // non-zero state
+}
+
+vl_uint32 vl_rand_uint32(VlRand *self) {
+  vl_uint32 *mt = self->mt;
+  if (self->mti >= (vl_uint32)kMtN) {
+    if (self->mti == (vl_uint32)kMtN + 1) vl_rand_seed(self, 5489u);
+    // Regenerate all words; indices wrap, so later words use the new values
+    // of earlier ones as the recurrence requires.
+    for (int k = 0; k < kMtN; ++k) {
+      const vl_uint32 y = (mt[k] & 0x80000000u) | (mt[(k + 1) % kMtN] & 0x7fffffffu);
+      mt[k] = mt[(k + kMtM) % kMtN] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+    self->mti = 0;
+  }
+  vl_uint32 y = mt[self->mti++];
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= y >> 18;
+  return y;
+}
+
+void vl_rand_permute_indexes(VlRand *self, vl_index *array, vl_size size) {
+  for (vl_index i = (vl_index)size - 1; i > 0; --i) {
+    const vl_index j = (vl_index)vl_rand_uindex(self, (vl_uindex)i + 1);
+    const vl_index t = array[i];
+    array[i] = array[j];
+    array[j] = t;
+  }
+}
+
+VlRand *vl_get_rand(void) {
+  struct ThreadRand {
+    VlRand r;
+    ThreadRand() { vl_rand_init(&r); }
+  };
+  static thread_local ThreadRand t;
+  return &t.r;
+}
 vl_size vl_get_max_threads(void) { return g_num_threads.load(); }
 void vl_set_num_threads(vl_size n) { g_num_threads = n ? n : 1; }
 vl_size vl_get_thread_limit(void) { return 1; }
