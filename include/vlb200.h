@@ -93,6 +93,21 @@ VL_EXPORT int vlb200_fisher_encode_batch_device(float *enc, float const *means, 
                                                 int flags, int precision, vl_uint64 *numTerms,
                                                 void *stream);
 
+/* Batched VLAD encoding (vl_vlad_encode, vl/vlad.h:45-50) of many images
+ * of uneven size in one call, with device pointers.  dataType: VL_TYPE_FLOAT
+ * or VL_TYPE_DOUBLE, for every array.  data: total x dimension rows; image j
+ * owns rows offsets[j] .. offsets[j+1]-1 of data and of assignments (total x
+ * numClusters weights); offsets: numImages+1 int64 (host).  enc: numImages x
+ * numClusters x dimension (device), image-major.  Each image's encoding is
+ * bit-equal to vl_vlad_encode on its rows.  dimension <= 1024.  Returns 0, or
+ * a VL_ERR_* code (recorded as the last error).  Returns once the encodings
+ * are written. */
+VL_EXPORT int vlb200_vlad_encode_batch_device(void *enc, vl_type dataType, void const *means,
+                                              vl_size dimension, vl_size numClusters,
+                                              void const *data, void const *assignments,
+                                              vl_int64 const *offsets, vl_size numImages,
+                                              int flags, void *stream);
+
 /* ------------------------------------------------------ batched encode plan
  * A plan binds the tensor-core batched encoder to one batch layout (offsets,
  * numImages), dimension, numClusters, flags and precision (FP32, BF16 or

@@ -10,7 +10,9 @@ does.
 * :class:`Reference` drives ``oracle/_ref/libvl_ref.so``, VLFeat's own CPU
   code compiled from the reference sources by ``oracle/Makefile`` (target
   ``ref``), through VLFeat's unchanged C API (vl/gmm.h:40-145,
-  vl/fisher.h:48-54).  It exists only where that library was built.
+  vl/fisher.h:48-54, vl/vlad.h:45-50).  It exists only where that library was
+  built.
+* :func:`vlad` restates VLAD encoding (vl/vlad.c:163-242) in NumPy.
 """
 from __future__ import annotations
 
@@ -30,6 +32,10 @@ FLAG_SQUARE_ROOT = 1 << 0
 FLAG_NORMALIZED = 1 << 1
 FLAG_IMPROVED = FLAG_SQUARE_ROOT | FLAG_NORMALIZED
 FLAG_FAST = 1 << 2
+VLAD_NORMALIZE_COMPONENTS = 1 << 0  # vl/vlad.h:23-26
+VLAD_SQUARE_ROOT = 1 << 1
+VLAD_UNNORMALIZED = 1 << 2
+VLAD_NORMALIZE_MASS = 1 << 3
 VL_GMM_RAND = 1    # VlGMMRand, vl/gmm.h:21-26
 VL_GMM_CUSTOM = 2  # VlGMMCustom
 
@@ -174,6 +180,8 @@ class Reference:
             f = getattr(L, "vl_get_gmm_data_posteriors" + s)
             f.restype = C.c_double
             f.argtypes = [_vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp]
+        L.vl_vlad_encode.restype = None
+        L.vl_vlad_encode.argtypes = [_vp, C.c_uint32, _vp, _sz, _sz, _vp, _sz, _vp, C.c_int]
         L.vl_set_num_threads.argtypes = [_sz]
         L.vl_get_max_threads.restype = _sz
         L.vl_set_simd_enabled.argtypes = [C.c_int]
@@ -286,6 +294,79 @@ class Reference:
             _ptr(np.ascontiguousarray(covs, dt)), _ptr(np.ascontiguousarray(priors, dt)),
             _ptr(np.ascontiguousarray(data)), N, int(flags))
         return enc, int(nt)
+
+
+    def vlad(self, data, means, assignments, flags):
+        """vl_vlad_encode (vl/vlad.h:45-50): K x D encoding of data's dtype."""
+        dt = data.dtype
+        N, D = data.shape
+        K = means.shape[0]
+        typ = VL_TYPE_FLOAT if dt == np.float32 else VL_TYPE_DOUBLE
+        enc = np.zeros(K * D, dt)
+        self.lib.vl_vlad_encode(
+            _ptr(enc), typ, _ptr(np.ascontiguousarray(means, dt)), D, K,
+            _ptr(np.ascontiguousarray(data)), N,
+            _ptr(np.ascontiguousarray(assignments, dt)), int(flags))
+        return enc
+
+
+def vlad(data, means, assignments, flags):
+    """VLAD encoding restated (vl/vlad.c:163-242) in the data type's scalar
+    arithmetic, vectorised over components and dimensions only: every
+    accumulation keeps the reference's order.
+
+    * enc_k += a_ik x_i for rows in order where a_ik > 0, each step computed
+      in double and rounded to the data type (vl/vlad.c:180-188); the mass
+      sum_i a_ik is a double;
+    * mass > 0: enc_k = enc_k / mass - mu_k (NORMALIZE_MASS, the divide in
+      double, the subtraction in the data type) or enc_k - mass mu_k in
+      double (vl/vlad.c:191-202);
+    * signed square root (vl/vlad.c:204-213);
+    * per-component and global L2 norms: sums of squares in the data type in
+      element order, square root, floored at 1e-12 in double
+      (vl/vlad.c:215-240).
+    """
+    T = data.dtype.type
+    x = np.asarray(data)
+    a = np.asarray(assignments, x.dtype)
+    mu = np.asarray(means, x.dtype)
+    N, D = x.shape
+    K = mu.shape[0]
+    enc = np.zeros((K, D), x.dtype)
+    mass = np.zeros(K, np.float64)
+    for i in range(N):
+        m = a[i] > 0
+        if not m.any():
+            continue
+        q = a[i, m].astype(np.float64)
+        mass[m] = mass[m] + q
+        enc[m] = (enc[m].astype(np.float64) + q[:, None] * x[i].astype(np.float64)[None, :]).astype(x.dtype)
+    pos = mass > 0
+    if flags & VLAD_NORMALIZE_MASS:
+        enc[pos] = (enc[pos].astype(np.float64) / mass[pos, None]).astype(x.dtype)
+        enc[pos] = enc[pos] - mu[pos]
+    else:
+        enc[pos] = (enc[pos].astype(np.float64) - mass[pos, None] * mu[pos].astype(np.float64)).astype(x.dtype)
+    if flags & VLAD_SQUARE_ROOT:
+        enc = np.where(enc >= 0, np.sqrt(np.abs(enc)), -np.sqrt(np.abs(enc))).astype(x.dtype)
+
+    def floor(n):
+        return np.where(n.astype(np.float64) > 1e-12, n, T(1e-12)).astype(x.dtype)
+
+    if flags & VLAD_NORMALIZE_COMPONENTS:
+        n = np.zeros(K, x.dtype)
+        for d in range(D):
+            n = n + enc[:, d] * enc[:, d]
+        n = floor(np.sqrt(n))
+        enc = enc / n[:, None]
+    enc = enc.ravel()
+    if not flags & VLAD_UNNORMALIZED:
+        n = T(0)
+        for z in enc:
+            n = T(n + T(z * z))
+        n = floor(np.sqrt(np.asarray(n, x.dtype)))
+        enc = enc / n
+    return enc
 
 
 def simple_fisher(data, means, covs, priors, flags):

@@ -151,6 +151,32 @@ def rand_case(ref, out):
                 out[f"rand_{name}_{tag}_t{T}_ll"] = np.float64(res["ll"])
 
 
+def vlad_case(ref, out):
+    """VLAD encodings (vl/vlad.c:163-242) for every combination of the four
+    flags: hard assignments to the nearest mean with one component left empty
+    (mass 0), soft assignments with zeroed and negative weights (only positive
+    weights count, vl/vlad.c:182), and an image without descriptors."""
+    r = rng(51)
+    x = W.mixture_data(400, 24, 10, seed=52)
+    mu = x[r.choice(400, 10, replace=False)] + 0.1 * r.standard_normal((10, 24))
+    d2 = ((x[:, None, :] - mu[None]) ** 2).sum(2)
+    d2[:, 4] = np.inf
+    hard = np.zeros((400, 10))
+    hard[np.arange(400), d2.argmin(1)] = 1.0
+    xs = r.standard_normal((300, 40)) * 2.0
+    mus = r.standard_normal((12, 40))
+    soft = r.dirichlet(np.ones(12) * 0.5, 300)
+    soft[soft < 0.02] = 0.0
+    soft[::11, 3] = -0.25
+    cases = {"hard": (x, mu, hard), "soft": (xs, mus, soft),
+             "empty": (np.zeros((0, 6)), r.standard_normal((3, 6)), np.zeros((0, 3)))}
+    for name, (cx, cm, ca) in cases.items():
+        out.update({f"vlad_{name}_data": cx, f"vlad_{name}_means": cm, f"vlad_{name}_assign": ca})
+        for dt, tag in ((np.float32, "f"), (np.float64, "d")):
+            for fl in range(16):
+                out[f"vlad_{name}_enc_{tag}_{fl}"] = ref.vlad(cx.astype(dt), cm.astype(dt), ca.astype(dt), fl)
+
+
 def main():
     ref = Reference(threads=1)
     out: dict = {}
@@ -160,6 +186,7 @@ def main():
     fv_case(ref, out)
     edge_cases(ref, out)
     rand_case(ref, out)
+    vlad_case(ref, out)
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")

@@ -10,7 +10,8 @@ import pytest
 
 from conftest import ROOT
 
-HEADERS = ["include/vl/generic.h", "include/vl/gmm.h", "include/vl/fisher.h", "include/vlb200.h"]
+HEADERS = ["include/vl/generic.h", "include/vl/random.h", "include/vl/gmm.h", "include/vl/fisher.h",
+           "include/vl/vlad.h", "include/vlb200.h"]
 
 
 def declared_symbols():
@@ -32,7 +33,8 @@ def libpath():
 def test_header_declarations_found():
     names = declared_symbols()
     assert {"vl_gmm_new", "vl_gmm_cluster", "vl_fisher_encode", "vl_get_gmm_data_posteriors_f",
-            "vlb200_fisher_encode_batch_device"} <= names
+            "vlb200_fisher_encode_batch_device", "vl_vlad_encode", "vl_rand_uint32",
+            "vlb200_vlad_encode_batch_device"} <= names
     assert len(names) > 60
 
 
@@ -116,3 +118,24 @@ def test_library_rng_matches_reference(libpath, golden):
     capi.rand_seed(int(golden["rng_seed"]))
     seq = [capi.rand_uint32() for _ in range(len(golden["rng_seq"]))]
     assert seq == [int(v) for v in golden["rng_seq"]]
+
+
+def test_vlad_argument_checks(libpath):
+    """VLAD's argument checks run before any device call: an unknown data
+    type, decreasing offsets and a dimension above 1024 fail with
+    VL_ERR_BAD_ARG through the last-error channel."""
+    import numpy as np
+    from vlfeat_b200 import capi
+    L = capi.lib()
+    enc = np.zeros(4, np.float32)
+    L.vl_set_last_error(0, b"")
+    L.vl_vlad_encode(enc.ctypes.data_as(C.c_void_p), 7, None, 2, 2, None, 0, None, 0)
+    assert L.vl_get_last_error() == 3
+    bad = np.array([0, 10, 5], np.int64)
+    assert L.vlb200_vlad_encode_batch_device(None, 1, None, 8, 4, None, None, capi._np_ptr(bad), 2, 0,
+                                             C.c_void_p(1)) == 3
+    assert L.vlb200_vlad_encode_batch_device(None, 9, None, 8, 4, None, None, capi._np_ptr(bad[:1]), 0, 0,
+                                             C.c_void_p(1)) == 3
+    offs = np.array([0, 10], np.int64)
+    assert L.vlb200_vlad_encode_batch_device(None, 1, None, 1025, 4, None, None, capi._np_ptr(offs), 1, 0,
+                                             C.c_void_p(1)) == 3

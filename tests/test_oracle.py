@@ -118,3 +118,21 @@ def test_rand_init_restatement(golden, tag):
     o = rand_init(x, K, MT19937(seed), lanes)
     for k in ("means", "covs", "priors"):
         assert np.array_equal(o[k], golden[f"rand_small_{tag}_t0_{k}"]), k
+
+
+@pytest.mark.parametrize("flags", range(16))
+@pytest.mark.parametrize("tag", ["f", "d"])
+@pytest.mark.parametrize("name", ["hard", "soft", "empty"])
+def test_vlad_restatement(golden, name, tag, flags):
+    """The NumPy VLAD restatement reproduces the reference's encodings bit for
+    bit: hard assignments with an empty component, soft assignments with
+    zero and negative weights, and an image without descriptors."""
+    from oracle.oracle import vlad
+    dt = np.float32 if tag == "f" else np.float64
+    x = golden[f"vlad_{name}_data"].astype(dt)
+    mu = golden[f"vlad_{name}_means"].astype(dt)
+    a = golden[f"vlad_{name}_assign"].astype(dt)
+    want = golden[f"vlad_{name}_enc_{tag}_{flags}"]
+    got = vlad(x, mu, a, flags)
+    assert got.dtype == want.dtype
+    np.testing.assert_array_equal(got.view(np.uint8), want.view(np.uint8))

@@ -22,6 +22,11 @@ FLAG_SQUARE_ROOT = 1 << 0
 FLAG_NORMALIZED = 1 << 1
 FLAG_IMPROVED = FLAG_SQUARE_ROOT | FLAG_NORMALIZED
 FLAG_FAST = 1 << 2
+# VLAD flags, vl/vlad.h:23-26
+VLAD_NORMALIZE_COMPONENTS = 1 << 0
+VLAD_SQUARE_ROOT = 1 << 1
+VLAD_UNNORMALIZED = 1 << 2
+VLAD_NORMALIZE_MASS = 1 << 3
 INIT_KMEANS, INIT_RAND, INIT_CUSTOM = 0, 1, 2  # VlGMMInitialization, vl/gmm.h:21-26
 
 PREC_DEFAULT, PREC_EXACT, PREC_FP32, PREC_BF16, PREC_BF16_ROUTER = 0, 1, 2, 3, 4
@@ -74,6 +79,9 @@ def _decl(L):
     for s in ("_f", "_d"):
         f("vl_get_gmm_data_posteriors" + s, C.c_double, _vp, _sz, _sz, _vp, _vp, _sz, _vp, _vp)
     f("vl_fisher_encode", _sz, _vp, C.c_uint32, _vp, _sz, _sz, _vp, _vp, _vp, _sz, C.c_int)
+    f("vl_vlad_encode", None, _vp, C.c_uint32, _vp, _sz, _sz, _vp, _sz, _vp, C.c_int)
+    f("vlb200_vlad_encode_batch_device", C.c_int, _vp, C.c_uint32, _vp, _sz, _sz, _vp, _vp, _vp, _sz,
+      C.c_int, _vp)
     f("vl_get_last_error", C.c_int)
     f("vl_get_last_error_message", C.c_char_p)
     f("vl_set_last_error", C.c_int, C.c_int, C.c_char_p)
@@ -359,6 +367,22 @@ def fisher_encode(data, means, covariances, priors, flags=FLAG_IMPROVED):
     return enc, int(nt)
 
 
+def vlad_encode(data, means, assignments, flags=0):
+    """vl_vlad_encode (vl/vlad.h:45-50) -> enc of K*D elements of data's dtype.
+    assignments: N x K weights (hard or soft)."""
+    data = np.ascontiguousarray(data)
+    dt = data.dtype
+    N, D = data.shape
+    K = np.asarray(means).shape[0]
+    enc = np.zeros(K * D, dt)
+    _clear()
+    lib().vl_vlad_encode(_np_ptr(enc), _dt(dt), _np_ptr(np.ascontiguousarray(means, dt)), D, K,
+                         _np_ptr(data), N, _np_ptr(np.ascontiguousarray(assignments, dt)), int(flags))
+    if lib().vl_get_last_error():
+        _raise_last("vl_vlad_encode")
+    return enc
+
+
 def rand_seed(s: int) -> None:
     """vl_rand_seed on the calling thread's generator (vl_get_rand)."""
     lib().vl_rand_seed(lib().vl_get_rand(), int(s))
@@ -423,6 +447,21 @@ def fisher_encode_batch_device(enc_t, means_t, covs_t, priors_t, data_t, offsets
         nterms_t.data_ptr() if nterms_t is not None else None, _stream(stream))
     if rc:
         _raise_last("vlb200_fisher_encode_batch_device")
+
+
+def vlad_encode_batch_device(enc_t, means_t, data_t, assign_t, offsets, flags=0, stream=None) -> None:
+    """VLAD of len(offsets)-1 images in one call (torch CUDA tensors of one
+    dtype, float32 or float64); enc_t is (numImages, K*D)."""
+    import torch
+    offs = np.ascontiguousarray(offsets, np.int64)
+    K, D = means_t.shape
+    typ = VL_TYPE_FLOAT if data_t.dtype == torch.float32 else VL_TYPE_DOUBLE
+    _clear()
+    rc = lib().vlb200_vlad_encode_batch_device(enc_t.data_ptr(), typ, means_t.data_ptr(), D, K,
+                                               data_t.data_ptr(), assign_t.data_ptr(), _np_ptr(offs),
+                                               len(offs) - 1, int(flags), _stream(stream))
+    if rc:
+        _raise_last("vlb200_vlad_encode_batch_device")
 
 
 class FisherPlan:

@@ -109,7 +109,14 @@ struct DevBuf {
 struct Scratch {
   DevBuf slot[32];
 };
-enum ScratchArena { kArenaApi = 0, kArenaExact = 1, kArenaTc = 2, kArenaRouter = 3, kNumArenas = 4 };
+enum ScratchArena {
+  kArenaApi = 0,
+  kArenaExact = 1,
+  kArenaTc = 2,
+  kArenaRouter = 3,
+  kArenaVlad = 4,
+  kNumArenas = 5
+};
 Scratch &thread_scratch(int arena = kArenaApi);
 
 // Pinned host staging buffer (per thread), for host-pointer API calls.

@@ -208,7 +208,7 @@ struct StreamHolder {
   }
 };
 thread_local StreamHolder g_stream;
-thread_local Scratch *g_scratch[kNumArenas] = {nullptr, nullptr, nullptr, nullptr};
+thread_local Scratch *g_scratch[kNumArenas] = {};
 thread_local DevBuf *g_pinned_dummy = nullptr;
 thread_local void *g_pinned = nullptr;
 thread_local size_t g_pinned_cap = 0;
