@@ -259,6 +259,13 @@ def cpu_baseline(wl, budget_s=12.0, kind_pref="reference"):
 
 
 # ------------------------------------------------------------- roofline
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
 def roofline(capi, wl, run, prec):
     """Dominant kernel's achieved rate from live CUDA-event timing of every
     launch (library profiling) of `run` (one eager encode), against the
@@ -436,6 +443,88 @@ def em_throughput(capi, iters=5, cpu=True):
     return out
 
 
+def vlad_throughput(capi, wl, steps=3, warmup=1, cpu=True, budget_s=8.0):
+    """VLAD (vl_vlad_encode, vl/vlad.c:163-242) of the Fisher workload's
+    images with hard assignments to the GMM means (vector quantisation, the
+    usual VLAD input), intra-normalised (VL_VLAD_FLAG_NORMALIZE_COMPONENTS,
+    then the global L2).  The batched device call's output is bit-equal to
+    the reference; timed with CUDA events on the launching stream, inputs
+    (descriptors N x D and assignments N x K, float32) resident in HBM and
+    larger than L2.  Algorithmic bytes: 4(D + K) per descriptor read plus
+    4KD per image written."""
+    import torch
+    x, mu, offs = wl["x"], wl["means"], wl["offs"]
+    N, nimg = int(x.shape[0]), len(offs) - 1
+    lab = torch.empty(N, dtype=torch.int64, device="cuda")
+    mu2 = (mu * mu).sum(1)
+    for i in range(0, N, 1 << 20):
+        xb = x[i:i + (1 << 20)]
+        lab[i:i + (1 << 20)] = (mu2[None, :] - 2.0 * xb @ mu.T).argmin(1)
+    a = torch.zeros((N, K), dtype=torch.float32, device="cuda")
+    a.scatter_(1, lab[:, None], 1.0)
+    del lab
+    flags = capi.VLAD_NORMALIZE_COMPONENTS
+    enc = torch.empty((nimg, K * D), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        capi.vlad_encode_batch_device(enc, mu, x, a, offs, flags)
+    torch.cuda.synchronize()
+    ms = []
+    l0 = capi.launch_count()
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        capi.vlad_encode_batch_device(enc, mu, x, a, offs, flags)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    launches = (capi.launch_count() - l0) // steps
+    t = float(np.median(ms))
+    capi.profile_reset()
+    capi.profile_enable(True)
+    capi.vlad_encode_batch_device(enc, mu, x, a, offs, flags)
+    torch.cuda.synchronize()
+    prof = capi.profile_read()
+    capi.profile_enable(False)
+    capi.profile_reset()
+    tot = sum(v[1] for v in prof.values()) or 1.0
+    shares = {k: {"launches": int(v[0]), "ms": round(v[1], 4), "share": round(v[1] / tot, 4)}
+              for k, v in prof.items()}
+    alg = 4.0 * (D + K) * N + 4.0 * K * D * nimg
+    peak = measured_peaks().get("hbm_gbs")
+    out = {"workload": f"{nimg} images, {N} descriptors, D={D}, K={K}, hard assignments (nearest mean), "
+                       "flags NORMALIZE_COMPONENTS", "ms_per_step": t, "value": N / (t * 1e-3),
+           "unit": "descriptors/s", "gpu_launches": launches, "kernels": shares,
+           "hbm": {"algorithmic_bytes": alg, "achieved_gbs": alg / (t * 1e-3) / 1e9, "peak_gbs": peak,
+                   "frac": (alg / (t * 1e-3) / 1e9 / peak) if peak else None}}
+    if cpu:
+        from oracle import oracle as O
+        try:
+            impl = O.Reference(threads=os.cpu_count() or 1)
+        except (FileNotFoundError, OSError):
+            impl = None
+        if impl is not None:
+            j, done, same = 0, 0, 0
+            xs = x[: int(offs[min(nimg, 256)])].cpu().numpy()
+            as_ = a[: int(offs[min(nimg, 256)])].cpu().numpy()
+            mun = mu.cpu().numpy()
+            got = enc[:min(nimg, 256)].cpu().numpy()
+            t0 = time.perf_counter()
+            while j < min(nimg, 256) and time.perf_counter() - t0 < budget_s:
+                r = impl.vlad(xs[offs[j]:offs[j + 1]], mun, as_[offs[j]:offs[j + 1]], flags)
+                same += int(np.array_equal(r.view(np.uint32), got[j].view(np.uint32)))
+                done += int(offs[j + 1] - offs[j])
+                j += 1
+            dt = time.perf_counter() - t0
+            out["cpu_baseline"] = {"kind": "reference", "cores": os.cpu_count() or 1, "value": done / dt,
+                                   "unit": "descriptors/s",
+                                   "sample": f"first {j} images ({done} descriptors), vl_vlad_encode per image"}
+            out["bit_exact_images"] = f"{same}/{j}"
+    del a, enc
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: VLFeat's own CPU code on the host cores."""
     if rank != 0:
@@ -485,6 +574,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-em", action="store_true", help="skip the EM iterations/s measurement")
+    ap.add_argument("--no-vlad", action="store_true", help="skip the VLAD descriptors/s measurement")
     ap.add_argument("--images", type=int, default=4096,
                     help="encode only the first IMAGES images of the workload (small profiling cases)")
     ap.add_argument("--plan", default=None,
@@ -561,6 +651,8 @@ def main():
             del encoders, eager_of
             torch.cuda.empty_cache()
             out["em"] = em_throughput(capi, cpu=not args.no_cpu)
+        if not args.no_vlad and world == 1:
+            out["vlad"] = vlad_throughput(capi, wl, cpu=not args.no_cpu)
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

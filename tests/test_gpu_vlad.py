@@ -49,9 +49,14 @@ def test_vlad_golden(vl, golden, name, tag, flags):
     assert np.array_equal(_bits(got), _bits(want))
 
 
-# Shapes over the kernel's register tilings (1, 2, 4 and 8 dimensions per
-# thread, ragged in the last) and component tiles (K not a multiple of 8).
-SHAPES = [(700, 5, 3, "hard"), (900, 130, 13, "soft"), (600, 257, 9, "hard"),
+# Shapes over both kernels.  Streaming kernel (row sizes multiples of 16
+# bytes, D <= 128): one or several component blocks per image, whole-row and
+# per-row copies, partial last block, 1-4 dimension registers per lane, 16
+# and 32 components per warp.  Tile kernel (the other shapes): 1, 2, 4 and 8
+# dimensions per thread, ragged, K not a multiple of 8.
+SHAPES = [(3000, 80, 256, "hard"), (2000, 128, 64, "soft"), (1500, 64, 300, "hard"),
+          (1000, 96, 520, "soft"), (700, 8, 4, "soft"), (2500, 32, 36, "hard"), (900, 112, 132, "hard"),
+          (700, 5, 3, "hard"), (900, 130, 13, "soft"), (600, 257, 9, "hard"),
           (400, 600, 21, "soft"), (300, 1024, 8, "hard")]
 
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "tc_common.cuh"
 
 extern "C" {
 #include "vl/vlad.h"
@@ -53,7 +54,10 @@ __global__ void __launch_bounds__(kVladThreads) k_vlad_accum(
     const T *__restrict__ A, const i64 *__restrict__ offs, i64 img0, int flags) {
   extern __shared__ unsigned char vlad_smem[];
   T *zs = (T *)vlad_smem;
-  const int img = blockIdx.x, k0 = blockIdx.y * kVladKT, tid = threadIdx.x;
+  // The component tiles of one image are adjacent in launch order, so the
+  // image's rows are read from HBM once and then from L2.
+  const i64 img = img0 + blockIdx.y;
+  const int k0 = blockIdx.x * kVladKT, tid = threadIdx.x;
   const int nk = min(kVladKT, K - k0);
   const i64 r0 = offs[img], r1 = offs[img + 1];
   T acc[kVladKT][JD];
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(kVladThreads) k_vlad_accum(
     }
     __syncthreads();
   }
-  T *out = enc + (img0 + img) * (i64)K * D;
+  T *out = enc + img * (i64)K * D;
   for (int c = 0; c < nk; ++c) {
     for (int d = tid; d < D; d += kVladThreads) {
       T z = zs[c * D + d];
@@ -140,24 +144,366 @@ __global__ void __launch_bounds__(kVladThreads) k_vlad_accum(
   }
 }
 
-// Global L2 of each image's KD values, summed in element order by one thread
-// per image (vl/vlad.c:226-237).
+// Global L2 of each image (vl/vlad.c:226-240), one warp per image: per chunk
+// of 256 values (8 loads per lane, issued while lane 0 sums the previous
+// chunk) the lanes square their values into shared memory and lane 0 adds the
+// squares in element order; the warp then divides its image by the floored
+// norm.
+constexpr int kGnChunk = 256;
+
 template <typename T>
-__global__ void k_vlad_global_norm(const T *__restrict__ enc, i64 KD, i64 nimg, T *__restrict__ norm) {
-  const i64 img = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_vlad_global_norm(T *__restrict__ enc, i64 KD, i64 nimg) {
+  __shared__ __align__(16) T sq[8][kGnChunk];
+  __shared__ T s_n[8];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const i64 img = (i64)blockIdx.x * 8 + w;
   if (img >= nimg) return;
-  const T *e = enc + img * KD;
+  T *e = enc + img * KD;
   T n = (T)0;
-  for (i64 i = 0; i < KD; ++i) n = add_t(n, mul_t(e[i], e[i]));
-  n = sqrt_t(n);
-  norm[img] = (T)fmax((double)n, 1e-12);
+  T z[kGnChunk / 32];
+  auto load = [&](i64 i0) {
+#pragma unroll
+    for (int q = 0; q < kGnChunk / 32; ++q) {
+      const i64 i = i0 + q * 32 + lane;
+      z[q] = i < KD ? e[i] : (T)0;
+    }
+  };
+  load(0);
+  for (i64 i0 = 0; i0 < KD; i0 += kGnChunk) {
+#pragma unroll
+    for (int q = 0; q < kGnChunk / 32; ++q) sq[w][q * 32 + lane] = mul_t(z[q], z[q]);
+    __syncwarp();
+    if (i0 + kGnChunk < KD) load(i0 + kGnChunk);  // next chunk in flight during the sum
+    if (lane == 0) {
+      const int lim = KD - i0 < kGnChunk ? (int)(KD - i0) : kGnChunk;
+      if (lim == kGnChunk) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 *v4 = (const float4 *)sq[w];
+#pragma unroll 16
+          for (int l = 0; l < kGnChunk / 4; ++l) {
+            const float4 v = v4[l];
+            n = add_t(add_t(add_t(add_t(n, v.x), v.y), v.z), v.w);
+          }
+        } else {
+#pragma unroll 32
+          for (int l = 0; l < kGnChunk; ++l) n = add_t(n, sq[w][l]);
+        }
+      } else {
+        for (int l = 0; l < lim; ++l) n = add_t(n, sq[w][l]);
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) s_n[w] = (T)fmax((double)sqrt_t(n), 1e-12);
+  __syncwarp();
+  n = s_n[w];
+  for (i64 i = lane; i < KD; i += 32) e[i] = div_t(e[i], n);
+}
+
+// ------------------------------------------------------------ streaming path
+// One block per (image, run of kVsWarps x CPW components).  A producer warp
+// streams the image's rows through shared memory with bulk asynchronous
+// copies (kVsStages stages of R rows: the block's slice of each assignment
+// row and the descriptor rows); kVsWarps consumer warps each own CPW
+// components with their accumulators in registers (lane l holds dimensions
+// l + 32j).  Per step a warp loads 32 weights, one per lane (32/CPW rows of
+// its CPW components), and a ballot skips the rows whose weights are all
+// <= 0, so hard assignments cost one shared-memory load per row and component
+// group.  Positive weights update the accumulators in row order, as the
+// reference's loop does: few per row through a branch tree on the component
+// index, many through a pass over all CPW components.  The mass step, signed
+// square root and the component norm (a serial sum in dimension order,
+// broadcast by shuffles) run in registers before the store.
+constexpr int kVsWarps = 8;
+constexpr int kVsThreads = (kVsWarps + 1) * 32;
+constexpr int kVsStages = 4;
+constexpr int kVsUnroll = 8;  // steps whose weights are loaded together
+
+struct VsParams {
+  void *enc;
+  const void *means, *X, *A;
+  const i64 *offs;
+  i64 img0;
+  int D, K, flags, R;
+  int *err;
+};
+
+template <typename T>
+__device__ __forceinline__ T vlad_mass_step(T z, T mu, double mass, int flags) {
+  if (!(mass > 0)) return z;
+  if (flags & VL_VLAD_FLAG_NORMALIZE_MASS) {
+    if constexpr (sizeof(T) == 4) z = __double2float_rn(__ddiv_rn((double)z, mass));
+    else z = __ddiv_rn(z, mass);
+    return sub_t(z, mu);
+  }
+  if constexpr (sizeof(T) == 4) return __double2float_rn(__dsub_rn((double)z, __dmul_rn(mass, (double)mu)));
+  else return __dsub_rn(z, __dmul_rn(mass, mu));
+}
+
+__device__ __forceinline__ bool vs_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
+  return tc::mbar_wait(bar, parity, abort_flag, err, 0x5600);
+}
+
+// acc[c] += av * xv for the component c in [LO, HI) (warp-uniform c): a
+// binary branch tree keeps every accumulator index static.  UNIT: float data
+// and av == 1, where (float)((double)acc + (double)x) is the float sum itself
+// (a sum of two floats rounded to double and then to float rounds as once to
+// float, since 53 >= 2 * 24 + 2: Figueroa, "When is double rounding
+// innocuous?", 1995).
+template <int LO, int HI, bool UNIT, typename T, int CPW, int JD>
+__device__ __forceinline__ void vs_update(int c, T (&acc)[CPW][JD], T av, const T (&xv)[JD]) {
+  if constexpr (HI - LO == 1) {
+#pragma unroll
+    for (int j = 0; j < JD; ++j) {
+      if constexpr (UNIT) acc[LO][j] = add_t(acc[LO][j], xv[j]);
+      else acc[LO][j] = acc_step(acc[LO][j], av, xv[j]);
+    }
+  } else {
+    constexpr int MID = (LO + HI) / 2;
+    if (c < MID) vs_update<LO, MID, UNIT>(c, acc, av, xv);
+    else vs_update<MID, HI, UNIT>(c, acc, av, xv);
+  }
+}
+
+// One step of a consumer warp: the 32/CPW rows whose weights gave the ballot
+// m (bit h*CPW + c: row h, component c of the warp); sa: the warp's first
+// weight of the first row (rows nkb apart), sx: the first row's descriptor,
+// both in shared memory.  Rows in order, components in any order (each
+// accumulator sees its rows in order).
+template <typename T, int JD, int CPW>
+__device__ __forceinline__ void vs_rows_step(T (&acc)[CPW][JD], unsigned m, const T *sa, int nkb, const T *sx,
+                                             int D, int lane) {
+  constexpr int RPS = 32 / CPW;
+  constexpr unsigned kMask = CPW == 32 ? 0xffffffffu : ((1u << CPW) - 1u);
+#pragma unroll
+  for (int h = 0; h < RPS; ++h) {
+    unsigned bits = (m >> (CPW * h)) & kMask;
+    if (bits == 0) continue;
+    const T *wa = sa + (size_t)h * nkb;
+    T xv[JD];
+#pragma unroll
+    for (int j = 0; j < JD; ++j) {
+      const int d = lane + 32 * j;
+      xv[j] = d < D ? sx[h * D + d] : (T)0;
+    }
+    if (__popc(bits) > 4) {
+#pragma unroll
+      for (int c = 0; c < CPW; ++c) {
+        if (bits & (1u << c)) {
+          const T av = wa[c];
+#pragma unroll
+          for (int j = 0; j < JD; ++j) acc[c][j] = acc_step(acc[c][j], av, xv[j]);
+        }
+      }
+    } else {
+      while (bits) {
+        const int c = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const T av = wa[c];
+        if (sizeof(T) == 4 && av == (T)1) vs_update<0, CPW, true>(c, acc, av, xv);
+        else vs_update<0, CPW, false>(c, acc, av, xv);
+      }
+    }
+  }
+}
+
+template <typename T, int JD, int CPW>
+__global__ void __launch_bounds__(kVsThreads, sizeof(T) == 4 && JD <= 3 ? 2 : 1) k_vlad_stream(const VsParams p) {
+  constexpr int RPS = 32 / CPW;  // rows per step
+  extern __shared__ __align__(128) unsigned char vs_smem[];
+  uint64_t *full = (uint64_t *)vs_smem;
+  uint64_t *empty = full + kVsStages;
+  volatile int *s_abort = (volatile int *)(empty + kVsStages);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int D = p.D, K = p.K, R = p.R;
+  const int k0 = blockIdx.x * (kVsWarps * CPW), nkb = min(kVsWarps * CPW, K - k0);
+  const i64 img = p.img0 + blockIdx.y;
+  const i64 r0 = p.offs[img], r1 = p.offs[img + 1];
+  const int ntiles = (int)((r1 - r0 + R - 1) / R);
+  const uint32_t aBytes = (uint32_t)(R * nkb * sizeof(T)), stageBytes = aBytes + (uint32_t)(R * D * sizeof(T));
+  unsigned char *stage0 = vs_smem + 128;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kVsStages; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], kVsWarps);
+    }
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const T *X = (const T *)p.X, *A = (const T *)p.A;
+  if (warp == kVsWarps) {
+    // Producer: one lane issues the copies of tile t into stage t % kVsStages.
+    if (lane == 0) {
+      int t = 0;
+      for (; t < ntiles; ++t) {
+        const int s = t % kVsStages;
+        if (t >= kVsStages && !vs_wait(&empty[s], ((t / kVsStages) + 1) & 1, s_abort, p.err)) break;
+        const i64 row0 = r0 + (i64)t * R;
+        const int rows = (int)(r1 - row0 < (i64)R ? r1 - row0 : (i64)R);
+        unsigned char *st = stage0 + (size_t)s * stageBytes;
+        const uint32_t ab = (uint32_t)(rows * nkb * sizeof(T)), xb = (uint32_t)(rows * D * sizeof(T));
+        tc::mbar_arrive_expect_tx(&full[s], ab + xb);
+        if (nkb == K) {
+          tc::bulk_g2s(tc::smem_u32(st), A + row0 * K, ab, &full[s]);
+        } else {
+          for (int r = 0; r < rows; ++r)
+            tc::bulk_g2s(tc::smem_u32(st + (size_t)r * nkb * sizeof(T)), A + (row0 + r) * K + k0,
+                         (uint32_t)(nkb * sizeof(T)), &full[s]);
+        }
+        tc::bulk_g2s(tc::smem_u32(st + aBytes), X + row0 * D, xb, &full[s]);
+      }
+      // The copies already issued land before the block exits (on an abort too).
+      for (int u = max(0, t - kVsStages); u < t; ++u) {
+        const unsigned long long t0 = tc::global_ns();
+        while (!tc::mbar_try_wait(&full[u % kVsStages], (u / kVsStages) & 1) &&
+               tc::global_ns() - t0 < tc::kWaitNs) {
+        }
+      }
+    }
+    return;
+  }
+  // Consumers.
+  const int cw = warp * CPW;  // first component of this warp within the block
+  T acc[CPW][JD];
+#pragma unroll
+  for (int c = 0; c < CPW; ++c)
+#pragma unroll
+    for (int j = 0; j < JD; ++j) acc[c][j] = (T)0;
+  double mass = 0.0;  // lane c < CPW: component cw + c
+  const int myc = cw + (lane % CPW);
+  const bool cvalid = myc < nkb;
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t % kVsStages;
+    if (!vs_wait(&full[s], (t / kVsStages) & 1, s_abort, p.err)) break;
+    const unsigned char *st = stage0 + (size_t)s * stageBytes;
+    const T *sA = (const T *)st, *sX = (const T *)(st + aBytes);
+    const i64 left = r1 - (r0 + (i64)t * R);
+    const int rows = (int)(left < (i64)R ? left : (i64)R);
+    // This lane's weight column, one row per step of RPS rows.
+    const T *pa = sA + (lane / CPW) * nkb + (cvalid ? myc : 0);
+    const int stride = RPS * nkb;
+    for (int r = 0; r < rows; r += RPS * kVsUnroll, pa += kVsUnroll * stride) {
+      T a[kVsUnroll];
+      unsigned m[kVsUnroll];
+      if (r + RPS * kVsUnroll <= rows && cvalid) {
+#pragma unroll
+        for (int u = 0; u < kVsUnroll; ++u) a[u] = pa[u * stride];
+      } else {
+#pragma unroll
+        for (int u = 0; u < kVsUnroll; ++u)
+          a[u] = (r + u * RPS + lane / CPW < rows && cvalid) ? pa[u * stride] : (T)0;
+      }
+      unsigned rowbits = 0;  // bit u: step u has a positive weight
+#pragma unroll
+      for (int u = 0; u < kVsUnroll; ++u) {
+        m[u] = __ballot_sync(0xffffffffu, a[u] > (T)0);  // vl/vlad.c:182
+        rowbits |= (m[u] != 0u) << u;
+      }
+      while (rowbits) {  // steps with a positive weight, in row order
+        const int u = __ffs(rowbits) - 1;
+        rowbits &= rowbits - 1;
+        unsigned mu = m[0];
+#pragma unroll
+        for (int v = 1; v < kVsUnroll; ++v) mu = u == v ? m[v] : mu;
+        // The step's weights are still in the stage: this lane's own (for the
+        // mass) and, per positive component, a broadcast read.
+        const T au = (cvalid && r + u * RPS + lane / CPW < rows) ? pa[u * stride] : (T)0;
+        // The mass of a component sums its positive weights in row order;
+        // the other weights would add 0.0, which leaves it unchanged.
+        const double am = au > (T)0 ? (double)au : 0.0;
+        mass += am;
+        if constexpr (RPS == 2) mass += __shfl_down_sync(0xffffffffu, am, 16);
+        const int rs = r + u * RPS;
+        vs_rows_step<T, JD, CPW>(acc, mu, sA + (size_t)rs * nkb + cw, nkb, sX + (size_t)rs * D, D, lane);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) tc::mbar_arrive(&empty[s]);
+  }
+  // Epilogue through shared memory (the stage area, free once every consumer
+  // warp is past its last tile; the producer has seen all its copies land):
+  // the warp stores its raw sums as rows of D + 1 values, lane c < CPW
+  // finishes component cw + c there (mass step, signed square root and the
+  // component norm in dimension order), and the warp writes the rows out
+  // coalesced.
+  tc::named_barrier(1, kVsWarps * 32);
+  if (*s_abort) return;
+  const int ncw = min(CPW, nkb - cw);
+  const int ld = D + 1;
+  T *zs = (T *)stage0 + (size_t)cw * ld;
+#pragma unroll
+  for (int c = 0; c < CPW; ++c) {
+#pragma unroll
+    for (int j = 0; j < JD; ++j) {
+      const int d = lane + 32 * j;
+      if (c < ncw && d < D) zs[c * ld + d] = acc[c][j];
+    }
+  }
+  __syncwarp();
+  if (lane < ncw) {
+    const T *mu = (const T *)p.means + (i64)(k0 + cw + lane) * D;
+    T *o = zs + lane * ld;
+    T n = (T)0;
+    for (int d = 0; d < D; ++d) {
+      T z = vlad_mass_step<T>(o[d], mu[d], mass, p.flags);
+      if (p.flags & VL_VLAD_FLAG_SQUARE_ROOT) z = z >= (T)0 ? sqrt_t(z) : -sqrt_t(-z);
+      n = add_t(n, mul_t(z, z));
+      o[d] = z;
+    }
+    if (p.flags & VL_VLAD_FLAG_NORMALIZE_COMPONENTS) {
+      n = (T)fmax((double)sqrt_t(n), 1e-12);
+      for (int d = 0; d < D; ++d) o[d] = div_t(o[d], n);
+    }
+  }
+  __syncwarp();
+  T *out = (T *)p.enc + img * (i64)K * D + (i64)(k0 + cw) * D;
+  for (int c = 0; c < ncw; ++c)
+    for (int d = lane; d < D; d += 32) out[(i64)c * D + d] = zs[c * ld + d];
+}
+
+// Components per consumer warp.  16 (two rows per step) keeps float
+// accumulators within the register budget of two blocks per SM.
+constexpr int kVsCpw = 16;
+
+// Rows per stage: stages of about 24 KB where two blocks share an SM (float
+// data, D <= 96), 32 KB otherwise.
+template <typename T>
+int vs_rows(int D, int K) {
+  const int rowBytes = (int)((std::min(K, kVsWarps * kVsCpw) + D) * sizeof(T));
+  const int target = sizeof(T) == 4 && D <= 96 ? 24 * 1024 : 32 * 1024;
+  return std::max(8, std::min(64, (target / rowBytes) & ~1));
 }
 
 template <typename T>
-__global__ void k_vlad_scale(T *__restrict__ enc, i64 KD, i64 nimg, const T *__restrict__ norm) {
-  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= KD * nimg) return;
-  enc[i] = div_t(enc[i], norm[i / KD]);
+bool vs_eligible(int D, int K, const void *X, const void *A) {
+  return D <= 128 && (D * sizeof(T)) % 16 == 0 && (K * sizeof(T)) % 16 == 0 && ((uintptr_t)X % 16) == 0 &&
+         ((uintptr_t)A % 16) == 0;
+}
+
+template <typename T, int JD, int CPW>
+void launch_stream_cpw(const VsParams &p0, i64 nimg, cudaStream_t s) {
+  constexpr int comps = kVsWarps * CPW;
+  VsParams p = p0;
+  const size_t stages = (size_t)kVsStages * p.R * (std::min(p.K, comps) + p.D) * sizeof(T);
+  const size_t epi = (size_t)std::min(p.K, comps) * (p.D + 1) * sizeof(T);
+  const size_t smem = 128 + std::max(stages, epi);
+  auto kern = k_vlad_stream<T, JD, CPW>;
+  VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (i64 img0 = 0; img0 < nimg; img0 += 65535) {
+    p.img0 = img0;
+    dim3 grid((unsigned)((p.K + comps - 1) / comps), (unsigned)std::min<i64>(65535, nimg - img0));
+    VLB_LAUNCH("vlad_stream", s, kern<<<grid, kVsThreads, smem, s>>>(p));
+  }
+}
+
+template <typename T, int JD>
+void launch_stream(T *enc, const T *means, int D, int K, const T *X, const T *A, const i64 *doffs, i64 nimg,
+                   int flags, int *derr, cudaStream_t s) {
+  VsParams p;
+  p.enc = enc; p.means = means; p.X = X; p.A = A; p.offs = doffs;
+  p.D = D; p.K = K; p.flags = flags; p.R = vs_rows<T>(D, K); p.err = derr;
+  launch_stream_cpw<T, JD, kVsCpw>(p, nimg, s);
 }
 
 template <typename T, int JD>
@@ -166,8 +512,20 @@ void launch_accum(T *enc, const T *means, int D, int K, const T *X, const T *A, 
   const size_t smem = sizeof(T) * kVladKT * D;
   auto kern = k_vlad_accum<T, JD>;
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid((unsigned)nimg, (unsigned)((K + kVladKT - 1) / kVladKT));
-  VLB_LAUNCH("vlad_accum", s, kern<<<grid, kVladThreads, smem, s>>>(enc, means, D, K, X, A, doffs, 0, flags));
+  for (i64 img0 = 0; img0 < nimg; img0 += 65535) {
+    dim3 grid((unsigned)((K + kVladKT - 1) / kVladKT), (unsigned)std::min<i64>(65535, nimg - img0));
+    VLB_LAUNCH("vlad_accum", s, kern<<<grid, kVladThreads, smem, s>>>(enc, means, D, K, X, A, doffs, img0, flags));
+  }
+}
+
+template <typename T>
+void vlad_tiles(T *enc, const T *means, i64 D, i64 K, const T *X, const T *A, const i64 *doffs, i64 nimg, int flags,
+                cudaStream_t s) {
+  const int jd = (int)((D + kVladThreads - 1) / kVladThreads);
+  if (jd <= 1) launch_accum<T, 1>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
+  else if (jd <= 2) launch_accum<T, 2>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
+  else if (jd <= 4) launch_accum<T, 4>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
+  else launch_accum<T, 8>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
 }
 
 }  // namespace
@@ -178,27 +536,34 @@ void vlad_batch(T *enc, const T *means, i64 D, i64 K, const T *X, const T *A, co
   VLB_CHECK(D >= 1 && K >= 1, VL_ERR_BAD_ARG, "VLAD: dimension and numClusters must be >= 1");
   VLB_CHECK(D <= 8 * kVladThreads, VL_ERR_BAD_ARG, "VLAD: dimension above 1024 is not supported");
   if (nimg <= 0) return;
+  // VLAD arena slots: 0 offsets, 6 error word (here); 2-5 the
+  // host entry point's staged inputs and output.
   Scratch &sc = thread_scratch(kArenaVlad);
   std::vector<i64> rel(nimg + 1);
   for (i64 j = 0; j <= nimg; ++j) rel[j] = h_offsets[j];
   i64 *doffs = sc.slot[0].get<i64>(nimg + 1);
   VLB_CUDA(cudaMemcpyAsync(doffs, rel.data(), sizeof(i64) * (nimg + 1), cudaMemcpyHostToDevice, s));
-  const int jd = (int)((D + kVladThreads - 1) / kVladThreads);
-  if (jd <= 1) launch_accum<T, 1>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
-  else if (jd <= 2) launch_accum<T, 2>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
-  else if (jd <= 4) launch_accum<T, 4>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
-  else launch_accum<T, 8>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, s);
-  if (!(flags & VL_VLAD_FLAG_UNNORMALIZED)) {
-    T *norm = sc.slot[1].get<T>(nimg);
-    const i64 KD = K * D;
-    VLB_LAUNCH("vlad_global_norm", s,
-               k_vlad_global_norm<T><<<(unsigned)((nimg + 127) / 128), 128, 0, s>>>(enc, KD, nimg, norm));
-    VLB_LAUNCH("vlad_scale", s,
-               k_vlad_scale<T><<<(unsigned)((KD * nimg + 255) / 256), 256, 0, s>>>(enc, KD, nimg, norm));
+  int *herr = (int *)pinned_host(sizeof(int));
+  *herr = 0;
+  if (vs_eligible<T>((int)D, (int)K, X, A)) {
+    int *derr = sc.slot[6].get<int>(1);
+    VLB_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), s));
+    const int jd = (int)((D + 31) / 32);
+    if (jd <= 1) launch_stream<T, 1>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
+    else if (jd == 2) launch_stream<T, 2>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
+    else if (jd == 3) launch_stream<T, 3>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
+    else launch_stream<T, 4>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
+    VLB_CUDA(cudaMemcpyAsync(herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  } else {
+    vlad_tiles<T>(enc, means, D, K, X, A, doffs, nimg, flags, s);
   }
+  if (!(flags & VL_VLAD_FLAG_UNNORMALIZED))
+    VLB_LAUNCH("vlad_global_norm", s,
+               k_vlad_global_norm<T><<<(unsigned)((nimg + 7) / 8), 256, 0, s>>>(enc, K * D, nimg));
   // The scratch above is reused by the next call on this thread, which may
   // use another stream: finish before returning.
   VLB_CUDA(cudaStreamSynchronize(s));
+  VLB_CHECK(*herr == 0, VL_ERR_ALLOC, "VLAD: a pipeline wait timed out on the device");
 }
 
 template void vlad_batch<float>(float *, const float *, i64, i64, const float *, const float *, const i64 *, i64,
