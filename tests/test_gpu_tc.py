@@ -158,3 +158,97 @@ def test_tc_deterministic(vl):
     a, _ = vl.fisher_encode(x, mu, cv, pr)
     b, _ = vl.fisher_encode(x, mu, cv, pr)
     assert np.array_equal(a, b)
+
+
+# ---------------------------------------------------------------- K > 256
+# Above 256 components the E-step runs as thread-block clusters: CTA r of a
+# cluster takes components [r Kb, (r+1) Kb) and the CTAs exchange each row's
+# (max, sum, argmax) through distributed shared memory before normalising.
+# K=300: 2 CTAs x 160; K=520: 3 x 192 (image padded from 576 to 640);
+# K=512 and 1024: 2 and 4 x 256 (D=128 streams W through the stages).
+CLUSTER_KD = [(1024, 80), (520, 80), (300, 64), (512, 128)]
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+@pytest.mark.parametrize("KD", CLUSTER_KD)
+def test_fv_cluster(vl, restatement, mode, KD):
+    from vlfeat_b200 import workloads as W
+    K, D = KD
+    pr, mu, cv = W.fv_gmm(K, D, seed=31)
+    x = W.pca_like(3000, D, seed=32)
+    ref, nref = restatement.fisher(x.astype(np.float64), mu.astype(np.float64), cv.astype(np.float64),
+                                   pr.astype(np.float64), FLAG_IMPROVED)
+    vl.set_precision(mode)
+    enc, nt = vl.fisher_encode(x, mu, cv, pr, FLAG_IMPROVED)
+    assert rel_err(enc, ref) < TOL[mode]
+    assert abs(nt - nref) <= max(2, 1e-3 * nref)
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+def test_fv_cluster_fast(vl, restatement, mode):
+    """FAST (hard assignment to the row's argmax) across the CTAs of a
+    cluster: the first maximum over all K wins."""
+    from vlfeat_b200 import workloads as W
+    pr, mu, cv = W.fv_gmm(1024, 80, seed=33)
+    x = W.pca_like(2000, 80, seed=34)
+    flags = FLAG_IMPROVED | FLAG_FAST
+    ref, nref = restatement.fisher(x.astype(np.float64), mu.astype(np.float64), cv.astype(np.float64),
+                                   pr.astype(np.float64), flags)
+    vl.set_precision(mode)
+    enc, nt = vl.fisher_encode(x, mu, cv, pr, flags)
+    assert rel_err(enc, ref) < 3 * TOL[mode]
+    assert nt == nref == 2000
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+def test_batched_uneven_cluster(vl, restatement, mode):
+    import torch
+    from vlfeat_b200 import workloads as W
+    K, D = 520, 80
+    pr, mu, cv = W.fv_gmm(K, D, seed=35)
+    counts = np.array([0, 1, 129, 3000, 0, 4100, 17])
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    x = W.pca_like(int(offs[-1]), D, seed=36)
+    enc = torch.zeros((len(counts), 2 * K * D), device="cuda")
+    nt = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+    vl.fisher_encode_batch_device(enc, _t(mu), _t(cv), _t(pr), _t(x), offs, FLAG_IMPROVED, mode, nt)
+    enc = enc.cpu().numpy()
+    nt = nt.cpu().numpy()
+    for j in range(len(counts)):
+        e, n = restatement.fisher(x[offs[j]:offs[j + 1]].astype(np.float64), mu.astype(np.float64),
+                                  cv.astype(np.float64), pr.astype(np.float64), FLAG_IMPROVED)
+        if counts[j] == 0:
+            assert np.all(enc[j] == 0) and nt[j] == 0
+        else:
+            assert rel_err(enc[j], e) < TOL[mode], j
+            assert abs(int(nt[j]) - n) <= max(2, 1e-3 * n), j
+
+
+@pytest.mark.parametrize("KD", [(1024, 80), (1024, 128), (520, 64)])
+def test_posteriors_cluster_fp32(vl, restatement, KD):
+    from vlfeat_b200 import workloads as W
+    K, D = KD
+    pr, mu, cv = W.fv_gmm(K, D, seed=37)
+    x = W.pca_like(4000, D, seed=38)
+    q64, ll64 = restatement.posteriors(x.astype(np.float64), pr.astype(np.float64),
+                                       mu.astype(np.float64), cv.astype(np.float64))
+    vl.set_precision("fp32")
+    q, ll = vl.get_gmm_data_posteriors(x, pr, mu, cv)
+    q_tol, ll_tol = {64: (1e-4, 1e-6), 80: (1e-4, 1e-6), 128: (2e-4, 4e-6)}[D]
+    assert np.max(np.abs(q - q64)) < q_tol
+    assert abs(ll - ll64) < ll_tol * abs(ll64)
+
+
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+def test_em_cluster_k1024(vl, restatement, mode):
+    """EM at K=1024, D=128 (the large-EM shape) on the SIFT-like generator at
+    reduced N: cluster E-step, statistics over 1,024 components."""
+    from vlfeat_b200 import workloads as W
+    c = W.config1(N=30000, K=1024, iters=2)
+    r = restatement.em(c["data"].astype(np.float64), c["priors"], c["means"], c["covs"],
+                       c["lower_bound"], 2)
+    m, ll = _em(vl, c, 2, mode)
+    assert abs(ll - r["ll"]) <= 2e-5 * abs(r["ll"])
+    assert rel_err(m.means, r["means"]) < EM_TOL[mode]
+    assert rel_err(m.covariances, r["covs"]) < EM_TOL[mode]
+    assert rel_err(m.priors, r["priors"]) < EM_TOL[mode]

@@ -122,6 +122,8 @@ void router_default_posteriors(const float *X, i64 N, const DevModel<float> &m, 
 // ------------------------------------------------------- tensor-core path
 // Implemented in k_tc.cu.  Available for float data only.
 bool tc_supported(i64 K, i64 D);
+// The tensor-core Fisher encoder (E-step, statistics and the cluster finalize).
+bool tc_fv_supported(i64 K, i64 D);
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
              bool fast, int precision, cudaStream_t s);
 // EM with the tensor-core M-step.  tc_estep_em is the E-step of tc_estep that

@@ -182,8 +182,11 @@ __host__ __device__ constexpr bool q_image32(int qf) { return qf == kQImg32 || q
 struct EParams {
   const float *X;
   i64 N;
-  int K, Kp, Kq, nst;  // Kq: components in the q image (Kp rounded up to 128)
-  i64 qpart;           // bytes of one part of the q image
+  // Kp: this CTA's components (at most 256); Kg: all padded components (the
+  // W image's and cst2's extent; Kp times the cluster size); Kq: components in
+  // the q image (Kg rounded up to 128).
+  int K, Kp, Kg, Kq, nst;
+  i64 qpart;  // bytes of one part of the q image
   const uint4 *wimg;
   const float *cst2;
   const float *ctr;
@@ -202,7 +205,7 @@ struct EParams {
 // image (hi + lo) is copied in once; with W streamed (SW true: W does not fit,
 // e.g. D=128 at K=256) each operand stage also holds the k-atom of W its
 // MMAs read, bulk-copied from global memory (L2) when the stage is filled.
-template <int DIM, bool SW = false>
+template <int DIM, bool SW = false, bool CL = false>
 struct ELayout {
   static constexpr int KD2 = 2 * DIM;
   static constexpr int NKA = KD2 / 32;
@@ -213,8 +216,10 @@ struct ELayout {
   __host__ __device__ static size_t wbytes(int Kp) { return (size_t)NKA * Kp * 64; }
   __host__ __device__ static size_t wstage(int Kp) { return SW ? (size_t)2 * Kp * 64 : 0; }
   __host__ __device__ static size_t stage(int Kp) { return kStage + wstage(Kp); }
+  // Cluster exchange slots: per TMEM buffer, 128 rows of (max, sum, argmax).
+  static constexpr int kXch = CL ? 2 * 128 * 16 : 0;
   static size_t fixed(int Kp) {
-    return (SW ? 0 : 2 * wbytes(Kp)) + 1024 /*cst*/ + 1024 /*ctr, bars*/ + kStaging + 1024 /*alignment*/;
+    return (SW ? 0 : 2 * wbytes(Kp)) + 1024 /*cst*/ + 1024 /*ctr, bars*/ + kStaging + kXch + 1024 /*alignment*/;
   }
   static int max_stages(int Kp) {
     return fixed(Kp) >= (size_t)kSmemLimit ? 0 : (int)((kSmemLimit - fixed(Kp)) / stage(Kp));
@@ -222,9 +227,14 @@ struct ELayout {
   static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * stage(Kp); }
 };
 
-template <int DIM, int QF, bool FAST, bool SW = false>
+// CL: the components are split over the CTAs of a thread-block cluster (K
+// above 256): CTA r computes the logits of components [r Kp, (r+1) Kp) for
+// every tile of its cluster, and after pass A the CTAs exchange each row's
+// running maximum and sum through distributed shared memory, so that pass B
+// normalises with the row's log-sum-exp over all K.
+template <int DIM, int QF, bool FAST, bool SW = false, bool CL = false>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
-  using L = ELayout<DIM, SW>;
+  using L = ELayout<DIM, SW, CL>;
   constexpr int NKA = L::NKA;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *base = align1024(smem_raw);
@@ -235,11 +245,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   uint8_t *sA = sW + (SW ? 0 : 2 * wbytes);
   float *s_cst = (float *)(sA + (size_t)p.nst * stageBytes);
   float *s_ctr = s_cst + 256;                     // DIM <= 128 floats
-  uint64_t *bars = (uint64_t *)(s_ctr + 128);     // 36 barriers, then TMEM base and abort flag
+  uint64_t *bars = (uint64_t *)(s_ctr + 128);     // 52 barriers, then TMEM base and abort flag
   uint64_t *full = bars, *empty = bars + 16, *accf = bars + 32, *acce = bars + 34;
-  uint32_t *s_tmem = (uint32_t *)(bars + 36);
+  uint64_t *xready = bars + 36, *xcons = bars + 44;  // cluster exchange: [buffer][epilogue warp]
+  uint32_t *s_tmem = (uint32_t *)(bars + 52);
   volatile int *s_abort = (volatile int *)(s_tmem + 1);
   uint8_t *s_stage = (uint8_t *)(s_cst + 512);   // 8 x 2 KB epilogue staging
+  float4 *s_xch = (float4 *)(s_stage + L::kStaging);  // [buffer][row] (max, sum, argmax) when CL
+  // This CTA's components and tiles: with CL the cluster shares each tile.
+  const int crank = CL ? (int)cluster_rank() : 0, ncta = CL ? (int)cluster_size() : 1;
+  const int kbase = crank * p.Kp;
+  const i64 tile0 = blockIdx.x / ncta, tstep = gridDim.x / ncta;
+  const size_t wbytesG = (size_t)NKA * p.Kg * 64;  // the global W image's part size
 
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   if (tid == 0) {
@@ -251,6 +268,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 128);
     }
+    if (CL)
+      for (int b = 0; b < 8; ++b) {
+        mbar_init(&xready[b], ncta);
+        mbar_init(&xcons[b], ncta);
+      }
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -258,13 +280,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     tmem_alloc(s_tmem, 512);
     tmem_relinquish();
   }
-  // Resident W (pre-swizzled image) and per-component constants.
+  // Resident W (this CTA's rows of the pre-swizzled image: per part and
+  // k-atom, Kp rows of 64 bytes) and per-component constants.
   {
     const uint4 *src = p.wimg;
     uint4 *dst = (uint4 *)sW;
     const int n16 = SW ? 0 : (int)(2 * wbytes / 16);
-    for (int i = tid; i < n16; i += kTcThreads) dst[i] = src[i];
-    for (int k = tid; k < 256; k += kTcThreads) s_cst[k] = k < p.Kp ? p.cst2[k] : -INFINITY;
+    const int part16 = (int)(wbytes / 16), atom16 = (int)(wpart / 16);
+    for (int i = tid; i < n16; i += kTcThreads) {
+      const int part = i / part16, rem = i % part16, c = rem / atom16, o = rem % atom16;
+      dst[i] = src[(part * wbytesG + (size_t)c * p.Kg * 64 + (size_t)kbase * 64) / 16 + o];
+    }
+    for (int k = tid; k < 256; k += kTcThreads) s_cst[k] = k < p.Kp ? p.cst2[kbase + k] : -INFINITY;
     for (int d = tid; d < DIM; d += kTcThreads) s_ctr[d] = p.ctr[d];
     fence_proxy_async_smem();
   }
@@ -295,14 +322,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     };
     // Positions (tile, chunk) of the chunk being converted and the next two,
     // whose rows are already in flight (a 3-deep register prefetch ring).
-    i64 t0 = blockIdx.x, t1, t2;
+    i64 t0 = tile0, t1, t2;
     int c0 = 0, c1, c2, it = 0;
     auto adv = [&](i64 t, int c, i64 &tn, int &cn) {
       tn = t;
       cn = c + 1;
       if (cn == NKA) {
         cn = 0;
-        tn += gridDim.x;
+        tn += tstep;
       }
     };
     adv(t0, c0, t1, c1);
@@ -317,10 +344,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       const uint32_t a_hi = smem_u32(sA + (size_t)stage * stageBytes);
       if (SW && warp == 0 && lane == 0) {
         // This stage's k-atom of W: its hi and lo parts, complete on full[stage].
-        const uint8_t *w = (const uint8_t *)p.wimg + (size_t)c0 * wpart;
+        const uint8_t *w = (const uint8_t *)p.wimg + (size_t)c0 * p.Kg * 64 + (size_t)kbase * 64;
         mbar_arrive_expect_tx(&full[stage], 2 * wpart);
         bulk_g2s(a_hi + L::kStage, w, wpart, &full[stage]);
-        bulk_g2s(a_hi + L::kStage + wpart, w + wbytes, wpart, &full[stage]);
+        bulk_g2s(a_hi + L::kStage + wpart, w + wbytesG, wpart, &full[stage]);
       }
       const int d0 = 16 * c0 + 4 * part;
       const float m0 = s_ctr[d0], m1 = s_ctr[d0 + 1], m2 = s_ctr[d0 + 2], m3 = s_ctr[d0 + 3];
@@ -360,11 +387,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     const int eg = (warp - 4) >> 2, ew = warp & 3;
     const int r = ew * 32 + lane;
     const int nch = p.Kp / 32;
-    const int ncw = q_image(QF) ? p.Kq / 32 : nch;
+    // Image chunks this CTA writes: its own, and (last CTA) the zero padding
+    // from Kg to Kq.
+    const int ncw = q_image(QF) ? nch + (crank == ncta - 1 ? (p.Kq - p.Kg) / 32 : 0) : nch;
     const unsigned long long *cst2v = (const unsigned long long *)s_cst;
     uint8_t *stg = s_stage + (warp - 4) * 2048;
     int tt = 0;
-    for (i64 tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x, ++tt) {
+    for (i64 tile = tile0; tile < p.ntiles; tile += tstep, ++tt) {
       const int buf = tt & 1;
       if (buf != eg) continue;
       if (!mbar_wait(&accf[buf], (tt >> 1) & 1, s_abort, p.err, 2)) break;
@@ -442,7 +471,40 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         mg[pc >> 1] = m;
       }
       tmem_wait_st();
-      const float mt = m, st = sum;
+      float mt = m, st = sum;
+      if constexpr (CL) {
+        // Exchange (max, sum, argmax) of each row with the cluster and
+        // combine them in rank order, identically in every CTA.
+        uint64_t *xr = &xready[buf * 4 + ew], *xc = &xcons[buf * 4 + ew];
+        float4 *slot = s_xch + buf * 128;
+        const int use = tt >> 1;
+        if (use > 0 && !mbar_wait_cluster(xc, (use + 1) & 1, s_abort, p.err, 5)) break;
+        slot[r] = make_float4(m, sum, __int_as_float(kbase + am), 0.f);
+        fence_acq_rel_cluster();
+        __syncwarp();
+        if (lane < ncta) mbar_arrive_remote(xr, (uint32_t)lane);
+        if (!mbar_wait_cluster(xr, use & 1, s_abort, p.err, 6)) break;
+        float4 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q < ncta) v[q] = ld_dsmem_f4(&slot[r], (uint32_t)q);
+        float M = -INFINITY, S = 0.f;
+        int amg = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q < ncta && v[q].x > M) {  // first rank wins ties: first index, vl/fisher.c:406
+            M = v[q].x;
+            amg = __float_as_int(v[q].z);
+          }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q < ncta && v[q].x != -INFINITY) S += v[q].y * ex2_approx(v[q].x - M);
+        __syncwarp();
+        if (lane < ncta) mbar_arrive_remote(xc, (uint32_t)lane);
+        mt = M;
+        st = S;
+        if (FAST) am = amg - kbase;
+      }
       const float inv = 1.f / st;
       const i64 row = tile * 128 + r;
       const bool valid = row < p.N;
@@ -464,8 +526,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const uint4 v = *(const uint4 *)(stg + (8 * i + a) * 64 + ((b ^ ((a >> 1) & 3)) << 4));
-          const size_t off = (size_t)(4 * ew + i) * (p.Kq / 64) * 1024 + (size_t)(cc >> 1) * 1024 +
-                             mnmajor_sw128_off((uint32_t)a, (uint32_t)((cc & 1) * 4 + b));
+          const int gc = kbase / 32 + cc;  // chunk of the whole image
+          const size_t off = (size_t)(4 * ew + i) * (p.Kq / 64) * 1024 + (size_t)(gc >> 1) * 1024 +
+                             mnmajor_sw128_off((uint32_t)a, (uint32_t)((gc & 1) * 4 + b));
           *(uint4 *)(ib + part_off + off) = v;
         }
         __syncwarp();
@@ -488,7 +551,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
           for (int j = 0; j < 16; ++j) {
             float x0, x1;
             if (FAST) {
-              x0 = (live && cc * 32 + 2 * j == am) ? 1.f : 0.f;
+              x0 = (live && cc * 32 + 2 * j == am) ? 1.f : 0.f;  // am: this CTA's columns
               x1 = (live && cc * 32 + 2 * j + 1 == am) ? 1.f : 0.f;
             } else {
               const unsigned long long q2 = mul2(f2u(__uint_as_float(va[2 * j]), __uint_as_float(va[2 * j + 1])), sc2);
@@ -516,7 +579,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         }
         if (q_rows(QF)) {
           if (live) {
-            const int k0 = cc * 32;
+            const int k0 = kbase + cc * 32;
             float *dst = (float *)p.q + row * p.ldq + k0;
             if (k0 + 32 <= p.K) {
 #pragma unroll
@@ -557,12 +620,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       }
       tc_fence_before();
       mbar_arrive(&acce[buf]);
-      if (valid && p.rowcnt) p.rowcnt[row] = (unsigned)(lo32(cnt2) + hi32(cnt2));
+      if (valid && p.rowcnt) {
+        const unsigned cnt = (unsigned)(lo32(cnt2) + hi32(cnt2));
+        if (CL) atomicAdd(&p.rowcnt[row], cnt);  // zeroed by the launcher
+        else p.rowcnt[row] = cnt;
+      }
       // Per-warp log-likelihood partial (fixed shuffle order): 4 per tile.
       double ll = valid ? ((double)mt + log2((double)st)) * kLn2 : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
-      if (lane == 0 && p.ll_part) p.ll_part[tile * 4 + ew] = ll;
+      if (lane == 0 && p.ll_part && crank == 0) p.ll_part[tile * 4 + ew] = ll;
     }
   } else if (warp == 12 && lane == 0) {
     // ---------------------------------------------------------- MMA
@@ -570,7 +637,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     const uint32_t w_hi = smem_u32(sW), w_lo = w_hi + wbytes;
     int it = 0, tt = 0;
     bool ok = true;
-    for (i64 tile = blockIdx.x; tile < p.ntiles && ok; tile += gridDim.x, ++tt) {
+    for (i64 tile = tile0; tile < p.ntiles && ok; tile += tstep, ++tt) {
       const int buf = tt & 1;
       if (!mbar_wait(&acce[buf], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 3)) break;
       tc_fence_after();
@@ -603,6 +670,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   }
   tc_fence_before();
   __syncthreads();
+  // No CTA leaves while another may still read its exchange slots (every
+  // role's waits are bounded, so every CTA arrives here).
+  if (CL) cg::this_cluster().sync();
   if (warp == 12) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
@@ -1132,7 +1202,17 @@ struct TcPrep {
   __nv_bfloat16 *wimg = nullptr;
 };
 
-int padK(i64 K) { return (int)((K + 31) / 32 * 32); }
+// Components of the tensor-core path, padded: a multiple of 32 up to 256; above
+// that nb = ceil(K / 256) CTAs of a cluster take Kb components each (Kb a
+// multiple of 32, at most 256) and K is padded to nb Kb.
+int padK(i64 K) {
+  const int k32 = (int)((K + 31) / 32 * 32);
+  if (k32 <= 256) return k32;
+  const int nb = (k32 + 255) / 256;
+  const int kb = ((k32 + nb - 1) / nb + 31) / 32 * 32;
+  return nb * kb;
+}
+int kblocks(int Kp) { return (Kp + 255) / 256; }
 
 void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &sc, cudaStream_t s) {
   tp.K = (int)m.K;
@@ -1140,7 +1220,7 @@ void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &
   tp.D = (int)m.D;
   const int KD2 = 2 * tp.D;
   tp.ctr = sc.slot[0].get<float>(256);
-  tp.cst2 = sc.slot[1].get<float>(256);
+  tp.cst2 = sc.slot[1].get<float>(std::max(256, tp.Kp));
   tp.wimg = sc.slot[2].get<__nv_bfloat16>((size_t)2 * tp.Kp * KD2);
   VLB_LAUNCH("tc_center", s, k_tc_center<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, tp.K, tp.D, tp.ctr));
   const i64 n = (i64)tp.Kp * KD2;
@@ -1173,47 +1253,79 @@ struct EOut {
   double qthr = 1e-6;  // vl/fisher.c:440 (the Fisher skip)
 };
 
-template <int DIM, int QF, bool SW>
+template <int DIM, int QF, bool SW, bool CL>
 i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
                       unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s,
                       const EOut &eo) {
-  using L = ELayout<DIM, SW>;
+  using L = ELayout<DIM, SW, CL>;
   const i64 ntiles = (N + 127) / 128;
   if (ntiles == 0) return 0;
-  const int nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(tp.Kp));
+  const int nb = CL ? kblocks(tp.Kp) : 1, Kb = tp.Kp / nb;
+  const int nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(Kb));
   VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
-  const size_t smem = L::bytes(tp.Kp, nst);
-  auto kern = k_tc_estep<DIM, QF, false, SW>;
+  const size_t smem = L::bytes(Kb, nst);
+  auto kern = k_tc_estep<DIM, QF, false, SW, CL>;
   if constexpr (!q_rows(QF) || QF == kQRow) {
-    if (fast) kern = k_tc_estep<DIM, QF, true, SW>;
+    if (fast) kern = k_tc_estep<DIM, QF, true, SW, CL>;
   } else {
     VLB_CHECK(!fast, VL_ERR_BAD_ARG, "tensor-core E-step: the combined formats have no FAST variant");
   }
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   EParams p;
-  p.X = X; p.N = N; p.K = tp.K; p.Kp = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
+  p.X = X; p.N = N; p.K = tp.K; p.Kp = Kb; p.Kg = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
   p.qpart = ntiles * 128 * (i64)p.Kq * 2;
   p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr;
   p.q = q; p.qimg = eo.qimg; p.ldq = ldq; p.fast = fast ? 1 : 0; p.qthr = float_at_least(eo.qthr);
   p.rowcnt = rowcnt; p.ll_part = ll_part;
   p.err = err; p.ntiles = ntiles;
-  const int grid = (int)std::min<i64>(ntiles, num_sms());
-  VLB_LAUNCH("tc_estep_bf16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
+  if constexpr (!CL) {
+    const int grid = (int)std::min<i64>(ntiles, num_sms());
+    VLB_LAUNCH("tc_estep_bf16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
+  } else {
+    // One cluster of nb CTAs per tile, as many clusters as fit at once
+    // (persistent: each cluster strides over the tiles).
+    if (rowcnt) VLB_CUDA(cudaMemsetAsync(rowcnt, 0, sizeof(unsigned) * (size_t)N, s));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)nb;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3((unsigned)(nb * std::max(1, num_sms() / nb)));
+    int maxc = 0;
+    VLB_CUDA(cudaOccupancyMaxActiveClusters(&maxc, kern, &cfg));
+    VLB_CHECK(maxc >= 1, VL_ERR_BAD_ARG, "tensor-core E-step: the CTA cluster does not fit on the device");
+    cfg.gridDim = dim3((unsigned)(nb * std::min<i64>(ntiles, maxc)));
+    VLB_LAUNCH("tc_estep_bf16x3", s, VLB_CUDA(cudaLaunchKernelEx(&cfg, kern, p)));
+  }
   return ntiles * 4;  // LL partials written
 }
 
 // W resident in shared memory when two operand stages fit beside it, else
-// streamed through the stages (built for D=128, the only supported dimension
-// whose W can exceed shared memory at K <= 256).
+// streamed through the stages (D=128 at 256 components per CTA).  Above 256
+// components the E-step runs as clusters of CTAs.
 template <int DIM, int QF>
 i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
                  unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s,
                  const EOut &eo) {
+  if (tp.Kp > 256) {
+    const int Kb = tp.Kp / kblocks(tp.Kp);
+    if constexpr (DIM == 128) {
+      if (ELayout<DIM, false, true>::max_stages(Kb) < 2)
+        return launch_estep_impl<DIM, QF, true, true>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
+    }
+    return launch_estep_impl<DIM, QF, false, true>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
+  }
   if constexpr (DIM == 128) {
     if (ELayout<DIM, false>::max_stages(tp.Kp) < 2)
-      return launch_estep_impl<DIM, QF, true>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
+      return launch_estep_impl<DIM, QF, true, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
   }
-  return launch_estep_impl<DIM, QF, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
+  return launch_estep_impl<DIM, QF, false, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
 }
 
 template <int DIM, int MT, int SPLIT>
@@ -1312,12 +1424,24 @@ void lpt_assign(const std::vector<SItem> &items, int gx, std::vector<int> &order
 
 bool tc_supported(i64 K, i64 D) {
   if (!(D == 64 || D == 80 || D == 128)) return false;
-  if (K < 8 || K > 256 || K % 8) return false;
-  // W resident beside two operand stages, or (D=128) streamed through them;
-  // TMEM holds two K_pad-column accumulators.
-  const int Kp = padK(K);
-  if (D == 128) return ELayout<128, true>::max_stages(Kp) >= 2;
-  return D == 64 ? ELayout<64, false>::max_stages(Kp) >= 2 : ELayout<80, false>::max_stages(Kp) >= 2;
+  if (K < 8 || K > 2048 || K % 8) return false;
+  // Per CTA: W resident beside two operand stages, or (D=128) streamed through
+  // them; TMEM holds two accumulators of the CTA's components.  Above 256
+  // components, clusters of up to 8 CTAs.
+  const int Kp = padK(K), nb = kblocks(Kp), Kb = Kp / nb;
+  if (nb > 8) return false;
+  if (nb == 1) {
+    if (D == 128) return ELayout<128, true>::max_stages(Kb) >= 2;
+    return D == 64 ? ELayout<64, false>::max_stages(Kb) >= 2 : ELayout<80, false>::max_stages(Kb) >= 2;
+  }
+  if (D == 128) return ELayout<128, true, true>::max_stages(Kb) >= 2;
+  return D == 64 ? ELayout<64, false, true>::max_stages(Kb) >= 2 : ELayout<80, false, true>::max_stages(Kb) >= 2;
+}
+
+bool tc_fv_supported(i64 K, i64 D) {
+  // The finalize keeps 2 (K / kFinCluster) D floats per CTA in shared memory.
+  return tc_supported(K, D) && K % kFinCluster == 0 &&
+         sizeof(float) * 2 * (size_t)(K / kFinCluster) * D <= (size_t)kSmemLimit;
 }
 
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part, bool fast,
@@ -1608,7 +1732,7 @@ void plan_build(TcFvPlan &p, cudaStream_t s) {
 
 TcFvPlan *tc_fv_plan_new(i64 D, i64 K, const i64 *offsets, i64 numImages, int flags, int precision,
                          cudaStream_t s) {
-  VLB_CHECK(tc_supported(K, D), VL_ERR_BAD_ARG, "batched Fisher plan: unsupported (numClusters, dimension)");
+  VLB_CHECK(tc_fv_supported(K, D), VL_ERR_BAD_ARG, "batched Fisher plan: unsupported (numClusters, dimension)");
   VLB_CHECK(precision == VLB200_PREC_FP32 || precision == VLB200_PREC_BF16 ||
                 precision == VLB200_PREC_BF16_ROUTER,
             VL_ERR_BAD_ARG, "batched Fisher plan: precision must be FP32, BF16 or BF16_ROUTER");
