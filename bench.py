@@ -378,7 +378,7 @@ def e2e(capi, wl, prec, config, steps=3):
             "d2h_bytes_per_step": int(NUM_IMAGES * (2 * K * D * 4 + 8)), "ms_per_step": ms}
 
 
-def em_throughput(capi, iters=5, cpu=True):
+def em_throughput(capi, iters=5, cpu=True, large=True):
     """EM iterations/s (a north-star throughput besides the Fisher metric).
 
     Config 1 (N=1,000,000 SIFT-like descriptors, D=128, K=256, custom init,
@@ -395,6 +395,11 @@ def em_throughput(capi, iters=5, cpu=True):
     out = {"timing": "wall clock around vlb200_gmm_em_device (blocking), after one untimed run"}
     cfgs = [("config1_sift_n1m_d128_k256", W.config1(N=1_000_000, K=256, iters=iters), iters),
             ("config0_n50k_d64_k64", W.config0(), 10)]
+    if large:
+        # Config 4's shape (SIFT-like, D=128, K=1024) at N=8,000,000 of its
+        # 20,000,000: the posteriors (N x K) and the M-step's posterior image
+        # stay in HBM (66 GB here, 164 GB at full N in FP32 mode).
+        cfgs.append(("config4_shape_sift_n8m_d128_k1024", W.config1(N=8_000_000, K=1024, iters=3), 3))
     for name, c, T in cfgs:
         x = torch.from_numpy(np.ascontiguousarray(c["data"])).cuda()
         N = int(x.shape[0])
@@ -440,6 +445,17 @@ def em_throughput(capi, iters=5, cpu=True):
                                "sample": f"config 1, first {n} descriptors, 2 iterations of vl_gmm_cluster",
                                "descriptor_iterations_per_s": n * 2 / dt,
                                "ms_per_iteration": 1e3 * dt / 2}
+        if large:
+            c4 = cfgs[-1][1]
+            n4 = 20_000
+            t0 = time.perf_counter()
+            impl.em(np.ascontiguousarray(c4["data"][:n4]), c4["priors"], c4["means"], c4["covs"],
+                    c4["lower_bound"], 1)
+            dt = time.perf_counter() - t0
+            out["cpu_baseline_config4_shape"] = {
+                "kind": kind, "cores": os.cpu_count() or 1,
+                "sample": f"config 4 shape, first {n4} descriptors, 1 iteration of vl_gmm_cluster",
+                "descriptor_iterations_per_s": n4 / dt}
     return out
 
 
