@@ -541,6 +541,73 @@ def vlad_throughput(capi, wl, steps=3, warmup=1, cpu=True, budget_s=8.0):
     return out
 
 
+def prologue_throughput(capi, wl, steps=3, warmup=1, cpu=True, budget_s=6.0):
+    """The recognition app's descriptor prologue (apps/recognition/
+    encodeImage.m:91-103) on the Fisher workload's images: 128-d descriptors ->
+    P (x - c) with P 80 x 128 -> L2 renormalisation -> 'xy' extension with the
+    frame normalised by its image's size (82-d output, the FV encoder's input
+    in the app).  Inputs resident in HBM, CUDA events on the launching stream.
+    Roofline: 2 x 128 x 80 fp32 FMA flop per descriptor on the CUDA cores
+    (nominal fp32 rate = SMs x 128 lanes x 2 x max SM clock) and 848 B per
+    descriptor of HBM traffic."""
+    import torch
+    offs = wl["offs"]
+    N, nimg, din, dout = int(offs[-1]), len(offs) - 1, 128, 80
+    g = torch.Generator(device="cuda")
+    g.manual_seed(71)
+    x = torch.rand((N, din), generator=g, device="cuda") * 255.0
+    P = torch.randn((dout, din), generator=g, device="cuda") / 11.3
+    c = torch.rand(din, generator=g, device="cuda") * 128.0
+    sizes = torch.tensor([[640.0, 480.0]], device="cuda").repeat(nimg, 1)
+    frames = torch.rand((N, 2), generator=g, device="cuda") * 400.0
+    out = torch.empty((N, dout + 2), device="cuda")
+    stream = torch.cuda.current_stream()
+    run = lambda: capi.pca_project_device(out, x, P, c, True, frames, offs, sizes)
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = float(np.median(ms))
+    props = torch.cuda.get_device_properties(0)
+    peaks = measured_peaks()
+    fp32_tflops = props.multi_processor_count * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    flop = 2.0 * din * dout * N
+    bytes_ = (4.0 * din + 8 + 4.0 * (dout + 2)) * N
+    res = {"workload": f"{nimg} images, {N} descriptors, 128 -> 80 + xy, renormalised", "ms_per_step": t,
+           "value": N / (t * 1e-3), "unit": "descriptors/s",
+           "fp32_cores": {"achieved_tflops": flop / (t * 1e-3) / 1e12, "nominal_tflops": fp32_tflops,
+                          "frac": flop / (t * 1e-3) / 1e12 / fp32_tflops},
+           "hbm": {"achieved_gbs": bytes_ / (t * 1e-3) / 1e9, "peak_gbs": peaks.get("hbm_gbs"),
+                   "frac": bytes_ / (t * 1e-3) / 1e9 / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None}}
+    if cpu:
+        from oracle import oracle as O
+        n = min(N, 2_000_000)
+        xs, fs = x[:n].cpu().numpy(), frames[:n].cpu().numpy()
+        Pn, cn = P.cpu().numpy(), c.cpu().numpy()
+        t0 = time.perf_counter()
+        done = 0
+        while done < n and time.perf_counter() - t0 < budget_s:
+            b = min(n - done, 250_000)
+            O.pca_project(xs[done:done + b], Pn, cn, True, fs[done:done + b], np.array([0, b]),
+                          np.array([[640.0, 480.0]]))
+            done += b
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"kind": "port", "cores": os.cpu_count() or 1, "value": done / dt,
+                               "unit": "descriptors/s",
+                               "sample": f"{done} descriptors through the float64 NumPy restatement "
+                                         "(multithreaded BLAS); the reference's step is MATLAB"}
+    del x, out, frames
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_reference(args, rank, world):
     """The reference arm: VLFeat's own CPU code on the host cores."""
     if rank != 0:
@@ -591,6 +658,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-em", action="store_true", help="skip the EM iterations/s measurement")
     ap.add_argument("--no-vlad", action="store_true", help="skip the VLAD descriptors/s measurement")
+    ap.add_argument("--no-prologue", action="store_true",
+                    help="skip the descriptor prologue (PCA projection) measurement")
     ap.add_argument("--images", type=int, default=4096,
                     help="encode only the first IMAGES images of the workload (small profiling cases)")
     ap.add_argument("--plan", default=None,
@@ -669,6 +738,8 @@ def main():
             out["em"] = em_throughput(capi, cpu=not args.no_cpu)
         if not args.no_vlad and world == 1:
             out["vlad"] = vlad_throughput(capi, wl, cpu=not args.no_cpu)
+        if not args.no_prologue and world == 1:
+            out["prologue"] = prologue_throughput(capi, wl, cpu=not args.no_cpu)
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

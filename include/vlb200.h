@@ -108,6 +108,35 @@ VL_EXPORT int vlb200_vlad_encode_batch_device(void *enc, vl_type dataType, void 
                                               vl_int64 const *offsets, vl_size numImages,
                                               int flags, void *stream);
 
+/* ---------------------------------------------------- descriptor prologue
+ * The recognition app's step before encoding (apps/recognition/encodeImage.m:
+ * 91-103): out = P (data - center), each row optionally L2-renormalised
+ * (times 1 / max(1e-12, norm)), then, when frames is not NULL, the frame
+ * position normalised by the image size appended ('xy' geometric extension,
+ * apps/recognition/extendDescriptorsWithGeometry.m:19-21): row i of out is
+ * [y_i, (fx - w/2)/w, (fy - h/2)/h].  All arrays are device pointers except
+ * offsets (numImages+1 int64, host).  projection: dimOut x dimIn, center:
+ * dimIn, data: numData x dimIn, out: numData x (dimOut + 2 if frames);
+ * frames: numData x 2 (pixel x, y); imageSizes: numImages x 2 (w, h), image j
+ * owning rows offsets[j] .. offsets[j+1]-1.  dimIn, dimOut <= 128.  FP32
+ * arithmetic.  Returns 0 or a VL_ERR_* code. */
+VL_EXPORT int vlb200_pca_project_device(float *out, vl_size dimOut, float const *data, vl_size dimIn,
+                                        vl_size numData, float const *projection, float const *center,
+                                        int renormalize, float const *frames, vl_int64 const *offsets,
+                                        float const *imageSizes, vl_size numImages, void *stream);
+
+/* PCA of a descriptor sample as the app learns it (apps/recognition/
+ * trainEncoder.m:150-171): center = mean, C = (data - center)^T (data -
+ * center) / numData (fp64 on the GPU), eigenvectors by decreasing eigenvalue
+ * d (cyclic Jacobi, fp64, host), d += whiteningRegul * max(d); projection
+ * (numPcaDimensions x dimIn, device) = the first eigenvectors as rows,
+ * scaled by 1/sqrt(d) when whitening, each with its largest-magnitude entry
+ * positive; center: dimIn (device); eigenvalues: numPcaDimensions regularised
+ * eigenvalues (host) or NULL.  dimIn <= 128. */
+VL_EXPORT int vlb200_pca_learn_device(float *projection, float *center, vl_size numPcaDimensions,
+                                      float const *data, vl_size dimIn, vl_size numData, int whitening,
+                                      double whiteningRegul, double *eigenvalues, void *stream);
+
 /* ------------------------------------------------------ batched encode plan
  * A plan binds the tensor-core batched encoder to one batch layout (offsets,
  * numImages), dimension, numClusters, flags and precision (FP32, BF16 or

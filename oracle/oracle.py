@@ -13,6 +13,10 @@ does.
   vl/fisher.h:48-54, vl/vlad.h:45-50).  It exists only where that library was
   built.
 * :func:`vlad` restates VLAD encoding (vl/vlad.c:163-242) in NumPy.
+* :func:`pca_learn` and :func:`pca_project` restate the recognition app's
+  descriptor prologue (apps/recognition/trainEncoder.m:150-171,
+  encodeImage.m:91-103), MATLAB code with no compiled form here: the
+  restatement follows the .m files and is not pinned to outputs of them.
 """
 from __future__ import annotations
 
@@ -367,6 +371,45 @@ def vlad(data, means, assignments, flags):
         n = floor(np.sqrt(np.asarray(n, x.dtype)))
         enc = enc / n
     return enc
+
+
+def pca_learn(descrs, num_pca, whitening=False, regul=0.0):
+    """PCA learning of apps/recognition/trainEncoder.m:150-171 restated in
+    float64: center = mean, X = x x^T / n, eigenvalues sorted decreasing,
+    d += regul * max(d), projection = first eigenvectors as rows (scaled by
+    1/sqrt(d) when whitening).  descrs: n x D (one descriptor per row).
+    Eigenvector signs are fixed as the library fixes them: the entry of
+    largest magnitude is positive."""
+    x = np.asarray(descrs, np.float64)
+    c = x.mean(0)
+    xc = x - c
+    X = xc.T @ xc / x.shape[0]
+    d, V = np.linalg.eigh(X)
+    perm = np.argsort(-d, kind="stable")
+    d, V = d[perm], V[:, perm]
+    d = d + regul * d.max()
+    m = min(num_pca, x.shape[1])
+    V = V[:, :m]
+    am = np.abs(V).argmax(0)
+    V = V * np.where(V[am, np.arange(m)] < 0, -1.0, 1.0)[None, :]
+    P = (V / np.sqrt(d[:m])[None, :]).T if whitening else V.T
+    return P, c, d[:m]
+
+
+def pca_project(descrs, P, c, renormalize=True, frames=None, offsets=None, sizes=None):
+    """Descriptor prologue of apps/recognition/encodeImage.m:91-103 in float64:
+    y = P (x - c), y / max(1e-12, |y|) per descriptor when renormalising, then
+    the 'xy' extension (extendDescriptorsWithGeometry.m:19-21) with frames
+    normalised by their image's size: (f - [w, h]/2) / [w, h]."""
+    y = (np.asarray(descrs, np.float64) - np.asarray(c, np.float64)) @ np.asarray(P, np.float64).T
+    if renormalize:
+        y = y / np.maximum(1e-12, np.sqrt((y * y).sum(1)))[:, None]
+    if frames is None:
+        return y
+    f = np.asarray(frames, np.float64)
+    img = np.searchsorted(np.asarray(offsets), np.arange(len(f)), side="right") - 1
+    wh = np.asarray(sizes, np.float64)[img]
+    return np.concatenate([y, (f - wh / 2) / wh], 1)
 
 
 def simple_fisher(data, means, covs, priors, flags):

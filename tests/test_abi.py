@@ -139,3 +139,17 @@ def test_vlad_argument_checks(libpath):
     offs = np.array([0, 10], np.int64)
     assert L.vlb200_vlad_encode_batch_device(None, 1, None, 1025, 4, None, None, capi._np_ptr(offs), 1, 0,
                                              C.c_void_p(1)) == 3
+
+
+def test_pca_argument_checks(libpath):
+    """Dimensions above 128 and frames without image sizes fail with
+    VL_ERR_BAD_ARG before any device work."""
+    import numpy as np
+    from vlfeat_b200 import capi
+    L = capi.lib()
+    offs = np.array([0, 10], np.int64)
+    assert L.vlb200_pca_project_device(None, 80, None, 129, 10, None, None, 1, None, None, None, 0,
+                                       C.c_void_p(1)) == 3
+    assert L.vlb200_pca_project_device(None, 80, None, 128, 10, None, None, 1, C.c_void_p(16), None, None, 1,
+                                       C.c_void_p(1)) == 3
+    assert L.vlb200_pca_learn_device(None, None, 81, None, 80, 10, 0, 0.0, None, C.c_void_p(1)) == 3

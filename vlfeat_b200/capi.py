@@ -82,6 +82,8 @@ def _decl(L):
     f("vl_vlad_encode", None, _vp, C.c_uint32, _vp, _sz, _sz, _vp, _sz, _vp, C.c_int)
     f("vlb200_vlad_encode_batch_device", C.c_int, _vp, C.c_uint32, _vp, _sz, _sz, _vp, _vp, _vp, _sz,
       C.c_int, _vp)
+    f("vlb200_pca_project_device", C.c_int, _vp, _sz, _vp, _sz, _sz, _vp, _vp, C.c_int, _vp, _vp, _vp, _sz, _vp)
+    f("vlb200_pca_learn_device", C.c_int, _vp, _vp, _sz, _vp, _sz, _sz, C.c_int, C.c_double, _vp, _vp)
     f("vl_get_last_error", C.c_int)
     f("vl_get_last_error_message", C.c_char_p)
     f("vl_set_last_error", C.c_int, C.c_int, C.c_char_p)
@@ -462,6 +464,39 @@ def vlad_encode_batch_device(enc_t, means_t, data_t, assign_t, offsets, flags=0,
                                                len(offs) - 1, int(flags), _stream(stream))
     if rc:
         _raise_last("vlb200_vlad_encode_batch_device")
+
+
+def pca_learn_device(data_t, num_pca_dimensions, whitening=False, whitening_regul=0.0, stream=None):
+    """PCA of a descriptor sample (vlb200_pca_learn_device): returns
+    (projection (m x D) and center (D) as torch CUDA tensors, eigenvalues)."""
+    import torch
+    N, D = data_t.shape
+    m = int(num_pca_dimensions)
+    P = torch.empty((m, D), dtype=torch.float32, device=data_t.device)
+    c = torch.empty(D, dtype=torch.float32, device=data_t.device)
+    ev = np.zeros(m, np.float64)
+    _clear()
+    rc = lib().vlb200_pca_learn_device(P.data_ptr(), c.data_ptr(), m, data_t.data_ptr(), D, N, int(bool(whitening)),
+                                       float(whitening_regul), _np_ptr(ev), _stream(stream))
+    if rc:
+        _raise_last("vlb200_pca_learn_device")
+    return P, c, ev
+
+
+def pca_project_device(out_t, data_t, projection_t, center_t, renormalize=True, frames_t=None, offsets=None,
+                       image_sizes_t=None, stream=None):
+    """The app's descriptor prologue (vlb200_pca_project_device): out_t is
+    N x (m + 2 if frames_t is given)."""
+    N, D = data_t.shape
+    m = projection_t.shape[0]
+    offs = np.ascontiguousarray(offsets if offsets is not None else [0, N], np.int64)
+    _clear()
+    rc = lib().vlb200_pca_project_device(
+        out_t.data_ptr(), m, data_t.data_ptr(), D, N, projection_t.data_ptr(), center_t.data_ptr(),
+        int(bool(renormalize)), frames_t.data_ptr() if frames_t is not None else None, _np_ptr(offs),
+        image_sizes_t.data_ptr() if image_sizes_t is not None else None, len(offs) - 1, _stream(stream))
+    if rc:
+        _raise_last("vlb200_pca_project_device")
 
 
 class FisherPlan:
