@@ -9,7 +9,7 @@ of 40,960 floats per image.  One step = one batched encode of all images.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Each path (exact CUDA-core fp32, tensor-core FP32 = bf16x3, BF16, BF16 +
+Each path (exact CUDA-core fp32, tensor-core FP32 = fp16x3, BF16, BF16 +
 router) is timed with CUDA events on the launching stream.  The tensor-core
 FP32 and BF16 paths run through a batched-encode plan (vlb200_fisher_plan_*):
 its tile shapes are autotuned on the workload and one whole encode is
@@ -315,8 +315,8 @@ def roofline(capi, wl, run, prec):
         pass
     # The same kernel against the HBM roofline: algorithmic bytes (x read,
     # q written or read) per descriptor.
-    alg_bytes = {"tc_estep_bf16x3": 320 + (2 if prec != "fp32" else 4) * K,
-                 "tc_stats_f16x2": 320 + 2 * K, "tc_stats_bf16x3": 320 + 4 * K}.get(name)
+    alg_bytes = {"tc_estep_f16x3": 320 + (2 if prec != "fp32" else 4) * K,
+                 "tc_stats_f16x2": 320 + 2 * K, "tc_stats_f16x3": 320 + 4 * K}.get(name)
     hbm_view = None
     if alg_bytes:
         gbs = units * alg_bytes / per_launch_s / 1e9
@@ -425,8 +425,8 @@ def em_throughput(capi, iters=5, cpu=True, large=True):
                          "iterations_per_s": its / dt, "descriptor_iterations_per_s": N * its / dt,
                          "log_likelihood": ll, "restarts": g.num_restarts,
                          "kernels": {"exact": "CUDA-core fp32 E-step and M-step",
-                                     "fp32": "tcgen05 bf16x3 E-step, bf16x3 M-step statistics",
-                                     "bf16": "tcgen05 bf16x3 E-step, fp16 M-step statistics"}[prec]}
+                                     "fp32": "tcgen05 fp16x3 E-step, fp16x3 M-step statistics",
+                                     "bf16": "tcgen05 fp16x3 E-step, fp16x2 M-step statistics"}[prec]}
         out[name] = res
         del x
     if cpu:
@@ -724,7 +724,7 @@ def main():
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": results[head]["ms_per_step"], "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None,
-               "dtype": {"exact": "f32", "fp32": "bf16x3", "bf16": "bf16", "bf16_router": "bf16"}[head],
+               "dtype": {"exact": "f32", "fp32": "f16x3", "bf16": "f16", "bf16_router": "f16"}[head],
                "data": "synthetic", "headline_path": head, "config": workload_desc(wl["total"]),
                "paths": results, "roofline": roof, "kernel_time_share": shares,
                "gpu_launches": launches_of[head], "clocks": clk.summary()}

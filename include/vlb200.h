@@ -19,11 +19,13 @@
  *  EXACT      direct (x-mu)^2/sigma^2 evaluation in the data type on CUDA cores
  *             (float or double), the reference's own formulation
  *             (vl/gmm.c:762-775, vl/fisher.c:442-447).
- *  FP32       tensor cores: E-step and statistics contractions in bf16x3
- *             split precision with fp32 accumulation (FP32-grade results).
- *  BF16       tensor cores: bf16x3 E-step, single-pass bf16 statistics.
+ *  FP32       tensor cores: E-step and statistics contractions in fp16x3
+ *             split precision (two fp16 parts per operand, power-of-two
+ *             scaled) with fp32 accumulation (FP32-grade results).
+ *  BF16       tensor cores: fp16x3 E-step, statistics with a single fp16 part
+ *             of the posteriors (rel err ~1e-4; the name is the mode's).
  *  BF16_ROUTER  learned router picks candidate components; exact posteriors
- *             on the candidates only; bf16 statistics; full E-step fallback
+ *             on the candidates only; fp16 statistics; full E-step fallback
  *             for descriptors whose predicted candidate mass is < 0.99.
  * DEFAULT resolves to the process-wide mode (vlb200_set_precision), which
  * starts as EXACT.  VL_TYPE_DOUBLE calls always run EXACT in double. */

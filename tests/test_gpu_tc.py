@@ -2,10 +2,12 @@
 
 Reference: the FP64 C restatement (oracle/), itself pinned to VLFeat's own
 double results.  Tolerances (relative L2 error of each Fisher vector):
-FP32 mode (bf16x3 on both contractions) 1e-4 -- its E-step split leaves
-~2e-5 on a 3,000-descriptor image and up to ~5e-5 on 200-descriptor images;
-BF16 mode 1e-3 (the metric's bound).  Posteriors: max |q - q64| <= 1e-4 in
-FP32 mode."""
+FP32 mode (fp16x3 on both contractions) 2e-5 -- measured 2.6e-6 to 4.9e-6 on
+200- and 3,000-descriptor images at K=64..1024, D=64..128, and 1.7e-5 on one
+1,000-descriptor image with the signed square root, whose slope near zero
+magnifies the absolute error of near-zero statistics (the exact CUDA-core
+path: 6.3e-6 on that image); BF16 mode 1e-3 (the metric's bound; measured
+~1e-4, set by the single fp16 part of q)."""
 import numpy as np
 import pytest
 
@@ -14,7 +16,7 @@ from oracle.oracle import FLAG_FAST, FLAG_IMPROVED, FLAG_NORMALIZED, FLAG_SQUARE
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp32": 1e-4, "bf16": 1e-3}
+TOL = {"fp32": 2e-5, "bf16": 1e-3}
 
 
 @pytest.fixture(autouse=True)
@@ -91,10 +93,11 @@ def test_posteriors_fp32(vl, restatement, D):
                                        mu.astype(np.float64), cv.astype(np.float64))
     vl.set_precision("fp32")
     q, ll = vl.get_gmm_data_posteriors(x, pr, mu, cv)
-    # Each score sums 2D bf16x3 products, so the error grows with D.  Bounds:
-    # D=80 max |q - q64| 1e-4, LL 1e-6 relative; D=128 2e-4 and 4e-6
-    # (measured 1.05e-4 and 2.6e-6).
-    q_tol, ll_tol = {80: (1e-4, 1e-6), 128: (2e-4, 4e-6)}[D]
+    # Each score sums 2D fp16x3 products, so the error grows with D.  Measured
+    # max |q - q64| 1.6e-5 (D=80), 2.7e-5 (D=128); LL relative 1.0e-6, 3.4e-6:
+    # the log-likelihood carries a small error common to a row's logits (the
+    # fp32 accumulation of the score), which the posteriors do not see.
+    q_tol, ll_tol = {80: (4e-5, 2e-6), 128: (6e-5, 6e-6)}[D]
     assert np.max(np.abs(q - q64)) < q_tol
     assert abs(ll - ll64) < ll_tol * abs(ll64)
 
@@ -234,7 +237,7 @@ def test_posteriors_cluster_fp32(vl, restatement, KD):
                                        mu.astype(np.float64), cv.astype(np.float64))
     vl.set_precision("fp32")
     q, ll = vl.get_gmm_data_posteriors(x, pr, mu, cv)
-    q_tol, ll_tol = {64: (1e-4, 1e-6), 80: (1e-4, 1e-6), 128: (2e-4, 4e-6)}[D]
+    q_tol, ll_tol = {64: (4e-5, 2e-6), 80: (4e-5, 2e-6), 128: (6e-5, 6e-6)}[D]
     assert np.max(np.abs(q - q64)) < q_tol
     assert abs(ll - ll64) < ll_tol * abs(ll64)
 

@@ -15,14 +15,18 @@
 //           an image's partials in double and forms the Fisher vector
 //           (vl/fisher.c:419-485) or the M-step update (vl/gmm.c:1169-1205).
 //
-// Precision: both operands are split into bf16 hi + lo parts and each product
-// is formed as hi.hi + hi.lo + lo.hi (bf16x3, ~2^-17 relative per product,
-// fp32 accumulation).  The BF16 mode keeps the split on the E-step (the
-// expanded quadratic cancels) and uses a single bf16 pass for the statistics.
+// Precision: both operands are split into fp16 hi + lo parts (22 bits) and
+// each product is formed as hi.hi + hi.lo + lo.hi (fp16x3, ~2^-21 relative per
+// product, fp32 accumulation).  Power-of-two scales keep the operands in
+// fp16's normal range: x' is multiplied by scale_d per dimension, W by one
+// global 2^-g (undone by the epilogue's fused multiply-add), q by 2^14 in the
+// image (undone by the finalizers).  The BF16 mode keeps the split on the
+// E-step (the expanded quadratic cancels) and uses a single fp16 q part for
+// the statistics.
 //
 // Both kernels are persistent and warp-specialised (288 threads):
 //   warps 0-3  producers: load fp32 rows, centre/square, split, and write the
-//              swizzled bf16 operand tiles into a ring of shared-memory stages;
+//              swizzled fp16 operand tiles into a ring of shared-memory stages;
 //   warps 4-7  epilogue: TMEM -> registers -> global;
 //   warp 8     TMEM allocation and, from one lane, tcgen05.mma issue.
 // Operand layouts: E-step A and W are K-major with the 64-byte swizzle (one
@@ -91,33 +95,65 @@ __global__ void k_tc_center(const float *__restrict__ means, int K, int D, float
   if (lane == 0) ctr[d] = (float)(s / (double)K);
 }
 
-// W image (hi then lo), K-major 64-byte-swizzled k-atoms of 32 elements:
+// Entries of the E-step's weight matrix for component k and K-order element
+// e (chunk c = e / 32 holds x''_d for d = 16c .. 16c+15, then x''_d^2 for the
+// same d, so that the producers read each element of x once):
+//   [mu'_kd / s2_kd / scale_d, -1/2 / s2_kd / scale_d^2] log2(e),
+// the producers multiplying x' by the power of two scale_d.
+__device__ __forceinline__ double tc_weight(const float *__restrict__ means, const float *__restrict__ covs,
+                                            const float *__restrict__ ctr, const float *__restrict__ scale, int k,
+                                            int e, int D) {
+  const int c = e / 32, ee = e % 32, d = 16 * c + (ee & 15);
+  const double s2 = (double)covs[(i64)k * D + d], sc = (double)scale[d];
+  const double mup = (double)means[(i64)k * D + d] - (double)ctr[d];
+  return (ee < 16 ? mup / s2 / sc : -0.5 / s2 / (sc * sc)) * 1.4426950408889634;
+}
+
+// max |w| over the model: one element per thread, a warp maximum, then an
+// atomic maximum on the float's bits (non-negative floats order as their bits;
+// *wmax is zeroed before the launch).  The maximum does not depend on order.
+__global__ void k_tc_wmax(const float *__restrict__ means, const float *__restrict__ covs,
+                          const float *__restrict__ ctr, const float *__restrict__ scale, int K, int D,
+                          float *__restrict__ wmax) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  float m = 0.f;
+  if (i < (i64)K * 2 * D)
+    m = (float)fabs(tc_weight(means, covs, ctr, scale, (int)(i / (2 * D)), (int)(i % (2 * D)), D));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax((unsigned *)wmax, __float_as_uint(m));
+}
+
+// W image (hi then lo, fp16), K-major 64-byte-swizzled k-atoms of 32 elements:
 // part p, atom c, row k, element e -> p*wbytes + c*Kp*64 + swizzled(k, e).
+// The entries are divided by 2^g, the power of two that puts max |w| in
+// [2^14, 2^15) (fp16 keeps 11 bits per part there); *wsc = 2^g, which the
+// E-step multiplies back onto every logit.
 __global__ void k_tc_wimg(const float *__restrict__ means, const float *__restrict__ covs,
-                          const float *__restrict__ ctr, int K, int Kp, int D,
-                          __nv_bfloat16 *__restrict__ wimg) {
+                          const float *__restrict__ ctr, const float *__restrict__ scale,
+                          const float *__restrict__ wmax, int K, int Kp, int D, __half *__restrict__ wimg,
+                          float *__restrict__ wsc) {
   const int KD2 = 2 * D;
   i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  int g = 0;
+  const float mx = *wmax;
+  if (mx > 0.f) {
+    frexpf(mx, &g);  // mx = m 2^g, m in [0.5, 1)
+    g -= 15;
+  }
+  if (idx == 0) *wsc = ldexpf(1.f, g);
   if (idx >= (i64)Kp * KD2) return;
   const int k = (int)(idx / KD2), e = (int)(idx % KD2);
-  // K order of the product: chunk c (32 elements) holds x'_d for
-  // d = 16c .. 16c+15, then x'_d^2 for the same d, so that the E-step's
-  // producers read each element of x once.
   const int c = e / 32, ee = e % 32;
-  double w = 0;
-  if (k < K) {
-    const int d = 16 * c + (ee & 15);
-    const double s2 = (double)covs[(i64)k * D + d];
-    const double mup = (double)means[(i64)k * D + d] - (double)ctr[d];
-    w = (ee < 16 ? mup / s2 : -0.5 / s2) * 1.4426950408889634;
-  }
-  __nv_bfloat16 hi, lo;
-  split_bf16((float)w, hi, lo);
+  float w = 0.f;
+  if (k < K) w = (float)ldexp(tc_weight(means, covs, ctr, scale, k, e, D), -g);
+  const __half hi = __float2half_rn(w);
+  const __half lo = __float2half_rn(w - __half2float(hi));
   const size_t wbytes = (size_t)(KD2 / 32) * Kp * 64;
   const size_t off = (size_t)c * Kp * 64 + kmajor_sw64_off(k, ee / 8) + (ee % 8) * 2;
   char *base = (char *)wimg;
-  *(__nv_bfloat16 *)(base + off) = hi;
-  *(__nv_bfloat16 *)(base + wbytes + off) = lo;
+  *(__half *)(base + off) = hi;
+  *(__half *)(base + wbytes + off) = lo;
 }
 
 // cst2_k = log2(e) * (log pi_k - D/2 log 2pi - 1/2 sum log s2 - 1/2 sum mu'^2/s2),
@@ -164,14 +200,21 @@ __global__ void k_tc_scale(const float *__restrict__ means, const float *__restr
 }
 
 // ============================================================ E-step
+__device__ __forceinline__ float clamp_f16(float v) { return fminf(fmaxf(v, -65504.f), 65504.f); }
+
+// The q image holds q * 2^14 in fp16 (one part, or hi and lo parts): every
+// posterior the statistics keep (q >= 1e-6) is then a normal fp16 number.
+// The statistics' finalizers multiply by 2^-14.
+constexpr float kQScale = 16384.f;
+
 // Output layouts of the posteriors written by the E-step.
 //   kQRow    fp32, row-major q[i * ldq + k] (VLFeat's layout; EM and API).
-//   kQImg16  fp16 operand image of q^T for the statistics GEMM: per 8-row
+//   kQImg16  fp16 operand image of q^T (times 2^14) for the statistics GEMM: per 8-row
 //            group g of a 128-row tile, Kq/64 MN-major 128-byte-swizzled
 //            1 KB atoms (64 components x 8 rows), so that a run of 8-row
 //            groups is exactly the MMA's A operand and moves with one bulk
 //            copy per group.
-//   kQImg32  the same image as two bf16 parts (hi, lo) for bf16x3 statistics.
+//   kQImg32  the same image as two fp16 parts (hi, lo) for fp16x3 statistics.
 //   kQRowImg16, kQRowImg32  both: the row-major posteriors (unthresholded)
 //            and the image (thresholded), for EM with the tensor-core M-step.
 constexpr int kQRow = 0, kQImg16 = 1, kQImg32 = 2, kQRowImg16 = 3, kQRowImg32 = 4;
@@ -190,6 +233,8 @@ struct EParams {
   const uint4 *wimg;
   const float *cst2;
   const float *ctr;
+  const float *scl;  // per-dimension power-of-two scale of x' (the operands are x'' = x' scale)
+  const float *wsc;  // the W image's power-of-two scale (one float, device)
   void *q;     // row-major posteriors (kQRow*) or the image (kQImg*)
   void *qimg;  // the image of the combined formats
   int ldq;
@@ -292,7 +337,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       dst[i] = src[(part * wbytesG + (size_t)c * p.Kg * 64 + (size_t)kbase * 64) / 16 + o];
     }
     for (int k = tid; k < 256; k += kTcThreads) s_cst[k] = k < p.Kp ? p.cst2[kbase + k] : -INFINITY;
-    for (int d = tid; d < DIM; d += kTcThreads) s_ctr[d] = p.ctr[d];
     fence_proxy_async_smem();
   }
   __syncthreads();
@@ -350,15 +394,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         bulk_g2s(a_hi + L::kStage + wpart, w + wbytesG, wpart, &full[stage]);
       }
       const int d0 = 16 * c0 + 4 * part;
-      const float m0 = s_ctr[d0], m1 = s_ctr[d0 + 1], m2 = s_ctr[d0 + 2], m3 = s_ctr[d0 + 3];
+      const float4 mm = __ldg((const float4 *)(p.ctr + d0)), sc = __ldg((const float4 *)(p.scl + d0));
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
-        const float v0 = cur[s].x - m0, v1 = cur[s].y - m1, v2 = cur[s].z - m2, v3 = cur[s].w - m3;
+        // x'' = (x - ctr) scale, kept inside fp16's range (an x'' beyond it
+        // is more than 255 model scales from the centre).
+        const float v0 = clamp_f16((cur[s].x - mm.x) * sc.x), v1 = clamp_f16((cur[s].y - mm.y) * sc.y);
+        const float v2 = clamp_f16((cur[s].z - mm.z) * sc.z), v3 = clamp_f16((cur[s].w - mm.w) * sc.w);
         uint32_t h0, l0, h1, l1, h2, l2, h3, l3;
-        split2<false>(v0, v1, h0, l0);
-        split2<false>(v2, v3, h1, l1);
-        split2<false>(v0 * v0, v1 * v1, h2, l2);
-        split2<false>(v2 * v2, v3 * v3, h3, l3);
+        split2<true>(v0, v1, h0, l0);
+        split2<true>(v2, v3, h1, l1);
+        split2<true>(clamp_f16(v0 * v0), clamp_f16(v1 * v1), h2, l2);
+        split2<true>(clamp_f16(v2 * v2), clamp_f16(v3 * v3), h3, l3);
         const uint32_t row = (uint32_t)(32 * warp + 8 * s + rr);
         const uint32_t o1 = kmajor_sw64_off(row, (uint32_t)(part >> 1)) + (part & 1) * 8;
         const uint32_t o2 = kmajor_sw64_off(row, (uint32_t)(2 + (part >> 1))) + (part & 1) * 8;
@@ -391,6 +438,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     // from Kg to Kq.
     const int ncw = q_image(QF) ? nch + (crank == ncta - 1 ? (p.Kq - p.Kg) / 32 : 0) : nch;
     const unsigned long long *cst2v = (const unsigned long long *)s_cst;
+    const float wsc = *p.wsc;
+    const unsigned long long wsc2 = f2u(wsc, wsc);
     uint8_t *stg = s_stage + (warp - 4) * 2048;
     int tt = 0;
     for (i64 tile = tile0; tile < p.ntiles; tile += tstep, ++tt) {
@@ -414,8 +463,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         int cam = 0;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const unsigned long long s = add2(f2u(__uint_as_float(va[2 * j]), __uint_as_float(va[2 * j + 1])),
-                                            cst2v[pc * 16 + j]);
+          const unsigned long long s = fma2(f2u(__uint_as_float(va[2 * j]), __uint_as_float(va[2 * j + 1])),
+                                            wsc2, cst2v[pc * 16 + j]);
           va[2 * j] = __float_as_uint(lo32(s));
           va[2 * j + 1] = __float_as_uint(hi32(s));
           if (FAST) {
@@ -428,8 +477,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         if (two) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
-            const unsigned long long s = add2(f2u(__uint_as_float(vb[2 * j]), __uint_as_float(vb[2 * j + 1])),
-                                              cst2v[pc * 16 + 16 + j]);
+            const unsigned long long s = fma2(f2u(__uint_as_float(vb[2 * j]), __uint_as_float(vb[2 * j + 1])),
+                                              wsc2, cst2v[pc * 16 + 16 + j]);
             vb[2 * j] = __float_as_uint(lo32(s));
             vb[2 * j + 1] = __float_as_uint(hi32(s));
             if (FAST) {
@@ -603,15 +652,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             if (!q_image32(QF)) {
-              wh[j].x = pack2<true>(qv[8 * j + 0], qv[8 * j + 1]);
-              wh[j].y = pack2<true>(qv[8 * j + 2], qv[8 * j + 3]);
-              wh[j].z = pack2<true>(qv[8 * j + 4], qv[8 * j + 5]);
-              wh[j].w = pack2<true>(qv[8 * j + 6], qv[8 * j + 7]);
+              wh[j].x = pack2<true>(qv[8 * j + 0] * kQScale, qv[8 * j + 1] * kQScale);
+              wh[j].y = pack2<true>(qv[8 * j + 2] * kQScale, qv[8 * j + 3] * kQScale);
+              wh[j].z = pack2<true>(qv[8 * j + 4] * kQScale, qv[8 * j + 5] * kQScale);
+              wh[j].w = pack2<true>(qv[8 * j + 6] * kQScale, qv[8 * j + 7] * kQScale);
             } else {
-              split2<false>(qv[8 * j + 0], qv[8 * j + 1], wh[j].x, wl[j].x);
-              split2<false>(qv[8 * j + 2], qv[8 * j + 3], wh[j].y, wl[j].y);
-              split2<false>(qv[8 * j + 4], qv[8 * j + 5], wh[j].z, wl[j].z);
-              split2<false>(qv[8 * j + 6], qv[8 * j + 7], wh[j].w, wl[j].w);
+              split2<true>(qv[8 * j + 0] * kQScale, qv[8 * j + 1] * kQScale, wh[j].x, wl[j].x);
+              split2<true>(qv[8 * j + 2] * kQScale, qv[8 * j + 3] * kQScale, wh[j].y, wl[j].y);
+              split2<true>(qv[8 * j + 4] * kQScale, qv[8 * j + 5] * kQScale, wh[j].z, wl[j].z);
+              split2<true>(qv[8 * j + 6] * kQScale, qv[8 * j + 7] * kQScale, wh[j].w, wl[j].w);
             }
           }
           stage_out(wh, cc, 0);
@@ -633,7 +682,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     }
   } else if (warp == 12 && lane == 0) {
     // ---------------------------------------------------------- MMA
-    const uint32_t idesc = idesc_bf16(128, p.Kp, false, false);
+    const uint32_t idesc = idesc_f16(128, p.Kp, false, false);
     const uint32_t w_hi = smem_u32(sW), w_lo = w_hi + wbytes;
     int it = 0, tt = 0;
     bool ok = true;
@@ -700,8 +749,9 @@ struct SParams {
   int *err;
 };
 
-// SPLIT 2: bf16x3 -- q and x both split hi/lo, products hi.hi + hi.lo + lo.hi.
-// SPLIT 1: fp16 operands -- q single fp16, x'' = x' * scale split hi/lo.
+// Operands are fp16: q 2^14 from the E-step's image and x'' = x' * scale.
+// SPLIT 2: both split hi/lo, products hi.hi + hi.lo + lo.hi (fp16x3).
+// SPLIT 1: q single fp16, x'' split hi/lo.
 template <int DIM, int MT, int SPLIT>
 struct SLayout {
   static constexpr int NST = 2 * DIM + 16;            // x', x'^2, [1, 0 x 15]
@@ -731,7 +781,7 @@ template <int DIM, int MT, int SPLIT>
 __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) {
   using L = SLayout<DIM, MT, SPLIT>;
   constexpr int NST = L::NST, NB = L::NB, NPA = L::NPA;
-  constexpr bool F16 = (SPLIT == 1);
+  constexpr bool F16 = true;  // fp16 operands: the q image and x'' = x' scale
   constexpr int NF4 = DIM / 4;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *base = align1024(smem_raw);
@@ -842,16 +892,16 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) 
           const int kr = rs & 7, kg = rs >> 3;
           uint32_t h0, l0, h1, l1;
           {
-            split2<F16>(v0, v1, h0, l0);
-            split2<F16>(v2, v3, h1, l1);
+            split2<F16>(clamp_f16(v0), clamp_f16(v1), h0, l0);
+            split2<F16>(clamp_f16(v2), clamp_f16(v3), h1, l1);
             const int f = d0;
             const uint32_t off = kg * (NB * 1024) + (f >> 6) * 1024 + mnmajor_sw128_off(kr, (f & 63) >> 3) + ((f >> 2) & 1) * 8;
             st_shared_v2(sb + off, h0, h1);
             st_shared_v2(sb + L::B_PART + off, l0, l1);
           }
           {
-            split2<F16>(v0 * v0, v1 * v1, h0, l0);
-            split2<F16>(v2 * v2, v3 * v3, h1, l1);
+            split2<F16>(clamp_f16(v0 * v0), clamp_f16(v1 * v1), h0, l0);
+            split2<F16>(clamp_f16(v2 * v2), clamp_f16(v3 * v3), h1, l1);
             const int f = DIM + d0;
             const uint32_t off = kg * (NB * 1024) + (f >> 6) * 1024 + mnmajor_sw128_off(kr, (f & 63) >> 3) + ((f >> 2) & 1) * 8;
             st_shared_v2(sb + off, h0, h1);
@@ -1020,6 +1070,7 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
   const double in = n > 0 ? 1.0 / (double)n : 0.0;
   const size_t slotStride = (size_t)Kp * NST;
   for (int d = tid; d < DIM; d += kFinThreads) s_is[d] = scale ? 1.0 / (double)scale[d] : 1.0;
+  const double iq = 1.0 / (double)kQScale;
   __syncthreads();
   double sq = 0;
   for (int el = tid; el < E; el += kFinThreads) {
@@ -1031,10 +1082,11 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
       S1 += (double)pp[d];
       S2 += (double)pp[DIM + d];
     }
-    // Statistics were taken on x'' = x' * scale (s_is = 1 without scaling).
+    // Statistics were taken on q 2^14 and x'' = x' * scale.
     const double is = s_is[d];
-    S1 *= is;
-    S2 *= is * is;
+    S0 *= iq;
+    S1 *= is * iq;
+    S2 *= is * is * iq;
     const double mup = cmu[e];
     const double u = cisd[e] * (S1 - mup * S0) * (cup[k] * in);
     const double v = ((S2 - 2.0 * mup * S1 + mup * mup * S0) * cis2[e] - S0) * (cvp[k] * in);
@@ -1124,9 +1176,10 @@ __global__ void k_tc_mstep_finalize(int nitems, int K, int Kp, int D, const floa
     S1 += (double)pp[d];
     S2 += (double)pp[D + d];
   }
-  const double is = scale ? 1.0 / (double)scale[d] : 1.0;
-  S1 *= is;
-  S2 *= is * is;
+  const double is = scale ? 1.0 / (double)scale[d] : 1.0, iq = 1.0 / (double)kQScale;
+  S0 *= iq;
+  S1 *= is * iq;
+  S2 *= is * is * iq;
   const double c = (double)ctr[d], oldmu = (double)means[idx], a = oldmu - c;
   const double mass = S0;
   double mu = S1 + c * S0, v = S2 - 2.0 * a * S1 + a * a * S0;
@@ -1143,7 +1196,7 @@ __global__ void k_tc_mstep_finalize(int nitems, int K, int Kp, int D, const floa
   if (d == 0) priors[k] = (float)mass;
 }
 
-// Row-major fp32 posteriors -> fp16 q^T operand image (the layout the
+// Row-major fp32 posteriors -> fp16 q^T operand image, times 2^14 (the layout the
 // E-step writes), with VLFeat's q < 1e-6 skip, the optional FAST one-hot of
 // the row's arg-max (vl/fisher.c:398-417) and per-row term counts.  One warp
 // per row; rows past n (tile padding) are written as zeros.
@@ -1183,10 +1236,10 @@ __global__ void k_rows_to_image16(const float *__restrict__ q, i64 n, int K, int
       v[t] = x < thr ? 0.f : x;
     }
     uint4 w;
-    w.x = pack2<true>(v[0], v[1]);
-    w.y = pack2<true>(v[2], v[3]);
-    w.z = pack2<true>(v[4], v[5]);
-    w.w = pack2<true>(v[6], v[7]);
+    w.x = pack2<true>(v[0] * kQScale, v[1] * kQScale);
+    w.y = pack2<true>(v[2] * kQScale, v[3] * kQScale);
+    w.z = pack2<true>(v[4] * kQScale, v[5] * kQScale);
+    w.w = pack2<true>(v[6] * kQScale, v[7] * kQScale);
     const int kk = g * 8;
     const uint32_t off = (uint32_t)((r >> 3) * (Kq / 64) * 1024 + (kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
     *(uint4 *)(tb + off) = w;
@@ -1198,8 +1251,8 @@ __global__ void k_rows_to_image16(const float *__restrict__ q, i64 n, int K, int
 // ================================================================ host
 struct TcPrep {
   int K = 0, Kp = 0, D = 0;
-  float *ctr = nullptr, *cst2 = nullptr, *scale = nullptr;
-  __nv_bfloat16 *wimg = nullptr;
+  float *ctr = nullptr, *cst2 = nullptr, *scale = nullptr, *wsc = nullptr;
+  __half *wimg = nullptr;
 };
 
 // Components of the tensor-core path, padded: a multiple of 32 up to 256; above
@@ -1214,27 +1267,34 @@ int padK(i64 K) {
 }
 int kblocks(int Kp) { return (Kp + 255) / 256; }
 
+// Model-derived operands of the tensor-core path: the centre, the
+// per-dimension scales, the fp16 W image with its scale, and the constants.
 void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &sc, cudaStream_t s) {
+  (void)want_scale;  // the E-step's operands are always scaled
   tp.K = (int)m.K;
   tp.Kp = padK(m.K);
   tp.D = (int)m.D;
   const int KD2 = 2 * tp.D;
   tp.ctr = sc.slot[0].get<float>(256);
   tp.cst2 = sc.slot[1].get<float>(std::max(256, tp.Kp));
-  tp.wimg = sc.slot[2].get<__nv_bfloat16>((size_t)2 * tp.Kp * KD2);
+  tp.wimg = sc.slot[2].get<__half>((size_t)2 * tp.Kp * KD2);
+  tp.scale = sc.slot[12].get<float>(256);
+  float *wm = sc.slot[19].get<float>(2);
+  tp.wsc = wm + 1;
   VLB_LAUNCH("tc_center", s, k_tc_center<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, tp.K, tp.D, tp.ctr));
+  VLB_LAUNCH("tc_scale", s,
+             k_tc_scale<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.D, tp.scale));
+  VLB_CUDA(cudaMemsetAsync(wm, 0, sizeof(float), s));
+  const i64 nw = (i64)tp.K * KD2;
+  VLB_LAUNCH("tc_wmax", s,
+             k_tc_wmax<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.scale, tp.K, tp.D, wm));
   const i64 n = (i64)tp.Kp * KD2;
   VLB_LAUNCH("tc_wimage", s,
-             k_tc_wimg<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.Kp,
-                                                                  tp.D, tp.wimg));
+             k_tc_wimg<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.scale, wm, tp.K,
+                                                                  tp.Kp, tp.D, tp.wimg, tp.wsc));
   VLB_LAUNCH("tc_constants", s,
              k_tc_cst<<<(tp.Kp + 7) / 8, 256, 0, s>>>(m.priors, m.means, m.covs, tp.ctr, tp.K,
                                                           tp.Kp, tp.D, tp.cst2));
-  if (want_scale) {
-    tp.scale = sc.slot[12].get<float>(256);
-    VLB_LAUNCH("tc_scale", s,
-               k_tc_scale<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.D, tp.scale));
-  }
 }
 
 int padQ(int Kp) { return (Kp + 127) / 128 * 128; }
@@ -1274,13 +1334,13 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   EParams p;
   p.X = X; p.N = N; p.K = tp.K; p.Kp = Kb; p.Kg = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
   p.qpart = ntiles * 128 * (i64)p.Kq * 2;
-  p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr;
+  p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr; p.scl = tp.scale; p.wsc = tp.wsc;
   p.q = q; p.qimg = eo.qimg; p.ldq = ldq; p.fast = fast ? 1 : 0; p.qthr = float_at_least(eo.qthr);
   p.rowcnt = rowcnt; p.ll_part = ll_part;
   p.err = err; p.ntiles = ntiles;
   if constexpr (!CL) {
     const int grid = (int)std::min<i64>(ntiles, num_sms());
-    VLB_LAUNCH("tc_estep_bf16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
+    VLB_LAUNCH("tc_estep_f16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
   } else {
     // One cluster of nb CTAs per tile, as many clusters as fit at once
     // (persistent: each cluster strides over the tiles).
@@ -1301,7 +1361,7 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
     VLB_CUDA(cudaOccupancyMaxActiveClusters(&maxc, kern, &cfg));
     VLB_CHECK(maxc >= 1, VL_ERR_BAD_ARG, "tensor-core E-step: the CTA cluster does not fit on the device");
     cfg.gridDim = dim3((unsigned)(nb * std::min<i64>(ntiles, maxc)));
-    VLB_LAUNCH("tc_estep_bf16x3", s, VLB_CUDA(cudaLaunchKernelEx(&cfg, kern, p)));
+    VLB_LAUNCH("tc_estep_f16x3", s, VLB_CUDA(cudaLaunchKernelEx(&cfg, kern, p)));
   }
   return ntiles * 4;  // LL partials written
 }
@@ -1337,7 +1397,7 @@ void launch_stats(const SParams &p0, int grid_x, int grid_y, int nst_req, cudaSt
   const size_t smem = L::bytes(p.nst);
   auto kern = k_tc_stats<DIM, MT, SPLIT>;
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  VLB_LAUNCH(SPLIT == 2 ? "tc_stats_bf16x3" : "tc_stats_f16x2", s,
+  VLB_LAUNCH(SPLIT == 2 ? "tc_stats_f16x3" : "tc_stats_f16x2", s,
              kern<<<dim3(grid_x, grid_y), kStatsThreads, smem, s>>>(p));
 }
 
@@ -1354,7 +1414,7 @@ struct Tc {
       default: return launch_estep<DIM, kQRow>(X, N, tp, q, ldq, fast, rowcnt, ll, err, nst, s, eo);
     }
   }
-  // split 2: bf16x3 statistics (q image in two bf16 parts); split 1: fp16.
+  // split 2: fp16x3 statistics (q image in two fp16 parts); split 1: one q part.
   // mt: 128-component M tiles per CTA (0: two when they fit in TMEM).
   static void stats(int split, const SParams &p, int grid_x, int mt, int nst, cudaStream_t s) {
     const int mtiles = p.Kq / 128;
@@ -1508,14 +1568,14 @@ void tc_mstep(const float *X, i64 N, float *means, float *covs, float *priors, i
     SParams sp;
     sp.X = X; sp.qimg = (const uint8_t *)sc.slot[4].p; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = 0;
     sp.K = (int)K; sp.Kp = Kp; sp.Kq = Kq; sp.nst = 0;
-    sp.ctr = (const float *)sc.slot[0].p; sp.scale = fp32 ? nullptr : (const float *)sc.slot[12].p;
+    sp.ctr = (const float *)sc.slot[0].p; sp.scale = (const float *)sc.slot[12].p;
     sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg; sp.partial = partial; sp.err = err;
     stats_dispatch((int)D, fp32 ? 2 : 1, sp, gx, 0, 0, s);
   }
   VLB_LAUNCH("tc_mstep_finalize", s,
              k_tc_mstep_finalize<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
                  nitems, (int)K, Kp, (int)D, partial, (const float *)sc.slot[0].p,
-                 fp32 ? nullptr : (const float *)sc.slot[12].p, lb, means, covs, priors));
+                 (const float *)sc.slot[12].p, lb, means, covs, priors));
   normalize_priors<float>(priors, K, s);
   check_err(err, s);
 }
@@ -1654,7 +1714,7 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
       SParams sp;
       sp.X = X; sp.qimg = (const uint8_t *)q; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = c.row0;
       sp.K = (int)K; sp.Kp = tp.Kp; sp.Kq = Kq; sp.nst = 0;
-      sp.ctr = tp.ctr; sp.scale = fp32 ? nullptr : tp.scale;
+      sp.ctr = tp.ctr; sp.scale = tp.scale;
       sp.items = ditems + c.items; sp.order = dorder + c.items; sp.cta_beg = dbeg + c.beg;
       sp.partial = partial; sp.err = err;
       stats_dispatch(tp.D, split, sp, c.gx, cfg.statsMT, cfg.statsStages, s);
@@ -1662,7 +1722,7 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
     VLB_LAUNCH("tc_fv_finalize", s,
                fin<<<(unsigned)(c.nimg * kFinCluster), kFinThreads, finSmem, s>>>(
                    (int)K, tp.Kp, partial, dslot0 + c.img, drow0 + c.img, cmu, cis2, cisd, cup, cvp,
-                   fp32 ? nullptr : tp.scale, c.nrows > 0 ? rowcnt : nullptr, c.row0, flags, c.img0, enc,
+                   tp.scale, c.nrows > 0 ? rowcnt : nullptr, c.row0, flags, c.img0, enc,
                    nterms));
     if (after) after(ci);
   }
