@@ -558,8 +558,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       const i64 row = tile * 128 + r;
       const bool valid = row < p.N;
       unsigned long long cnt2 = 0ull;  // (+0.0f, +0.0f): per-row term counts, exact below 2^24
-      // -prev(qthr) * 2^64, prev(qthr) the largest float below qthr (> 0).
-      const float nthr = -__uint_as_float(__float_as_uint(p.qthr) - 1u) * 0x1p64f;
+      // The image-only formats form q 2^14 directly (the scale folded into the
+      // row's normaliser) and test it against qthr 2^14: power-of-two scaling
+      // keeps every comparison, and the flags, exact.
+      constexpr bool kImgOnly = (QF == kQImg16 || QF == kQImg32);
+      constexpr float kQs = kImgOnly ? kQScale : 1.f;   // scale of qv below
+      constexpr float kPack = kImgOnly ? 1.f : kQScale;  // still to apply when packing the image
+      // -prev(qthr) * 2^64 (times the scale), prev(qthr) the largest float below qthr (> 0).
+      const float nthr = -__uint_as_float(__float_as_uint(p.qthr) - 1u) * (0x1p64f * kQs);
       // q image of this tile; this warp's rows are its 8-row groups 4 ew .. 4 ew + 3.
       uint8_t *ib = (uint8_t *)(q_rows(QF) ? p.qimg : p.q) + (size_t)tile * 128 * p.Kq * 2;
       // Image stores go through this warp's staging (32 rows x 64 B, 16-byte
@@ -594,14 +600,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
           uint32_t va[32];
           tmem_ld32(tb + cc * 32, va);
           tmem_wait_ld();
-          const float sc = live ? ex2_approx(mg[cc >> 1] - mt) * inv : 0.f;
+          const float sc = live ? ex2_approx(mg[cc >> 1] - mt) * (inv * kQs) : 0.f;
           const unsigned long long sc2 = f2u(sc, sc);
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             float x0, x1;
             if (FAST) {
-              x0 = (live && cc * 32 + 2 * j == am) ? 1.f : 0.f;  // am: this CTA's columns
-              x1 = (live && cc * 32 + 2 * j + 1 == am) ? 1.f : 0.f;
+              x0 = (live && cc * 32 + 2 * j == am) ? kQs : 0.f;  // am: this CTA's columns
+              x1 = (live && cc * 32 + 2 * j + 1 == am) ? kQs : 0.f;
             } else {
               const unsigned long long q2 = mul2(f2u(__uint_as_float(va[2 * j]), __uint_as_float(va[2 * j + 1])), sc2);
               x0 = lo32(q2);
@@ -652,15 +658,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             if (!q_image32(QF)) {
-              wh[j].x = pack2<true>(qv[8 * j + 0] * kQScale, qv[8 * j + 1] * kQScale);
-              wh[j].y = pack2<true>(qv[8 * j + 2] * kQScale, qv[8 * j + 3] * kQScale);
-              wh[j].z = pack2<true>(qv[8 * j + 4] * kQScale, qv[8 * j + 5] * kQScale);
-              wh[j].w = pack2<true>(qv[8 * j + 6] * kQScale, qv[8 * j + 7] * kQScale);
+              wh[j].x = pack2<true>(qv[8 * j + 0] * kPack, qv[8 * j + 1] * kPack);
+              wh[j].y = pack2<true>(qv[8 * j + 2] * kPack, qv[8 * j + 3] * kPack);
+              wh[j].z = pack2<true>(qv[8 * j + 4] * kPack, qv[8 * j + 5] * kPack);
+              wh[j].w = pack2<true>(qv[8 * j + 6] * kPack, qv[8 * j + 7] * kPack);
             } else {
-              split2<true>(qv[8 * j + 0] * kQScale, qv[8 * j + 1] * kQScale, wh[j].x, wl[j].x);
-              split2<true>(qv[8 * j + 2] * kQScale, qv[8 * j + 3] * kQScale, wh[j].y, wl[j].y);
-              split2<true>(qv[8 * j + 4] * kQScale, qv[8 * j + 5] * kQScale, wh[j].z, wl[j].z);
-              split2<true>(qv[8 * j + 6] * kQScale, qv[8 * j + 7] * kQScale, wh[j].w, wl[j].w);
+              split2<true>(qv[8 * j + 0] * kPack, qv[8 * j + 1] * kPack, wh[j].x, wl[j].x);
+              split2<true>(qv[8 * j + 2] * kPack, qv[8 * j + 3] * kPack, wh[j].y, wl[j].y);
+              split2<true>(qv[8 * j + 4] * kPack, qv[8 * j + 5] * kPack, wh[j].z, wl[j].z);
+              split2<true>(qv[8 * j + 6] * kPack, qv[8 * j + 7] * kPack, wh[j].w, wl[j].w);
             }
           }
           stage_out(wh, cc, 0);
