@@ -40,7 +40,8 @@ VLAD_NORMALIZE_COMPONENTS = 1 << 0  # vl/vlad.h:23-26
 VLAD_SQUARE_ROOT = 1 << 1
 VLAD_UNNORMALIZED = 1 << 2
 VLAD_NORMALIZE_MASS = 1 << 3
-VL_GMM_RAND = 1    # VlGMMRand, vl/gmm.h:21-26
+VL_GMM_KMEANS = 0  # VlGMMKMeans, vl/gmm.h:21-26
+VL_GMM_RAND = 1    # VlGMMRand
 VL_GMM_CUSTOM = 2  # VlGMMCustom
 
 _vp = C.c_void_p
@@ -167,6 +168,8 @@ class Reference:
         L.vl_gmm_get_posteriors.argtypes = [_vp]
         L.vl_gmm_get_posteriors.restype = _vp
         L.vl_gmm_set_initialization.argtypes = [_vp, C.c_int]
+        L.vl_gmm_init_with_kmeans.restype = None
+        L.vl_gmm_init_with_kmeans.argtypes = [_vp, _vp, _sz, _vp]
         L.vl_gmm_set_max_num_iterations.argtypes = [_vp, _sz]
         L.vl_gmm_set_num_repetitions.argtypes = [_vp, _sz]
         L.vl_gmm_set_verbosity.argtypes = [_vp, C.c_int]
@@ -254,8 +257,9 @@ class Reference:
         """vl_rand_seed on the calling thread's generator (vl/random.c:109-127)."""
         self.lib.vl_rand_seed(self.lib.vl_get_rand(), int(s))
 
-    def rand_init(self, data, K, seed, max_iter=0, lb=1e-4):
-        """vl_gmm_cluster with VlGMMRand initialisation (vl/gmm.c:1416-1443)
+    def rand_init(self, data, K, seed, max_iter=0, lb=1e-4, init=VL_GMM_RAND):
+        """vl_gmm_cluster with VlGMMRand (vl/gmm.c:1416-1443) or, with
+        init=VL_GMM_KMEANS, VlGMMKMeans initialisation (vl/gmm.c:1315-1370)
         after seeding the thread's generator; max_iter=0 leaves the initial
         parameters (one E-step, no M-step)."""
         L = self.lib
@@ -263,7 +267,7 @@ class Reference:
         N, D = data.shape
         g = L.vl_gmm_new(VL_TYPE_FLOAT if dt == np.float32 else VL_TYPE_DOUBLE, D, K)
         try:
-            L.vl_gmm_set_initialization(g, VL_GMM_RAND)
+            L.vl_gmm_set_initialization(g, int(init))
             L.vl_gmm_set_max_num_iterations(g, int(max_iter))
             L.vl_gmm_set_covariance_lower_bound(g, float(lb))
             self.seed(seed)
@@ -277,6 +281,35 @@ class Reference:
             return dict(ll=ll, priors=grab(L.vl_gmm_get_priors(g), K),
                         means=grab(L.vl_gmm_get_means(g), K * D).reshape(K, D),
                         covs=grab(L.vl_gmm_get_covariances(g), K * D).reshape(K, D))
+        finally:
+            L.vl_gmm_delete(g)
+
+    def kmeans_init(self, data, K, seed, lb=1e-4):
+        """vl_gmm_init_with_kmeans (vl/gmm.c:1315-1370) after seeding the
+        thread's generator: the GMM parameters of the one-hot M-step, the
+        k-means assignment of every row (the one-hot posteriors) and the
+        generator's next draw (which shows how many draws the initialisation
+        took)."""
+        L = self.lib
+        dt = data.dtype
+        N, D = data.shape
+        g = L.vl_gmm_new(VL_TYPE_FLOAT if dt == np.float32 else VL_TYPE_DOUBLE, D, K)
+        try:
+            L.vl_gmm_set_covariance_lower_bound(g, float(lb))
+            self.seed(seed)
+            dat = np.ascontiguousarray(data)
+            L.vl_gmm_init_with_kmeans(g, _ptr(dat), N, None)
+            nxt = int(L.vl_rand_uint32(L.vl_get_rand()))
+            ct = C.c_float if dt == np.float32 else C.c_double
+
+            def grab(p, n):
+                return np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape=(n,)).copy()
+
+            post = grab(L.vl_gmm_get_posteriors(g), N * K).reshape(N, K)
+            return dict(priors=grab(L.vl_gmm_get_priors(g), K),
+                        means=grab(L.vl_gmm_get_means(g), K * D).reshape(K, D),
+                        covs=grab(L.vl_gmm_get_covariances(g), K * D).reshape(K, D),
+                        assign=np.argmax(post, axis=1).astype(np.int64), next_draw=nxt)
         finally:
             L.vl_gmm_delete(g)
 
@@ -570,3 +603,248 @@ def rand_init(data, K, rng, lanes):
                 break
             x += 1
     return dict(priors=priors, means=centers, covs=covs)
+
+
+# ----------------------------------------------------- KMeans initialisation
+def _l2_rows(q, C, lanes, T):
+    """_l2_ordered of q against every row of C, vectorised over the rows (each
+    NumPy operation rounds to T, so every element follows the scalar order)."""
+    K, D = C.shape
+    q = np.asarray(q, T)
+    v = [np.zeros(K, T) for _ in range(lanes)]
+    i = 0
+    while i + lanes <= D:
+        for l in range(lanes):
+            d = (q[i + l] - C[:, i + l]).astype(T)
+            v[l] = (v[l] + (d * d).astype(T)).astype(T)
+        i += lanes
+    if lanes == 8:
+        acc = ((v[0] + v[1]) + (v[4] + v[5])) + ((v[2] + v[3]) + (v[6] + v[7]))
+    elif lanes == 4:
+        acc = (v[0] + v[2]) + (v[1] + v[3])
+    elif lanes == 2:
+        acc = v[0] + v[1]
+    else:
+        acc = v[0]
+    acc = acc.astype(T)
+    while i < D:
+        d = (q[i] - C[:, i]).astype(T)
+        acc = (acc + (d * d).astype(T)).astype(T)
+        i += 1
+    return acc
+
+
+def _kd_tree(C, rng):
+    """One kd-tree of a one-tree forest over the rows of C with median
+    thresholds (vl/kdtree.c:165-325, 491-576; vl/kmeans.c:723-726).  Nodes are
+    [lowerChild, upperChild, splitDimension, threshold, lowerBound,
+    upperBound]; entries [index, value].  Draws from rng as the reference."""
+    K, D = C.shape
+    nodes, ent = [], [[k, 0.0] for k in range(K)]
+
+    def new():
+        nodes.append([0, 0, 0, 0.0, 0.0, 0.0])
+        return len(nodes) - 1
+
+    def build(n, b, e):
+        if e - b <= 1:
+            nodes[n][0], nodes[n][1] = -b - 1, -e - 1
+            return
+        have, bd, bv = False, 0, 0.0
+        for d in range(D):
+            full = e - b <= 1024
+            ns = e - b if full else 1024
+            mean = sec = 0.0
+            for i in range(ns):
+                si = i if full else rng.uint32() % 1024
+                datum = float(C[ent[b + si][0], d])
+                mean += datum
+                sec += datum * datum
+            mean /= ns
+            sec /= ns
+            var = sec - mean * mean
+            if var <= 0:
+                continue
+            if not have or bv < var:
+                have, bd, bv = True, d, var
+        if not have:
+            nodes[n][0], nodes[n][1] = -b - 1, -e - 1
+            return
+        rng.uint32()  # the dice over the kept dimensions (one tree: one)
+        nodes[n][2] = bd
+        for i in range(b, e):
+            ent[i][1] = float(C[ent[i][0], bd])
+        ent[b:e] = sorted(ent[b:e], key=lambda t: t[1])
+        med = (b + e - 1) // 2
+        nodes[n][3] = ent[med][1]
+        lc = new()
+        nodes[n][0] = lc
+        build(lc, b, med + 1)
+        uc = new()
+        nodes[n][1] = uc
+        build(uc, med + 1, e)
+
+    build(new(), 0, K)
+    sb = [-np.inf, np.inf] * D
+
+    def bounds(n):
+        i, t = nodes[n][2], nodes[n][3]
+        nodes[n][4], nodes[n][5] = sb[2 * i], sb[2 * i + 1]
+        if nodes[n][0] > 0:
+            sb[2 * i + 1] = t
+            bounds(nodes[n][0])
+            sb[2 * i + 1] = nodes[n][5]
+        if nodes[n][1] > 0:
+            sb[2 * i] = t
+            bounds(nodes[n][1])
+            sb[2 * i] = nodes[n][4]
+
+    bounds(0)
+    return nodes, [e[0] for e in ent]
+
+
+def _kd_query(q, dists, nodes, ent, max_comp):
+    """Best-bin-first search for one neighbour (vl/kdtree.c:583-725,
+    774-840) with the binary heap of vl/heap-def.h; dists[k] is the distance
+    of the query to centre k.  Returns (distance, index)."""
+    exact = max_comp == 0
+    heap = [(0.0, 0)]
+    comps, have, best, bi = 0, False, 0.0, 0
+    while exact or comps < max_comp:
+        if not heap:
+            break
+        n = len(heap) - 1
+        heap[0], heap[n] = heap[n], heap[0]
+        top = heap.pop()
+        i = 0
+        while True:  # vl/heap-def.h up()
+            l, r = 2 * i + 1, 2 * i + 2
+            if l >= len(heap):
+                break
+            if r >= len(heap):
+                if heap[i][0] > heap[l][0]:
+                    heap[i], heap[l] = heap[l], heap[i]
+                break
+            c = l if heap[l][0] < heap[r][0] else r
+            if heap[i][0] > heap[c][0]:
+                heap[i], heap[c] = heap[c], heap[i]
+                i = c
+            else:
+                break
+        lb, node = top
+        if have and best < lb:
+            break
+        dist = lb
+        while True:
+            lo, up, dim, x2, x1, x3 = nodes[node]
+            if lo < 0:
+                for it in range(-lo - 1, -up - 1):
+                    if not (exact or comps < max_comp):
+                        break
+                    di = ent[it]
+                    dd = float(dists[di])
+                    comps += 1
+                    if not have:
+                        have, best, bi = True, dd, di
+                    elif best > dd:
+                        best, bi = dd, di
+                break
+            x = float(q[dim])
+            delta = x - x2
+            save = dist + delta * delta
+            if x <= x2:
+                nxt, sv = lo, up
+                if x <= x1:
+                    delta = x - x1
+                    save -= delta * delta
+            else:
+                nxt, sv = up, lo
+                if x > x3:
+                    delta = x - x3
+                    save -= delta * delta
+            if not have or best > save:
+                heap.append((save, sv))
+                j = len(heap) - 1
+                while j > 0:  # vl/heap-def.h down()
+                    p = (j - 1) // 2
+                    if heap[j][0] < heap[p][0]:
+                        heap[j], heap[p] = heap[p], heap[j]
+                        j = p
+                    else:
+                        break
+            node = nxt
+    return best, bi
+
+
+def kmeans_init(data, K, rng, lanes):
+    """The k-means of VlGMMKMeans restated (vl/gmm.c:1336-1364 with
+    vl/kmeans.c:528-582, 708-771, 1003-1150, 656-702) for small cases:
+    random-selection seeding, ANN refinement (one tree, max(N/4, 10)
+    comparisons, 5 iterations), exact quantisation.  Returns the centres, the
+    assignment of every row and the energy."""
+    T = data.dtype.type
+    N, D = data.shape
+    perm = list(range(N))
+    n = N
+    while n > 1:  # vl/shuffle-def.h:82-91
+        k = rng.uindex(n)
+        n -= 1
+        perm[n], perm[k] = perm[k], perm[n]
+    C = np.zeros((K, D), data.dtype)
+    k = i = 0
+    while k < K:
+        if K - k < N - i and k > 0:
+            d = np.array([_l2_rows(data[perm[i]], C[j:j + 1], lanes, T)[0] for j in range(k)])
+            if np.any(d == 0):
+                i += 1
+                continue
+        C[k] = data[perm[i]]
+        k += 1
+        i += 1
+    max_comp = max(N // 4, 10)
+    assign = np.zeros(N, np.int64)
+    dist = np.zeros(N, data.dtype)
+    energy = prev = initial = np.inf
+    it = 0
+    while True:
+        nodes, ent = _kd_tree(C, rng)
+        for x in range(N):
+            dd = _l2_rows(data[x], C, lanes, T)
+            nd, ni = _kd_query(data[x], dd, nodes, ent, max_comp)
+            if it == 0:
+                dist[x], assign[x] = T(nd), ni
+            else:
+                pd = dd[assign[x]]
+                if pd > T(nd):
+                    dist[x], assign[x] = T(nd), ni
+                else:
+                    dist[x] = pd
+        energy = 0.0
+        for x in range(N):
+            energy += float(dist[x])
+        if it >= 5 or energy == prev:
+            break
+        if it == 0:
+            initial = energy
+        elif (prev - energy) / (initial - energy) < 1e-4:
+            break
+        prev = energy
+        mass = np.bincount(assign, minlength=K)
+        acc = np.zeros((K, D), data.dtype)
+        for x in range(N):
+            acc[assign[x]] = (acc[assign[x]] + data[x]).astype(T)
+        for c in range(K):
+            if mass[c] > 0:
+                C[c] = (acc[c] / T(mass[c])).astype(T)
+            else:
+                C[c] = data[rng.uindex(N)]
+        it += 1
+    final = np.zeros(N, np.int64)
+    for x in range(N):
+        dd = _l2_rows(data[x], C, lanes, T)
+        best, bi = T(np.inf), 0
+        for c in range(K):
+            if dd[c] < best:
+                best, bi = dd[c], c
+        final[x] = bi
+    return dict(centers=C, assign=final, energy=energy)

@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle.oracle import (FLAG_FAST, FLAG_IMPROVED, FLAG_NORMALIZED,  # noqa: E402
-                           FLAG_SQUARE_ROOT, Reference)
+                           FLAG_SQUARE_ROOT, Reference, VL_GMM_KMEANS)
 from vlfeat_b200 import workloads as W  # noqa: E402
 
 FLAG_SETS = [0, FLAG_SQUARE_ROOT, FLAG_NORMALIZED, FLAG_IMPROVED, FLAG_IMPROVED | FLAG_FAST, FLAG_FAST]
@@ -177,6 +177,56 @@ def vlad_case(ref, out):
                 out[f"vlad_{name}_enc_{tag}_{fl}"] = ref.vlad(cx.astype(dt), cm.astype(dt), ca.astype(dt), fl)
 
 
+def kmeans_data(name):
+    """Inputs of the KMeans-initialisation cases (regenerated by the tests from
+    the same seeds): uniform rows, an integer grid (many equal distances and
+    split values), 25 distinct rows repeated (duplicate seeds, constant
+    leaves), too few rows for a full search (N/4 < K: the comparison budget
+    cuts the search), a mixture, more than 1024 centres (the kd-tree samples
+    variances with random draws), and SIFT-sized rows."""
+    if name == "small":
+        return rng(61).random((400, 5)), 8, 611
+    if name == "grid":
+        return rng(62).integers(0, 4, (500, 3)).astype(np.float64), 16, 621
+    if name == "dup":
+        base = rng(63).random((25, 5))
+        return base[rng(631).integers(0, 25, 200)], 30, 632
+    if name == "trunc":
+        return rng(64).random((60, 4)), 20, 641
+    if name == "mix":
+        return W.mixture_data(20000, 16, 64, seed=65, dtype=np.float64), 64, 651
+    if name == "wide":
+        return W.mixture_data(6000, 6, 300, seed=66, dtype=np.float64), 1100, 661
+    if name == "sift":
+        return W.mixture_data(50000, 80, 256, seed=67, dtype=np.float64), 256, 671
+    raise KeyError(name)
+
+
+KMEANS_CASES = {"small": ("f", "d"), "grid": ("f",), "dup": ("f",), "trunc": ("f",), "mix": ("f", "d"),
+                "wide": ("f",), "sift": ("f",)}
+
+
+def kmeans_case(ref, out):
+    """VlGMMKMeans initialisation (vl/gmm.c:1315-1370) from a seeded thread
+    generator through vl_gmm_init_with_kmeans: the k-means assignment of every
+    row, the generator's next draw, the one-hot M-step's parameters; and
+    vl_gmm_cluster with KMeans initialisation and 5 EM iterations for two cases."""
+    for name, tags in KMEANS_CASES.items():
+        x, K, seed = kmeans_data(name)
+        for tag in tags:
+            dt = np.float32 if tag == "f" else np.float64
+            res = ref.kmeans_init(x.astype(dt), K, seed)
+            out[f"km_{name}_{tag}_assign"] = res["assign"].astype(np.int32)
+            out[f"km_{name}_{tag}_next"] = np.uint32(res["next_draw"])
+            for k in ("means", "covs", "priors"):
+                out[f"km_{name}_{tag}_{k}"] = res[k]
+            if name in ("small", "mix"):
+                em = ref.rand_init(x.astype(dt), K, seed, max_iter=5, lb=1e-4, init=VL_GMM_KMEANS)
+                out[f"km_{name}_{tag}_t5_ll"] = np.float64(em["ll"])
+                for k in ("means", "covs", "priors"):
+                    out[f"km_{name}_{tag}_t5_{k}"] = em[k]
+
+
 def main():
     ref = Reference(threads=1)
     out: dict = {}
@@ -187,6 +237,7 @@ def main():
     edge_cases(ref, out)
     rand_case(ref, out)
     vlad_case(ref, out)
+    kmeans_case(ref, out)
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")

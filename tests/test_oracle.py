@@ -2,6 +2,8 @@
 produced by VLFeat's own code (tests/golden/make_golden.py), and the FP64
 NumPy statement of the Fisher vector pins the known-answer case the way
 toolbox/xtest/vl_test_fisher.m does (absTol 1e-10 in double)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -118,6 +120,29 @@ def test_rand_init_restatement(golden, tag):
     o = rand_init(x, K, MT19937(seed), lanes)
     for k in ("means", "covs", "priors"):
         assert np.array_equal(o[k], golden[f"rand_small_{tag}_t0_{k}"]), k
+
+
+@pytest.mark.parametrize("name,tag", [("small", "f"), ("small", "d"), ("grid", "f"), ("dup", "f"),
+                                      ("trunc", "f")])
+def test_kmeans_init_restatement(golden, name, tag):
+    """The k-means of the KMeans initialisation restated (oracle.kmeans_init:
+    seeding shuffle and duplicate test, one-tree kd-forest with its random
+    draws, best-bin-first search, ordered centre sums, exact quantisation)
+    against the reference's: every assignment and the generator's next draw
+    equal."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import kmeans_data
+    from oracle.oracle import MT19937, kmeans_init
+    x, K, seed = kmeans_data(name)
+    dt = np.float32 if tag == "f" else np.float64
+    lanes = int(golden["rand_lanes"])
+    if dt == np.float64:
+        lanes = {8: 4, 4: 2, 1: 1}[lanes]
+    rng = MT19937(seed)
+    o = kmeans_init(x.astype(dt), K, rng, lanes)
+    assert np.array_equal(o["assign"], golden[f"km_{name}_{tag}_assign"])
+    assert rng.uint32() == int(golden[f"km_{name}_{tag}_next"])
 
 
 @pytest.mark.parametrize("flags", range(16))

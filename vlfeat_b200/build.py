@@ -26,8 +26,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 SOURCES = ["runtime.cpp", "gmm_api.cpp", "fisher_api.cpp", "fisher_plan.cpp", "k_exact.cu", "k_tc.cu", "k_noalloc.cu",
-           "k_router.cu", "k_vlad.cu", "k_pca.cu"]
-HEADERS = ["common.h", "engine.h", "tc_common.cuh"]
+           "k_router.cu", "k_vlad.cu", "k_pca.cu", "k_kmeans.cu"]
+HEADERS = ["common.h", "engine.h", "tc_common.cuh", "exact_math.cuh"]
 
 
 def _newer(src: str, dst: str, deps) -> bool:
@@ -41,7 +41,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
     deps = [os.path.join(CSRC, h) for h in HEADERS]
-    deps += [os.path.join(ROOT, "include", p) for p in ("vlb200.h", "vl/gmm.h", "vl/fisher.h", "vl/random.h", "vl/vlad.h",
+    deps += [os.path.join(ROOT, "include", p) for p in ("vlb200.h", "vl/gmm.h", "vl/fisher.h", "vl/random.h", "vl/vlad.h", "vl/kmeans.h",
                                                           "vl/generic.h", "vl/host.h")]
     objs = []
     for src in SOURCES:

@@ -115,7 +115,8 @@ enum ScratchArena {
   kArenaTc = 2,
   kArenaRouter = 3,
   kArenaVlad = 4,
-  kNumArenas = 5
+  kArenaKMeans = 5,
+  kNumArenas = 6
 };
 Scratch &thread_scratch(int arena = kArenaApi);
 

@@ -66,6 +66,27 @@ template <typename T>
 void kmeanspp(const T *X, i64 N, i64 D, i64 K, T *centers, i64 x0, const std::vector<T> &thresh, int lanes,
               cudaStream_t s);
 
+// KMeans initialisation (vl/gmm.c:1315-1370).  The settings of the k-means
+// object that the GMM creates for it (vl/gmm.c:1336-1356); the object itself
+// is struct _VlKMeans (k_kmeans.cu).
+struct KMeansSettings {
+  i64 maxNumIterations = 5;
+  i64 maxNumComparisons = 10;
+  i64 numRepetitions = 1;
+  double minEnergyVariation = 1e-4;  // vl/kmeans.c:416
+};
+// vl_kmeans_cluster with random-selection seeding and ANN refinement over a
+// one-tree kd-forest (vl/kmeans.c:2024-2093, 528-582, 1003-1150), then
+// vl_kmeans_quantize (vl/kmeans.c:656-702).  centers (K x D) and assign (N)
+// are device outputs; random draws come from the calling thread's generator in
+// the reference's order; lanes as for kmeanspp.  Returns the best energy.
+template <typename T>
+double kmeans_ann(const T *X, i64 N, i64 D, i64 K, const KMeansSettings &cfg, int lanes, T *centers,
+                  uint32_t *assign, cudaStream_t s);
+// q (N x K) = the one-hot rows of assign (vl/gmm.c:1361-1364).
+template <typename T>
+void onehot_posteriors(const uint32_t *assign, i64 N, i64 K, T *q, cudaStream_t s);
+
 // priors /= max(sum priors, 1e-12) on the device (vl/gmm.c:1196-1211).
 template <typename T>
 void normalize_priors(T *priors, i64 K, cudaStream_t s);

@@ -6,6 +6,7 @@
 // the data is staged to device memory once per call, parameters live on the
 // device during the loop and are copied back at the end; posteriors are
 // copied back lazily on the first vl_gmm_get_posteriors() call.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -19,6 +20,15 @@ extern "C" {
 
 using vlb::i64;
 
+// The k-means object of the KMeans initialisation.  The library creates one
+// the first time a GMM needs it, with the reference's settings
+// (vl/gmm.c:1336-1356), and owns it; objects from elsewhere are refused.
+struct _VlKMeans {
+  static constexpr uint32_t kMagic = 0x4b4d6231u;
+  uint32_t magic = kMagic;
+  vlb::KMeansSettings cfg;
+};
+
 struct _VlGMM {
   vl_type dataType = VL_TYPE_FLOAT;
   vl_size dimension = 0, numClusters = 0, numData = 0;
@@ -30,10 +40,11 @@ struct _VlGMM {
   double *sigmaLowBound = nullptr;
   VlGMMInitialization initialization = VlGMMRand;
   VlKMeans *kmeansInit = nullptr;
+  bool kmeansInitIsOwner = false;
   double LL = 0;
   // GPU state.
   bool postOnDevice = false;  // the device buffer holds the current posteriors
-  vlb::DevBuf dX, dq, dmeans, dcovs, dpriors, dlb, dtmp;
+  vlb::DevBuf dX, dq, dmeans, dcovs, dpriors, dlb, dtmp, dassign;
   std::vector<double> llTrace;
   vl_size numRestarts = 0;
 };
@@ -261,6 +272,22 @@ const T *stage_data(VlGMM *self, const void *data, i64 N) {
   return dX;
 }
 
+// Lanes of the reference's distance kernel on this host (vl/mathop.c:489-510):
+// AVX, SSE2 or scalar.
+int simd_lanes(bool isFloat) {
+  if (vl_get_simd_enabled()) {
+    if (vl_cpu_has_avx()) return isFloat ? 8 : 4;
+    if (vl_cpu_has_sse2()) return isFloat ? 4 : 2;
+  }
+  return 1;
+}
+
+void drop_kmeans(VlGMM *self) {
+  if (self->kmeansInit && self->kmeansInitIsOwner) delete self->kmeansInit;
+  self->kmeansInit = nullptr;
+  self->kmeansInitIsOwner = false;
+}
+
 // Rand initialisation, vl/gmm.c:1416-1443, on device data: uniform priors,
 // every covariance the global data variance, means by k-means++ seeding.  The
 // random draws come from the calling thread's generator in the reference's
@@ -280,11 +307,7 @@ void init_rand(VlGMM *self, const T *dX, i64 N) {
   const i64 x0 = (i64)vl_rand_uindex(r, (vl_uindex)N);
   std::vector<T> thresh((size_t)K);
   for (i64 k = 0; k < K; ++k) thresh[k] = (T)vl_rand_real1(r);
-  int lanes = 1;
-  if (vl_get_simd_enabled()) {
-    if (vl_cpu_has_avx()) lanes = sizeof(T) == 4 ? 8 : 4;
-    else if (vl_cpu_has_sse2()) lanes = sizeof(T) == 4 ? 4 : 2;
-  }
+  const int lanes = simd_lanes(sizeof(T) == 4);
   T *dsigma = self->dtmp.get<T>(D);
   T *dcenters = self->dmeans.get<T>(K * D);
   vlb::global_variance<T>(dX, N, D, dsigma, s);
@@ -295,6 +318,48 @@ void init_rand(VlGMM *self, const T *dX, i64 N) {
   VLB_CUDA(cudaStreamSynchronize(s));
   T *cv = (T *)self->covariances;
   for (i64 k = 0; k < K; ++k) memcpy(cv + k * D, sigma.data(), sizeof(T) * D);
+}
+
+// KMeans initialisation, vl/gmm.c:1315-1370, on device data: k-means (the
+// GMM's own object, created on first use with numData/4 comparisons, at least
+// 10), exact assignment of every row, then one M-step from the one-hot
+// posteriors and zero parameters.  Parameters go to the host arrays; the
+// one-hot posteriors stay on the device as the current posteriors.
+template <typename T>
+void init_kmeans(VlGMM *self, const T *dX, i64 N) {
+  VLB_CHECK(N >= 1, VL_ERR_BAD_ARG, "KMeans initialisation needs at least one data point");
+  if (!self->kmeansInit) {
+    VlKMeans *k = new VlKMeans();
+    k->cfg.maxNumComparisons = std::max<i64>(N / 4, 10);
+    k->cfg.maxNumIterations = 5;
+    k->cfg.numRepetitions = 1;
+    self->kmeansInit = k;
+    self->kmeansInitIsOwner = true;
+  }
+  VLB_CHECK(self->kmeansInit->magic == VlKMeans::kMagic, VL_ERR_BAD_ARG,
+            "KMeans initialisation: only the library's own k-means object is supported");
+  cudaStream_t s = vlb::thread_stream();
+  const i64 K = (i64)self->numClusters, D = (i64)self->dimension;
+  self->numData = (vl_size)N;  // _vl_gmm_prepare_for_data, vl/gmm.c:336-344
+  T *dcenters = self->dtmp.get<T>(K * D);
+  uint32_t *dassign = self->dassign.get<uint32_t>(N);
+  vlb::kmeans_ann<T>(dX, N, D, K, self->kmeansInit->cfg, simd_lanes(sizeof(T) == 4), dcenters, dassign, s);
+  T *dmeans = self->dmeans.get<T>(K * D);
+  T *dcovs = self->dcovs.get<T>(K * D);
+  T *dpriors = self->dpriors.get<T>(K);
+  double *dlb = self->dlb.get<double>(D);
+  T *dq = self->dq.get<T>(N * K);
+  vlb::onehot_posteriors<T>(dassign, N, K, dq, s);
+  VLB_CUDA(cudaMemsetAsync(dmeans, 0, sizeof(T) * K * D, s));  // vl/gmm.c:1326-1328
+  VLB_CUDA(cudaMemsetAsync(dcovs, 0, sizeof(T) * K * D, s));
+  VLB_CUDA(cudaMemsetAsync(dpriors, 0, sizeof(T) * K, s));
+  VLB_CUDA(cudaMemcpyAsync(dlb, self->sigmaLowBound, sizeof(double) * D, cudaMemcpyHostToDevice, s));
+  vlb::exact_mstep<T>(dX, N, dq, dmeans, dcovs, dpriors, K, D, dlb, s);
+  VLB_CUDA(cudaMemcpyAsync(self->means, dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaMemcpyAsync(self->covariances, dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaMemcpyAsync(self->priors, dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  self->postOnDevice = true;
 }
 
 double em_host(VlGMM *self, const void *data, vl_size N) {
@@ -350,7 +415,7 @@ void vl_gmm_reset(VlGMM *self) {
   }
   self->numData = 0;
   self->postOnDevice = false;
-  self->kmeansInit = nullptr;
+  drop_kmeans(self);
 }
 
 void vl_gmm_delete(VlGMM *self) {
@@ -360,6 +425,7 @@ void vl_gmm_delete(VlGMM *self) {
   vl_free(self->priors);
   vl_free(self->posteriors);
   vl_free(self->sigmaLowBound);
+  drop_kmeans(self);
   delete self;
 }
 
@@ -397,7 +463,11 @@ vl_size vl_gmm_get_dimension(VlGMM const *self) { return self->dimension; }
 VlGMMInitialization vl_gmm_get_initialization(VlGMM const *self) { return self->initialization; }
 void vl_gmm_set_initialization(VlGMM *self, VlGMMInitialization init) { self->initialization = init; }
 VlKMeans *vl_gmm_get_kmeans_init_object(VlGMM const *self) { return self->kmeansInit; }
-void vl_gmm_set_kmeans_init_object(VlGMM *self, VlKMeans *k) { self->kmeansInit = k; }
+void vl_gmm_set_kmeans_init_object(VlGMM *self, VlKMeans *k) {  // vl/gmm.c:628-638
+  drop_kmeans(self);
+  self->kmeansInit = k;
+  self->kmeansInitIsOwner = false;
+}
 double const *vl_gmm_get_covariance_lower_bounds(VlGMM const *self) { return self->sigmaLowBound; }
 void vl_gmm_set_covariance_lower_bounds(VlGMM *self, double const *b) {
   memcpy(self->sigmaLowBound, b, sizeof(double) * self->dimension);
@@ -430,11 +500,17 @@ void vl_gmm_init_with_rand_data(VlGMM *self, void const *data, vl_size numData) 
       0);
 }
 
-void vl_gmm_init_with_kmeans(VlGMM *self, void const *, vl_size, VlKMeans *) {
-  vl_set_last_error(VL_ERR_BAD_ARG,
-                    "vl_gmm_init_with_kmeans: k-means initialisation is not available in the GPU "
-                    "library; use VlGMMCustom");
-  (void)self;
+void vl_gmm_init_with_kmeans(VlGMM *self, void const *data, vl_size numData, VlKMeans *kmeansInit) {
+  guarded(
+      [&]() -> int {
+        if (kmeansInit) vl_gmm_set_kmeans_init_object(self, kmeansInit);  // vl/gmm.c:1333
+        if (self->dataType == VL_TYPE_FLOAT)
+          init_kmeans<float>(self, stage_data<float>(self, data, (i64)numData), (i64)numData);
+        else
+          init_kmeans<double>(self, stage_data<double>(self, data, (i64)numData), (i64)numData);
+        return 0;
+      },
+      0);
 }
 
 double vl_gmm_em(VlGMM *self, void const *data, vl_size numData) {
@@ -447,9 +523,6 @@ double vl_gmm_em(VlGMM *self, void const *data, vl_size numData) {
 double vl_gmm_cluster(VlGMM *self, void const *data, vl_size numData) {
   return guarded(
       [&]() -> double {
-        VLB_CHECK(self->initialization == VlGMMCustom || self->initialization == VlGMMRand,
-                  VL_ERR_BAD_ARG,
-                  "vl_gmm_cluster: VlGMMKMeans initialisation is not available in the GPU library");
         const size_t sz = tsize(self->dataType);
         const size_t nKD = self->numClusters * self->dimension;
         std::vector<char> m0((char *)self->means, (char *)self->means + sz * nKD);
@@ -471,6 +544,11 @@ double vl_gmm_cluster(VlGMM *self, void const *data, vl_size numData) {
               init_rand<float>(self, (const float *)dX, (i64)numData);
             else
               init_rand<double>(self, (const double *)dX, (i64)numData);
+          } else if (self->initialization == VlGMMKMeans) {
+            if (self->dataType == VL_TYPE_FLOAT)
+              init_kmeans<float>(self, (const float *)dX, (i64)numData);
+            else
+              init_kmeans<double>(self, (const double *)dX, (i64)numData);
           } else if (rep > 0) {
             memcpy(self->means, m0.data(), m0.size());
             memcpy(self->covariances, c0.data(), c0.size());
