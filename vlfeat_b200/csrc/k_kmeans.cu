@@ -187,6 +187,17 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ X, i64 N, int D,
   }
 }
 
+// Distance of the query (stride qs) to centre row c; VEC reads the row in
+// 16-byte vectors (row starts 16-byte aligned, whole vectors per lane group).
+template <typename T, int L, bool VEC>
+__device__ __forceinline__ T row_dist(const T *q, int qs, const T *__restrict__ c, int D) {
+  if constexpr (VEC && (L * sizeof(T)) % 16 == 0) {
+    return l2_ordered_sv<T, L>(q, qs, c, D);
+  } else {
+    return l2_ordered_s<T, L>(q, qs, c, D);
+  }
+}
+
 // One query of the forest, vl/kdtree.c:774-840 with numNeighbors = 1, the
 // recursion of vl/kdtree.c:583-725 unrolled into a loop.  The search heap of
 // this thread lives at hk[e * G], hn[e * G] (entry e), capacity cap = the
@@ -195,7 +206,7 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ X, i64 N, int D,
 // the root while strictly smaller, pop moves the last entry to the root and
 // sifts it down towards the smaller child (the right one on ties) while it
 // is strictly larger.
-template <typename T, int L>
+template <typename T, int L, bool VEC>
 __device__ __forceinline__ int kd_query(const T *q, int qs, const T *__restrict__ C, int D, const KdDev &tr,
                                         i64 maxComp, double *__restrict__ hk, int *__restrict__ hn, i64 G,
                                         int cap, double &bestOut, int *__restrict__ err) {
@@ -250,7 +261,7 @@ __device__ __forceinline__ int kd_query(const T *q, int qs, const T *__restrict_
         const int b = -lc - 1, e = -tr.upper[n] - 1;
         for (int it = b; it < e && (exact || comps < maxComp); ++it) {
           const int di = tr.ent[it];
-          const double dd = (double)l2_ordered_s<T, L>(q, qs, C + (i64)di * D, D);
+          const double dd = (double)row_dist<T, L, VEC>(q, qs, C + (i64)di * D, D);
           ++comps;
           if (!have) {
             have = true;
@@ -313,7 +324,7 @@ __device__ __forceinline__ int kd_query(const T *q, int qs, const T *__restrict_
 // ANN assignment, vl/kmeans.c:708-771: the forest's nearest centre of each
 // row; after the first iteration (update) the previous assignment is kept
 // unless the new centre is strictly closer.  Persistent blocks of TB rows.
-template <typename T, int L>
+template <typename T, int L, bool VEC>
 __global__ void k_km_ann(const T *__restrict__ X, i64 N, int D, const T *__restrict__ C, KdDev tr, i64 maxComp,
                          int update, uint32_t *__restrict__ assign, T *__restrict__ dist,
                          double *__restrict__ hkey, int *__restrict__ hnode, int cap, int *__restrict__ err) {
@@ -330,13 +341,13 @@ __global__ void k_km_ann(const T *__restrict__ X, i64 N, int D, const T *__restr
     if (x >= N) continue;
     const T *q = sq + threadIdx.x;
     double nd;
-    const int ni = kd_query<T, L>(q, TB, C, D, tr, maxComp, hkey + g, hnode + g, G, cap, nd, err);
+    const int ni = kd_query<T, L, VEC>(q, TB, C, D, tr, maxComp, hkey + g, hnode + g, G, cap, nd, err);
     const T ndt = (T)nd;  // exact: the distance was computed in T
     if (!update) {
       dist[x] = ndt;
       assign[x] = (uint32_t)ni;
     } else {
-      const T prev = l2_ordered_s<T, L>(q, TB, C + (i64)assign[x] * D, D);
+      const T prev = row_dist<T, L, VEC>(q, TB, C + (i64)assign[x] * D, D);
       if (prev > ndt) {
         dist[x] = ndt;
         assign[x] = (uint32_t)ni;
@@ -350,7 +361,7 @@ __global__ void k_km_ann(const T *__restrict__ X, i64 N, int D, const T *__restr
 // Exact quantisation, vl/kmeans.c:656-702: the first centre of least
 // distance (strict <, starting from +inf; rows whose distances are all NaN
 // keep centre 0, where the reference leaves the assignment unset).
-template <typename T, int L>
+template <typename T, int L, bool VEC>
 __global__ void k_km_quantize(const T *__restrict__ X, i64 N, int D, const T *__restrict__ C, int K,
                               uint32_t *__restrict__ assign) {
   extern __shared__ __align__(16) unsigned char km_smem[];
@@ -367,7 +378,7 @@ __global__ void k_km_quantize(const T *__restrict__ X, i64 N, int D, const T *__
     T best = (T)INFINITY;
     uint32_t bi = 0;
     for (int k = 0; k < K; ++k) {
-      const T dd = l2_ordered_s<T, L>(q, TB, C + (i64)k * D, D);
+      const T dd = row_dist<T, L, VEC>(q, TB, C + (i64)k * D, D);
       if (dd < best) {
         best = dd;
         bi = (uint32_t)k;
@@ -546,6 +557,10 @@ struct KMeansRun {
     return 32;
   }
 
+  // Centre rows can be read in 16-byte vectors: every row start 16-byte
+  // aligned and each lane group whole vectors.
+  bool vec(int L) const { return (D * sizeof(T)) % 16 == 0 && (L * sizeof(T)) % 16 == 0; }
+
   template <template <typename, int> class Launch, typename... A>
   void by_lanes(A &&...a) {
     switch (lanes) {
@@ -675,15 +690,19 @@ struct KMeansRun {
       const int TB = r.tile_rows();
       const int cap = tr.numNodes;
       const i64 perThread = (i64)cap * (sizeof(double) + sizeof(int));
-      i64 blocks = std::min<i64>((r.N + TB - 1) / TB, (i64)num_sms() * 8);
+      i64 blocks = std::min<i64>((r.N + TB - 1) / TB, (i64)num_sms() * 12);
       blocks = std::max<i64>(1, std::min<i64>(blocks, (i64)(kHeapBudget / (size_t)(perThread * TB))));
       const i64 G = blocks * TB;
       double *hk = r.sc.slot[5].template get<double>(G * cap);
       int *hn = r.sc.slot[6].template get<int>(G * cap);
       const size_t smem = sizeof(TT) * (size_t)TB * (size_t)r.D;
-      VLB_CUDA(cudaFuncSetAttribute(k_km_ann<TT, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      VLB_LAUNCH("km_ann", r.s, (k_km_ann<TT, L><<<(int)blocks, TB, smem, r.s>>>(
-                                    r.X, r.N, (int)r.D, centers, tr, maxComp, update, assign, dist, hk, hn, cap, err)));
+      auto go = [&](auto kern) {
+        VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        VLB_LAUNCH("km_ann", r.s, (kern<<<(int)blocks, TB, smem, r.s>>>(r.X, r.N, (int)r.D, centers, tr, maxComp,
+                                                                         update, assign, dist, hk, hn, cap, err)));
+      };
+      if (r.vec(L)) go(k_km_ann<TT, L, true>);
+      else go(k_km_ann<TT, L, false>);
     }
   };
 
@@ -693,9 +712,13 @@ struct KMeansRun {
       const int TB = r.tile_rows();
       const i64 blocks = std::min<i64>((r.N + TB - 1) / TB, (i64)num_sms() * 16);
       const size_t smem = sizeof(TT) * (size_t)TB * (size_t)r.D;
-      VLB_CUDA(cudaFuncSetAttribute(k_km_quantize<TT, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      VLB_LAUNCH("km_quantize", r.s, (k_km_quantize<TT, L><<<(int)blocks, TB, smem, r.s>>>(
-                                         r.X, r.N, (int)r.D, centers, (int)r.K, assign)));
+      auto go = [&](auto kern) {
+        VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        VLB_LAUNCH("km_quantize", r.s, (kern<<<(int)blocks, TB, smem, r.s>>>(r.X, r.N, (int)r.D, centers,
+                                                                              (int)r.K, assign)));
+      };
+      if (r.vec(L)) go(k_km_quantize<TT, L, true>);
+      else go(k_km_quantize<TT, L, false>);
     }
   };
 
