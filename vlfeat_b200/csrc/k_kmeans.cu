@@ -173,8 +173,9 @@ struct KdDev {
 
 // ---------------------------------------------------------------- kernels
 // Loads rows [base, base + TB) of X into the block's transposed tile
-// sq[d * TB + r] (row r's element d), so that each thread reads its row with
-// stride TB and a warp's reads hit distinct banks.
+// sq[d * (TB + 1) + r] (row r's element d): each thread reads its row with
+// stride TB + 1, and both the warp's reads and the tile's stores hit
+// distinct banks.
 template <typename T>
 __device__ __forceinline__ void load_rows(const T *__restrict__ X, i64 N, int D, i64 base, T *sq) {
   const int TB = blockDim.x;
@@ -183,9 +184,11 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ X, i64 N, int D,
   for (i64 e = threadIdx.x; e < rows * D; e += TB) {
     const i64 r = e / D;
     const int d = (int)(e - r * D);
-    sq[(i64)d * TB + r] = src[e];
+    sq[(i64)d * (TB + 1) + r] = src[e];
   }
 }
+
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 // Distance of the query (stride qs) to centre row c; VEC reads the row in
 // 16-byte vectors (row starts 16-byte aligned, whole vectors per lane group).
@@ -324,30 +327,54 @@ __device__ __forceinline__ int kd_query(const T *q, int qs, const T *__restrict_
 // ANN assignment, vl/kmeans.c:708-771: the forest's nearest centre of each
 // row; after the first iteration (update) the previous assignment is kept
 // unless the new centre is strictly closer.  Persistent blocks of TB rows.
-template <typename T, int L, bool VEC>
+// With a row list, the kernel serves only rows list[0 .. count).  SH: the
+// search heaps live in shared memory after the query tile (entry e of thread
+// t at e * TB + t), else in global memory (entry e at e * G + global thread).
+template <typename T, int L, bool VEC, bool SH>
 __global__ void k_km_ann(const T *__restrict__ X, i64 N, int D, const T *__restrict__ C, KdDev tr, i64 maxComp,
                          int update, uint32_t *__restrict__ assign, T *__restrict__ dist,
-                         double *__restrict__ hkey, int *__restrict__ hnode, int cap, int *__restrict__ err) {
+                         double *__restrict__ hkey, int *__restrict__ hnode, int cap, int *__restrict__ err,
+                         const uint32_t *__restrict__ list, i64 count) {
   extern __shared__ __align__(16) unsigned char km_smem[];
   T *sq = (T *)km_smem;
   const int TB = blockDim.x;
+  const int QS = TB + 1;
   const i64 G = (i64)gridDim.x * TB;
   const i64 g = (i64)blockIdx.x * TB + threadIdx.x;
-  for (i64 base = (i64)blockIdx.x * TB; base < N; base += G) {
+  double *hk;
+  int *hn;
+  i64 hG;
+  if constexpr (SH) {
+    double *hkS = (double *)(km_smem + align16(sizeof(T) * (size_t)QS * D));
+    hk = hkS + threadIdx.x;
+    hn = (int *)(hkS + (size_t)TB * cap) + threadIdx.x;
+    hG = TB;
+  } else {
+    hk = hkey + g;
+    hn = hnode + g;
+    hG = G;
+  }
+  const i64 M = list ? count : N;
+  for (i64 base = (i64)blockIdx.x * TB; base < M; base += G) {
     __syncthreads();
-    load_rows(X, N, D, base, sq);
+    if (!list) {
+      load_rows(X, N, D, base, sq);
+    } else if (base + threadIdx.x < M) {
+      const T *src = X + (i64)list[base + threadIdx.x] * D;
+      for (int d = 0; d < D; ++d) sq[(i64)d * QS + threadIdx.x] = src[d];
+    }
     __syncthreads();
-    const i64 x = base + threadIdx.x;
-    if (x >= N) continue;
+    if (base + threadIdx.x >= M) continue;
+    const i64 x = list ? (i64)list[base + threadIdx.x] : base + threadIdx.x;
     const T *q = sq + threadIdx.x;
     double nd;
-    const int ni = kd_query<T, L, VEC>(q, TB, C, D, tr, maxComp, hkey + g, hnode + g, G, cap, nd, err);
+    const int ni = kd_query<T, L, VEC>(q, QS, C, D, tr, maxComp, hk, hn, hG, cap, nd, err);
     const T ndt = (T)nd;  // exact: the distance was computed in T
     if (!update) {
       dist[x] = ndt;
       assign[x] = (uint32_t)ni;
     } else {
-      const T prev = row_dist<T, L, VEC>(q, TB, C + (i64)assign[x] * D, D);
+      const T prev = row_dist<T, L, VEC>(q, QS, C + (i64)assign[x] * D, D);
       if (prev > ndt) {
         dist[x] = ndt;
         assign[x] = (uint32_t)ni;
@@ -358,33 +385,163 @@ __global__ void k_km_ann(const T *__restrict__ X, i64 N, int D, const T *__restr
   }
 }
 
-// Exact quantisation, vl/kmeans.c:656-702: the first centre of least
-// distance (strict <, starting from +inf; rows whose distances are all NaN
-// keep centre 0, where the reference leaves the assignment unset).
+// A lane group of L elements of a centre row, in 16-byte vectors when VEC.
 template <typename T, int L, bool VEC>
-__global__ void k_km_quantize(const T *__restrict__ X, i64 N, int D, const T *__restrict__ C, int K,
-                              uint32_t *__restrict__ assign) {
+__device__ __forceinline__ void load_group(const T *__restrict__ p, T *out) {
+  if constexpr (VEC && (L * sizeof(T)) % 16 == 0) {
+    constexpr int V = 16 / sizeof(T);
+#pragma unroll
+    for (int u = 0; u < L / V; ++u) {
+      const float4 w = __ldg(reinterpret_cast<const float4 *>(p) + u);
+      const T *wp = reinterpret_cast<const T *>(&w);
+#pragma unroll
+      for (int e = 0; e < V; ++e) out[u * V + e] = wp[e];
+    }
+  } else {
+#pragma unroll
+    for (int l = 0; l < L; ++l) out[l] = __ldg(p + l);
+  }
+}
+
+template <typename T, int L>
+__device__ __forceinline__ T lane_sum(const T *v) {  // the SIMD horizontal sum of l2_ordered_s
+  if constexpr (L == 8) {
+    return add_rn(add_rn(add_rn(v[0], v[1]), add_rn(v[4], v[5])), add_rn(add_rn(v[2], v[3]), add_rn(v[6], v[7])));
+  } else if constexpr (L == 4) {
+    return add_rn(add_rn(v[0], v[2]), add_rn(v[1], v[3]));
+  } else if constexpr (L == 2) {
+    return add_rn(v[0], v[1]);
+  } else {
+    return v[0];
+  }
+}
+
+enum : int { kNearestQuantize = 0, kNearestScreen = 1 };
+
+// Every distance of a row to the K centres, each in the reference's order
+// (l2_ordered_s), with a register tile of TC centres sharing each lane group
+// of the query.
+//
+// kNearestQuantize: exact quantisation, vl/kmeans.c:656-702: the first centre
+// of least distance (strict <, from +inf; rows whose distances are all NaN
+// keep centre 0, where the reference leaves the assignment unset).
+//
+// kNearestScreen: the ANN assignment (vl/kmeans.c:708-771) when the search
+// budget covers every centre (K <= maxNumComparisons, one tree): the search
+// is then exhaustive up to pruning by exact lower bounds, so when the least
+// distance is below every other by more than the distances' rounding
+// (margin, relative) the search returns that centre; such rows are assigned
+// here (with the update rule: keep the previous centre unless strictly
+// farther).  Rows with a near tie, a NaN or an infinite distance go to the
+// row list for the kd-tree search itself.
+template <typename T, int L, bool VEC, int TC>
+__global__ void k_km_nearest(const T *__restrict__ X, i64 N, int D, const T *__restrict__ C, int K, int KC,
+                             int mode, int update, uint32_t *__restrict__ assign, T *__restrict__ dist, T margin,
+                             uint32_t *__restrict__ list, unsigned long long *__restrict__ count) {
   extern __shared__ __align__(16) unsigned char km_smem[];
-  T *sq = (T *)km_smem;
   const int TB = blockDim.x;
+  const int QS = TB + 1;
+  T *sq = (T *)km_smem;
+  T *sc = (T *)(km_smem + align16(sizeof(T) * (size_t)QS * D));  // KC centre rows
   const i64 G = (i64)gridDim.x * TB;
   for (i64 base = (i64)blockIdx.x * TB; base < N; base += G) {
     __syncthreads();
     load_rows(X, N, D, base, sq);
-    __syncthreads();
     const i64 x = base + threadIdx.x;
-    if (x >= N) continue;
+    const bool active = x < N;
     const T *q = sq + threadIdx.x;
-    T best = (T)INFINITY;
+    const uint32_t pa = (active && mode == kNearestScreen && update) ? assign[x] : 0xffffffffu;
+    T best = (T)INFINITY, second = (T)INFINITY, prevd = (T)0;
     uint32_t bi = 0;
-    for (int k = 0; k < K; ++k) {
-      const T dd = row_dist<T, L, VEC>(q, TB, C + (i64)k * D, D);
-      if (dd < best) {
-        best = dd;
-        bi = (uint32_t)k;
+    bool nan = false;
+    for (int k0 = 0; k0 < K; k0 += KC) {
+      // The next KC centres into shared memory (every thread reads the same
+      // centre element at a time: broadcast loads).
+      const int kn = min(KC, K - k0);
+      __syncthreads();
+      if constexpr (VEC) {
+        const float4 *src = reinterpret_cast<const float4 *>(C + (i64)k0 * D);
+        float4 *dst = reinterpret_cast<float4 *>(sc);
+        const int n4 = (int)((size_t)kn * D * sizeof(T) / 16);
+        for (int e = threadIdx.x; e < n4; e += TB) dst[e] = __ldg(src + e);
+      } else {
+        for (int e = threadIdx.x; e < kn * D; e += TB) sc[e] = __ldg(C + (i64)k0 * D + e);
+      }
+      __syncthreads();
+      if (!active) continue;
+      for (int c0 = 0; c0 < kn; c0 += TC) {
+        T acc[TC][L];
+#pragma unroll
+        for (int t = 0; t < TC; ++t)
+#pragma unroll
+          for (int l = 0; l < L; ++l) acc[t][l] = (T)0;
+        int i = 0;
+        for (; i + L <= D; i += L) {
+          T qv[L];
+#pragma unroll
+          for (int l = 0; l < L; ++l) qv[l] = q[(i + l) * QS];
+#pragma unroll
+          for (int t = 0; t < TC; ++t) {
+            const T *cr = sc + (size_t)min(c0 + t, kn - 1) * D + i;  // a partial tile repeats the last row
+            T cg[L];
+            if constexpr (VEC && (L * sizeof(T)) % 16 == 0) {
+              constexpr int V = 16 / sizeof(T);
+#pragma unroll
+              for (int u = 0; u < L / V; ++u) {
+                const float4 w = reinterpret_cast<const float4 *>(cr)[u];
+                const T *wp = reinterpret_cast<const T *>(&w);
+#pragma unroll
+                for (int e = 0; e < V; ++e) cg[u * V + e] = wp[e];
+              }
+            } else {
+#pragma unroll
+              for (int l = 0; l < L; ++l) cg[l] = cr[l];
+            }
+#pragma unroll
+            for (int l = 0; l < L; ++l) {
+              const T dl = sub_rn(qv[l], cg[l]);
+              acc[t][l] = add_rn(acc[t][l], mul_rn(dl, dl));
+            }
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < TC; ++t) {
+          const int cl = c0 + t;
+          if (cl >= kn) break;
+          const int c = k0 + cl;
+          T d = lane_sum<T, L>(acc[t]);
+          for (int j = i; j < D; ++j) {
+            const T dl = sub_rn(q[j * QS], sc[(size_t)cl * D + j]);
+            d = add_rn(d, mul_rn(dl, dl));
+          }
+          nan |= d != d;
+          if ((uint32_t)c == pa) prevd = d;
+          if (d < best) {
+            second = best;
+            best = d;
+            bi = (uint32_t)c;
+          } else if (d < second) {
+            second = d;
+          }
+        }
       }
     }
-    assign[x] = bi;
+    if (!active) continue;
+    if (mode == kNearestQuantize) {
+      assign[x] = bi;
+      continue;
+    }
+    const bool clear = !nan && best != (T)INFINITY && (K == 1 || second - best > margin * second);
+    if (!clear) {
+      list[atomicAdd(count, 1ull)] = (uint32_t)x;
+      continue;
+    }
+    if (!update || prevd > best) {
+      dist[x] = best;
+      assign[x] = bi;
+    } else {
+      dist[x] = prevd;
+    }
   }
 }
 
@@ -501,32 +658,63 @@ __global__ void k_km_scatter(const uint32_t *__restrict__ assign, i64 N, int K, 
   }
 }
 
-// New centres, vl/kmeans.c:1078-1098: one thread per (centre, dimension) adds
-// the centre's rows in data order from 0, then divides by the mass rounded to
-// T.  Empty centres are left for the host's restarts.
+// New centres, vl/kmeans.c:1078-1098: block c adds centre c's rows in data
+// order from 0, thread t owning dimensions t, t + blockDim, ... (up to
+// kSumDims per thread), then divides by the mass rounded to T.  The rows come
+// through a shared-memory tile of R rows: the loads of the next tile (into
+// registers) overlap the ordered additions of the current one.  Empty
+// centres are left for the host's restarts.
+constexpr int kSumThreads = 256;
+constexpr int kSumDims = 4;          // D <= kSumThreads * kSumDims
+constexpr int kSumTileElems = 2048;  // R * D <= this
+constexpr int kSumPer = kSumTileElems / kSumThreads;
+
 template <typename T>
-__global__ void k_km_sums(const T *__restrict__ X, int D, int K, const i64 *__restrict__ off,
-                          const uint32_t *__restrict__ order, T *__restrict__ C) {
-  const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (i64)K * D) return;
-  const int c = (int)(e / D);
-  const int d = (int)(e - (i64)c * D);
+__global__ void __launch_bounds__(kSumThreads) k_km_sums(const T *__restrict__ X, int D, int R,
+                                                         const i64 *__restrict__ off,
+                                                         const uint32_t *__restrict__ order, T *__restrict__ C) {
+  __shared__ T tile[kSumTileElems];
+  const int c = blockIdx.x;
   const i64 b = off[c], n = off[c + 1] - off[c];
   if (n == 0) return;
-  T acc = (T)0;
-  i64 j = 0;
-  for (; j + 8 <= n; j += 8) {
-    uint32_t idx[8];
-    T v[8];
+  const int t = threadIdx.x;
+  T acc[kSumDims];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) idx[u] = order[b + j + u];
+  for (int u = 0; u < kSumDims; ++u) acc[u] = (T)0;
+  const int te = R * D;
+  T nxt[kSumPer];
+  auto fetch = [&](i64 j) {  // tile starting at segment position j, into registers
 #pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = X[(i64)idx[u] * D + d];
+    for (int u = 0; u < kSumPer; ++u) {
+      const int e = t + u * kSumThreads;
+      const int r = e / D;
+      nxt[u] = (e < te && j + r < n) ? __ldg(X + (i64)__ldg(order + b + j + r) * D + (e - r * D)) : (T)0;
+    }
+  };
+  fetch(0);
+  for (i64 j = 0; j < n; j += R) {
+    __syncthreads();
 #pragma unroll
-    for (int u = 0; u < 8; ++u) acc = add_rn(acc, v[u]);
+    for (int u = 0; u < kSumPer; ++u) {
+      const int e = t + u * kSumThreads;
+      if (e < te) tile[e] = nxt[u];
+    }
+    __syncthreads();
+    if (j + R < n) fetch(j + R);
+    const int rows = (int)min((i64)R, n - j);
+#pragma unroll
+    for (int u = 0; u < kSumDims; ++u) {
+      const int d = t + u * kSumThreads;
+      if (d < D)
+        for (int r = 0; r < rows; ++r) acc[u] = add_rn(acc[u], tile[r * D + d]);
+    }
   }
-  for (; j < n; ++j) acc = add_rn(acc, X[(i64)order[b + j] * D + d]);
-  C[e] = div_rn(acc, (T)(unsigned long long)n);
+  const T m = (T)(unsigned long long)n;
+#pragma unroll
+  for (int u = 0; u < kSumDims; ++u) {
+    const int d = t + u * kSumThreads;
+    if (d < D) C[(i64)c * D + d] = div_rn(acc[u], m);
+  }
 }
 
 template <typename T>
@@ -551,8 +739,8 @@ struct KMeansRun {
   // must fit the shared memory this kernel may use.
   int tile_rows() const {
     for (int tb : {128, 64, 32})
-      if ((size_t)tb * D * sizeof(T) <= (size_t)96 * 1024) return tb;
-    VLB_CHECK((size_t)32 * D * sizeof(T) <= (size_t)200 * 1024, VL_ERR_BAD_ARG,
+      if ((size_t)(tb + 1) * D * sizeof(T) <= (size_t)96 * 1024) return tb;
+    VLB_CHECK((size_t)33 * D * sizeof(T) <= (size_t)200 * 1024, VL_ERR_BAD_ARG,
               "k-means initialisation: dimension too large");
     return 32;
   }
@@ -686,39 +874,75 @@ struct KMeansRun {
   template <typename TT, int L>
   struct AnnLaunch {
     static void run(KMeansRun &r, const TT *centers, const KdDev &tr, i64 maxComp, int update, uint32_t *assign,
-                    TT *dist, int *err) {
-      const int TB = r.tile_rows();
+                    TT *dist, int *err, const uint32_t *list, i64 count) {
       const int cap = tr.numNodes;
-      const i64 perThread = (i64)cap * (sizeof(double) + sizeof(int));
-      i64 blocks = std::min<i64>((r.N + TB - 1) / TB, (i64)num_sms() * 12);
-      blocks = std::max<i64>(1, std::min<i64>(blocks, (i64)(kHeapBudget / (size_t)(perThread * TB))));
+      const size_t perThread = (size_t)cap * (sizeof(double) + sizeof(int));
+      const i64 M = list ? count : r.N;
+      // Heaps in shared memory when at least 8 threads' heaps and query
+      // columns fit the block's 200 KB: the search's pops and pushes are
+      // then shared-memory latency instead of global-memory latency.
+      const size_t rowBytes = sizeof(TT) * (size_t)r.D;
+      const size_t smemCap = (size_t)200 * 1024 - 32 - rowBytes;
+      const int tbSh = (int)std::min<size_t>((size_t)r.tile_rows(), smemCap / (perThread + rowBytes));
+      if (tbSh >= 8) {
+        const int TB = tbSh;
+        const i64 blocks = std::max<i64>(1, std::min<i64>((M + TB - 1) / TB, (i64)num_sms()));
+        const size_t smem = align16(rowBytes * (TB + 1)) + perThread * TB;
+        auto go = [&](auto kern) {
+          VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          VLB_LAUNCH("km_ann", r.s, (kern<<<(int)blocks, TB, smem, r.s>>>(
+                                        r.X, r.N, (int)r.D, centers, tr, maxComp, update, assign, dist,
+                                        (double *)nullptr, (int *)nullptr, cap, err, list, count)));
+        };
+        if (r.vec(L)) go(k_km_ann<TT, L, true, true>);
+        else go(k_km_ann<TT, L, false, true>);
+        return;
+      }
+      const int TB = r.tile_rows();
+      i64 blocks = std::min<i64>((M + TB - 1) / TB, (i64)num_sms() * 12);
+      blocks = std::max<i64>(1, std::min<i64>(blocks, (i64)(kHeapBudget / (perThread * TB))));
       const i64 G = blocks * TB;
       double *hk = r.sc.slot[5].template get<double>(G * cap);
       int *hn = r.sc.slot[6].template get<int>(G * cap);
-      const size_t smem = sizeof(TT) * (size_t)TB * (size_t)r.D;
+      const size_t smem = rowBytes * (TB + 1);
       auto go = [&](auto kern) {
         VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         VLB_LAUNCH("km_ann", r.s, (kern<<<(int)blocks, TB, smem, r.s>>>(r.X, r.N, (int)r.D, centers, tr, maxComp,
-                                                                         update, assign, dist, hk, hn, cap, err)));
+                                                                         update, assign, dist, hk, hn, cap, err,
+                                                                         list, count)));
       };
-      if (r.vec(L)) go(k_km_ann<TT, L, true>);
-      else go(k_km_ann<TT, L, false>);
+      if (r.vec(L)) go(k_km_ann<TT, L, true, false>);
+      else go(k_km_ann<TT, L, false, false>);
     }
   };
 
   template <typename TT, int L>
-  struct QuantLaunch {
-    static void run(KMeansRun &r, const TT *centers, uint32_t *assign) {
+  struct NearestLaunch {
+    static void run(KMeansRun &r, const TT *centers, int mode, int update, uint32_t *assign, TT *dist,
+                    uint32_t *list, unsigned long long *count) {
       const int TB = r.tile_rows();
       const i64 blocks = std::min<i64>((r.N + TB - 1) / TB, (i64)num_sms() * 16);
-      const size_t smem = sizeof(TT) * (size_t)TB * (size_t)r.D;
+      constexpr int TC = sizeof(TT) == 4 ? 8 : 4;
+      // Centre rows staged per chunk of KC (a multiple of TC, about 16 KB).
+      const size_t rowBytes = sizeof(TT) * (size_t)r.D;
+      int KC = (int)std::max<size_t>(1, (size_t)16384 / rowBytes) / TC * TC;
+      KC = std::max(TC, std::min(KC, 64));
+      const size_t smem = align16(rowBytes * (TB + 1)) + rowBytes * KC;
+      // The distances' rounding: a difference, a square and at most D - 1
+      // additions per distance, each rounded once (unit roundoff u), bound
+      // the error of a distance d by (D + 6) u d; a relative gap above
+      // 2 (D + 8) u between the least and the second least distance keeps
+      // the least one's exact value below every other's and below the
+      // search's lower bounds for the other centres.
+      const TT margin = (TT)((double)(r.D + 8) * (sizeof(TT) == 4 ? 0x1p-23 : 0x1p-52));
       auto go = [&](auto kern) {
         VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        VLB_LAUNCH("km_quantize", r.s, (kern<<<(int)blocks, TB, smem, r.s>>>(r.X, r.N, (int)r.D, centers,
-                                                                              (int)r.K, assign)));
+        VLB_LAUNCH(mode == kNearestQuantize ? "km_quantize" : "km_screen", r.s,
+                   (kern<<<(int)blocks, TB, smem, r.s>>>(r.X, r.N, (int)r.D, centers, (int)r.K, KC, mode, update,
+                                                         assign, dist, margin, list, count)));
       };
-      if (r.vec(L)) go(k_km_quantize<TT, L, true>);
-      else go(k_km_quantize<TT, L, false>);
+      if (r.vec(L)) go(k_km_nearest<TT, L, true, TC>);
+      else go(k_km_nearest<TT, L, false, TC>);
     }
   };
 
@@ -744,8 +968,8 @@ struct KMeansRun {
     const size_t bsm = sizeof(i64) * (size_t)K;
     VLB_CUDA(cudaFuncSetAttribute(k_km_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
     VLB_LAUNCH("km_scatter", s, k_km_scatter<<<nb, 32, bsm, s>>>(assign, N, (int)K, nb, H, off, order));
-    VLB_LAUNCH("km_sums", s, k_km_sums<T><<<blocks_for(K * D, kKmThreads), kKmThreads, 0, s>>>(
-                                 X, (int)D, (int)K, off, order, centers));
+    const int R = (int)std::max<i64>(1, std::min<i64>(64, kSumTileElems / D));
+    VLB_LAUNCH("km_sums", s, k_km_sums<T><<<(int)K, kSumThreads, 0, s>>>(X, (int)D, R, off, order, centers));
     for (i64 c = 0; c < K; ++c) {
       if (hc[(size_t)c] != 0) continue;
       const i64 x = (i64)vl_rand_uindex(rand, (vl_uindex)N);
@@ -758,12 +982,29 @@ struct KMeansRun {
   double refine(const KMeansSettings &cfg, T *centers, uint32_t *assign) {
     T *dist = sc.slot[7].get<T>(N);
     int *err = sc.slot[13].get<int>(1);
+    // With a budget of at least K comparisons (one tree) the search is exact
+    // up to ties: screen every row by brute force, search the near ties.
+    const bool screen = K <= cfg.maxNumComparisons;
+    uint32_t *list = sc.slot[15].get<uint32_t>(N);
+    unsigned long long *cnt = sc.slot[16].get<unsigned long long>(1);
     VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     double energy = INFINITY, prev = INFINITY, initial = INFINITY;
     for (i64 it = 0;; ++it) {
       const KdDev tr = tree(centers);
-      by_lanes<AnnLaunch>(*this, (const T *)centers, tr, (i64)cfg.maxNumComparisons, it > 0 ? 1 : 0, assign, dist,
-                          err);
+      const int update = it > 0 ? 1 : 0;
+      if (screen) {
+        VLB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
+        by_lanes<NearestLaunch>(*this, (const T *)centers, (int)kNearestScreen, update, assign, dist, list, cnt);
+        unsigned long long hc = 0;
+        VLB_CUDA(cudaMemcpyAsync(&hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, s));
+        VLB_CUDA(cudaStreamSynchronize(s));
+        if (hc > 0)
+          by_lanes<AnnLaunch>(*this, (const T *)centers, tr, (i64)cfg.maxNumComparisons, update, assign, dist, err,
+                              (const uint32_t *)list, (i64)hc);
+      } else {
+        by_lanes<AnnLaunch>(*this, (const T *)centers, tr, (i64)cfg.maxNumComparisons, update, assign, dist, err,
+                            (const uint32_t *)nullptr, (i64)0);
+      }
       energy = this->energy(dist);
       if (it >= cfg.maxNumIterations) break;
       if (energy == prev) break;
@@ -790,6 +1031,7 @@ template <typename T>
 double kmeans_ann(const T *X, i64 N, i64 D, i64 K, const KMeansSettings &cfg, int lanes, T *centers,
                   uint32_t *assign, cudaStream_t s) {
   VLB_CHECK(N >= 1 && D >= 1 && K >= 1, VL_ERR_BAD_ARG, "k-means: empty data or no centres");
+  VLB_CHECK(D <= (i64)kSumThreads * kSumDims, VL_ERR_BAD_ARG, "k-means initialisation: dimension above 1024");
   VLB_CHECK(N >= K, VL_ERR_BAD_ARG, "k-means: fewer data points than centres");
   VLB_CHECK(N < ((i64)1 << 32) && K <= 16384, VL_ERR_BAD_ARG, "k-means: too many data points or centres");
   VLB_CHECK(cfg.numRepetitions >= 1, VL_ERR_BAD_ARG, "k-means: at least one repetition");
@@ -805,7 +1047,9 @@ double kmeans_ann(const T *X, i64 N, i64 D, i64 K, const KMeansSettings &cfg, in
         VLB_CUDA(cudaMemcpyAsync(centers, work, sizeof(T) * K * D, cudaMemcpyDeviceToDevice, s));
     }
   }
-  r.template by_lanes<KMeansRun<T>::template QuantLaunch>(r, (const T *)centers, assign);
+  r.template by_lanes<KMeansRun<T>::template NearestLaunch>(r, (const T *)centers, (int)kNearestQuantize, 0, assign,
+                                                             (T *)nullptr, (uint32_t *)nullptr,
+                                                             (unsigned long long *)nullptr);
   return bestEnergy;
 }
 
