@@ -1,8 +1,10 @@
 """The recognition app's descriptor prologue on the GPU (PCA learning,
 projection, renormalisation and the 'xy' geometric extension,
 apps/recognition/trainEncoder.m:150-171, encodeImage.m:91-103) against the
-float64 NumPy restatement in oracle.oracle.  The library projects in fp32:
-relative error bound 1e-5 per descriptor; the PCA (fp64 covariance, Jacobi
+float64 NumPy restatement in oracle.oracle.  The library projects on the
+tensor cores in scaled fp16x3 (rows on 16-byte boundaries with a multiple of 4
+input dimensions) or on the CUDA cores in fp32: relative error bound 1e-5 per
+descriptor either way; the PCA (fp64 covariance, Jacobi
 eigenvectors) matches to 1e-6 where the eigenvalues are well separated."""
 import numpy as np
 import pytest
@@ -90,8 +92,10 @@ def test_pca_prologue_then_fisher(vl, restatement):
 
 
 def test_pca_project_unaligned_rows(vl):
-    """Rows that do not start on 16-byte boundaries take the plain-load path;
-    the result is bit-equal to the bulk-copy path on the same values."""
+    """Rows that do not start on 16-byte boundaries take the CUDA-core kernel
+    (plain loads, fp32); aligned rows take the tensor-core kernel (fp16x3).
+    Both are within the 1e-5 per-descriptor bound of the float64 restatement,
+    and so within 2e-5 of each other."""
     import torch
     r = np.random.default_rng(9)
     x = _data(5000, 128, seed=10)
@@ -105,4 +109,10 @@ def test_pca_project_unaligned_rows(vl):
     b = torch.empty((5000, 80), device="cuda")
     vl.pca_project_device(a, xu, P, c, True)
     vl.pca_project_device(b, torch.from_numpy(x).cuda(), P, c, True)
-    assert torch.equal(a, b)
+    from oracle.oracle import pca_project
+    want = pca_project(x, P.cpu().numpy(), c.cpu().numpy(), True)[:, :80]
+    for got in (a, b):
+        g = got.cpu().numpy().astype(np.float64)
+        assert (np.linalg.norm(g - want, axis=1) / np.linalg.norm(want, axis=1)).max() < 1e-5
+    d = (a - b).double().norm(dim=1) / b.double().norm(dim=1)
+    assert float(d.max()) < 2e-5

@@ -192,6 +192,283 @@ __global__ void __launch_bounds__(16 * NC, 2) k_pca_project(const PcaParams p) {
   }
 }
 
+// ------------------------------------------------ tensor-core projection
+// The projection as a tcgen05 GEMM per tile of 128 descriptors, in scaled
+// fp16x3 (two fp16 parts per operand, products hi.hi + hi.lo + lo.hi with fp32
+// accumulation in TMEM):
+//  - x' = x - c per descriptor is scaled by 2^s (s per row: max |x'| into
+//    [2^14, 2^15)), P by 2^g (one g: max |P| into [2^14, 2^15)); the epilogue
+//    undoes both exactly, so fp16's range holds any input and each operand
+//    keeps 22 significant bits;
+//  - roles: warps 0-7 producers (16 rows each; a lane converts 4 dimensions of
+//    a row: coalesced 512-byte row loads, a warp max for the row's scale, the
+//    hi/lo split, stores into the K-major 64-byte-swizzled A tile), warps 8-11
+//    epilogue (one row per thread: TMEM -> scale -> renormalisation -> 'xy'
+//    -> store), warp 12 TMEM allocation and the MMA issue;
+//  - two A stages and two TMEM accumulators of np columns; P's image stays in
+//    shared memory for the CTA's life.
+constexpr int kPtThreads = 416;
+constexpr int kPtOffsCache = 2048;  // image offsets cached in shared memory up to this many images
+
+struct PcaTcParams {
+  float *out;
+  int ldo, din, dout, renorm, nka, np, vec_out, offs_cached;  // vec_out: 4, 2 or 1 floats per store
+  i64 N, nimg, ntiles;
+  const float *X, *P, *c, *frames, *sizes;
+  const i64 *offs;
+  int *err;
+};
+
+// Dynamic shared memory from a 1024-aligned base: A stages (2 x nka x 16 KB:
+// hi atoms then lo atoms), P image (hi nka x np x 64 B, then lo), control
+// block (barriers, flags, row exponents), image offsets.
+__host__ __device__ inline size_t pt_a_bytes(int nka) { return (size_t)2 * nka * 16384; }
+__host__ __device__ inline size_t pt_p_bytes(int nka, int np) { return (size_t)nka * np * 128; }
+constexpr size_t kPtCtl = 128 + 2 * 128 * sizeof(int);
+__host__ inline size_t pt_smem(int nka, int np, bool cache, i64 nimg) {
+  return 1024 + pt_a_bytes(nka) + pt_p_bytes(nka, np) + kPtCtl + (cache ? sizeof(i64) * (size_t)(nimg + 1) : 0);
+}
+
+__device__ __forceinline__ float pow2f(int e) {  // 2^e for e in [-126, 127]
+  return __int_as_float((e + 127) << 23);
+}
+
+__global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
+  using namespace tc;
+  extern __shared__ __align__(16) unsigned char pt_raw[];
+  const uint32_t raw_s = smem_u32(pt_raw);
+  const uint32_t base_s = (raw_s + 1023u) & ~1023u;
+  unsigned char *base = pt_raw + (base_s - raw_s);
+  const int nka = p.nka, np = p.np;
+  const uint32_t a_s = base_s;                         // stage st: hi at a_s + st*nka*16K, lo + nka*8K
+  const uint32_t p_s = base_s + (uint32_t)pt_a_bytes(nka);  // P hi; lo at + nka*np*64
+  unsigned char *ctl = base + pt_a_bytes(nka) + pt_p_bytes(nka, np);
+  uint64_t *full = (uint64_t *)ctl;       // [2], producers' arrivals
+  uint64_t *accf = full + 2;              // [2], MMA commit
+  uint64_t *acce = full + 4;              // [2], epilogue arrivals
+  volatile int *s_abort = (volatile int *)(full + 6);
+  uint32_t *s_tmem = (uint32_t *)(full + 7);
+  int *s_g = (int *)(full + 8);
+  float *s_red = (float *)(full + 9);     // 13 warp maxima (up to full + 16)
+  int *sexp = (int *)(ctl + 128);         // [2][128] row exponents
+  i64 *soffs = (i64 *)(ctl + kPtCtl);
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  if (tid == 0) {
+    mbar_init(&full[0], 256);
+    mbar_init(&full[1], 256);
+    mbar_init(&accf[0], 1);
+    mbar_init(&accf[1], 1);
+    mbar_init(&acce[0], 128);
+    mbar_init(&acce[1], 128);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // P's scale: g with max |P| 2^g in [2^14, 2^15).
+  float mx = 0.f;
+  const int nP = p.dout * p.din;
+  for (int e = tid; e < nP; e += kPtThreads) mx = fmaxf(mx, fabsf(__ldg(p.P + e)));
+  mx = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(mx)));
+  if (lane == 0) s_red[warp] = mx;
+  if (warp == 12) tmem_alloc(s_tmem, 256);
+  if (warp == 12) tmem_relinquish();
+  __syncthreads();
+  if (tid == 0) {
+    float m = 0.f;
+    for (int w = 0; w < kPtThreads / 32; ++w) m = fmaxf(m, s_red[w]);
+    int e = 0;
+    if (m > 0.f) frexpf(m, &e);
+    *s_g = m > 0.f ? max(-126, min(126, 15 - e)) : 0;
+  }
+  __syncthreads();
+  const int g = *s_g;
+  {
+    // P image: row n (output), element k (input dimension), zero padded.
+    const float sg = pow2f(g);
+    const int kmax = nka * 32;
+    for (int e = tid; e < np * kmax; e += kPtThreads) {
+      const int n = e / kmax, k = e - n * kmax;
+      const float v = (n < p.dout && k < p.din) ? __ldg(p.P + (i64)n * p.din + k) * sg : 0.f;
+      const __half hi = __float2half_rn(v);
+      const __half lo = __float2half_rn(v - __half2float(hi));
+      const uint32_t off = (uint32_t)(k >> 5) * (uint32_t)np * 64u + kmajor_sw64_off((uint32_t)n, (uint32_t)((k & 31) >> 3)) +
+                           (uint32_t)(k & 7) * 2u;
+      *(__half *)(base + pt_a_bytes(nka) + off) = hi;
+      *(__half *)(base + pt_a_bytes(nka) + (size_t)nka * np * 64 + off) = lo;
+    }
+    if (p.offs_cached)
+      for (i64 i = tid; i <= p.nimg; i += kPtThreads) soffs[i] = p.offs[i];
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  if (warp < 8) {
+    // ------------------------------------------------------- producers
+    const int k0 = 4 * lane;
+    const bool in = k0 < p.din, pad = k0 < nka * 32;
+    float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (in) cv = __ldg((const float4 *)(p.c + k0));
+    const uint32_t aoff = (uint32_t)(lane >> 3) * 8192u;  // atom of this lane's 4 dimensions
+    const uint32_t chunk = (uint32_t)((lane & 7) >> 1), half8 = (uint32_t)(lane & 1) * 8u;
+    int tt = 0;
+    for (i64 t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tt) {
+      const int st = tt & 1;
+      if (tt >= 2 && !mbar_wait(&acce[st], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 11)) break;
+      const i64 r0 = t * 128 + 16 * warp;
+      float4 xv[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const i64 row = r0 + u;
+        xv[u] = (in && row < p.N) ? __ldg((const float4 *)(p.X + row * p.din + k0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      const uint32_t ahi = a_s + (uint32_t)st * (uint32_t)nka * 16384u, alo = ahi + (uint32_t)nka * 8192u;
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const bool live = in && r0 + u < p.N;
+        const float v0 = live ? __fsub_rn(xv[u].x, cv.x) : 0.f, v1 = live ? __fsub_rn(xv[u].y, cv.y) : 0.f;
+        const float v2 = live ? __fsub_rn(xv[u].z, cv.z) : 0.f, v3 = live ? __fsub_rn(xv[u].w, cv.w) : 0.f;
+        const float m = fmaxf(fmaxf(fabsf(v0), fabsf(v1)), fmaxf(fabsf(v2), fabsf(v3)));
+        const float rm = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m)));
+        int e = 0;
+        if (rm > 0.f) frexpf(rm, &e);
+        const int sx = rm > 0.f ? max(-126, min(126, 15 - e)) : 0;
+        const float f = pow2f(sx);
+        uint32_t h0, l0, h1, l1;
+        split2<true>(v0 * f, v1 * f, h0, l0);
+        split2<true>(v2 * f, v3 * f, h1, l1);
+        const uint32_t rl = (uint32_t)(16 * warp + u);
+        if (pad) {
+          const uint32_t off = aoff + kmajor_sw64_off(rl, chunk) + half8;
+          st_shared_v2(ahi + off, h0, h1);
+          st_shared_v2(alo + off, l0, l1);
+        }
+        if (lane == 0) sexp[st * 128 + rl] = sx;
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(&full[st]);
+    }
+  } else if (warp < 12) {
+    // -------------------------------------------------------- epilogue
+    const int ew = warp - 8, rl = 32 * ew + lane;
+    const int nch = (np + 31) / 32;
+    int tt = 0;
+    i64 img = 0;
+    for (i64 t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tt) {
+      const int buf = tt & 1;
+      if (!mbar_wait(&accf[buf], (tt >> 1) & 1, s_abort, p.err, 12)) break;
+      tc_fence_after();
+      const i64 row = t * 128 + rl;
+      const bool valid = row < p.N;
+      const int sx = sexp[buf * 128 + rl];
+      // acc 2^-(s + g), as two exact power-of-two factors.
+      const float f1 = pow2f(-sx), f2 = pow2f(-g);
+      const uint32_t taddr = tmem + (uint32_t)(buf * 128) + ((uint32_t)(32 * ew) << 16);
+      float inv = 1.f;
+      if (p.renorm) {
+        float ss = 0.f;
+        for (int ch = 0; ch < nch; ++ch) {
+          uint32_t v[32];
+          tmem_ld32(taddr + (uint32_t)(ch * 32), v);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const float y = __uint_as_float(v[j]) * f1 * f2;
+            if (ch * 32 + j < p.dout) ss = __fmaf_rn(y, y, ss);
+          }
+        }
+        inv = 1.f / fmaxf(1e-12f, sqrtf(ss));
+      }
+      float *o = p.out + row * p.ldo;
+      for (int ch = 0; ch < nch; ++ch) {
+        uint32_t v[32];
+        tmem_ld32(taddr + (uint32_t)(ch * 32), v);
+        tmem_wait_ld();
+        if (!valid) continue;
+        const int j0 = ch * 32;
+        if (p.vec_out == 4) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            if (j0 + 4 * q < p.dout) {
+              float4 w;
+              w.x = __uint_as_float(v[4 * q]) * f1 * f2 * inv;
+              w.y = __uint_as_float(v[4 * q + 1]) * f1 * f2 * inv;
+              w.z = __uint_as_float(v[4 * q + 2]) * f1 * f2 * inv;
+              w.w = __uint_as_float(v[4 * q + 3]) * f1 * f2 * inv;
+              *(float4 *)(o + j0 + 4 * q) = w;
+            }
+          }
+        } else if (p.vec_out == 2) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            if (j0 + 2 * q < p.dout) {
+              float2 w;
+              w.x = __uint_as_float(v[2 * q]) * f1 * f2 * inv;
+              w.y = __uint_as_float(v[2 * q + 1]) * f1 * f2 * inv;
+              *(float2 *)(o + j0 + 2 * q) = w;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (j0 + j < p.dout) o[j0 + j] = __uint_as_float(v[j]) * f1 * f2 * inv;
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[buf]);
+      if (p.frames && valid) {
+        // The last image whose first row is <= row (offsets non-decreasing).
+        i64 lo = img, hi = p.nimg;
+        const i64 *of = p.offs_cached ? soffs : p.offs;
+        if (of[lo] > row) lo = 0;
+        while (hi - lo > 1) {
+          const i64 mid = (lo + hi) / 2;
+          if (of[mid] <= row) lo = mid;
+          else hi = mid;
+        }
+        img = lo;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const float sz = __ldg(p.sizes + 2 * img + i);
+          o[p.dout + i] = (__ldg(p.frames + 2 * row + i) - sz * 0.5f) * (1.f / sz);
+        }
+      }
+    }
+  } else if (lane == 0) {
+    // ------------------------------------------------------------- MMA
+    const uint32_t idesc = idesc_f16(128, np, false, false);
+    const uint32_t phi = p_s, plo = p_s + (uint32_t)nka * (uint32_t)np * 64u;
+    int tt = 0;
+    for (i64 t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tt) {
+      const int buf = tt & 1;
+      if (!mbar_wait(&acce[buf], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 13)) break;
+      if (!mbar_wait(&full[buf], (tt >> 1) & 1, s_abort, p.err, 14)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + (uint32_t)(buf * 128);
+      const uint32_t ahi = a_s + (uint32_t)buf * (uint32_t)nka * 16384u, alo = ahi + (uint32_t)nka * 8192u;
+      for (int a = 0; a < nka; ++a) {
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+          const uint64_t ah = sdesc(ahi + (uint32_t)a * 8192u + ks * 32, 16, 512, kSw64);
+          const uint64_t al = sdesc(alo + (uint32_t)a * 8192u + ks * 32, 16, 512, kSw64);
+          const uint64_t bh = sdesc(phi + (uint32_t)a * (uint32_t)np * 64u + ks * 32, 16, 512, kSw64);
+          const uint64_t bl = sdesc(plo + (uint32_t)a * (uint32_t)np * 64u + ks * 32, 16, 512, kSw64);
+          mma_bf16(d, ah, bh, idesc, (a > 0 || ks > 0) ? 1u : 0u);
+          mma_bf16(d, ah, bl, idesc, 1u);
+          mma_bf16(d, al, bh, idesc, 1u);
+        }
+      }
+      mma_commit(&accf[buf]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 12) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
 // Per-dimension sums (fp64) of a slab of rows: slab b writes sums[b][d].
 __global__ void k_pca_colsum(const float *__restrict__ X, int din, i64 N, i64 slab, double *__restrict__ sums) {
   const int d = threadIdx.x;
@@ -324,6 +601,28 @@ void pca_project(float *out, i64 ldo, const float *X, i64 din, i64 N, i64 dout, 
   p.out = out; p.ldo = (int)ldo; p.din = (int)din; p.dout = (int)dout; p.renorm = renorm ? 1 : 0;
   p.N = N; p.nimg = nimg; p.X = X; p.P = P; p.c = c; p.frames = frames; p.sizes = sizes; p.offs = doffs;
   p.err = derr;
+  if (din % 4 == 0 && (uintptr_t)X % 16 == 0 && (uintptr_t)c % 16 == 0) {
+    // Tensor-core path: fp16x3 tcgen05 GEMM with the fused epilogue.
+    PcaTcParams q;
+    q.out = out; q.ldo = (int)ldo; q.din = (int)din; q.dout = (int)dout; q.renorm = renorm ? 1 : 0;
+    q.nka = (int)((din + 31) / 32);
+    q.np = (int)((dout + 15) / 16 * 16);
+    q.vec_out = (ldo % 4 == 0 && dout % 4 == 0 && (uintptr_t)out % 16 == 0)  ? 4
+                : (ldo % 2 == 0 && dout % 2 == 0 && (uintptr_t)out % 8 == 0) ? 2
+                                                                               : 1;
+    q.N = N; q.nimg = frames ? nimg : 0; q.ntiles = (N + 127) / 128;
+    q.offs_cached = (frames && nimg + 1 <= kPtOffsCache) ? 1 : 0;
+    q.X = X; q.P = P; q.c = c; q.frames = frames; q.sizes = sizes; q.offs = doffs; q.err = derr;
+    const size_t smem = pt_smem(q.nka, q.np, q.offs_cached != 0, q.nimg);
+    const int grid = (int)std::min<i64>(q.ntiles, (i64)sm_count());
+    VLB_CUDA(cudaFuncSetAttribute(k_pca_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    VLB_LAUNCH("pca_project_tc", s, k_pca_tc<<<grid, kPtThreads, smem, s>>>(q));
+    int herr = 0;
+    VLB_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+    VLB_CHECK(herr == 0, VL_ERR_ALLOC, "PCA projection: a pipeline wait timed out on the device");
+    return;
+  }
   const bool bulk = (din % 4) == 0 && ((uintptr_t)X % 16) == 0;
   const size_t tile = sizeof(float) * (size_t)kPcaRows * pca_ldx((int)din);
   const size_t smem = 128 + sizeof(float) * ((size_t)((din + 3) / 4 * 4) * pca_ldp((int)dout) + pca_ldx((int)din)) +
