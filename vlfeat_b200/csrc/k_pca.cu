@@ -208,11 +208,11 @@ __global__ void __launch_bounds__(16 * NC, 2) k_pca_project(const PcaParams p) {
 //  - two A stages and two TMEM accumulators of np columns; P's image stays in
 //    shared memory for the CTA's life.
 constexpr int kPtThreads = 416;
-constexpr int kPtOffsCache = 2048;  // image offsets cached in shared memory up to this many images
 
 struct PcaTcParams {
   float *out;
-  int ldo, din, dout, renorm, nka, np, vec_out, offs_cached;  // vec_out: 4, 2 or 1 floats per store
+  int ldo, din, dout, renorm, nka, np, vec_out;  // vec_out: 4, 2 or 1 floats per store
+  int vec_xy;                                    // frames and xy outputs as float2
   i64 N, nimg, ntiles;
   const float *X, *P, *c, *frames, *sizes;
   const i64 *offs;
@@ -221,13 +221,11 @@ struct PcaTcParams {
 
 // Dynamic shared memory from a 1024-aligned base: A stages (2 x nka x 16 KB:
 // hi atoms then lo atoms), P image (hi nka x np x 64 B, then lo), control
-// block (barriers, flags, row exponents), image offsets.
+// block (barriers, flags, row exponents, the image of each stage's first row).
 __host__ __device__ inline size_t pt_a_bytes(int nka) { return (size_t)2 * nka * 16384; }
 __host__ __device__ inline size_t pt_p_bytes(int nka, int np) { return (size_t)nka * np * 128; }
-constexpr size_t kPtCtl = 128 + 2 * 128 * sizeof(int);
-__host__ inline size_t pt_smem(int nka, int np, bool cache, i64 nimg) {
-  return 1024 + pt_a_bytes(nka) + pt_p_bytes(nka, np) + kPtCtl + (cache ? sizeof(i64) * (size_t)(nimg + 1) : 0);
-}
+constexpr size_t kPtCtl = 128 + 2 * 128 * sizeof(int) + 16;
+__host__ inline size_t pt_smem(int nka, int np) { return 1024 + pt_a_bytes(nka) + pt_p_bytes(nka, np) + kPtCtl; }
 
 __device__ __forceinline__ float pow2f(int e) {  // 2^e for e in [-126, 127]
   return __int_as_float((e + 127) << 23);
@@ -251,7 +249,7 @@ __global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
   int *s_g = (int *)(full + 8);
   float *s_red = (float *)(full + 9);     // 13 warp maxima (up to full + 16)
   int *sexp = (int *)(ctl + 128);         // [2][128] row exponents
-  i64 *soffs = (i64 *)(ctl + kPtCtl);
+  i64 *timg = (i64 *)(ctl + 128 + 2 * 128 * sizeof(int));  // [2] image of each stage's first row
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   if (tid == 0) {
     mbar_init(&full[0], 256);
@@ -295,8 +293,6 @@ __global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
       *(__half *)(base + pt_a_bytes(nka) + off) = hi;
       *(__half *)(base + pt_a_bytes(nka) + (size_t)nka * np * 64 + off) = lo;
     }
-    if (p.offs_cached)
-      for (i64 i = tid; i <= p.nimg; i += kPtThreads) soffs[i] = p.offs[i];
   }
   fence_proxy_async_smem();
   tc_fence_before();
@@ -312,16 +308,42 @@ __global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
     const uint32_t aoff = (uint32_t)(lane >> 3) * 8192u;  // atom of this lane's 4 dimensions
     const uint32_t chunk = (uint32_t)((lane & 7) >> 1), half8 = (uint32_t)(lane & 1) * 8u;
     int tt = 0;
-    for (i64 t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tt) {
-      const int st = tt & 1;
-      if (tt >= 2 && !mbar_wait(&acce[st], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 11)) break;
+    // The rows of the next tile are loaded as soon as the current tile's are
+    // converted, before waiting for a free stage, so their latency overlaps
+    // that wait.
+    float4 xv[16];
+    auto load = [&](i64 t) {
       const i64 r0 = t * 128 + 16 * warp;
-      float4 xv[16];
 #pragma unroll
       for (int u = 0; u < 16; ++u) {
         const i64 row = r0 + u;
-        xv[u] = (in && row < p.N) ? __ldg((const float4 *)(p.X + row * p.din + k0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        xv[u] = (in && t < p.ntiles && row < p.N) ? __ldg((const float4 *)(p.X + row * p.din + k0))
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
       }
+    };
+    load(blockIdx.x);
+    i64 pimg = 0;  // image of the previous tile's first row (rows only increase)
+    for (i64 t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tt) {
+      const int st = tt & 1;
+      if (tt >= 2 && !mbar_wait(&acce[st], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 11)) break;
+      if (p.frames && tid == 0) {
+        // The last image whose first row is <= the tile's first row: gallop
+        // forward from the previous tile's, then bisect (offs[nimg] = N).
+        const i64 f0 = t * 128;
+        i64 lo = pimg, hi = lo + 1, step = 1;
+        while (hi < p.nimg && __ldg(p.offs + hi) <= f0) {
+          lo = hi;
+          step *= 2;
+          hi = min(p.nimg, lo + step);
+        }
+        while (hi - lo > 1) {
+          const i64 mid = (lo + hi) / 2;
+          if (__ldg(p.offs + mid) <= f0) lo = mid;
+          else hi = mid;
+        }
+        timg[st] = pimg = lo;
+      }
+      const i64 r0 = t * 128 + 16 * warp;
       const uint32_t ahi = a_s + (uint32_t)st * (uint32_t)nka * 16384u, alo = ahi + (uint32_t)nka * 8192u;
 #pragma unroll
       for (int u = 0; u < 16; ++u) {
@@ -347,13 +369,13 @@ __global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
       }
       fence_proxy_async_smem();
       mbar_arrive(&full[st]);
+      load(t + gridDim.x);
     }
   } else if (warp < 12) {
     // -------------------------------------------------------- epilogue
     const int ew = warp - 8, rl = 32 * ew + lane;
     const int nch = (np + 31) / 32;
     int tt = 0;
-    i64 img = 0;
     for (i64 t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++tt) {
       const int buf = tt & 1;
       if (!mbar_wait(&accf[buf], (tt >> 1) & 1, s_abort, p.err, 12)) break;
@@ -361,6 +383,7 @@ __global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
       const i64 row = t * 128 + rl;
       const bool valid = row < p.N;
       const int sx = sexp[buf * 128 + rl];
+      const i64 img0 = p.frames ? timg[buf] : 0;  // read before the stage is released below
       // acc 2^-(s + g), as two exact power-of-two factors.
       const float f1 = pow2f(-sx), f2 = pow2f(-g);
       const uint32_t taddr = tmem + (uint32_t)(buf * 128) + ((uint32_t)(32 * ew) << 16);
@@ -417,20 +440,19 @@ __global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
       tc_fence_before();
       mbar_arrive(&acce[buf]);
       if (p.frames && valid) {
-        // The last image whose first row is <= row (offsets non-decreasing).
-        i64 lo = img, hi = p.nimg;
-        const i64 *of = p.offs_cached ? soffs : p.offs;
-        if (of[lo] > row) lo = 0;
-        while (hi - lo > 1) {
-          const i64 mid = (lo + hi) / 2;
-          if (of[mid] <= row) lo = mid;
-          else hi = mid;
-        }
-        img = lo;
+        // Forward from the image of the tile's first row.
+        i64 img = img0;
+        while (img + 1 < p.nimg && __ldg(p.offs + img + 1) <= row) ++img;
+        if (p.vec_xy) {
+          const float2 fr = __ldg((const float2 *)(p.frames + 2 * row));
+          const float2 sz = __ldg((const float2 *)(p.sizes + 2 * img));
+          *(float2 *)(o + p.dout) = make_float2((fr.x - sz.x * 0.5f) * (1.f / sz.x), (fr.y - sz.y * 0.5f) * (1.f / sz.y));
+        } else {
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const float sz = __ldg(p.sizes + 2 * img + i);
-          o[p.dout + i] = (__ldg(p.frames + 2 * row + i) - sz * 0.5f) * (1.f / sz);
+          for (int i = 0; i < 2; ++i) {
+            const float sz = __ldg(p.sizes + 2 * img + i);
+            o[p.dout + i] = (__ldg(p.frames + 2 * row + i) - sz * 0.5f) * (1.f / sz);
+          }
         }
       }
     }
@@ -611,9 +633,10 @@ void pca_project(float *out, i64 ldo, const float *X, i64 din, i64 N, i64 dout, 
                 : (ldo % 2 == 0 && dout % 2 == 0 && (uintptr_t)out % 8 == 0) ? 2
                                                                                : 1;
     q.N = N; q.nimg = frames ? nimg : 0; q.ntiles = (N + 127) / 128;
-    q.offs_cached = (frames && nimg + 1 <= kPtOffsCache) ? 1 : 0;
+    q.vec_xy = (frames && (uintptr_t)frames % 8 == 0 && (uintptr_t)sizes % 8 == 0 && ldo % 2 == 0 &&
+                dout % 2 == 0 && (uintptr_t)out % 8 == 0) ? 1 : 0;
     q.X = X; q.P = P; q.c = c; q.frames = frames; q.sizes = sizes; q.offs = doffs; q.err = derr;
-    const size_t smem = pt_smem(q.nka, q.np, q.offs_cached != 0, q.nimg);
+    const size_t smem = pt_smem(q.nka, q.np);
     const int grid = (int)std::min<i64>(q.ntiles, (i64)sm_count());
     VLB_CUDA(cudaFuncSetAttribute(k_pca_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     VLB_LAUNCH("pca_project_tc", s, k_pca_tc<<<grid, kPtThreads, smem, s>>>(q));
