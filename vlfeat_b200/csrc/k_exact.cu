@@ -823,20 +823,77 @@ __global__ void k_fill(T *__restrict__ p, i64 n, T v) {
   if (i < n) p[i] = v;
 }
 
-// The next centre, vl/kmeans.c:631-641, by one thread: the energy (sum of
-// minDist in order), then the first x with acc >= thresh * energy, or N - 1.
+// The next centre, vl/kmeans.c:631-641: the energy (sum of minDist in
+// order), then the first x with acc >= thresh * energy, or N - 1.
+// The scan's running sum acc is the energy's own prefix sum (both add minDist
+// in order from 0).  So the energy pass keeps every 32nd prefix; the scan
+// bisects these checkpoints (prefixes of non-negative terms never decrease, and
+// a NaN prefix, then every later one, fails the test as in the loop) and
+// re-adds at most 32 terms from the checkpoint before, which reproduces the
+// prefixes exactly.  One sequential pass of N additions instead of two.
+// One block: thread 0 adds in order out of shared memory while the warps on
+// the other three schedulers stage the next chunk of minDist, so the chain
+// waits on no load and shares its scheduler with no loader.
+constexpr int kKppCk = 32;  // terms per checkpoint
+
 template <typename T>
-__global__ void k_kpp_select(const T *__restrict__ minDist, i64 N, T thresh, i64 *__restrict__ xOut) {
+__global__ void __launch_bounds__(1024) k_kpp_select(const T *__restrict__ minDist, i64 N, T thresh,
+                                                     T *__restrict__ ck, i64 *__restrict__ xOut) {
+  constexpr int kChunk = 16384 / (int)sizeof(T);  // 32 KB of staging in all
+  __shared__ T buf[2][kChunk];
+  const int tid = threadIdx.x;
+  const i64 nch = (N + kChunk - 1) / kChunk;
+  auto stage = [&](i64 ch, int b, int t0, int nt) {
+    const i64 base = ch * kChunk;
+    const int n = (int)min((i64)kChunk, N - base);
+    for (int e = t0; e < n; e += nt) buf[b][e] = minDist[base + e];
+  };
+  stage(0, 0, tid, blockDim.x);
+  __syncthreads();
   T energy = (T)0;
-  for (i64 x = 0; x < N; ++x) energy = add_rn(energy, minDist[x]);
+  for (i64 ch = 0; ch < nch; ++ch) {
+    const int b = (int)(ch & 1);
+    if (tid == 0) {
+      const i64 base = ch * kChunk;
+      const int n = (int)min((i64)kChunk, N - base);
+      int e = 0;
+      for (; e + kKppCk <= n; e += kKppCk) {  // kChunk is a multiple of kKppCk
+#pragma unroll
+        for (int g = 0; g < kKppCk; g += 8) {
+          T v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) v[u] = buf[b][e + g + u];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) energy = add_rn(energy, v[u]);
+        }
+        ck[(base + e) / kKppCk] = energy;
+      }
+      for (; e < n; ++e) energy = add_rn(energy, buf[b][e]);
+    } else if ((tid >> 5) & 3) {
+      const int w = tid >> 5, li = (w - w / 4 - 1) * 32 + (tid & 31), nl = (int)blockDim.x / 4 * 3;
+      if (ch + 1 < nch) stage(ch + 1, b ^ 1, li, nl);
+    }
+    __syncthreads();
+  }
+  if (tid != 0) return;
   const T t = mul_rn(thresh, energy);
-  T acc = (T)0;
-  i64 x = 0;
-  for (; x < N - 1; ++x) {
+  // The first checkpoint j with ck[j] >= t (nck if none); the answer lies in
+  // terms [32 j, 32 j + 32), re-added from checkpoint j - 1.
+  const i64 nck = N / kKppCk;
+  i64 lo = 0, hi = nck;
+  while (lo < hi) {
+    const i64 mid = lo + (hi - lo) / 2;
+    if (ck[mid] >= t) hi = mid;
+    else lo = mid + 1;
+  }
+  T acc = lo > 0 ? ck[lo - 1] : (T)0;
+  i64 x = lo * kKppCk;
+  const i64 end = min(N, x + kKppCk);
+  for (; x < end; ++x) {
     acc = add_rn(acc, minDist[x]);
     if (acc >= t) break;
   }
-  *xOut = x;
+  *xOut = min(x, N - 1);  // none before N - 1: the last row
 }
 
 // centers[c] = X[x] with x the selected row (device) or the first row (host).
@@ -860,6 +917,7 @@ void kmeanspp(const T *X, i64 N, i64 D, i64 K, T *centers, i64 x0, const std::ve
   Scratch &sc = thread_scratch(kArenaExact);
   T *minDist = sc.slot[20].get<T>(N);
   i64 *xdev = sc.slot[21].get<i64>(1);
+  T *ck = sc.slot[22].get<T>(N / kKppCk + 1);
   const T inf = (T)INFINITY;
   VLB_LAUNCH("kpp_fill", s, k_fill<T><<<grid1(N, kThreads), kThreads, 0, s>>>(minDist, N, inf));
   const size_t smem = sizeof(T) * D;
@@ -874,7 +932,7 @@ void kmeanspp(const T *X, i64 N, i64 D, i64 K, T *centers, i64 x0, const std::ve
       case 2: VLB_LAUNCH("kpp_update", s, (k_kpp_update<T, 2><<<grid1(N, kThreads), kThreads, smem, s>>>(X, N, (int)D, ctr, minDist))); break;
       default: VLB_LAUNCH("kpp_update", s, (k_kpp_update<T, 1><<<grid1(N, kThreads), kThreads, smem, s>>>(X, N, (int)D, ctr, minDist))); break;
     }
-    VLB_LAUNCH("kpp_select", s, k_kpp_select<T><<<1, 1, 0, s>>>(minDist, N, thresh[c], xdev));
+    VLB_LAUNCH("kpp_select", s, k_kpp_select<T><<<1, 1024, 0, s>>>(minDist, N, thresh[c], ck, xdev));
   }
 }
 
