@@ -649,6 +649,17 @@ def kmeans_init_throughput(capi, cpu=True, n=1_000_000, n_cpu=25_000):
               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:8]}
     out = {"workload": f"N={n} rows, D=80, K={K}, float32, vl_gmm_init_with_kmeans", "ms": 1e3 * dt,
            "value": n / dt, "unit": "rows/s", "gpu_launches": int(launches), "kernels": shares}
+    # Dominant kernel: the brute-force screen, N x K x D elements per launch at
+    # three separately rounded fp32 operations each (the reference's order, no
+    # fused multiply-add), against the nominal fp32 issue rate of the CUDA cores.
+    scr = prof.get("km_screen")
+    if scr and scr[0] > 0:
+        props = torch.cuda.get_device_properties(0)
+        peak = props.multi_processor_count * 128 * measured_peaks().get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+        ach = 3.0 * n * K * 80 / (scr[1] / scr[0] * 1e-3) / 1e12
+        out["roofline"] = {"kernel": "k_km_nearest (screen)", "bound": "fp32 issue", "achieved": ach,
+                           "peak": peak, "unit": "T fp32 ops/s", "frac": ach / peak,
+                           "ops_per_element": 3}
     if cpu:
         from oracle import oracle as O
         try:

@@ -30,6 +30,7 @@
 
 #include "engine.h"
 #include "exact_math.cuh"
+#include "tc_common.cuh"
 
 extern "C" {
 #include "vl/random.h"
@@ -476,31 +477,76 @@ __global__ void k_km_nearest(const T *__restrict__ X, i64 N, int D, const T *__r
 #pragma unroll
           for (int l = 0; l < L; ++l) acc[t][l] = (T)0;
         int i = 0;
-        for (; i + L <= D; i += L) {
-          T qv[L];
+        if constexpr (sizeof(T) == 4 && L % 2 == 0) {
+          // Packed fp32x2: lanes l and l + 1 of the lane sums in one
+          // instruction each for the difference, the square and the sum,
+          // every half rounded exactly as the scalar operation.
+          constexpr unsigned long long kNeg = 0x8000000080000000ull;
+          unsigned long long ap[TC][L / 2];
 #pragma unroll
-          for (int l = 0; l < L; ++l) qv[l] = q[(i + l) * QS];
+          for (int t = 0; t < TC; ++t)
 #pragma unroll
-          for (int t = 0; t < TC; ++t) {
-            const T *cr = sc + (size_t)min(c0 + t, kn - 1) * D + i;  // a partial tile repeats the last row
-            T cg[L];
-            if constexpr (VEC && (L * sizeof(T)) % 16 == 0) {
-              constexpr int V = 16 / sizeof(T);
+            for (int l = 0; l < L / 2; ++l) ap[t][l] = 0ull;
+          for (; i + L <= D; i += L) {
+            unsigned long long qn[L / 2];  // -q, pairs
 #pragma unroll
-              for (int u = 0; u < L / V; ++u) {
-                const float4 w = reinterpret_cast<const float4 *>(cr)[u];
-                const T *wp = reinterpret_cast<const T *>(&w);
+            for (int l = 0; l < L / 2; ++l) qn[l] = tc::f2u(q[(i + 2 * l) * QS], q[(i + 2 * l + 1) * QS]) ^ kNeg;
 #pragma unroll
-                for (int e = 0; e < V; ++e) cg[u * V + e] = wp[e];
+            for (int t = 0; t < TC; ++t) {
+              const float *cr = (const float *)sc + (size_t)min(c0 + t, kn - 1) * D + i;
+              unsigned long long cp[L / 2];
+              if constexpr (VEC && L % 4 == 0) {
+#pragma unroll
+                for (int u = 0; u < L / 4; ++u) {
+                  const ulonglong2 w = reinterpret_cast<const ulonglong2 *>(cr)[u];
+                  cp[2 * u] = w.x;
+                  cp[2 * u + 1] = w.y;
+                }
+              } else {
+#pragma unroll
+                for (int l = 0; l < L / 2; ++l) cp[l] = tc::f2u(cr[2 * l], cr[2 * l + 1]);
               }
-            } else {
 #pragma unroll
-              for (int l = 0; l < L; ++l) cg[l] = cr[l];
+              for (int l = 0; l < L / 2; ++l) {
+                const unsigned long long dl = tc::add2(cp[l], qn[l]);  // c - q: squared alike
+                ap[t][l] = tc::add2(ap[t][l], tc::mul2(dl, dl));
+              }
             }
+          }
 #pragma unroll
-            for (int l = 0; l < L; ++l) {
-              const T dl = sub_rn(qv[l], cg[l]);
-              acc[t][l] = add_rn(acc[t][l], mul_rn(dl, dl));
+          for (int t = 0; t < TC; ++t)
+#pragma unroll
+            for (int l = 0; l < L / 2; ++l) {
+              acc[t][2 * l] = (T)tc::lo32(ap[t][l]);
+              acc[t][2 * l + 1] = (T)tc::hi32(ap[t][l]);
+            }
+        } else {
+          for (; i + L <= D; i += L) {
+            T qv[L];
+#pragma unroll
+            for (int l = 0; l < L; ++l) qv[l] = q[(i + l) * QS];
+#pragma unroll
+            for (int t = 0; t < TC; ++t) {
+              const T *cr = sc + (size_t)min(c0 + t, kn - 1) * D + i;  // a partial tile repeats the last row
+              T cg[L];
+              if constexpr (VEC && (L * sizeof(T)) % 16 == 0) {
+                constexpr int V = 16 / sizeof(T);
+#pragma unroll
+                for (int u = 0; u < L / V; ++u) {
+                  const float4 w = reinterpret_cast<const float4 *>(cr)[u];
+                  const T *wp = reinterpret_cast<const T *>(&w);
+#pragma unroll
+                  for (int e = 0; e < V; ++e) cg[u * V + e] = wp[e];
+                }
+              } else {
+#pragma unroll
+                for (int l = 0; l < L; ++l) cg[l] = cr[l];
+              }
+#pragma unroll
+              for (int l = 0; l < L; ++l) {
+                const T dl = sub_rn(qv[l], cg[l]);
+                acc[t][l] = add_rn(acc[t][l], mul_rn(dl, dl));
+              }
             }
           }
         }
