@@ -191,201 +191,6 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ X, i64 N, int D,
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
-// Distance of the query (stride qs) to centre row c; VEC reads the row in
-// 16-byte vectors (row starts 16-byte aligned, whole vectors per lane group).
-template <typename T, int L, bool VEC>
-__device__ __forceinline__ T row_dist(const T *q, int qs, const T *__restrict__ c, int D) {
-  if constexpr (VEC && (L * sizeof(T)) % 16 == 0) {
-    return l2_ordered_sv<T, L>(q, qs, c, D);
-  } else {
-    return l2_ordered_s<T, L>(q, qs, c, D);
-  }
-}
-
-// One query of the forest, vl/kdtree.c:774-840 with numNeighbors = 1, the
-// recursion of vl/kdtree.c:583-725 unrolled into a loop.  The search heap of
-// this thread lives at hk[e * G], hn[e * G] (entry e), capacity cap = the
-// tree's node count, which bounds the pushes of one query (each node is
-// pushed at most once).  Heap moves follow vl/heap-def.h: push sifts towards
-// the root while strictly smaller, pop moves the last entry to the root and
-// sifts it down towards the smaller child (the right one on ties) while it
-// is strictly larger.
-template <typename T, int L, bool VEC>
-__device__ __forceinline__ int kd_query(const T *q, int qs, const T *__restrict__ C, int D, const KdDev &tr,
-                                        i64 maxComp, double *__restrict__ hk, int *__restrict__ hn, i64 G,
-                                        int cap, double &bestOut, int *__restrict__ err) {
-  const bool exact = maxComp == 0;
-  i64 comps = 0;
-  int nh = 1;
-  hk[0] = 0.0;
-  hn[0] = 0;
-  bool have = false;
-  double best = 0.0;
-  int bestIdx = 0;
-  while (exact || comps < maxComp) {
-    if (nh == 0) break;
-    // Pop (vl/heap-def.h pop + up).
-    nh -= 1;
-    const double pk = hk[0];
-    const int pn = hn[0];
-    if (nh > 0) {
-      const double lk = hk[(i64)nh * G];
-      const int ln = hn[(i64)nh * G];
-      int i = 0;
-      if (nh > 1) {
-        while (true) {
-          const int l = 2 * i + 1, r = l + 1;
-          if (l >= nh) break;
-          int c;
-          if (r >= nh) {
-            c = l;
-          } else {
-            c = hk[(i64)l * G] < hk[(i64)r * G] ? l : r;
-          }
-          const double ck = hk[(i64)c * G];
-          if (lk > ck) {
-            hk[(i64)i * G] = ck;
-            hn[(i64)i * G] = hn[(i64)c * G];
-            i = c;
-            if (r >= nh) break;  // a lone left child is the last entry: stop
-          } else {
-            break;
-          }
-        }
-      }
-      hk[(i64)i * G] = lk;
-      hn[(i64)i * G] = ln;
-    }
-    if (have && best < pk) break;  // no better neighbour can remain
-    double dist = pk;
-    int n = pn;
-    while (true) {
-      const int lc = tr.lower[n];
-      if (lc < 0) {  // leaf
-        const int b = -lc - 1, e = -tr.upper[n] - 1;
-        for (int it = b; it < e && (exact || comps < maxComp); ++it) {
-          const int di = tr.ent[it];
-          const double dd = (double)row_dist<T, L, VEC>(q, qs, C + (i64)di * D, D);
-          ++comps;
-          if (!have) {
-            have = true;
-            best = dd;
-            bestIdx = di;
-          } else if (best > dd) {
-            best = dd;
-            bestIdx = di;
-          }
-        }
-        break;
-      }
-      const double xv = (double)q[(i64)tr.dim[n] * qs];
-      const double x1 = tr.lb[n], x2 = tr.thr[n], x3 = tr.ub[n];
-      double delta = __dsub_rn(xv, x2);
-      double save = __dadd_rn(dist, __dmul_rn(delta, delta));
-      int next, sv;
-      if (xv <= x2) {
-        next = lc;
-        sv = tr.upper[n];
-        if (xv <= x1) {
-          delta = __dsub_rn(xv, x1);
-          save = __dsub_rn(save, __dmul_rn(delta, delta));
-        }
-      } else {
-        next = tr.upper[n];
-        sv = lc;
-        if (xv > x3) {
-          delta = __dsub_rn(xv, x3);
-          save = __dsub_rn(save, __dmul_rn(delta, delta));
-        }
-      }
-      if (!have || best > save) {
-        if (nh >= cap) {
-          atomicOr(err, 1);  // cannot happen: pushes per query <= nodes
-        } else {
-          int i = nh++;
-          while (i > 0) {
-            const int p = (i - 1) / 2;
-            const double pkk = hk[(i64)p * G];
-            if (save < pkk) {
-              hk[(i64)i * G] = pkk;
-              hn[(i64)i * G] = hn[(i64)p * G];
-              i = p;
-            } else {
-              break;
-            }
-          }
-          hk[(i64)i * G] = save;
-          hn[(i64)i * G] = sv;
-        }
-      }
-      n = next;
-    }
-  }
-  bestOut = best;
-  return bestIdx;
-}
-
-// ANN assignment, vl/kmeans.c:708-771: the forest's nearest centre of each
-// row; after the first iteration (update) the previous assignment is kept
-// unless the new centre is strictly closer.  Persistent blocks of TB rows.
-// With a row list, the kernel serves only rows list[0 .. count).  SH: the
-// search heaps live in shared memory after the query tile (entry e of thread
-// t at e * TB + t), else in global memory (entry e at e * G + global thread).
-template <typename T, int L, bool VEC, bool SH>
-__global__ void k_km_ann(const T *__restrict__ X, i64 N, int D, const T *__restrict__ C, KdDev tr, i64 maxComp,
-                         int update, uint32_t *__restrict__ assign, T *__restrict__ dist,
-                         double *__restrict__ hkey, int *__restrict__ hnode, int cap, int *__restrict__ err,
-                         const uint32_t *__restrict__ list, i64 count) {
-  extern __shared__ __align__(16) unsigned char km_smem[];
-  T *sq = (T *)km_smem;
-  const int TB = blockDim.x;
-  const int QS = TB + 1;
-  const i64 G = (i64)gridDim.x * TB;
-  const i64 g = (i64)blockIdx.x * TB + threadIdx.x;
-  double *hk;
-  int *hn;
-  i64 hG;
-  if constexpr (SH) {
-    double *hkS = (double *)(km_smem + align16(sizeof(T) * (size_t)QS * D));
-    hk = hkS + threadIdx.x;
-    hn = (int *)(hkS + (size_t)TB * cap) + threadIdx.x;
-    hG = TB;
-  } else {
-    hk = hkey + g;
-    hn = hnode + g;
-    hG = G;
-  }
-  const i64 M = list ? count : N;
-  for (i64 base = (i64)blockIdx.x * TB; base < M; base += G) {
-    __syncthreads();
-    if (!list) {
-      load_rows(X, N, D, base, sq);
-    } else if (base + threadIdx.x < M) {
-      const T *src = X + (i64)list[base + threadIdx.x] * D;
-      for (int d = 0; d < D; ++d) sq[(i64)d * QS + threadIdx.x] = src[d];
-    }
-    __syncthreads();
-    if (base + threadIdx.x >= M) continue;
-    const i64 x = list ? (i64)list[base + threadIdx.x] : base + threadIdx.x;
-    const T *q = sq + threadIdx.x;
-    double nd;
-    const int ni = kd_query<T, L, VEC>(q, QS, C, D, tr, maxComp, hk, hn, hG, cap, nd, err);
-    const T ndt = (T)nd;  // exact: the distance was computed in T
-    if (!update) {
-      dist[x] = ndt;
-      assign[x] = (uint32_t)ni;
-    } else {
-      const T prev = row_dist<T, L, VEC>(q, QS, C + (i64)assign[x] * D, D);
-      if (prev > ndt) {
-        dist[x] = ndt;
-        assign[x] = (uint32_t)ni;
-      } else {
-        dist[x] = prev;
-      }
-    }
-  }
-}
-
 // A lane group of L elements of a centre row, in 16-byte vectors when VEC.
 template <typename T, int L, bool VEC>
 __device__ __forceinline__ void load_group(const T *__restrict__ p, T *out) {
@@ -587,6 +392,217 @@ __global__ void k_km_nearest(const T *__restrict__ X, i64 N, int D, const T *__r
       assign[x] = bi;
     } else {
       dist[x] = prevd;
+    }
+  }
+}
+
+// Distance of query row q (shared memory) to centre row c in the reference's
+// order, by one warp: lane l < L adds (q_i - c_i)^2 for i = l, l + L, ... in
+// order (a warp load reads L consecutive elements), the L lane sums are
+// gathered into every lane and reduced in the SIMD horizontal-sum pattern, and
+// every lane adds the D mod L remaining elements in order.  Every lane returns
+// the same value.
+template <typename T, int L>
+__device__ __forceinline__ T warp_row_dist(const T *q, const T *__restrict__ c, int D, int lane) {
+  T a = (T)0;
+  const int full = D / L * L;
+  if (lane < L)
+    for (int i = lane; i < full; i += L) {
+      const T dl = sub_rn(q[i], __ldg(c + i));
+      a = add_rn(a, mul_rn(dl, dl));
+    }
+  T v[L];
+#pragma unroll
+  for (int l = 0; l < L; ++l) v[l] = __shfl_sync(0xffffffffu, a, l);
+  T d = lane_sum<T, L>(v);
+  for (int i = full; i < D; ++i) {
+    const T dl = sub_rn(q[i], __ldg(c + i));
+    d = add_rn(d, mul_rn(dl, dl));
+  }
+  return d;
+}
+
+// One query of the forest by one warp, vl/kdtree.c:774-840 with numNeighbors
+// = 1 and the recursion of vl/kdtree.c:583-725 unrolled into a loop.  Every
+// lane follows the same path (the decisions depend only on values all lanes
+// hold); lane 0 alone keeps the search heap (hk, hn: capacity cap = the
+// tree's node count, which bounds the pushes of one query, each node being
+// pushed at most once) and hands each popped entry to the warp.  Heap moves
+// follow vl/heap-def.h: push sifts towards the root while strictly smaller,
+// pop moves the last entry to the root and sifts it towards the smaller
+// child (the right one on ties) while strictly larger.
+template <typename T, int L>
+__device__ int kd_query_warp(const T *q, const T *__restrict__ C, int D, const KdDev &tr, i64 maxComp,
+                             double *__restrict__ hk, int *__restrict__ hn, int cap, double &bestOut,
+                             int *__restrict__ err, int lane) {
+  const bool exact = maxComp == 0;
+  i64 comps = 0;
+  int nh = 1;
+  if (lane == 0) {
+    hk[0] = 0.0;
+    hn[0] = 0;
+  }
+  bool have = false;
+  double best = 0.0;
+  int bestIdx = 0;
+  while (exact || comps < maxComp) {
+    if (nh == 0) break;
+    nh -= 1;
+    double pk = 0.0;
+    int pn = 0;
+    if (lane == 0) {
+      pk = hk[0];
+      pn = hn[0];
+      if (nh > 0) {
+        const double lk = hk[nh];
+        const int ln = hn[nh];
+        int i = 0;
+        if (nh > 1) {
+          while (true) {
+            const int l = 2 * i + 1, r = l + 1;
+            if (l >= nh) break;
+            const int c = (r >= nh) ? l : (hk[l] < hk[r] ? l : r);
+            const double ck = hk[c];
+            if (lk > ck) {
+              hk[i] = ck;
+              hn[i] = hn[c];
+              i = c;
+              if (r >= nh) break;  // a lone left child is the last entry: stop
+            } else {
+              break;
+            }
+          }
+        }
+        hk[i] = lk;
+        hn[i] = ln;
+      }
+    }
+    pk = __shfl_sync(0xffffffffu, pk, 0);
+    pn = __shfl_sync(0xffffffffu, pn, 0);
+    if (have && best < pk) break;  // no better neighbour can remain
+    const double dist = pk;
+    int n = pn;
+    while (true) {
+      const int lc = __ldg(tr.lower + n);
+      if (lc < 0) {  // leaf
+        const int b = -lc - 1, e = -__ldg(tr.upper + n) - 1;
+        for (int it = b; it < e && (exact || comps < maxComp); ++it) {
+          const int di = __ldg(tr.ent + it);
+          const double dd = (double)warp_row_dist<T, L>(q, C + (i64)di * D, D, lane);
+          ++comps;
+          if (!have) {
+            have = true;
+            best = dd;
+            bestIdx = di;
+          } else if (best > dd) {
+            best = dd;
+            bestIdx = di;
+          }
+        }
+        break;
+      }
+      const int up = __ldg(tr.upper + n);
+      const double xv = (double)q[__ldg(tr.dim + n)];
+      const double x1 = __ldg(tr.lb + n), x2 = __ldg(tr.thr + n), x3 = __ldg(tr.ub + n);
+      double delta = __dsub_rn(xv, x2);
+      double save = __dadd_rn(dist, __dmul_rn(delta, delta));
+      int next, sv;
+      if (xv <= x2) {
+        next = lc;
+        sv = up;
+        if (xv <= x1) {
+          delta = __dsub_rn(xv, x1);
+          save = __dsub_rn(save, __dmul_rn(delta, delta));
+        }
+      } else {
+        next = up;
+        sv = lc;
+        if (xv > x3) {
+          delta = __dsub_rn(xv, x3);
+          save = __dsub_rn(save, __dmul_rn(delta, delta));
+        }
+      }
+      if (!have || best > save) {
+        if (nh >= cap) {
+          if (lane == 0) atomicOr(err, 1);  // cannot happen: pushes per query <= nodes
+        } else {
+          if (lane == 0) {
+            int i = nh;
+            while (i > 0) {
+              const int p = (i - 1) / 2;
+              const double pkk = hk[p];
+              if (save < pkk) {
+                hk[i] = pkk;
+                hn[i] = hn[p];
+                i = p;
+              } else {
+                break;
+              }
+            }
+            hk[i] = save;
+            hn[i] = sv;
+          }
+          ++nh;
+        }
+      }
+      n = next;
+    }
+  }
+  bestOut = best;
+  return bestIdx;
+}
+
+// ANN assignment, vl/kmeans.c:708-771: the forest's nearest centre of each
+// row; after the first iteration (update) the previous assignment is kept
+// unless the new centre is strictly closer.  One warp per row, WPB warps per
+// block; with a row list only rows list[0 .. count) are served.  SH: each
+// warp's query row and search heap live in shared memory, else the heap is
+// the warp's slice of hkey / hnode.
+template <typename T, int L, bool SH>
+__global__ void k_km_ann(const T *__restrict__ X, i64 N, int D, const T *__restrict__ C, KdDev tr, i64 maxComp,
+                         int update, uint32_t *__restrict__ assign, T *__restrict__ dist,
+                         double *__restrict__ hkey, int *__restrict__ hnode, int cap, int *__restrict__ err,
+                         const uint32_t *__restrict__ list, i64 count) {
+  extern __shared__ __align__(16) unsigned char km_smem[];
+  const int WPB = blockDim.x / 32, warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  // Each warp's region (query row, then heap keys and nodes) starts 16-byte aligned.
+  const size_t per = align16(align16(sizeof(T) * (size_t)D) + (SH ? (size_t)cap * (sizeof(double) + sizeof(int)) : 0));
+  unsigned char *mine = km_smem + per * warp;
+  T *q = (T *)mine;
+  const i64 gw = (i64)blockIdx.x * WPB + warp, GW = (i64)gridDim.x * WPB;
+  double *hk;
+  int *hn;
+  if constexpr (SH) {
+    hk = (double *)(mine + align16(sizeof(T) * (size_t)D));
+    hn = (int *)(hk + cap);
+  } else {
+    hk = hkey + gw * cap;
+    hn = hnode + gw * cap;
+  }
+  const i64 M = list ? count : N;
+  for (i64 pidx = gw; pidx < M; pidx += GW) {
+    const i64 x = list ? (i64)list[pidx] : pidx;
+    __syncwarp();
+    for (int d = lane; d < D; d += 32) q[d] = X[x * D + d];
+    __syncwarp();
+    double nd;
+    const int ni = kd_query_warp<T, L>(q, C, D, tr, maxComp, hk, hn, cap, nd, err, lane);
+    const T ndt = (T)nd;  // exact: the distance was computed in T
+    if (!update) {
+      if (lane == 0) {
+        dist[x] = ndt;
+        assign[x] = (uint32_t)ni;
+      }
+    } else {
+      const T prev = warp_row_dist<T, L>(q, C + (i64)assign[x] * D, D, lane);
+      if (lane == 0) {
+        if (prev > ndt) {
+          dist[x] = ndt;
+          assign[x] = (uint32_t)ni;
+        } else {
+          dist[x] = prev;
+        }
+      }
     }
   }
 }
@@ -922,43 +938,36 @@ struct KMeansRun {
     static void run(KMeansRun &r, const TT *centers, const KdDev &tr, i64 maxComp, int update, uint32_t *assign,
                     TT *dist, int *err, const uint32_t *list, i64 count) {
       const int cap = tr.numNodes;
-      const size_t perThread = (size_t)cap * (sizeof(double) + sizeof(int));
+      const size_t heap = (size_t)cap * (sizeof(double) + sizeof(int));
+      const size_t rowB = align16(sizeof(TT) * (size_t)r.D);
       const i64 M = list ? count : r.N;
-      // Heaps in shared memory when at least 8 threads' heaps and query
-      // columns fit the block's 200 KB: the search's pops and pushes are
-      // then shared-memory latency instead of global-memory latency.
-      const size_t rowBytes = sizeof(TT) * (size_t)r.D;
-      const size_t smemCap = (size_t)200 * 1024 - 32 - rowBytes;
-      const int tbSh = (int)std::min<size_t>((size_t)r.tile_rows(), smemCap / (perThread + rowBytes));
-      if (tbSh >= 8) {
-        const int TB = tbSh;
-        const i64 blocks = std::max<i64>(1, std::min<i64>((M + TB - 1) / TB, (i64)num_sms()));
-        const size_t smem = align16(rowBytes * (TB + 1)) + perThread * TB;
-        auto go = [&](auto kern) {
-          VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-          VLB_LAUNCH("km_ann", r.s, (kern<<<(int)blocks, TB, smem, r.s>>>(
-                                        r.X, r.N, (int)r.D, centers, tr, maxComp, update, assign, dist,
-                                        (double *)nullptr, (int *)nullptr, cap, err, list, count)));
-        };
-        if (r.vec(L)) go(k_km_ann<TT, L, true, true>);
-        else go(k_km_ann<TT, L, false, true>);
+      // Up to 8 warps (rows) per block, as many as fit 200 KB with their query
+      // rows and, when possible, their heaps.
+      const size_t budget = (size_t)200 * 1024;
+      const size_t perW = align16(rowB + heap);
+      int wpb = (int)std::min<size_t>(8, budget / perW);
+      if (wpb >= 1) {
+        const i64 blocks = std::max<i64>(1, std::min<i64>((M + wpb - 1) / wpb, (i64)num_sms() * 8));
+        const size_t smem = perW * wpb;
+        auto kern = k_km_ann<TT, L, true>;
+        VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        VLB_LAUNCH("km_ann", r.s, (kern<<<(int)blocks, 32 * wpb, smem, r.s>>>(
+                                      r.X, r.N, (int)r.D, centers, tr, maxComp, update, assign, dist,
+                                      (double *)nullptr, (int *)nullptr, cap, err, list, count)));
         return;
       }
-      const int TB = r.tile_rows();
-      i64 blocks = std::min<i64>((M + TB - 1) / TB, (i64)num_sms() * 12);
-      blocks = std::max<i64>(1, std::min<i64>(blocks, (i64)(kHeapBudget / (perThread * TB))));
-      const i64 G = blocks * TB;
-      double *hk = r.sc.slot[5].template get<double>(G * cap);
-      int *hn = r.sc.slot[6].template get<int>(G * cap);
-      const size_t smem = rowBytes * (TB + 1);
-      auto go = [&](auto kern) {
-        VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        VLB_LAUNCH("km_ann", r.s, (kern<<<(int)blocks, TB, smem, r.s>>>(r.X, r.N, (int)r.D, centers, tr, maxComp,
-                                                                         update, assign, dist, hk, hn, cap, err,
-                                                                         list, count)));
-      };
-      if (r.vec(L)) go(k_km_ann<TT, L, true, false>);
-      else go(k_km_ann<TT, L, false, false>);
+      wpb = 8;
+      i64 blocks = std::min<i64>((M + wpb - 1) / wpb, (i64)num_sms() * 8);
+      blocks = std::max<i64>(1, std::min<i64>(blocks, (i64)(kHeapBudget / (heap * wpb))));
+      const i64 GW = blocks * wpb;
+      double *hk = r.sc.slot[5].template get<double>(GW * cap);
+      int *hn = r.sc.slot[6].template get<int>(GW * cap);
+      const size_t smem = rowB * wpb;
+      auto kern = k_km_ann<TT, L, false>;
+      VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      VLB_LAUNCH("km_ann", r.s, (kern<<<(int)blocks, 32 * wpb, smem, r.s>>>(r.X, r.N, (int)r.D, centers, tr, maxComp,
+                                                                             update, assign, dist, hk, hn, cap, err,
+                                                                             list, count)));
     }
   };
 
