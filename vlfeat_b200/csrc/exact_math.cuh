@@ -60,45 +60,4 @@ __device__ __forceinline__ T l2_ordered(const T *__restrict__ a, const T *__rest
   return l2_ordered_s<T, L>(a, 1, b, D);
 }
 
-// l2_ordered_s with b read in 16-byte vectors: b must be 16-byte aligned and
-// L * sizeof(T) a multiple of 16 (float L = 4, 8; double L = 2, 4).  Same
-// arithmetic, same order.
-template <typename T, int L>
-__device__ __forceinline__ T l2_ordered_sv(const T *__restrict__ a, int as, const T *__restrict__ b, int D) {
-  static_assert((L * sizeof(T)) % 16 == 0, "groups must be whole 16-byte vectors");
-  constexpr int V = 16 / sizeof(T);  // elements per vector
-  T v[L];
-#pragma unroll
-  for (int l = 0; l < L; ++l) v[l] = (T)0;
-  int i = 0;
-  for (; i + L <= D; i += L) {
-    T bb[L];
-#pragma unroll
-    for (int u = 0; u < L / V; ++u) {
-      const float4 w = __ldg(reinterpret_cast<const float4 *>(b + i) + u);
-      const T *wp = reinterpret_cast<const T *>(&w);
-#pragma unroll
-      for (int e = 0; e < V; ++e) bb[u * V + e] = wp[e];
-    }
-#pragma unroll
-    for (int l = 0; l < L; ++l) {
-      const T dl = sub_rn(a[(i + l) * as], bb[l]);
-      v[l] = add_rn(v[l], mul_rn(dl, dl));
-    }
-  }
-  T acc;
-  if constexpr (L == 8) {
-    acc = add_rn(add_rn(add_rn(v[0], v[1]), add_rn(v[4], v[5])), add_rn(add_rn(v[2], v[3]), add_rn(v[6], v[7])));
-  } else if constexpr (L == 4) {
-    acc = add_rn(add_rn(v[0], v[2]), add_rn(v[1], v[3]));
-  } else {
-    acc = add_rn(v[0], v[1]);
-  }
-  for (; i < D; ++i) {
-    const T dl = sub_rn(a[i * as], b[i]);
-    acc = add_rn(acc, mul_rn(dl, dl));
-  }
-  return acc;
-}
-
 }  // namespace vlb

@@ -191,24 +191,6 @@ __device__ __forceinline__ void load_rows(const T *__restrict__ X, i64 N, int D,
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
-// A lane group of L elements of a centre row, in 16-byte vectors when VEC.
-template <typename T, int L, bool VEC>
-__device__ __forceinline__ void load_group(const T *__restrict__ p, T *out) {
-  if constexpr (VEC && (L * sizeof(T)) % 16 == 0) {
-    constexpr int V = 16 / sizeof(T);
-#pragma unroll
-    for (int u = 0; u < L / V; ++u) {
-      const float4 w = __ldg(reinterpret_cast<const float4 *>(p) + u);
-      const T *wp = reinterpret_cast<const T *>(&w);
-#pragma unroll
-      for (int e = 0; e < V; ++e) out[u * V + e] = wp[e];
-    }
-  } else {
-#pragma unroll
-    for (int l = 0; l < L; ++l) out[l] = __ldg(p + l);
-  }
-}
-
 template <typename T, int L>
 __device__ __forceinline__ T lane_sum(const T *v) {  // the SIMD horizontal sum of l2_ordered_s
   if constexpr (L == 8) {
