@@ -9,9 +9,11 @@
 // (vl/gmm.c:1152-1166).
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "engine.h"
 #include "exact_math.cuh"
+#include "tc_common.cuh"
 
 namespace vlb {
 
@@ -57,24 +59,33 @@ __global__ void k_prepare(const T *__restrict__ priors, const T *__restrict__ co
 // ------------------------------------------------------------ E-step
 // Log-densities of a TM x TK tile of (descriptor, component) pairs.  The
 // dimension is streamed through shared memory in chunks of DC.  Each thread
-// owns one component and RPT descriptors.
+// owns a register tile of 8 descriptors x 4 components: per dimension, 16-byte
+// shared loads of its 8 x values, 4 means and 4 inverse variances feed 32
+// updates acc += (x - mu)^2 / sigma^2.  Per (descriptor, component) the sum
+// runs over the dimensions in ascending order.
 template <typename T, int TM, int TK, int DC>
 __global__ void __launch_bounds__(kThreads) k_logp(const T *__restrict__ X, i64 N, int D, int K,
                                                   const T *__restrict__ means,
                                                   const T *__restrict__ inv,
                                                   const double *__restrict__ cst,
                                                   T *__restrict__ q) {
-  constexpr int RPT = TM * TK / kThreads;
-  __shared__ T sx[DC][TM + 1];
-  __shared__ T smu[DC][TK + 1];
-  __shared__ T siv[DC][TK + 1];
+  constexpr int RR = 8, CC = 4, NCG = TK / CC;
+  static_assert(TM * TK == kThreads * RR * CC, "one 8 x 4 register tile per thread");
+  constexpr int XP = TM + 16 / (int)sizeof(T), MP = TK + 16 / (int)sizeof(T);  // padded, 16-byte rows
+  constexpr int VW = 16 / (int)sizeof(T);                                     // elements per vector
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  __shared__ __align__(16) T sx[DC][XP];
+  __shared__ __align__(16) T smu[DC][MP];
+  __shared__ __align__(16) T siv[DC][MP];
   const int tid = threadIdx.x;
-  const int tk = tid % TK, tg = tid / TK;
+  const int tc = tid % NCG, tr = tid / NCG;
   const i64 i0 = (i64)blockIdx.x * TM;
   const int k0 = blockIdx.y * TK;
-  T acc[RPT];
+  T acc[RR][CC];
 #pragma unroll
-  for (int r = 0; r < RPT; ++r) acc[r] = 0;
+  for (int r = 0; r < RR; ++r)
+#pragma unroll
+    for (int c = 0; c < CC; ++c) acc[r][c] = 0;
 
   for (int d0 = 0; d0 < D; d0 += DC) {
     for (int e = tid; e < TM * DC; e += kThreads) {
@@ -93,22 +104,62 @@ __global__ void __launch_bounds__(kThreads) k_logp(const T *__restrict__ X, i64 
     __syncthreads();
     const int dl = min(DC, D - d0);
     for (int dd = 0; dd < dl; ++dd) {
-      const T m = smu[dd][tk], iv = siv[dd][tk];
+      T x[RR], m[CC], iv[CC];
 #pragma unroll
-      for (int r = 0; r < RPT; ++r) {
-        T diff = sx[dd][tg * RPT + r] - m;
-        acc[r] += diff * diff * iv;
+      for (int u = 0; u < RR / VW; ++u) {
+        const V w = *reinterpret_cast<const V *>(&sx[dd][tr * RR + u * VW]);
+        const T *wp = reinterpret_cast<const T *>(&w);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) x[u * VW + e] = wp[e];
+      }
+#pragma unroll
+      for (int u = 0; u < CC / VW; ++u) {
+        const V a = *reinterpret_cast<const V *>(&smu[dd][tc * CC + u * VW]);
+        const V b = *reinterpret_cast<const V *>(&siv[dd][tc * CC + u * VW]);
+        const T *ap = reinterpret_cast<const T *>(&a);
+        const T *bp = reinterpret_cast<const T *>(&b);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+          m[u * VW + e] = ap[e];
+          iv[u * VW + e] = bp[e];
+        }
+      }
+      if constexpr (sizeof(T) == 4) {
+        // Packed fp32x2 over component pairs: each half is the scalar
+        // x - mu, (x - mu)^2 and the fused (x - mu)^2 iv + acc.
+        constexpr unsigned long long kNeg = 0x8000000080000000ull;
+#pragma unroll
+        for (int c = 0; c < CC; c += 2) {
+          const unsigned long long mn = tc::f2u(m[c], m[c + 1]) ^ kNeg, ivp = tc::f2u(iv[c], iv[c + 1]);
+#pragma unroll
+          for (int r = 0; r < RR; ++r) {
+            const unsigned long long df = tc::add2(tc::f2u(x[r], x[r]), mn);
+            const unsigned long long a = tc::fma2(tc::mul2(df, df), ivp, tc::f2u(acc[r][c], acc[r][c + 1]));
+            acc[r][c] = tc::lo32(a);
+            acc[r][c + 1] = tc::hi32(a);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < RR; ++r)
+#pragma unroll
+          for (int c = 0; c < CC; ++c) {
+            T diff = x[r] - m[c];
+            acc[r][c] += diff * diff * iv[c];
+          }
       }
     }
     __syncthreads();
   }
-  const int k = k0 + tk;
-  if (k < K) {
-    const double c = cst[k];
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      i64 i = i0 + tg * RPT + r;
-      if (i < N) q[i * K + k] = (T)(c - 0.5 * (double)acc[r]);
+  for (int c = 0; c < CC; ++c) {
+    const int k = k0 + tc * CC + c;
+    if (k >= K) continue;
+    const double cc = cst[k];
+#pragma unroll
+    for (int r = 0; r < RR; ++r) {
+      const i64 i = i0 + tr * RR + r;
+      if (i < N) q[i * K + k] = (T)(cc - 0.5 * (double)acc[r][c]);
     }
   }
 }
@@ -236,17 +287,50 @@ __global__ void __launch_bounds__(kThreads) k_mstep_stats(
       sq[r][cc] = ((double)v < thr) ? (T)0 : v;
     }
     __syncthreads();
-    for (int r = 0; r < rc; ++r) {
-      const T p = sq[r][c];
-      if (p == (T)0) continue;
-      mass += p;
+    if constexpr (sizeof(T) == 4 && JMAX % 2 == 0) {
+      // Packed fp32x2 over dimension pairs (j, j + 1): each half is the
+      // scalar x - mu_old, its square, p x + s1 and p (x - mu_old)^2 + s2.
+      constexpr unsigned long long kNeg = 0x8000000080000000ull;
+      unsigned long long mo[JMAX / 2], a1[JMAX / 2], a2[JMAX / 2];
 #pragma unroll
-      for (int j = 0; j < JMAX; ++j) {
-        const int dd = dg + 8 * j;
-        const T x = sx[r][dd];
-        const T diff = x - smo[dd][c];
-        s1[j] += p * x;
-        s2[j] += p * (diff * diff);
+      for (int j = 0; j < JMAX; j += 2) {
+        mo[j / 2] = tc::f2u(smo[dg + 8 * j][c], smo[dg + 8 * j + 8][c]) ^ kNeg;
+        a1[j / 2] = tc::f2u(s1[j], s1[j + 1]);
+        a2[j / 2] = tc::f2u(s2[j], s2[j + 1]);
+      }
+      for (int r = 0; r < rc; ++r) {
+        const T p = sq[r][c];
+        if (p == (T)0) continue;
+        mass += p;
+        const unsigned long long pp = tc::f2u(p, p);
+#pragma unroll
+        for (int j = 0; j < JMAX; j += 2) {
+          const unsigned long long xp = tc::f2u(sx[r][dg + 8 * j], sx[r][dg + 8 * j + 8]);
+          const unsigned long long df = tc::add2(xp, mo[j / 2]);
+          a1[j / 2] = tc::fma2(pp, xp, a1[j / 2]);
+          a2[j / 2] = tc::fma2(pp, tc::mul2(df, df), a2[j / 2]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < JMAX; j += 2) {
+        s1[j] = tc::lo32(a1[j / 2]);
+        s1[j + 1] = tc::hi32(a1[j / 2]);
+        s2[j] = tc::lo32(a2[j / 2]);
+        s2[j + 1] = tc::hi32(a2[j / 2]);
+      }
+    } else {
+      for (int r = 0; r < rc; ++r) {
+        const T p = sq[r][c];
+        if (p == (T)0) continue;
+        mass += p;
+#pragma unroll
+        for (int j = 0; j < JMAX; ++j) {
+          const int dd = dg + 8 * j;
+          const T x = sx[r][dd];
+          const T diff = x - smo[dd][c];
+          s1[j] += p * x;
+          s2[j] += p * (diff * diff);
+        }
       }
     }
   }
@@ -554,7 +638,7 @@ template <typename T>
 i64 exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,
                 double *ll_part, bool fast, cudaStream_t s) {
   if (N <= 0) return 0;
-  constexpr int TM = 32, TK = 64, DC = 32;
+  constexpr int TM = 128, TK = 64, DC = sizeof(T) == 4 ? 32 : 16;  // 34 KB of tiles either way
   dim3 g(grid1(N, TM), grid1(m.K, TK));
   VLB_LAUNCH("exact_logp", s,
              (k_logp<T, TM, TK, DC><<<g, kThreads, 0, s>>>(X, N, (int)m.D, (int)m.K, m.means,
@@ -751,7 +835,7 @@ void exact_fisher_single_fixed(const float *X, i64 N, const DevModel<float> &m, 
                                unsigned long long *nterms, int flags, const ExactFvScratch &sc,
                                cudaStream_t s) {
   constexpr int TKC = 32, RC = 32, JMAX = 10, DB = 8 * JMAX;
-  constexpr int TM = 32, TK = 64, DC = 32;
+  constexpr int TM = 128, TK = 64, DC = 32;
   const i64 K = m.K, D = m.D, nseg = exact_fv_segments(N);
   VLB_LAUNCH_PLAIN(s, k_single_segments<<<1, 32, 0, s>>>(N, nseg, sc.segs, sc.segBegin, sc.rows));
   VLB_LAUNCH_PLAIN(s, k_prepare<float><<<grid1(K, 128), 128, 0, s>>>(
