@@ -183,7 +183,8 @@ def kmeans_data(name):
     split values), 25 distinct rows repeated (duplicate seeds, constant
     leaves), too few rows for a full search (N/4 < K: the comparison budget
     cuts the search), a mixture, more than 1024 centres (the kd-tree samples
-    variances with random draws), and SIFT-sized rows."""
+    variances with random draws), SIFT-sized rows, and the edge shapes K = 1,
+    N = K and D = 1."""
     if name == "small":
         return rng(61).random((400, 5)), 8, 611
     if name == "grid":
@@ -199,11 +200,17 @@ def kmeans_data(name):
         return W.mixture_data(6000, 6, 300, seed=66, dtype=np.float64), 1100, 661
     if name == "sift":
         return W.mixture_data(50000, 80, 256, seed=67, dtype=np.float64), 256, 671
+    if name == "k1":  # one centre: a one-leaf tree
+        return rng(68).random((40, 3)), 1, 681
+    if name == "nk":  # as many rows as centres: every row becomes a centre
+        return rng(69).random((12, 2)), 12, 691
+    if name == "d1":  # one dimension
+        return rng(70).random((300, 1)), 5, 701
     raise KeyError(name)
 
 
 KMEANS_CASES = {"small": ("f", "d"), "grid": ("f",), "dup": ("f",), "trunc": ("f",), "mix": ("f", "d"),
-                "wide": ("f",), "sift": ("f",)}
+                "wide": ("f",), "sift": ("f",), "k1": ("f",), "nk": ("f", "d"), "d1": ("f",)}
 
 
 def kmeans_case(ref, out):

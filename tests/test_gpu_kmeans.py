@@ -7,8 +7,11 @@ vl_gmm_init_with_kmeans leaves) and the generator's next draw after the
 initialisation (the number of random draws: seeding shuffle, kd-tree builds,
 restarts).  Within tolerance: the parameters of the one-hot M-step (the
 library's M-step sums in another order than the reference's: float 2e-5,
-double 1e-10 relative) and five EM iterations after the initialisation (the
-bounds of the other EM tests: float 2e-4, double 1e-9)."""
+double 1e-10 relative; float covariances 1e-4, because this M-step starts from
+zero means (vl/gmm.c:1326-1328), so the variance is E[x^2] - mean^2 and both
+implementations' float rounding is amplified by mean^2 / variance, about 125
+on the one-dimensional case) and five EM iterations after the initialisation
+(the bounds of the other EM tests: float 2e-4, double 1e-9)."""
 import ctypes as C
 import os
 import sys
@@ -25,6 +28,7 @@ pytestmark = pytest.mark.gpu
 
 DT = {"f": np.float32, "d": np.float64}
 TOL = {"f": 2e-5, "d": 1e-10}
+TOL_COVS = {"f": 1e-4, "d": 1e-10}
 EM_TOL = {"f": 2e-4, "d": 1e-9}
 CASES = [(n, t) for n, tags in KMEANS_CASES.items() for t in tags]
 
@@ -70,7 +74,8 @@ def test_kmeans_init_matches_reference(vl, golden, name, tag):
     assert np.array_equal(assign, ref), f"{int((assign != ref).sum())} rows assigned differently"
     assert nxt == int(golden[f"km_{name}_{tag}_next"])
     for k, got in (("means", m.means), ("covs", m.covariances), ("priors", m.priors)):
-        assert rel_err(got, golden[f"km_{name}_{tag}_{k}"]) < TOL[tag], k
+        tol = TOL_COVS[tag] if k == "covs" else TOL[tag]
+        assert rel_err(got, golden[f"km_{name}_{tag}_{k}"]) < tol, k
 
 
 @pytest.mark.parametrize("name,tag", [("small", "f"), ("small", "d"), ("mix", "f"), ("mix", "d")])

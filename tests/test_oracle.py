@@ -123,7 +123,7 @@ def test_rand_init_restatement(golden, tag):
 
 
 @pytest.mark.parametrize("name,tag", [("small", "f"), ("small", "d"), ("grid", "f"), ("dup", "f"),
-                                      ("trunc", "f")])
+                                      ("trunc", "f"), ("k1", "f"), ("nk", "f"), ("nk", "d"), ("d1", "f")])
 def test_kmeans_init_restatement(golden, name, tag):
     """The k-means of the KMeans initialisation restated (oracle.kmeans_init:
     seeding shuffle and duplicate test, one-tree kd-forest with its random
