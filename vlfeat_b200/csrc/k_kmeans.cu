@@ -10,13 +10,17 @@
 //    draws, then one draw per empty centre;
 //  - the kd-tree over the K centres is built on the host exactly as
 //    vl/kdtree.c:165-325 and 491-576 build it (its shape decides the draws);
-//  - each data point's query is one GPU thread running the reference's
-//    best-bin-first search (vl/kdtree.c:583-725, 774-840) with the same heap
-//    discipline (vl/heap-def.h), comparison budget and tie rules;
+//  - each row's assignment: when the comparison budget covers every centre,
+//    an exact brute-force screen settles every row whose nearest centre is
+//    clear of the second by more than the distances' rounding (the search
+//    must return that centre); the other rows, and every row when the budget
+//    is smaller, get the reference's best-bin-first search (vl/kdtree.c:
+//    583-725, 774-840) by one warp each, with the same heap discipline
+//    (vl/heap-def.h), comparison budget and tie rules;
 //  - distances use the summation order of the reference's SIMD kernel;
 //  - a centre is the sum of its points in data order (a stable counting sort
-//    by centre, then one thread per centre and dimension adding in order),
-//    divided by its mass rounded to the data type (vl/kmeans.c:1078-1098).
+//    by centre, then one block per centre adding its rows in order), divided
+//    by its mass rounded to the data type (vl/kmeans.c:1078-1098).
 //
 // The energy (sum of the point distances, in double) is summed in a fixed
 // parallel order instead of the reference's data order; it only steers the
