@@ -531,16 +531,50 @@ __global__ void __launch_bounds__(kThreads) k_fisher_stats(
     }
     __syncthreads();
     if (!active) continue;
-    for (int r = 0; r < rc; ++r) {
-      const T p = sq[r][c];
-      if (p == (T)0) continue;
-      ++nt;
+    if constexpr (sizeof(T) == 4 && JMAX % 2 == 0) {
+      // Packed fp32x2 over dimension pairs (j, j + 1): each half is the
+      // scalar (x - mu) sigma^-1, p df + u and p (df^2 - 1) + v.
+      constexpr unsigned long long kNeg = 0x8000000080000000ull, kMinus1 = 0xbf800000bf800000ull;
+      unsigned long long mn[JMAX / 2], si[JMAX / 2], au[JMAX / 2], av[JMAX / 2];
 #pragma unroll
-      for (int j = 0; j < JMAX; ++j) {
-        const int dd = dg + 8 * j;
-        const T df = (sx[r][dd] - smu[dd][c]) * ssi[dd][c];
-        u[j] += p * df;
-        v[j] += p * (df * df - (T)1);
+      for (int j = 0; j < JMAX; j += 2) {
+        mn[j / 2] = tc::f2u(smu[dg + 8 * j][c], smu[dg + 8 * j + 8][c]) ^ kNeg;
+        si[j / 2] = tc::f2u(ssi[dg + 8 * j][c], ssi[dg + 8 * j + 8][c]);
+        au[j / 2] = tc::f2u(u[j], u[j + 1]);
+        av[j / 2] = tc::f2u(v[j], v[j + 1]);
+      }
+      for (int r = 0; r < rc; ++r) {
+        const T p = sq[r][c];
+        if (p == (T)0) continue;
+        ++nt;
+        const unsigned long long pp = tc::f2u(p, p);
+#pragma unroll
+        for (int j = 0; j < JMAX; j += 2) {
+          const unsigned long long xp = tc::f2u(sx[r][dg + 8 * j], sx[r][dg + 8 * j + 8]);
+          const unsigned long long df = tc::mul2(tc::add2(xp, mn[j / 2]), si[j / 2]);
+          au[j / 2] = tc::fma2(pp, df, au[j / 2]);
+          av[j / 2] = tc::fma2(pp, tc::fma2(df, df, kMinus1), av[j / 2]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < JMAX; j += 2) {
+        u[j] = tc::lo32(au[j / 2]);
+        u[j + 1] = tc::hi32(au[j / 2]);
+        v[j] = tc::lo32(av[j / 2]);
+        v[j + 1] = tc::hi32(av[j / 2]);
+      }
+    } else {
+      for (int r = 0; r < rc; ++r) {
+        const T p = sq[r][c];
+        if (p == (T)0) continue;
+        ++nt;
+#pragma unroll
+        for (int j = 0; j < JMAX; ++j) {
+          const int dd = dg + 8 * j;
+          const T df = (sx[r][dd] - smu[dd][c]) * ssi[dd][c];
+          u[j] += p * df;
+          v[j] += p * (df * df - (T)1);
+        }
       }
     }
   }
