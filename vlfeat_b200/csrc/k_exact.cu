@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kThreads) k_mstep_stats(
     const T *__restrict__ oldMeans, double *__restrict__ pmass, double *__restrict__ ps1,
     double *__restrict__ ps2) {
   constexpr int DB = 8 * JMAX;
-  __shared__ T sx[RC][DB];
+  __shared__ __align__(16) T sx[RC][DB];
   __shared__ T sq[RC][TKC];
   __shared__ T smo[DB][TKC + 1];
   const int tid = threadIdx.x, c = tid % TKC, dg = tid / TKC;
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(kThreads) k_fisher_stats(
     const T *__restrict__ priors, double *__restrict__ pu, double *__restrict__ pv,
     unsigned long long *__restrict__ pnt) {
   constexpr int DB = 8 * JMAX;
-  __shared__ T sx[RC][DB];
+  __shared__ __align__(16) T sx[RC][DB];
   __shared__ T sq[RC][TKC];
   __shared__ T smu[DB][TKC + 1];
   __shared__ T ssi[DB][TKC + 1];
@@ -538,8 +538,8 @@ __global__ void __launch_bounds__(kThreads) k_fisher_stats(
       unsigned long long mn[JMAX / 2], si[JMAX / 2], au[JMAX / 2], av[JMAX / 2];
 #pragma unroll
       for (int j = 0; j < JMAX; j += 2) {
-        mn[j / 2] = tc::f2u(smu[dg + 8 * j][c], smu[dg + 8 * j + 8][c]) ^ kNeg;
-        si[j / 2] = tc::f2u(ssi[dg + 8 * j][c], ssi[dg + 8 * j + 8][c]);
+        mn[j / 2] = tc::f2u(smu[dg * JMAX + j][c], smu[dg * JMAX + j + 1][c]) ^ kNeg;
+        si[j / 2] = tc::f2u(ssi[dg * JMAX + j][c], ssi[dg * JMAX + j + 1][c]);
         au[j / 2] = tc::f2u(u[j], u[j + 1]);
         av[j / 2] = tc::f2u(v[j], v[j + 1]);
       }
@@ -548,9 +548,10 @@ __global__ void __launch_bounds__(kThreads) k_fisher_stats(
         if (p == (T)0) continue;
         ++nt;
         const unsigned long long pp = tc::f2u(p, p);
+        const unsigned long long *xr = reinterpret_cast<const unsigned long long *>(&sx[r][dg * JMAX]);
 #pragma unroll
         for (int j = 0; j < JMAX; j += 2) {
-          const unsigned long long xp = tc::f2u(sx[r][dg + 8 * j], sx[r][dg + 8 * j + 8]);
+          const unsigned long long xp = xr[j / 2];
           const unsigned long long df = tc::mul2(tc::add2(xp, mn[j / 2]), si[j / 2]);
           au[j / 2] = tc::fma2(pp, df, au[j / 2]);
           av[j / 2] = tc::fma2(pp, tc::fma2(df, df, kMinus1), av[j / 2]);
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(kThreads) k_fisher_stats(
         ++nt;
 #pragma unroll
         for (int j = 0; j < JMAX; ++j) {
-          const int dd = dg + 8 * j;
+          const int dd = dg * JMAX + j;
           const T df = (sx[r][dd] - smu[dd][c]) * ssi[dd][c];
           u[j] += p * df;
           v[j] += p * (df * df - (T)1);
@@ -582,7 +583,7 @@ __global__ void __launch_bounds__(kThreads) k_fisher_stats(
     const i64 base = ((i64)sidx * K + k) * D;
 #pragma unroll
     for (int j = 0; j < JMAX; ++j) {
-      const int d = dbase + dg + 8 * j;
+      const int d = dbase + dg * JMAX + j;
       if (d < D) {
         pu[base + d] = (double)u[j];
         pv[base + d] = (double)v[j];
