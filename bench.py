@@ -375,7 +375,7 @@ def e2e(capi, wl, prec, config, steps=3):
 
 
 def em_throughput(capi, iters=5, cpu=True, large=True):
-    """EM iterations/s (a north-star throughput besides the Fisher metric).
+    """EM iterations/s, reported beside the Fisher metric.
 
     Config 1 (N=1,000,000 SIFT-like descriptors, D=128, K=256, custom init,
     variance floor 1e-4 x max global variance) and config 0 (N=50,000, D=64,

@@ -58,7 +58,7 @@ def test_training_gains_over_untrained_router(vl):
     pr, mu, cv, x = _mixture(K, D, 60000, seed=21)
     xtr, xte = x[:50000], x[50000:]
     prt, mut, cvt = _t(pr), _t(mu), _t(cv)
-    # Full E-step posteriors (exact path) are the labels and the judge.
+    # Full E-step posteriors (exact path) are the labels and the measure of missed mass.
     qtr = torch.zeros((xtr.shape[0], K), device="cuda")
     vl.gmm_posteriors_device(qtr, prt, mut, cvt, _t(xtr), "exact")
     tidx = torch.zeros((xtr.shape[0], 8), dtype=torch.int32, device="cuda")
