@@ -203,39 +203,55 @@ __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float
 }
 
 // Candidates: top-m logits of each row and the router's softmax mass on them.
-template <int MM>
+// One warp per row; lane l holds logits l, l + 32, ... in registers (KPL of
+// them, K <= 32 KPL).  Each of the m rounds takes the largest logit not yet
+// taken (ties: lowest index), found by a lane scan and a warp arg-max; the
+// owner lane marks it taken in a bit mask.
+template <int KPL>
 __global__ void k_select(const float *__restrict__ Zl, i64 n, int K, int m, int *__restrict__ cand,
                          float *__restrict__ cmass) {
   const i64 row = (i64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   if (row >= n) return;
   const float *z = Zl + row * K;
+  float zv[KPL];
   float mx = -INFINITY;
-  for (int k = lane; k < K; k += 32) mx = fmaxf(mx, z[k]);
+#pragma unroll
+  for (int i = 0; i < KPL; ++i) {
+    const int k = lane + 32 * i;
+    zv[i] = k < K ? z[k] : -INFINITY;
+    if (k < K) mx = fmaxf(mx, zv[i]);
+  }
   for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   float s = 0.f;
-  for (int k = lane; k < K; k += 32) s += expf(z[k] - mx);
+#pragma unroll
+  for (int i = 0; i < KPL; ++i)
+    if (lane + 32 * i < K) s += expf(zv[i] - mx);
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  int taken[MM];
+  uint32_t taken = 0;
+  int mine = 0;
   float sel = 0.f;
   for (int t = 0; t < m; ++t) {
     float bv = -INFINITY;
     int bi = 0x7fffffff;
-    for (int k = lane; k < K; k += 32) {
-      bool used = false;
-      for (int u = 0; u < t; ++u) used |= (taken[u] == k);
-      const float v = z[k];
-      if (!used && (v > bv || (v == bv && k < bi))) { bv = v; bi = k; }
+#pragma unroll
+    for (int i = 0; i < KPL; ++i) {
+      const int k = lane + 32 * i;
+      if (k < K && !((taken >> i) & 1u) && (zv[i] > bv || (zv[i] == bv && k < bi))) {
+        bv = zv[i];
+        bi = k;
+      }
     }
     for (int o = 16; o > 0; o >>= 1) {
       const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
       const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
-    taken[t] = bi;
+    if (lane == (bi & 31)) taken |= 1u << (bi >> 5);
+    if (lane == t) mine = bi;
     sel += expf(bv - mx);
   }
-  if (lane < m) cand[row * m + lane] = taken[lane];
+  if (lane < m) cand[row * m + lane] = mine;
   if (lane == 0) cmass[row] = sel / s;
 }
 
@@ -575,6 +591,7 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
                              void *stream) {
   return guarded([&] {
     VLB_CHECK(m >= 1 && m <= 32 && (int)m <= r->K, VL_ERR_BAD_ARG, "router: m must be in [1, 32]");
+    VLB_CHECK(r->K <= 1024, VL_ERR_BAD_ARG, "router: at most 1024 components");
     cudaStream_t s = vlb::pick_stream(stream);
     vlb::Scratch &sc = vlb::thread_scratch(vlb::kArenaRouter);
     const int L = nlayers(r), K = r->K, D = r->D;
@@ -595,8 +612,15 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
       float *cm = sc.slot[26].get<float>(chunk);
       unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
       forward(r, X + i0 * D, B, act, s);
-      VLB_LAUNCH("router_select", s,
-                 vlb::k_select<32><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+      if (K <= 256)
+        VLB_LAUNCH("router_select", s,
+                   vlb::k_select<8><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+      else if (K <= 512)
+        VLB_LAUNCH("router_select", s,
+                   vlb::k_select<16><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+      else
+        VLB_LAUNCH("router_select", s,
+                   vlb::k_select<32><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
       VLB_LAUNCH("router_candidate_estep", s,
                  vlb::k_candidate_estep<<<vlb::gridn(B, 8), 256, 0, s>>>(
                      X + i0 * D, B, D, K, means, der.inv, der.cst, cand, cm, (int)m, threshold,
