@@ -273,20 +273,37 @@ __global__ void k_candidate_estep(const float *__restrict__ X, i64 n, int D, int
   const int nc = fb ? K : m;
   for (int k = lane; k < K; k += 32) qr[k] = 0.f;
   __syncwarp();
-  // Pass 1: log-densities (stored temporarily in q) and their maximum.
+  // Pass 1: log-densities (stored temporarily in q) and their maximum.  Four
+  // candidates at a time, so that their loads and shuffle reductions overlap.
   float mx = -INFINITY;
-  for (int c = 0; c < nc; ++c) {
-    const int k = fb ? c : cand[row * m + c];
-    const float *mu = means + (i64)k * D, *iv = inv + (i64)k * D;
-    float acc = 0.f;
-    for (int d = lane; d < D; d += 32) {
-      const float df = x[d] - mu[d];
-      acc += df * df * iv[d];
+  for (int c0 = 0; c0 < nc; c0 += 4) {
+    int kk[4];
+    float acc[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int c = min(c0 + u, nc - 1);  // a partial group repeats the last candidate
+      kk[u] = fb ? c : cand[row * m + c];
+      acc[u] = 0.f;
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    const float p = (float)(cst[k] - 0.5 * (double)acc);
-    if (lane == 0) qr[k] = p;
-    mx = fmaxf(mx, p);
+    for (int d = lane; d < D; d += 32) {
+      const float xd = x[d];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float df = xd - means[(i64)kk[u] * D + d];
+        acc[u] += df * df * inv[(i64)kk[u] * D + d];
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (c0 + u >= nc) break;
+      const float p = (float)(cst[kk[u]] - 0.5 * (double)acc[u]);
+      if (lane == 0) qr[kk[u]] = p;
+      mx = fmaxf(mx, p);
+    }
   }
   __syncwarp();
   float s = 0.f;
