@@ -116,3 +116,31 @@ def test_pca_project_unaligned_rows(vl):
         assert (np.linalg.norm(g - want, axis=1) / np.linalg.norm(want, axis=1)).max() < 1e-5
     d = (a - b).double().norm(dim=1) / b.double().norm(dim=1)
     assert float(d.max()) < 2e-5
+
+
+@pytest.mark.parametrize("xscale,pscale", [(1e-20, 1.0), (1e15, 1.0), (1.0, 1e-15), (1.0, 1e15), (3e5, 7e-4)])
+def test_pca_project_scales(vl, xscale, pscale):
+    """The tensor-core projection scales each row of x - c and the matrix P by
+    powers of two into fp16's range, so data far outside it (tiny, huge, or a
+    mix with a tiny P) stays within the 1e-5 per-descriptor bound; rows equal to
+    the centre give zeros (and renormalise to zeros).  The renormalisation
+    squares in single precision as the app's MATLAB code does on single
+    descriptors, so norms above about 1.8e19 overflow there as in MATLAB; the
+    scales here stay below that."""
+    import torch
+    from oracle.oracle import pca_project
+    r = np.random.default_rng(11)
+    x = (_data(3_000, 128, seed=12).astype(np.float64) * xscale).astype(np.float32)
+    P = (r.standard_normal((80, 128)) / np.sqrt(128) * pscale).astype(np.float32)
+    c = (r.uniform(0, 2, 128) * xscale).astype(np.float32)
+    x[7] = c  # a row equal to the centre
+    for renorm in (False, True):
+        want = pca_project(x, P, c, renorm)[:, :80]
+        out = torch.empty((len(x), 80), device="cuda")
+        vl.pca_project_device(out, torch.from_numpy(x).cuda(), torch.from_numpy(P).cuda(),
+                              torch.from_numpy(c).cuda(), renorm)
+        got = out.cpu().numpy().astype(np.float64)
+        assert np.all(got[7] == 0.0)
+        keep = np.arange(len(x)) != 7
+        rel = np.linalg.norm(got[keep] - want[keep], axis=1) / np.linalg.norm(want[keep], axis=1)
+        assert rel.max() < 1e-5, (renorm, rel.max())
