@@ -37,6 +37,14 @@
 
 VL_EXPORT int vlb200_set_precision(int precision);
 VL_EXPORT int vlb200_get_precision(void);
+/* The arithmetic (VLB200_PREC_EXACT .. BF16_ROUTER) that the calling
+ * thread's most recent Fisher encode, E-step or EM iteration actually ran; 0
+ * before any such call.  A tensor-core mode requested for a shape the
+ * tensor-core kernels do not take (tensor-core E-step: 8 <= numClusters <=
+ * 2048, numClusters % 8 == 0, dimension <= 128; Fisher encoding also needs
+ * numClusters % 4 == 0 and the finalisation's shared memory) runs EXACT,
+ * and this reports it.  No reference counterpart. */
+VL_EXPORT int vlb200_last_precision(void);
 
 /* Library / device information. */
 VL_EXPORT char const *vlb200_version(void);
@@ -73,6 +81,17 @@ VL_EXPORT double vlb200_gmm_em_device(VlGMM *self, float const *data, vl_size nu
 VL_EXPORT vl_size vlb200_gmm_get_ll_trace(VlGMM const *self, double *trace, vl_size maxEntries);
 /* Number of empty modes re-seeded in the last EM run. */
 VL_EXPORT vl_size vlb200_gmm_get_num_restarts(VlGMM const *self);
+/* Parameter trace of EM runs (off by default; no reference counterpart: the
+ * reference returns only the final parameters, vl/gmm.c:1220-1308).  When on,
+ * each EM iteration first copies the parameters its E-step uses back to the
+ * host, so entry t holds them after t M-steps (t = 0 .. the number of
+ * iterations).  get copies entry `iteration` as double (means and covariances
+ * numClusters x dimension, priors numClusters; each pointer may be NULL) and
+ * returns the number of entries, writing nothing when iteration is past
+ * them. */
+VL_EXPORT void vlb200_gmm_set_param_trace(VlGMM *self, int on);
+VL_EXPORT vl_size vlb200_gmm_get_param_trace(VlGMM const *self, vl_size iteration, double *means,
+                                             double *covariances, double *priors);
 
 /* Fisher encoding of one image with device pointers (vl_fisher_encode,
  * vl/fisher.h:48-54).  enc: 2*D*K floats, device.  numTerms: host pointer or
@@ -243,9 +262,9 @@ VL_EXPORT int vlb200_router_set_default(VlB200Router *router, vl_size m, float t
 
 /* Fisher encoding of one image that allocates nothing.  No counterpart in
  * the reference: it exists for callers that cannot allocate device memory on
- * the call path (work being recorded into a CUDA graph by stream capture,
- * services that forbid allocation after start-up, hosts with a fixed memory
- * budget).  The caller passes inputs and outputs as device pointers, as for
+ * the call path (services that forbid allocation after start-up, loops that
+ * cannot accept cudaMalloc's implicit device synchronisation, hosts with a
+ * fixed memory budget).  The caller passes inputs and outputs as device pointers, as for
  * vlb200_fisher_encode_device; the scratch is a fixed 8 MiB device array
  * inside the library, held by every GPU that loads it until the process
  * exits.  Limits: numData <= 4096, numClusters <= 256, dimension <= 128;

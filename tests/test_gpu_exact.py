@@ -93,7 +93,9 @@ def test_em_per_iteration(vl, golden, tag):
     g = golden
     dt = DT[tag]
     T = int(g["em_T"])
-    tol = {"f": 2e-4, "d": 1e-9}[tag]
+    # Float: measured maxima over t = 0..T against VLFeat's float run: LL
+    # 3.6e-8, priors 9.3e-7, means 7.9e-7, covariances 1.8e-6, posteriors 3.6e-6.
+    tol = {"f": 1e-5, "d": 1e-9}[tag]
     for t in range(T + 1):
         m, ll = _em(vl, g, dt, t)
         ref_ll = g[f"em_ll_{tag}"][t]
@@ -112,7 +114,9 @@ def test_config0_em_and_fv(vl, restatement):
     restatement."""
     from vlfeat_b200 import workloads as W
     c = W.config0()
-    for dt, tol in ((np.float64, 1e-9), (np.float32, 2e-4)):
+    # Float against the C restatement in float (its own float rounding):
+    # measured LL 1.9e-9, priors 2.4e-6, means 6.2e-6, covariances 1.0e-5.
+    for dt, tol in ((np.float64, 1e-9), (np.float32, 5e-5)):
         d = c["data"].astype(dt)
         ref = restatement.em(d, c["priors"], c["means"], c["covs"], c["lower_bound"], c["iters"])
         m = vl.GMM(c["D"], c["K"], dt)
@@ -209,7 +213,8 @@ def test_rand_init_then_em(vl, golden, name, tag):
     if not _lanes_match(vl, golden):
         pytest.skip("this host's SIMD support differs from the fixture host's")
     m, ll = _rand_em(vl, golden, name, tag, 5)
-    tol = {"f": 2e-4, "d": 1e-9}[tag]
+    # Float: measured at most 1.1e-6 (means) against VLFeat's float run.
+    tol = {"f": 1e-5, "d": 1e-9}[tag]
     ref_ll = float(golden[f"rand_{name}_{tag}_t5_ll"])
     assert abs(ll - ref_ll) <= tol * abs(ref_ll)
     assert rel_err(m.means, golden[f"rand_{name}_{tag}_t5_means"]) < tol

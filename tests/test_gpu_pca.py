@@ -118,7 +118,8 @@ def test_pca_project_unaligned_rows(vl):
     assert float(d.max()) < 2e-5
 
 
-@pytest.mark.parametrize("xscale,pscale", [(1e-20, 1.0), (1e15, 1.0), (1.0, 1e-15), (1.0, 1e15), (3e5, 7e-4)])
+@pytest.mark.parametrize("xscale,pscale", [(1e-20, 1.0), (1e15, 1.0), (1.0, 1e-15), (1.0, 1e15), (3e5, 7e-4),
+                                           (1e36, 1e-27), (1e-30, 1e25)])
 def test_pca_project_scales(vl, xscale, pscale):
     """The tensor-core projection scales each row of x - c and the matrix P by
     powers of two into fp16's range, so data far outside it (tiny, huge, or a

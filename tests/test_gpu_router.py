@@ -112,3 +112,31 @@ def test_router_fisher_vector_within_metric(vl, restatement):
     finally:
         vl.set_precision("exact")
     assert rel_err(enc, ref) < 1e-3
+
+
+def test_nan_descriptor_falls_back_without_touching_other_rows(vl):
+    """A NaN descriptor gives NaN logits: the top-m selection must still name
+    valid components (the lowest untaken ones) and the row must fall back to
+    the full E-step (its candidate mass is NaN), so every access stays in
+    bounds.  The other rows' posteriors are unchanged."""
+    import torch
+    from vlfeat_b200.router import Router
+    K, D = 64, 16
+    pr, mu, cv, x = _mixture(K, D, 512, seed=41)
+    r = Router(D, K, hidden=(32,), seed=9)
+    r.set_input_transform(x.mean(0), 1.0 / x.std(0))
+    prt, mut, cvt = _t(pr), _t(mu), _t(cv)
+    clean = torch.zeros((x.shape[0], K), device="cuda")
+    r.posteriors(clean, prt, mut, cvt, _t(x), m=8, threshold=0.5)
+    xn = x.copy()
+    xn[100] = np.nan
+    xn[200, 3] = np.nan
+    q = torch.zeros((x.shape[0], K), device="cuda")
+    r.posteriors(q, prt, mut, cvt, _t(xn), m=8, threshold=0.5)
+    torch.cuda.synchronize()
+    qh, ch = q.cpu().numpy(), clean.cpu().numpy()
+    keep = np.ones(x.shape[0], bool)
+    keep[[100, 200]] = False
+    assert np.array_equal(qh[keep], ch[keep])
+    for row in (100, 200):
+        assert np.all(np.isnan(qh[row]) | np.isfinite(qh[row]))

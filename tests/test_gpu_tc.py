@@ -1,13 +1,20 @@
 """GPU parity of the tensor-core (tcgen05) paths through the C-ABI.
 
 Reference: the FP64 C restatement (oracle/), itself pinned to VLFeat's own
-double results.  Tolerances (relative L2 error of each Fisher vector):
-FP32 mode (fp16x3 on both contractions) 2e-5 -- measured 2.6e-6 to 4.9e-6 on
-200- and 3,000-descriptor images at K=64..1024, D=64..128, and 1.7e-5 on one
-1,000-descriptor image with the signed square root, whose slope near zero
-magnifies the absolute error of near-zero statistics (the exact CUDA-core
-path: 6.3e-6 on that image); BF16 mode 1e-3 (the metric's bound; measured
-~1e-4, set by the single fp16 part of q)."""
+double results.  Bounds on the relative L2 error of each Fisher vector:
+
+* FP32 mode (fp16x3 on both contractions, fp32 accumulation): 1e-5, or --
+  where VLFeat's own float path (oracle/_ref, the same image) is further
+  than that from FP64 -- VLFeat's float error.  The improved Fisher vector's
+  signed square root magnifies the absolute error of near-zero statistics, so
+  fp32 arithmetic of either kind exceeds 1e-5 on a few images: on 256 images
+  of the benchmark's shape VLFeat's float path measured max 1.5e-5 (median
+  4.3e-6, 2 images above 1e-5), this path max 1.2e-5 (median 3.4e-6, 2
+  images above 1e-5), the exact CUDA-core path max 1.7e-5.
+* BF16 mode: 1e-3 (the metric's bound; measured ~1-2e-4, set by the single
+  fp16 part of q)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -16,7 +23,27 @@ from oracle.oracle import FLAG_FAST, FLAG_IMPROVED, FLAG_NORMALIZED, FLAG_SQUARE
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp32": 2e-5, "bf16": 1e-3}
+TOL = {"fp32": 1e-5, "bf16": 1e-3}
+
+
+@pytest.fixture(scope="module")
+def vlfeat_float():
+    """VLFeat's own CPU library (float path), or None where it is not built."""
+    from oracle.oracle import Reference
+    try:
+        return Reference(threads=os.cpu_count() or 1)
+    except (FileNotFoundError, OSError):
+        return None
+
+
+def fv_bound(mode, ref64, vf, x, mu, cv, pr, flags):
+    """The bound for one Fisher vector: TOL[mode], raised for FP32 mode to
+    VLFeat's own float error on the same input when that is larger."""
+    if mode != "fp32" or vf is None:
+        return TOL[mode]
+    e, _ = vf.fisher(x.astype(np.float32), mu.astype(np.float32), cv.astype(np.float32),
+                     pr.astype(np.float32), flags)
+    return max(TOL[mode], rel_err(e, ref64))
 
 
 @pytest.fixture(autouse=True)
@@ -33,7 +60,7 @@ def _t(a, dev="cuda"):
 @pytest.mark.parametrize("mode", ["fp32", "bf16"])
 # (256, 128): W does not fit in shared memory and streams through the stages.
 @pytest.mark.parametrize("KD", [(256, 80), (64, 64), (128, 80), (64, 128), (256, 128)])
-def test_fv_single(vl, restatement, mode, KD):
+def test_fv_single(vl, restatement, vlfeat_float, mode, KD):
     from vlfeat_b200 import workloads as W
     K, D = KD
     pr, mu, cv = W.fv_gmm(K, D, seed=3)
@@ -42,13 +69,14 @@ def test_fv_single(vl, restatement, mode, KD):
                                    pr.astype(np.float64), FLAG_IMPROVED)
     vl.set_precision(mode)
     enc, nt = vl.fisher_encode(x, mu, cv, pr, FLAG_IMPROVED)
-    assert rel_err(enc, ref) < TOL[mode]
+    assert vl.last_precision() == mode
+    assert rel_err(enc, ref) < fv_bound(mode, ref, vlfeat_float, x, mu, cv, pr, FLAG_IMPROVED)
     assert abs(nt - nref) <= max(2, 1e-3 * nref)
 
 
 @pytest.mark.parametrize("mode", ["fp32", "bf16"])
 @pytest.mark.parametrize("flags", [0, FLAG_SQUARE_ROOT, FLAG_NORMALIZED, FLAG_IMPROVED | FLAG_FAST])
-def test_fv_flags(vl, restatement, mode, flags):
+def test_fv_flags(vl, restatement, vlfeat_float, mode, flags):
     from vlfeat_b200 import workloads as W
     pr, mu, cv = W.fv_gmm(256, 80, seed=7)
     x = W.pca_like(1000, 80, seed=8)
@@ -56,12 +84,12 @@ def test_fv_flags(vl, restatement, mode, flags):
                                    pr.astype(np.float64), flags)
     vl.set_precision(mode)
     enc, nt = vl.fisher_encode(x, mu, cv, pr, flags)
-    tol = TOL[mode] * (3 if flags & FLAG_FAST else 1)
+    tol = fv_bound(mode, ref, vlfeat_float, x, mu, cv, pr, flags) * (3 if flags & FLAG_FAST else 1)
     assert rel_err(enc, ref) < tol
 
 
 @pytest.mark.parametrize("mode", ["fp32", "bf16"])
-def test_batched_uneven(vl, restatement, mode):
+def test_batched_uneven(vl, restatement, vlfeat_float, mode):
     import torch
     from vlfeat_b200 import workloads as W
     K, D = 256, 80
@@ -80,7 +108,8 @@ def test_batched_uneven(vl, restatement, mode):
         if counts[j] == 0:
             assert np.all(enc[j] == 0) and nt[j] == 0
         else:
-            assert rel_err(enc[j], e) < TOL[mode], j
+            xj = x[offs[j]:offs[j + 1]]
+            assert rel_err(enc[j], e) < fv_bound(mode, e, vlfeat_float, xj, mu, cv, pr, FLAG_IMPROVED), j
             assert abs(int(nt[j]) - n) <= max(2, 1e-3 * n), j
 
 
@@ -94,10 +123,9 @@ def test_posteriors_fp32(vl, restatement, D):
     vl.set_precision("fp32")
     q, ll = vl.get_gmm_data_posteriors(x, pr, mu, cv)
     # Each score sums 2D fp16x3 products, so the error grows with D.  Measured
-    # max |q - q64| 1.6e-5 (D=80), 2.7e-5 (D=128); LL relative 1.0e-6, 3.4e-6:
-    # the log-likelihood carries a small error common to a row's logits (the
-    # fp32 accumulation of the score), which the posteriors do not see.
-    q_tol, ll_tol = {80: (4e-5, 2e-6), 128: (6e-5, 6e-6)}[D]
+    # max |q - q64| 1.3e-5 (D=80), 2.0e-5 (D=128) -- the exact CUDA-core path,
+    # VLFeat's formulation in fp32: 2.1e-5, 4.6e-5; LL relative 8.7e-7, 1.7e-6.
+    q_tol, ll_tol = {80: (2.5e-5, 2e-6), 128: (4e-5, 4e-6)}[D]
     assert np.max(np.abs(q - q64)) < q_tol
     assert abs(ll - ll64) < ll_tol * abs(ll64)
 
@@ -175,7 +203,7 @@ CLUSTER_KD = [(1024, 80), (520, 80), (300, 64), (512, 128)]
 
 @pytest.mark.parametrize("mode", ["fp32", "bf16"])
 @pytest.mark.parametrize("KD", CLUSTER_KD)
-def test_fv_cluster(vl, restatement, mode, KD):
+def test_fv_cluster(vl, restatement, vlfeat_float, mode, KD):
     from vlfeat_b200 import workloads as W
     K, D = KD
     pr, mu, cv = W.fv_gmm(K, D, seed=31)
@@ -184,7 +212,7 @@ def test_fv_cluster(vl, restatement, mode, KD):
                                    pr.astype(np.float64), FLAG_IMPROVED)
     vl.set_precision(mode)
     enc, nt = vl.fisher_encode(x, mu, cv, pr, FLAG_IMPROVED)
-    assert rel_err(enc, ref) < TOL[mode]
+    assert rel_err(enc, ref) < fv_bound(mode, ref, vlfeat_float, x, mu, cv, pr, FLAG_IMPROVED)
     assert abs(nt - nref) <= max(2, 1e-3 * nref)
 
 
@@ -205,7 +233,7 @@ def test_fv_cluster_fast(vl, restatement, mode):
 
 
 @pytest.mark.parametrize("mode", ["fp32", "bf16"])
-def test_batched_uneven_cluster(vl, restatement, mode):
+def test_batched_uneven_cluster(vl, restatement, vlfeat_float, mode):
     import torch
     from vlfeat_b200 import workloads as W
     K, D = 520, 80
@@ -224,7 +252,8 @@ def test_batched_uneven_cluster(vl, restatement, mode):
         if counts[j] == 0:
             assert np.all(enc[j] == 0) and nt[j] == 0
         else:
-            assert rel_err(enc[j], e) < TOL[mode], j
+            xj = x[offs[j]:offs[j + 1]]
+            assert rel_err(enc[j], e) < fv_bound(mode, e, vlfeat_float, xj, mu, cv, pr, FLAG_IMPROVED), j
             assert abs(int(nt[j]) - n) <= max(2, 1e-3 * n), j
 
 
@@ -238,7 +267,7 @@ def test_posteriors_cluster_fp32(vl, restatement, KD):
                                        mu.astype(np.float64), cv.astype(np.float64))
     vl.set_precision("fp32")
     q, ll = vl.get_gmm_data_posteriors(x, pr, mu, cv)
-    q_tol, ll_tol = {64: (4e-5, 2e-6), 80: (4e-5, 2e-6), 128: (6e-5, 6e-6)}[D]
+    q_tol, ll_tol = {64: (2.5e-5, 2e-6), 80: (2.5e-5, 2e-6), 128: (4e-5, 4e-6)}[D]
     assert np.max(np.abs(q - q64)) < q_tol
     assert abs(ll - ll64) < ll_tol * abs(ll64)
 
@@ -256,3 +285,47 @@ def test_em_cluster_k1024(vl, restatement, mode):
     assert rel_err(m.means, r["means"]) < EM_TOL[mode]
     assert rel_err(m.covariances, r["covs"]) < EM_TOL[mode]
     assert rel_err(m.priors, r["priors"]) < EM_TOL[mode]
+
+
+def test_config1_full_size_em_per_iteration(vl):
+    """Config 1 at its stated size: N = 1,000,000 SIFT-like descriptors, D =
+    128, K = 256, custom initialisation from 256 seeded rows, variance floor
+    1e-4 x the largest global variance, 20 iterations.  Every iteration's
+    parameters (after t M-steps, t = 0..20) and log-likelihood are compared
+    with an FP64 run on the GPU from the same initialisation (the library's
+    exact double kernels, which match VLFeat's double path to 1e-10).
+    Measured maxima over the 21 snapshots (relative L2): FP32 mode means
+    7.8e-6, covariances 1.2e-5, priors 6.3e-6, LL 1.3e-7; EXACT (VLFeat's
+    float formulation) 8.3e-6, 1.3e-5, 3.8e-5, 2.3e-7; BF16 5.6e-5, 8.6e-5,
+    4.3e-5, 1.4e-7.  The errors grow about linearly with the iterations."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    c = W.config1(N=1_000_000, K=256, iters=20)
+
+    def model(dt):
+        m = vl.GMM(128, 256, dt)
+        m.set_initialization("custom")
+        m.set_max_num_iterations(20)
+        m.set_covariance_lower_bound(c["lower_bound"])
+        m.set_means(c["means"])
+        m.set_covariances(c["covs"])
+        m.set_priors(c["priors"])
+        m.set_param_trace(True)
+        return m
+    m64 = model(np.float64)
+    m64.cluster(c["data"].astype(np.float64))
+    tr64, ll64 = m64.param_trace(), m64.ll_trace
+    assert len(tr64) == 21
+    x = torch.from_numpy(c["data"]).cuda()
+    bounds = {"fp32": (2e-5, 2e-5, 2e-5, 5e-7), "exact": (2e-5, 3e-5, 8e-5, 5e-7),
+              "bf16": (1.5e-4, 2e-4, 1e-4, 5e-7)}
+    for mode, (bm, bc, bp, bl) in bounds.items():
+        m = model(np.float32)
+        m.em_device(x, mode)
+        tr, ll = m.param_trace(), m.ll_trace
+        assert len(tr) == 21 and len(ll) == 21, mode
+        for t in range(21):
+            assert rel_err(tr[t][0], tr64[t][0]) < bm, (mode, t)
+            assert rel_err(tr[t][1], tr64[t][1]) < bc, (mode, t)
+            assert rel_err(tr[t][2], tr64[t][2]) < bp, (mode, t)
+            assert abs(ll[t] - ll64[t]) < bl * abs(ll64[t]), (mode, t)

@@ -1,6 +1,7 @@
 """GPU test of vlb200_fisher_encode_noalloc, the entry point for callers that
-cannot allocate device memory on the call path (stream capture, services
-that forbid allocation after start-up, fixed memory budgets).
+cannot allocate device memory on the call path (services that forbid
+allocation after start-up, loops that cannot accept cudaMalloc's implicit
+synchronisation, fixed memory budgets).
 
 It is called through the C-ABI and compared with the allocating entry point
 vlb200_fisher_encode_device in the same (exact fp32) arithmetic, within the
@@ -68,3 +69,43 @@ def test_noalloc_rejects_oversized_request(vl):
                  t(x).data_ptr(), N, vl.FLAG_IMPROVED, None, None)
     assert rc == 3  # VL_ERR_BAD_ARG
     assert b"exceeds" in lib.vl_get_last_error_message()
+
+
+def test_noalloc_empty_image_and_null_term_count(vl):
+    """numData = 0 gives the zero vector and no terms, as vl/fisher.c:
+    383, 450 and 481-484 do (the memset, no prefix, norm floored at 1e-12);
+    a NULL numTerms is accepted.  Two calls in a row on the shared scratch."""
+    import torch
+    lib = vl.lib()
+    noalloc = _bind(lib)
+    stream = torch.cuda.current_stream()
+    handle = C.c_void_p(stream.cuda_stream if stream.cuda_stream else 1)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    K, D = 32, 16
+    pr, mu, cv, x = _case(5, K, D, 700)
+    mu_t, cv_t, pr_t, x_t = t(mu), t(cv), t(pr), t(x)
+    enc = torch.full((2 * K * D,), float("nan"), device="cuda")
+    nt = torch.full((1,), 123, dtype=torch.int64, device="cuda")
+    rc = noalloc(enc.data_ptr(), mu_t.data_ptr(), D, K, cv_t.data_ptr(), pr_t.data_ptr(),
+                 x_t.data_ptr(), 0, vl.FLAG_IMPROVED, nt.data_ptr(), handle)
+    assert rc == 0, lib.vl_get_last_error_message()
+    torch.cuda.synchronize()
+    assert np.array_equal(enc.cpu().numpy(), np.zeros(2 * K * D, np.float32))
+    assert int(nt.item()) == 0
+    ref = torch.zeros(2 * K * D, device="cuda")
+    vl.fisher_encode_device(ref, mu_t, cv_t, pr_t, x_t, vl.FLAG_IMPROVED, "exact", stream)
+    enc.fill_(float("nan"))
+    rc = noalloc(enc.data_ptr(), mu_t.data_ptr(), D, K, cv_t.data_ptr(), pr_t.data_ptr(),
+                 x_t.data_ptr(), x.shape[0], vl.FLAG_IMPROVED, None, handle)
+    assert rc == 0, lib.vl_get_last_error_message()
+    torch.cuda.synchronize()
+    assert rel_err(enc.cpu().numpy(), ref.cpu().numpy()) < 2e-5
+
+
+def test_noalloc_rejects_sizes_that_wrap_when_signed(vl):
+    """Sizes of 2^63 and above are refused before any arithmetic on them."""
+    lib = vl.lib()
+    noalloc = _bind(lib)
+    for n, k, d in ((1 << 63, 8, 8), (16, (1 << 64) - 1, 8), (16, 8, 1 << 63)):
+        rc = noalloc(None, None, d, k, None, None, None, n, vl.FLAG_IMPROVED, None, None)
+        assert rc == 3  # VL_ERR_BAD_ARG

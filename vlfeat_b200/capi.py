@@ -94,6 +94,7 @@ def _decl(L):
     f("vlb200_device_ok", C.c_int)
     f("vlb200_set_precision", C.c_int, C.c_int)
     f("vlb200_get_precision", C.c_int)
+    f("vlb200_last_precision", C.c_int)
     f("vlb200_launch_count", C.c_uint64)
     f("vlb200_profile_enable", None, C.c_int)
     f("vlb200_profile_reset", None)
@@ -103,6 +104,8 @@ def _decl(L):
     f("vlb200_gmm_em_device", C.c_double, _vp, _vp, _sz, C.c_int)
     f("vlb200_gmm_get_ll_trace", _sz, _vp, _vp, _sz)
     f("vlb200_gmm_get_num_restarts", _sz, _vp)
+    f("vlb200_gmm_set_param_trace", None, _vp, C.c_int)
+    f("vlb200_gmm_get_param_trace", _sz, _vp, _sz, _vp, _vp, _vp)
     f("vlb200_fisher_encode_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _sz, C.c_int,
       C.c_int, C.POINTER(C.c_uint64), _vp)
     f("vlb200_fisher_encode_batch_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _sz,
@@ -173,6 +176,13 @@ def set_precision(p) -> None:
 
 def get_precision() -> int:
     return int(lib().vlb200_get_precision())
+
+
+def last_precision() -> str:
+    """Arithmetic the calling thread's last encode / E-step / EM iteration
+    actually ran ("exact", "fp32", "bf16", "bf16_router"; "" before any)."""
+    v = int(lib().vlb200_last_precision())
+    return {k: n for n, k in PRECISIONS.items() if n != "default"}.get(v, "")
 
 
 def device_ok() -> bool:
@@ -331,6 +341,20 @@ class GMM:
     @property
     def num_restarts(self) -> int:
         return int(lib().vlb200_gmm_get_num_restarts(self._h))
+
+    def set_param_trace(self, on: bool = True) -> None:
+        """Keep every EM iteration's parameters (vlb200_gmm_set_param_trace)."""
+        lib().vlb200_gmm_set_param_trace(self._h, 1 if on else 0)
+
+    def param_trace(self):
+        """[(means, covariances, priors)] as float64, entry t after t M-steps."""
+        out = []
+        n = int(lib().vlb200_gmm_get_param_trace(self._h, 1 << 62, None, None, None))
+        for t in range(n):
+            mu = np.zeros((self.K, self.D)); cv = np.zeros((self.K, self.D)); pr = np.zeros(self.K)
+            lib().vlb200_gmm_get_param_trace(self._h, t, _np_ptr(mu), _np_ptr(cv), _np_ptr(pr))
+            out.append((mu, cv, pr))
+        return out
 
 
 def get_gmm_data_posteriors(data, priors, means, covariances):

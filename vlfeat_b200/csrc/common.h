@@ -126,6 +126,10 @@ void *pinned_host(size_t bytes);
 // Process-wide precision default (VLB200_PREC_*).
 int default_precision();
 int resolve_precision(int precision, bool is_double);
+// Records the arithmetic a call actually used (VLB200_PREC_*), per thread:
+// a request for a tensor-core mode on a shape the tensor-core kernels do not
+// take runs EXACT, and vlb200_last_precision() reports that.
+void note_precision(int used);
 
 // Host-side printf through the VLFeat hook.
 #define VLB_PRINTF(...) ((*vl_get_printf_func())(__VA_ARGS__))

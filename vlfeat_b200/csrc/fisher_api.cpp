@@ -34,11 +34,13 @@ void encode_batch(T *enc, const vlb::DevModel<T> &m, const T *X, const i64 *h_of
   if constexpr (sizeof(T) == 4) {
     if (precision != VLB200_PREC_EXACT && vlb::tc_fv_supported(m.K, m.D)) {
       vlb::tc_fisher_batch(X, h_offsets, numImages, m, enc, nterms, flags, precision, s);
+      vlb::note_precision(precision);
       return;
     }
   }
-  vlb::exact_fisher_batch<T>(X, h_offsets, numImages, m, enc, nterms, flags, s,
-                             sizeof(T) == 4 && precision == VLB200_PREC_BF16_ROUTER);
+  const bool router = sizeof(T) == 4 && precision == VLB200_PREC_BF16_ROUTER;
+  vlb::exact_fisher_batch<T>(X, h_offsets, numImages, m, enc, nterms, flags, s, router);
+  vlb::note_precision(router ? VLB200_PREC_BF16_ROUTER : VLB200_PREC_EXACT);
 }
 
 template <typename T>

@@ -47,6 +47,10 @@ struct _VlGMM {
   vlb::DevBuf dX, dq, dmeans, dcovs, dpriors, dlb, dtmp, dassign;
   std::vector<double> llTrace;
   vl_size numRestarts = 0;
+  // Parameter snapshots of the last EM run (vlb200_gmm_set_param_trace):
+  // entry t holds means, covariances and priors after t M-steps, in double.
+  bool traceParams = false;
+  std::vector<std::vector<double>> paramTrace;
 };
 
 namespace {
@@ -100,6 +104,7 @@ double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int pr
       nparts = em_image ? vlb::tc_estep_em(dX, N, m, dq, llp, precision, s)
                         : vlb::tc_estep(dX, N, m, dq, llp, fast, precision, s);
       done = true;
+      vlb::note_precision(precision);
     }
   }
   if (!done) {
@@ -109,6 +114,7 @@ double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int pr
     der.cst = sc.slot[19].get<double>(m.K);
     vlb::exact_prepare(m, der, s);
     nparts = vlb::exact_estep(dX, N, m, der, dq, llp, fast, s);
+    vlb::note_precision(VLB200_PREC_EXACT);
   }
   if (N <= 0) return 0.0;
   vlb::sum_doubles(llp, nparts, dll, s);
@@ -200,6 +206,7 @@ double em_device(VlGMM *self, const T *dX, i64 N, int precision) {
   VLB_CUDA(cudaMemcpyAsync(dlb, self->sigmaLowBound, sizeof(double) * D, cudaMemcpyHostToDevice, s));
   self->numData = (vl_size)N;  // _vl_gmm_prepare_for_data, vl/gmm.c:336-344
   self->llTrace.clear();
+  self->paramTrace.clear();
   self->numRestarts = 0;
 
   vlb::DevModel<T> m;
@@ -215,7 +222,17 @@ double em_device(VlGMM *self, const T *dX, i64 N, int precision) {
   bool tcm = false;
   if constexpr (sizeof(T) == 4) tcm = precision != VLB200_PREC_EXACT && vlb::tc_supported(K, D);
   double prevLL = -INFINITY, LL = -INFINITY;
+  std::vector<T> snap;
   for (vl_size it = 0;; ++it) {
+    if (self->traceParams) {
+      // The parameters this iteration's E-step uses: after `it` M-steps.
+      snap.resize((size_t)(2 * K * D + K));
+      VLB_CUDA(cudaMemcpyAsync(snap.data(), dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaMemcpyAsync(snap.data() + K * D, dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaMemcpyAsync(snap.data() + 2 * K * D, dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaStreamSynchronize(s));
+      self->paramTrace.emplace_back(snap.begin(), snap.end());
+    }
     LL = device_estep<T>(dX, N, m, dq, precision, false, s, tcm);
     self->llTrace.push_back(LL);
     if (self->verbosity)
@@ -675,5 +692,22 @@ vl_size vlb200_gmm_get_ll_trace(VlGMM const *self, double *trace, vl_size maxEnt
 }
 
 vl_size vlb200_gmm_get_num_restarts(VlGMM const *self) { return self->numRestarts; }
+
+void vlb200_gmm_set_param_trace(VlGMM *self, int on) {
+  self->traceParams = on != 0;
+  if (!on) self->paramTrace.clear();
+}
+
+vl_size vlb200_gmm_get_param_trace(VlGMM const *self, vl_size iteration, double *means,
+                                   double *covariances, double *priors) {
+  const vl_size n = self->paramTrace.size();
+  if (iteration >= n) return n;
+  const std::vector<double> &v = self->paramTrace[iteration];
+  const size_t KD = (size_t)self->numClusters * self->dimension;
+  if (means) std::copy(v.begin(), v.begin() + KD, means);
+  if (covariances) std::copy(v.begin() + KD, v.begin() + 2 * KD, covariances);
+  if (priors) std::copy(v.begin() + 2 * KD, v.begin() + 2 * KD + self->numClusters, priors);
+  return n;
+}
 
 }  // extern "C"

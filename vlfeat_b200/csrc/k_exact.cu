@@ -667,7 +667,9 @@ void exact_prepare(const DevModel<T> &m, DevDerived<T> &der, cudaStream_t s) {
                                                           der.cst, der.sis));
 }
 
-i64 estep_ll_parts(i64 N) { return (N + 7) / 8 + 1; }  // capacity bound for any E-step kernel
+// Capacity bound for any E-step kernel: the exact kernels write one partial
+// per 8 rows; the tensor-core E-step 8 per 128-row tile.
+i64 estep_ll_parts(i64 N) { return std::max<i64>((N + 7) / 8 + 1, 8 * ((N + 127) / 128) + 8); }
 
 template <typename T>
 i64 exact_estep(const T *X, i64 N, const DevModel<T> &m, const DevDerived<T> &der, T *q,

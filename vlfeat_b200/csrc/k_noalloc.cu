@@ -1,9 +1,9 @@
 // Fisher encoding of one image without any allocation.
 //
-// Some callers cannot allocate device memory on the call path: code running
-// under a CUDA stream capture that must not add allocation nodes, real-time
-// or embedded services that forbid allocation after start-up, and hosts that
-// hand the library a fixed memory budget.  vlb200_fisher_encode_noalloc
+// Some callers cannot allocate device memory on the call path: real-time or
+// embedded services that forbid allocation after start-up, loops that cannot
+// accept the implicit device synchronisation of cudaMalloc / cudaFree, and
+// hosts that hand the library a fixed memory budget.  vlb200_fisher_encode_noalloc
 // serves them: its scratch (posteriors, per-component constants, partial
 // statistics, segment tables) lives in one file-scope device array of fixed
 // size, and the call performs no cudaMalloc / cudaFree, no host-to-device
@@ -84,8 +84,10 @@ extern "C" int vlb200_fisher_encode_noalloc(float *enc, float const *means, vl_s
     using vlb::i64;
     VLB_CHECK(numClusters >= 1 && dimension >= 1, VL_ERR_BAD_ARG,
               "vlb200_fisher_encode_noalloc: numClusters and dimension must be >= 1");
-    VLB_CHECK((i64)numData <= vlb::kMaxData && (i64)numClusters <= vlb::kMaxClusters &&
-                  (i64)dimension <= vlb::kMaxDim,
+    // Compared as unsigned sizes before any conversion to i64, so that no
+    // size of 2^63 or more can wrap to a negative value and pass.
+    VLB_CHECK(numData <= (vl_size)vlb::kMaxData && numClusters <= (vl_size)vlb::kMaxClusters &&
+                  dimension <= (vl_size)vlb::kMaxDim,
               VL_ERR_BAD_ARG,
               "vlb200_fisher_encode_noalloc: request exceeds the fixed scratch "
               "(numData <= 4096, numClusters <= 256, dimension <= 128)");

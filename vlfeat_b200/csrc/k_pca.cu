@@ -384,8 +384,13 @@ __global__ void __launch_bounds__(kPtThreads, 1) k_pca_tc(const PcaTcParams p) {
       const bool valid = row < p.N;
       const int sx = sexp[buf * 128 + rl];
       const i64 img0 = p.frames ? timg[buf] : 0;  // read before the stage is released below
-      // acc 2^-(s + g), as two exact power-of-two factors.
-      const float f1 = pow2f(-sx), f2 = pow2f(-g);
+      // acc 2^-(s + g).  The combined exponent e is applied as 2^e1 2^(e - e1)
+      // with e1 the part within a float's normal range: the second factor is 1
+      // unless |e| > 126, and the first product cannot overflow (or leave the
+      // normal range) when the final value is finite and normal, whatever the
+      // signs of s and g.
+      const int e = -(sx + g), e1 = e > 126 ? 126 : (e < -126 ? -126 : e);
+      const float f1 = pow2f(e1), f2 = pow2f(e - e1);
       const uint32_t taddr = tmem + (uint32_t)(buf * 128) + ((uint32_t)(32 * ew) << 16);
       float inv = 1.f;
       if (p.renorm) {

@@ -247,6 +247,19 @@ __global__ void k_select(const float *__restrict__ Zl, i64 n, int K, int m, int 
       const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
+    if (bi == 0x7fffffff) {
+      // No remaining logit compares above -inf (NaN or -inf logits): take the
+      // lowest untaken index, so that every candidate is a valid component.
+      int li = 0x7fffffff;
+#pragma unroll
+      for (int i = 0; i < KPL; ++i) {
+        const int k = lane + 32 * i;
+        if (k < K && !((taken >> i) & 1u) && k < li) li = k;
+      }
+      for (int o = 16; o > 0; o >>= 1) li = min(li, __shfl_xor_sync(0xffffffffu, li, o));
+      bi = li;  // < K: m <= K components are taken in all
+      bv = -INFINITY;
+    }
     if (lane == (bi & 31)) taken |= 1u << (bi >> 5);
     if (lane == t) mine = bi;
     sel += expf(bv - mx);
@@ -269,7 +282,7 @@ __global__ void k_candidate_estep(const float *__restrict__ X, i64 n, int D, int
   if (row >= n) return;
   const float *x = X + row * D;
   float *qr = q + row * K;
-  const bool fb = cmass[row] < thr;
+  const bool fb = !(cmass[row] >= thr);  // a NaN mass (NaN logits) falls back too
   const int nc = fb ? K : m;
   for (int k = lane; k < K; k += 32) qr[k] = 0.f;
   __syncwarp();

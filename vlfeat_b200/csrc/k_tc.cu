@@ -95,30 +95,55 @@ __global__ void k_tc_center(const float *__restrict__ means, int K, int D, float
   if (lane == 0) ctr[d] = (float)(s / (double)K);
 }
 
+// The x''^2 weight of component k and dimension d, -1/2 / s2_kd / scale_d^2
+// log2(e), before the common part is taken out.
+__device__ __forceinline__ double tc_weight2(const float *__restrict__ covs, const float *__restrict__ scale,
+                                             int k, int d, int D) {
+  const double s2 = (double)covs[(i64)k * D + d], sc = (double)scale[d];
+  return -0.5 / s2 / (sc * sc) * 1.4426950408889634;
+}
+
+// Common part of the x''^2 weights: wbar_d = mean over the components of
+// tc_weight2 (fixed-order sums, one warp per dimension).  The logits of a
+// row change by the same amount sum_d wbar_d x''_d^2 when it is taken out of
+// every component's weights, so the posteriors do not change, while the
+// terms the fp32 accumulator adds (and the logit it rounds) shrink by about
+// an order of magnitude; the log-likelihood adds the common part back.
+__global__ void k_tc_wbar(const float *__restrict__ covs, const float *__restrict__ scale, int K, int D,
+                          float *__restrict__ wbar) {
+  const int d = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (d >= D) return;
+  double s = 0;
+  for (int k = lane; k < K; k += 32) s += tc_weight2(covs, scale, k, d, D);
+  s = warp_sum(s);
+  if (lane == 0) wbar[d] = (float)(s / (double)K);
+}
+
 // Entries of the E-step's weight matrix for component k and K-order element
 // e (chunk c = e / 32 holds x''_d for d = 16c .. 16c+15, then x''_d^2 for the
 // same d, so that the producers read each element of x once):
-//   [mu'_kd / s2_kd / scale_d, -1/2 / s2_kd / scale_d^2] log2(e),
+//   [mu'_kd / s2_kd / scale_d, -1/2 / s2_kd / scale_d^2 - wbar_d] log2(e),
 // the producers multiplying x' by the power of two scale_d.
 __device__ __forceinline__ double tc_weight(const float *__restrict__ means, const float *__restrict__ covs,
-                                            const float *__restrict__ ctr, const float *__restrict__ scale, int k,
-                                            int e, int D) {
+                                            const float *__restrict__ ctr, const float *__restrict__ scale,
+                                            const float *__restrict__ wbar, int k, int e, int D) {
   const int c = e / 32, ee = e % 32, d = 16 * c + (ee & 15);
+  if (ee >= 16) return tc_weight2(covs, scale, k, d, D) - (double)wbar[d];
   const double s2 = (double)covs[(i64)k * D + d], sc = (double)scale[d];
   const double mup = (double)means[(i64)k * D + d] - (double)ctr[d];
-  return (ee < 16 ? mup / s2 / sc : -0.5 / s2 / (sc * sc)) * 1.4426950408889634;
+  return mup / s2 / sc * 1.4426950408889634;
 }
 
 // max |w| over the model: one element per thread, a warp maximum, then an
 // atomic maximum on the float's bits (non-negative floats order as their bits;
 // *wmax is zeroed before the launch).  The maximum does not depend on order.
 __global__ void k_tc_wmax(const float *__restrict__ means, const float *__restrict__ covs,
-                          const float *__restrict__ ctr, const float *__restrict__ scale, int K, int D,
-                          float *__restrict__ wmax) {
+                          const float *__restrict__ ctr, const float *__restrict__ scale,
+                          const float *__restrict__ wbar, int K, int D, float *__restrict__ wmax) {
   const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   float m = 0.f;
   if (i < (i64)K * 2 * D)
-    m = (float)fabs(tc_weight(means, covs, ctr, scale, (int)(i / (2 * D)), (int)(i % (2 * D)), D));
+    m = (float)fabs(tc_weight(means, covs, ctr, scale, wbar, (int)(i / (2 * D)), (int)(i % (2 * D)), D));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax((unsigned *)wmax, __float_as_uint(m));
@@ -131,8 +156,8 @@ __global__ void k_tc_wmax(const float *__restrict__ means, const float *__restri
 // E-step multiplies back onto every logit.
 __global__ void k_tc_wimg(const float *__restrict__ means, const float *__restrict__ covs,
                           const float *__restrict__ ctr, const float *__restrict__ scale,
-                          const float *__restrict__ wmax, int K, int Kp, int D, __half *__restrict__ wimg,
-                          float *__restrict__ wsc) {
+                          const float *__restrict__ wbar, const float *__restrict__ wmax, int K, int Kp,
+                          int D, __half *__restrict__ wimg, float *__restrict__ wsc) {
   const int KD2 = 2 * D;
   i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   int g = 0;
@@ -146,7 +171,7 @@ __global__ void k_tc_wimg(const float *__restrict__ means, const float *__restri
   const int k = (int)(idx / KD2), e = (int)(idx % KD2);
   const int c = e / 32, ee = e % 32;
   float w = 0.f;
-  if (k < K) w = (float)ldexp(tc_weight(means, covs, ctr, scale, k, e, D), -g);
+  if (k < K) w = (float)ldexp(tc_weight(means, covs, ctr, scale, wbar, k, e, D), -g);
   const __half hi = __float2half_rn(w);
   const __half lo = __float2half_rn(w - __half2float(hi));
   const size_t wbytes = (size_t)(KD2 / 32) * Kp * 64;
@@ -156,16 +181,16 @@ __global__ void k_tc_wimg(const float *__restrict__ means, const float *__restri
   *(__half *)(base + wbytes + off) = lo;
 }
 
-// cst2_k = log2(e) * (log pi_k - D/2 log 2pi - 1/2 sum log s2 - 1/2 sum mu'^2/s2),
-// -inf for padding and for priors below 1e-6 (vl/gmm.c:746-747).
+// c_k = log2(e) * (log pi_k - D/2 log 2pi - 1/2 sum log s2 - 1/2 sum mu'^2/s2)
+// in double, -inf for padding and for priors below 1e-6 (vl/gmm.c:746-747).
 __global__ void k_tc_cst(const float *__restrict__ priors, const float *__restrict__ means,
                          const float *__restrict__ covs, const float *__restrict__ ctr, int K,
-                         int Kp, int D, float *__restrict__ cst2) {
+                         int Kp, int D, double *__restrict__ cst64) {
   // One warp per component; lanes take dimensions d = lane, lane + 32, ...
   const int k = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x % 32;
   if (k >= Kp) return;
   if (k >= K || (double)priors[k] < 1e-6) {
-    if (lane == 0) cst2[k] = -INFINITY;
+    if (lane == 0) cst64[k] = -INFINITY;
     return;
   }
   double c = 0;
@@ -175,7 +200,27 @@ __global__ void k_tc_cst(const float *__restrict__ priors, const float *__restri
     c += 0.5 * log(s2) + 0.5 * mup * mup / s2;
   }
   c = log((double)priors[k]) - 0.5 * (double)D * log(2.0 * 3.141592653589793) - warp_sum(c);
-  if (lane == 0) cst2[k] = (float)(c * 1.4426950408889634);
+  if (lane == 0) cst64[k] = c * 1.4426950408889634;
+}
+
+// cst2_k = c_k - cbar in float, with cbar the mean of the finite c_k (one
+// warp, fixed-order sums; 0 when every component is skipped).  Like wbar,
+// cbar is common to all components: the posteriors do not see it, the float
+// constants carry less rounding, and the log-likelihood adds it back.
+__global__ void k_tc_cst_center(const double *__restrict__ cst64, int Kp, float *__restrict__ cst2,
+                                double *__restrict__ cbar) {
+  const int lane = threadIdx.x;
+  double s = 0, n = 0;
+  for (int k = lane; k < Kp; k += 32)
+    if (cst64[k] != -INFINITY) {
+      s += cst64[k];
+      n += 1;
+    }
+  s = warp_sum(s);
+  n = warp_sum(n);
+  const double c = n > 0 ? s / n : 0.0;
+  for (int k = lane; k < Kp; k += 32) cst2[k] = cst64[k] == -INFINITY ? -INFINITY : (float)(cst64[k] - c);
+  if (lane == 0) *cbar = c;
 }
 
 // Per-dimension power-of-two scale for fp16 statistics operands, chosen from
@@ -235,6 +280,8 @@ struct EParams {
   const float *ctr;
   const float *scl;  // per-dimension power-of-two scale of x' (the operands are x'' = x' scale)
   const float *wsc;  // the W image's power-of-two scale (one float, device)
+  const float *wbar;   // common part of the x''^2 weights (log2 units), taken out of W
+  const double *cbar;  // common part of the constants (log2 units), taken out of cst2
   void *q;     // row-major posteriors (kQRow*) or the image (kQImg*)
   void *qimg;  // the image of the combined formats
   int ldq;
@@ -368,6 +415,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     // whose rows are already in flight (a 3-deep register prefetch ring).
     i64 t0 = tile0, t1, t2;
     int c0 = 0, c1, c2, it = 0;
+    // Log-likelihood: the common parts taken out of the logits, per row
+    // sum_d wbar_d x''_d^2 + cbar (log2 units), summed in double in a fixed
+    // order (this lane's rows and dimensions over the tile's chunks, then the
+    // warp's butterfly) and written as the warp's partial for the tile, after
+    // the epilogue's partials (ll_part[4 ntiles + 4 tile + warp]).
+    const bool want_ll = p.ll_part != nullptr && crank == 0;
+    const double cb = want_ll ? *p.cbar : 0.0;
+    double cacc = 0.0;
     auto adv = [&](i64 t, int c, i64 &tn, int &cn) {
       tn = t;
       cn = c + 1;
@@ -395,12 +450,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       }
       const int d0 = 16 * c0 + 4 * part;
       const float4 mm = __ldg((const float4 *)(p.ctr + d0)), sc = __ldg((const float4 *)(p.scl + d0));
+      const float4 wb = want_ll ? __ldg((const float4 *)(p.wbar + d0)) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         // x'' = (x - ctr) scale, kept inside fp16's range (an x'' beyond it
         // is more than 255 model scales from the centre).
         const float v0 = clamp_f16((cur[s].x - mm.x) * sc.x), v1 = clamp_f16((cur[s].y - mm.y) * sc.y);
         const float v2 = clamp_f16((cur[s].z - mm.z) * sc.z), v3 = clamp_f16((cur[s].w - mm.w) * sc.w);
+        if (want_ll && t0 * 128 + 32 * warp + 8 * s + rr < p.N)
+          cacc += (double)wb.x * ((double)v0 * v0) + (double)wb.y * ((double)v1 * v1) +
+                  (double)wb.z * ((double)v2 * v2) + (double)wb.w * ((double)v3 * v3);
         uint32_t h0, l0, h1, l1, h2, l2, h3, l3;
         split2<true>(v0, v1, h0, l0);
         split2<true>(v2, v3, h1, l1);
@@ -416,6 +475,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       }
       fence_proxy_async_smem();
       mbar_arrive(&full[stage]);
+      if (want_ll && c0 == NKA - 1) {
+        const double v = warp_sum(cacc);
+        if (lane == 0) {
+          const i64 r0 = t0 * 128 + 32 * warp;
+          const i64 nv = p.N - r0 < 0 ? 0 : (p.N - r0 > 32 ? 32 : p.N - r0);
+          p.ll_part[p.ntiles * 4 + t0 * 4 + warp] = (v + (double)nv * cb) * kLn2;
+        }
+        cacc = 0.0;
+      }
       ++it;
       t0 = t1; c0 = c1;
       t1 = t2; c1 = c2;
@@ -1257,7 +1325,8 @@ __global__ void k_rows_to_image16(const float *__restrict__ q, i64 n, int K, int
 // ================================================================ host
 struct TcPrep {
   int K = 0, Kp = 0, D = 0;
-  float *ctr = nullptr, *cst2 = nullptr, *scale = nullptr, *wsc = nullptr;
+  float *ctr = nullptr, *cst2 = nullptr, *scale = nullptr, *wsc = nullptr, *wbar = nullptr;
+  double *cbar = nullptr;
   __half *wimg = nullptr;
 };
 
@@ -1287,20 +1356,26 @@ void tc_prepare(const DevModel<float> &m, TcPrep &tp, bool want_scale, Scratch &
   tp.scale = sc.slot[12].get<float>(256);
   float *wm = sc.slot[19].get<float>(2);
   tp.wsc = wm + 1;
+  tp.wbar = sc.slot[20].get<float>(256);
+  double *c64 = sc.slot[21].get<double>((size_t)std::max(256, tp.Kp) + 1);
+  tp.cbar = c64 + std::max(256, tp.Kp);
   VLB_LAUNCH("tc_center", s, k_tc_center<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, tp.K, tp.D, tp.ctr));
   VLB_LAUNCH("tc_scale", s,
              k_tc_scale<<<(tp.D + 7) / 8, 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.K, tp.D, tp.scale));
+  VLB_LAUNCH("tc_wbar", s, k_tc_wbar<<<(tp.D + 7) / 8, 256, 0, s>>>(m.covs, tp.scale, tp.K, tp.D, tp.wbar));
   VLB_CUDA(cudaMemsetAsync(wm, 0, sizeof(float), s));
   const i64 nw = (i64)tp.K * KD2;
   VLB_LAUNCH("tc_wmax", s,
-             k_tc_wmax<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.scale, tp.K, tp.D, wm));
+             k_tc_wmax<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.scale, tp.wbar,
+                                                                    tp.K, tp.D, wm));
   const i64 n = (i64)tp.Kp * KD2;
   VLB_LAUNCH("tc_wimage", s,
-             k_tc_wimg<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.scale, wm, tp.K,
-                                                                  tp.Kp, tp.D, tp.wimg, tp.wsc));
+             k_tc_wimg<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(m.means, m.covs, tp.ctr, tp.scale, tp.wbar,
+                                                                  wm, tp.K, tp.Kp, tp.D, tp.wimg, tp.wsc));
   VLB_LAUNCH("tc_constants", s,
              k_tc_cst<<<(tp.Kp + 7) / 8, 256, 0, s>>>(m.priors, m.means, m.covs, tp.ctr, tp.K,
-                                                          tp.Kp, tp.D, tp.cst2));
+                                                          tp.Kp, tp.D, c64));
+  VLB_LAUNCH("tc_constants_center", s, k_tc_cst_center<<<1, 32, 0, s>>>(c64, tp.Kp, tp.cst2, tp.cbar));
 }
 
 int padQ(int Kp) { return (Kp + 127) / 128 * 128; }
@@ -1341,6 +1416,7 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   p.X = X; p.N = N; p.K = tp.K; p.Kp = Kb; p.Kg = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
   p.qpart = ntiles * 128 * (i64)p.Kq * 2;
   p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr; p.scl = tp.scale; p.wsc = tp.wsc;
+  p.wbar = tp.wbar; p.cbar = tp.cbar;
   p.q = q; p.qimg = eo.qimg; p.ldq = ldq; p.fast = fast ? 1 : 0; p.qthr = float_at_least(eo.qthr);
   p.rowcnt = rowcnt; p.ll_part = ll_part;
   p.err = err; p.ntiles = ntiles;
@@ -1369,7 +1445,7 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
     cfg.gridDim = dim3((unsigned)(nb * std::min<i64>(ntiles, maxc)));
     VLB_LAUNCH("tc_estep_f16x3", s, VLB_CUDA(cudaLaunchKernelEx(&cfg, kern, p)));
   }
-  return ntiles * 4;  // LL partials written
+  return ll_part ? ntiles * 8 : ntiles * 4;  // LL partials written: epilogue's, then the common parts
 }
 
 // W resident in shared memory when two operand stages fit beside it, else

@@ -252,6 +252,9 @@ void *pinned_host(size_t bytes) {
 
 int default_precision() { return g_precision.load(); }
 
+thread_local int t_last_precision = 0;
+void note_precision(int used) { t_last_precision = used; }
+
 int resolve_precision(int p, bool is_double) {
   if (is_double) return VLB200_PREC_EXACT;
   if (p == VLB200_PREC_DEFAULT) p = g_precision.load();
@@ -289,6 +292,8 @@ void launch_end(const char *name, cudaStream_t s) {
 }  // namespace vlb
 
 extern "C" {
+
+int vlb200_last_precision(void) { return vlb::t_last_precision; }
 
 vl_uint64 vlb200_launch_count(void) { return vlb::g_launches.load(); }
 
