@@ -281,4 +281,19 @@ VL_EXPORT int vlb200_fisher_encode_noalloc(float *enc, float const *means, vl_si
                                            vl_size numData, int flags, vl_uint64 *numTerms,
                                            void *stream);
 
+/* ------------------------------------------------------ failure checks
+ * No reference counterpart.  Every wait of the library's tcgen05 kernels on
+ * an mbarrier is bounded (2 s): a wait that expires records a code in the
+ * launch's error word, raises the block's abort flag so that every role
+ * leaves its loop and TMEM is freed, and the host raises VL_ERR_BAD_ARG with
+ * "gave up waiting (code N)".  vlb200_selftest_bounded_wait runs that
+ * mechanism on a barrier that nothing arrives on, with a wait limit of
+ * limit_ms (0 < limit_ms <= 1000): it returns VL_ERR_BAD_ARG with the
+ * message of an expired wait (code 99), and the CUDA context stays usable.
+ * vlb200_debug_fail_allocations(n) makes the library's next n device
+ * allocations fail as a failed cudaMalloc does (VL_ERR_ALLOC, the call
+ * returns its error sentinel); 0 clears it. */
+VL_EXPORT int vlb200_selftest_bounded_wait(double limit_ms);
+VL_EXPORT void vlb200_debug_fail_allocations(vl_size n);
+
 #endif /* VLB200_H */

@@ -67,6 +67,11 @@ bool profile_swap(bool on);
     ::vlb::count_launch();             \
   } while (0)
 
+// Host-side fault injection (vlb200_debug_fail_allocations): the next n
+// device allocations of the library's buffers fail as cudaMalloc failures
+// do.  Returns true when this allocation is to fail.
+bool take_injected_alloc_failure();
+
 // Grow-only device buffer.  Contents are not preserved across growth.
 struct DevBuf {
   void *p = nullptr;
@@ -91,7 +96,7 @@ struct DevBuf {
     if (bytes > cap) {
       release();
       size_t want = bytes + bytes / 8;
-      cudaError_t e = cudaMalloc(&p, want);
+      cudaError_t e = take_injected_alloc_failure() ? cudaErrorMemoryAllocation : cudaMalloc(&p, want);
       if (e != cudaSuccess) {
         p = nullptr;
         cudaGetLastError();

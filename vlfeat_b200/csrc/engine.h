@@ -143,6 +143,9 @@ void router_default_posteriors(const float *X, i64 N, const DevModel<float> &m, 
 // ------------------------------------------------------- tensor-core path
 // Implemented in k_tc.cu.  Available for float data only.
 bool tc_supported(i64 K, i64 D);
+// Runs the bounded-wait self-test kernel with a wait limit of limit_ms and
+// raises the error a kernel's expired wait raises.
+void wait_selftest(double limit_ms, cudaStream_t s);
 // The tensor-core Fisher encoder (E-step, statistics and the cluster finalize).
 bool tc_fv_supported(i64 K, i64 D);
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,

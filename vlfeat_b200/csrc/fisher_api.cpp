@@ -146,4 +146,13 @@ int vlb200_fisher_encode_batch_device(float *enc, float const *means, vl_size di
       (int)VL_ERR_BAD_ARG);
 }
 
+int vlb200_selftest_bounded_wait(double limit_ms) {
+  return guarded(
+      [&]() -> int {
+        vlb::wait_selftest(limit_ms, vlb::thread_stream());
+        return 0;
+      },
+      (int)VL_ERR_BAD_ARG);
+}
+
 }  // extern "C"

@@ -179,6 +179,7 @@ vl_size restart_empty_modes(VlGMM *self, const T *dX, i64 N, T *dq, T *dmeans, T
         bv = (double)cv[best * D + d];
         bd = d;
       }
+    if (bd < 0) continue;  // every variance NaN: no dimension to split along
     vlb::restart_split<T>(dq, dX, N, K, D, icl, best, bd, mu[best * D + bd], s);
     vlb::exact_mstep<T>(dX, N, dq, dmeans, dcovs, dpriors, K, D, dlb, s);
     VLB_CUDA(cudaMemcpyAsync(pr.data(), dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));

@@ -245,7 +245,12 @@ __global__ void k_tc_scale(const float *__restrict__ means, const float *__restr
 }
 
 // ============================================================ E-step
-__device__ __forceinline__ float clamp_f16(float v) { return fminf(fmaxf(v, -65504.f), 65504.f); }
+// Finite values beyond fp16's range are clamped to it; NaN and +-inf pass
+// through, so that a non-finite descriptor gives a non-finite result, as in
+// the reference's float arithmetic.
+__device__ __forceinline__ float clamp_f16(float v) {
+  return fabsf(v) < INFINITY ? fminf(fmaxf(v, -65504.f), 65504.f) : v;
+}
 
 // The q image holds q * 2^14 in fp16 (one part, or hi and lo parts): every
 // posterior the statistics keep (q >= 1e-6) is then a normal fp16 number.
@@ -1562,7 +1567,36 @@ void lpt_assign(const std::vector<SItem> &items, int gx, std::vector<int> &order
   beg[gx] = (int)order.size();
 }
 
+// Self-test of the bounded waits of the tcgen05 kernels (mbar_wait): one CTA,
+// an mbarrier that nothing arrives on.  Thread 0 waits with `limit_ns`, gives
+// up, records code 99 in *err and raises the abort flag, as any role of the
+// kernels above does when its producer or consumer never comes; warp 1 waits
+// on the same barrier with the kernels' own limit and leaves on the flag.
+// Every wait is bounded, so the kernel returns in either case.
+__global__ void k_wait_selftest(unsigned long long limit_ns, int *err) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait(&bar, 0, (volatile int *)&abort_flag, err, 99, limit_ns);
+  else if (threadIdx.x == 32) mbar_wait(&bar, 0, (volatile int *)&abort_flag, err, 98);
+  __syncthreads();
+}
+
 }  // namespace
+
+void wait_selftest(double limit_ms, cudaStream_t s) {
+  VLB_CHECK(limit_ms > 0 && limit_ms <= 1000, VL_ERR_BAD_ARG, "wait self-test: limit must be in (0, 1000] ms");
+  Scratch &sc = thread_scratch(kArenaTc);
+  int *err = sc.slot[3].get<int>(1);
+  VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  VLB_LAUNCH("wait_selftest", s, k_wait_selftest<<<1, 64, 0, s>>>((unsigned long long)(limit_ms * 1e6), err));
+  check_err(err, s);
+}
 
 bool tc_supported(i64 K, i64 D) {
   if (!(D == 64 || D == 80 || D == 128)) return false;

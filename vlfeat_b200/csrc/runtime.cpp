@@ -255,6 +255,12 @@ int default_precision() { return g_precision.load(); }
 thread_local int t_last_precision = 0;
 void note_precision(int used) { t_last_precision = used; }
 
+std::atomic<long long> g_fail_allocs{0};
+bool take_injected_alloc_failure() {
+  if (g_fail_allocs.load() <= 0) return false;
+  return g_fail_allocs.fetch_sub(1) > 0;
+}
+
 int resolve_precision(int p, bool is_double) {
   if (is_double) return VLB200_PREC_EXACT;
   if (p == VLB200_PREC_DEFAULT) p = g_precision.load();
@@ -294,6 +300,8 @@ void launch_end(const char *name, cudaStream_t s) {
 extern "C" {
 
 int vlb200_last_precision(void) { return vlb::t_last_precision; }
+
+void vlb200_debug_fail_allocations(vl_size n) { vlb::g_fail_allocs.store((long long)n); }
 
 vl_uint64 vlb200_launch_count(void) { return vlb::g_launches.load(); }
 

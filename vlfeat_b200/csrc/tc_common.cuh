@@ -58,13 +58,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // false) when the block's abort flag is raised or after kWaitNs; in the latter
 // case records `code` in *err and raises the abort flag.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
-                                          int *err, int code) {
+                                          int *err, int code, unsigned long long limit_ns = kWaitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort_flag) return false;
-    if (global_ns() - t0 > kWaitNs) {
+    if (global_ns() - t0 > limit_ns) {
       atomicCAS(err, 0, code);
       *abort_flag = 1;
       return false;
