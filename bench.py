@@ -432,11 +432,7 @@ def em_throughput(capi, iters=5, cpu=True, large=True):
     out = {"timing": "wall clock around vlb200_gmm_em_device (blocking), after one untimed run"}
     cfgs = [("config1_sift_n1m_d128_k256", W.config1(N=1_000_000, K=256, iters=20), 20),
             ("config0_n50k_d64_k64", W.config0(), 10)]
-    if large:
-        # Config 4's shape (SIFT-like, D=128, K=1024) at N=8,000,000 of its
-        # 20,000,000: the posteriors (N x K) and the M-step's posterior image
-        # stay in HBM (66 GB here, 164 GB at full N in FP32 mode).
-        cfgs.append(("config4_shape_sift_n8m_d128_k1024", W.config1(N=8_000_000, K=1024, iters=3), 3))
+
     def trace_errors(g, ref):
         """Per-iteration relative L2 errors of the parameters (after t M-steps)
         and of the log-likelihood against the FP64 run."""
@@ -515,17 +511,97 @@ def em_throughput(capi, iters=5, cpu=True, large=True):
                                "sample": f"config 1, first {n} descriptors, 2 iterations of vl_gmm_cluster",
                                "descriptor_iterations_per_s": n * 2 / dt,
                                "ms_per_iteration": 1e3 * dt / 2}
-        if large:
-            c4 = cfgs[-1][1]
-            n4 = 20_000
-            t0 = time.perf_counter()
-            impl.em(np.ascontiguousarray(c4["data"][:n4]), c4["priors"], c4["means"], c4["covs"],
-                    c4["lower_bound"], 1)
-            dt = time.perf_counter() - t0
-            out["cpu_baseline_config4_shape"] = {
-                "kind": kind, "cores": os.cpu_count() or 1,
-                "sample": f"config 4 shape, first {n4} descriptors, 1 iteration of vl_gmm_cluster",
-                "descriptor_iterations_per_s": n4 / dt}
+    if large:
+        out["config4_streamed_n20m_d128_k1024"] = em_config4(capi, cpu=cpu)
+    return out
+
+
+def em_config4(capi, N=20_000_000, K=1024, D=128, T=15, m=8, threshold=0.99, judge_every=5, cpu=True):
+    """Config 4: streamed EM at N = 20,000,000 SIFT-like descriptors (10 GB
+    resident), D = 128, K = 1,024, 15 iterations from a custom initialisation
+    (1,024 seeded rows, unbiased global variance, uniform priors, variance
+    floor 1e-4 x the largest global variance); the N x K posteriors are never
+    resident (82 GB in fp32).  Runs: the plain FP32 path (fp16x3 tensor-core
+    E-step and statistics); the BF16 path (fp16x3 E-step, one fp16 q part in
+    the statistics); BF16 with router-pruned E-steps (MLP 128-256-256-1024,
+    m = 8, full E-step below 0.99 predicted candidate mass) and a full E-step
+    every 5th iteration, which re-fits the router and judges its missed
+    posterior mass.  All three reduce the M-step in f64.  The BF16 runs'
+    final log-likelihood and parameters are compared with the FP32 run's."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    from vlfeat_b200.router import Router
+    x = W.sift_like_device(N, D, seed=400)
+    pr, mu, cv, lb = W.custom_init_device(x, K, seed=401)
+
+    def model():
+        g = capi.GMM(D, K, np.float32)
+        g.set_initialization("custom")
+        g.set_max_num_iterations(T)
+        g.set_covariance_lower_bound(lb)
+        g.set_means(mu)
+        g.set_covariances(cv)
+        g.set_priors(pr)
+        return g
+
+    def rel(a, b):
+        return float(np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b))
+
+    out = {"N": N, "D": D, "K": K, "max_iterations": T, "data": "SIFT-like, generated on the GPU (seed 400)",
+           "timing": "wall clock around vlb200_gmm_em_stream_device (blocking)"}
+    runs = {}
+    for name, prec, use_router in (("fp32", "fp32", False), ("bf16", "bf16", False),
+                                   ("bf16_router", "bf16", True)):
+        r = None
+        if use_router:
+            r = Router(D, K, hidden=(256, 256), seed=5)
+            xm = x[:1 << 20].mean(0).cpu().numpy()
+            xs = x[:1 << 20].std(0).clamp_min(1e-3).cpu().numpy()
+            r.set_input_transform(xm, (1.0 / xs).astype(np.float32))
+        g = model()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ll = g.em_stream_device(x, prec, router=r, m=m, threshold=threshold, judge_every=judge_every)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        rep = g.stream_report()
+        its = len(rep) - 1
+        res = {"seconds": dt, "iterations": its, "ms_per_iteration": 1e3 * dt / max(1, its),
+               "descriptor_iterations_per_s": N * its / dt, "log_likelihood": ll, "restarts": g.num_restarts,
+               "e_step_ms": [round(row["ms"], 1) for row in rep]}
+        if use_router:
+            res["router"] = {"m": m, "threshold": threshold, "judge_every": judge_every,
+                             "judged_missed_mass": {str(t): rep[t]["missed_mass"] for t in range(len(rep))
+                                                    if rep[t]["judged"]},
+                             "fallback_fraction": {str(t): rep[t]["fallback_rows"] / N for t in range(len(rep))
+                                                   if rep[t]["routed"]}}
+        runs[name] = (g, res)
+        out[name] = res
+        del r
+    ga = runs["fp32"][0]
+    for name in ("bf16", "bf16_router"):
+        g = runs[name][0]
+        out[name]["vs_fp32_path"] = {
+            "log_likelihood_rel": abs(g.loglikelihood - ga.loglikelihood) / abs(ga.loglikelihood),
+            "means_rel": rel(g.means, ga.means), "covariances_rel": rel(g.covariances, ga.covariances),
+            "priors_rel": rel(g.priors, ga.priors)}
+    out["bf16_router_vs_fp32_speed"] = out["fp32"]["seconds"] / out["bf16_router"]["seconds"]
+    if cpu:
+        from oracle import oracle as O
+        n4 = 20_000
+        try:
+            impl, kind = O.Reference(threads=os.cpu_count() or 1), "reference"
+        except (FileNotFoundError, OSError):
+            impl, kind = O.Restatement(), "port"
+        xs = x[:n4].cpu().numpy()
+        t0 = time.perf_counter()
+        impl.em(np.ascontiguousarray(xs), pr, mu, cv, lb, 1)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"kind": kind, "cores": os.cpu_count() or 1,
+                               "sample": f"first {n4} descriptors, 1 iteration of vl_gmm_cluster",
+                               "descriptor_iterations_per_s": n4 / dt}
+    del runs, x
+    torch.cuda.empty_cache()
     return out
 
 
@@ -756,6 +832,89 @@ def kmeans_init_throughput(capi, cpu=True, n=1_000_000, n_cpu=25_000):
     return out
 
 
+def router_config3(capi, n_train=2_000_000, n_eval=10_000_000, ms=(4, 8, 16), threshold=0.99,
+                   epochs=6, fv_images=1000, fv_rows=3000):
+    """The learned router at its own configuration: K = 1,024, D = 80, a
+    seeded 1,024-component mixture (sigma ~ U[0.3, 1.5]); an MLP 80 -> 256 ->
+    256 -> 1024 (ReLU) trained by the library's own forward / backward / Adam
+    kernels on the top-8 posteriors of the full E-step of 2,000,000
+    descriptors, then evaluated on 10,000,000 held-out descriptors at m in
+    {4, 8, 16}: missed posterior mass without fallback, the fraction of rows
+    whose predicted candidate mass is below 0.99 (those fall back to the full
+    E-step) and the missed mass with that fallback, against the full E-step's
+    posteriors; and the improved Fisher vectors of 1,000 held-out images of
+    3,000 descriptors through the router path against the FP32 path."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    from vlfeat_b200.router import Router, missed_mass, targets
+    K3, D3 = 1024, 80
+    params = W.config3_params(K3, D3)
+    pr, mu, cv = (torch.from_numpy(a).cuda() for a in params)
+    out = {"workload": f"K={K3}, D={D3}, mixture sigma ~ U[0.3, 1.5]; MLP {D3}-256-256-{K3}; "
+                       f"{n_train} training / {n_eval} held-out descriptors", "threshold": threshold}
+    xtr = W.config3_data_device(n_train, params, seed=501)
+    q = torch.empty((n_train, K3), device="cuda")
+    capi.gmm_posteriors_device(q, pr, mu, cv, xtr, "fp32")
+    tidx = torch.empty((n_train, 8), dtype=torch.int32, device="cuda")
+    tw = torch.empty((n_train, 8), dtype=torch.float32, device="cuda")
+    targets(q, tidx, tw)
+    del q
+    r = Router(D3, K3, hidden=(256, 256), seed=3)
+    xm, xs = xtr.mean(0).cpu().numpy(), xtr.std(0).cpu().numpy()
+    r.set_input_transform(xm, (1.0 / xs).astype(np.float32))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = r.train(xtr, tidx, tw, epochs=epochs, batch=1024, lr=2e-3)
+    torch.cuda.synchronize()
+    out["training"] = {"epochs": epochs, "batch": 1024, "last_epoch_loss": loss,
+                       "seconds": time.perf_counter() - t0}
+    del xtr, tidx, tw
+    xev = W.config3_data_device(n_eval, params, seed=502)
+    chunk = 1 << 20
+    per_m = {}
+    for m in ms:
+        mm0 = mm1 = 0.0
+        fb = 0
+        t_router = 0.0
+        for i in range(0, n_eval, chunk):
+            xb = xev[i:i + chunk]
+            b = xb.shape[0]
+            qf = torch.empty((b, K3), device="cuda")
+            capi.gmm_posteriors_device(qf, pr, mu, cv, xb, "fp32")
+            qc = torch.empty_like(qf)
+            r.posteriors(qc, pr, mu, cv, xb, m=m, threshold=0.0)
+            mm0 += missed_mass(qf, qc) * b
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            fb += r.posteriors(qc, pr, mu, cv, xb, m=m, threshold=threshold)
+            torch.cuda.synchronize()
+            t_router += time.perf_counter() - t1
+            mm1 += missed_mass(qf, qc) * b
+            del qf, qc
+        per_m[str(m)] = {"missed_mass_without_fallback": mm0 / n_eval,
+                         "fallback_fraction": fb / n_eval, "missed_mass_with_fallback": mm1 / n_eval,
+                         "router_posteriors_rows_per_s": n_eval / t_router}
+    out["eval"] = per_m
+    # Fisher vectors of held-out images through the router path (m = 8).
+    n_img = min(fv_images, n_eval // fv_rows)
+    offs = np.arange(n_img + 1, dtype=np.int64) * fv_rows
+    xi = xev[: n_img * fv_rows].contiguous()
+    ref = torch.empty((n_img, 2 * K3 * D3), device="cuda")
+    capi.fisher_encode_batch_device(ref, mu, cv, pr, xi, offs, FLAGS, "fp32")
+    enc = torch.empty_like(ref)
+    fv = {}
+    for m in ms:
+        r.set_default(m=m, threshold=threshold)
+        capi.fisher_encode_batch_device(enc, mu, cv, pr, xi, offs, FLAGS, "bf16_router")
+        e = ((enc.double() - ref.double()).norm(dim=1) / ref.double().norm(dim=1)).cpu().numpy()
+        fv[str(m)] = {"max": float(e.max()), "p50": float(np.median(e)), "images": int(n_img)}
+    out["fv_rel_err_vs_fp32_path"] = fv
+    capi.lib().vlb200_router_set_default(None, 8, 0.99)
+    del r, xev, xi, ref, enc
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: VLFeat's own CPU code on the host cores."""
     if rank != 0:
@@ -810,6 +969,8 @@ def main():
                     help="skip the descriptor prologue (PCA projection) measurement")
     ap.add_argument("--no-kmeans", action="store_true",
                     help="skip the GMM KMeans-initialisation measurement")
+    ap.add_argument("--no-router-eval", action="store_true",
+                    help="skip the learned router's evaluation at K=1024 (train 2M, evaluate 10M)")
     ap.add_argument("--images", type=int, default=4096,
                     help="encode only the first IMAGES images of the workload (small profiling cases)")
     ap.add_argument("--plan", default=None,
@@ -921,6 +1082,11 @@ def main():
             out["prologue"] = prologue_throughput(capi, wl, cpu=not args.no_cpu)
         if not args.no_kmeans and world == 1:
             out["kmeans_init"] = kmeans_init_throughput(capi, cpu=not args.no_cpu)
+        if not args.no_router_eval and world == 1:
+            if router is not None:
+                capi.lib().vlb200_router_set_default(None, 8, 0.99)
+                del router
+            out["router_config3"] = router_config3(capi)
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

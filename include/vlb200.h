@@ -15,6 +15,8 @@
 #include "vl/generic.h"
 #include "vl/gmm.h"
 
+struct _VlB200Router; /* the learned router, declared below */
+
 /* Arithmetic used on the GPU.
  *  EXACT      direct (x-mu)^2/sigma^2 evaluation in the data type on CUDA cores
  *             (float or double), the reference's own formulation
@@ -75,6 +77,36 @@ VL_EXPORT int vlb200_gmm_posteriors_device(float *posteriors, vl_size numCluster
  * copies visible through vl_gmm_get_*; posteriors are fetched lazily. */
 VL_EXPORT double vlb200_gmm_em_device(VlGMM *self, float const *data, vl_size numData,
                                       int precision);
+
+/* EM on device-resident data whose N x numClusters posteriors are never
+ * resident (no reference counterpart; the loop is vl_gmm_em's, vl/gmm.c:
+ * 1220-1308, with the reference's stopping rules and empty-mode restarts).
+ * Each E-step pass runs in chunks of about chunkRows rows (0: about 8 GB of
+ * posteriors per chunk), and the chunk's M-step statistics, column masses and
+ * log-likelihood are accumulated while its posteriors exist; the M-step is
+ * reduced in f64.  With a router (not NULL, trained or not; numClusters and
+ * dimension as the model's, set_input_transform applied), iterations that
+ * are not multiples of judgeEvery take the exact posteriors of each row's m
+ * router candidates only (full E-step for rows whose predicted candidate
+ * mass is below threshold; their log-likelihood is the log-sum-exp over the
+ * components evaluated), and every judgeEvery-th iteration runs the full
+ * E-step, re-fits the router on the first 2^20 rows' posteriors (4 epochs at
+ * iteration 0, then 1) and measures its missed posterior mass on the other
+ * rows.  vl_gmm_get_posteriors afterwards recomputes the final E-step chunk
+ * by chunk from `data`, which must then still be valid.  vl_gmm_em and
+ * vl_gmm_cluster take this path by themselves when the posteriors would not
+ * fit in free device memory.  Returns the final log-likelihood (NaN on
+ * error). */
+VL_EXPORT double vlb200_gmm_em_stream_device(VlGMM *self, float const *data, vl_size numData,
+                                             int precision, vl_size chunkRows,
+                                             struct _VlB200Router *router, vl_size m,
+                                             float threshold, vl_size judgeEvery);
+/* One row of 6 doubles per E-step of the last streamed EM: log-likelihood,
+ * judged (1: full E-step with the router judged), routed (1: router E-step),
+ * mean missed posterior mass of the router on the judged rows (NaN when not
+ * judged), rows that fell back to the full E-step, milliseconds (wall clock,
+ * the E-step pass with its statistics).  Returns the rows written. */
+VL_EXPORT vl_size vlb200_gmm_get_stream_report(VlGMM const *self, double *rows, vl_size maxIterations);
 
 /* Per-iteration log-likelihood trace of the last EM run (up to maxEntries
  * values; returns the number written). */

@@ -105,6 +105,8 @@ def _decl(L):
     f("vlb200_gmm_get_ll_trace", _sz, _vp, _vp, _sz)
     f("vlb200_gmm_get_num_restarts", _sz, _vp)
     f("vlb200_gmm_set_param_trace", None, _vp, C.c_int)
+    f("vlb200_gmm_em_stream_device", C.c_double, _vp, _vp, _sz, C.c_int, _sz, _vp, _sz, C.c_float, _sz)
+    f("vlb200_gmm_get_stream_report", _sz, _vp, _vp, _sz)
     f("vlb200_gmm_get_param_trace", _sz, _vp, _sz, _vp, _vp, _vp)
     f("vlb200_fisher_encode_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _sz, C.c_int,
       C.c_int, C.POINTER(C.c_uint64), _vp)
@@ -299,6 +301,28 @@ class GMM:
         if lib().vl_get_last_error():
             _raise_last("vlb200_gmm_em_device")
         return ll
+
+    def em_stream_device(self, data_t, precision="default", chunk_rows=0, router=None, m=8,
+                         threshold=0.99, judge_every=5) -> float:
+        """Streamed EM on a (N, D) float32 CUDA tensor, posteriors never
+        resident (vlb200_gmm_em_stream_device); `router` a router.Router or
+        None.  `data_t` must stay alive while the posteriors may be read."""
+        _clear()
+        ll = lib().vlb200_gmm_em_stream_device(self._h, data_t.data_ptr(), data_t.shape[0], _prec(precision),
+                                               int(chunk_rows), router._h if router is not None else None,
+                                               int(m), float(threshold), int(judge_every))
+        if lib().vl_get_last_error():
+            _raise_last("vlb200_gmm_em_stream_device")
+        return ll
+
+    def stream_report(self):
+        """Per E-step of the last streamed EM: dicts of log-likelihood,
+        judged, routed, missed_mass, fallback_rows, ms."""
+        buf = np.zeros((4096, 6), np.float64)
+        n = int(lib().vlb200_gmm_get_stream_report(self._h, _np_ptr(buf), 4096))
+        keys = ("loglikelihood", "judged", "routed", "missed_mass", "fallback_rows", "ms")
+        return [{k: (bool(v) if k in ("judged", "routed") else float(v)) for k, v in zip(keys, row)}
+                for row in buf[:n]]
 
     def _get(self, fn, n):
         ct = C.c_float if self.dtype == np.float32 else C.c_double

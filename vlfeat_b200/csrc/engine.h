@@ -53,6 +53,20 @@ void sum_doubles(const double *part, i64 n, double *out, cudaStream_t s);
 template <typename T>
 void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i64 K, i64 D,
                  const double *lb, cudaStream_t s);
+// The same M-step over rows streamed in chunks: the rows are cut into slabs
+// of `rps` rows (exact_mstep_slab_rows(N) is exact_mstep's own choice), each
+// chunk starting on a slab boundary; exact_mstep_stats_rows writes the slab
+// partials of rows [row0, row0 + n) (posteriors q: n x K) centred on
+// oldMeans; exact_mstep_finalize_slabs reduces nslab slabs in order and
+// updates the parameters.  pmass: nslab x K, ps1/ps2: nslab x K x D doubles.
+i64 exact_mstep_slab_rows(i64 N);
+template <typename T>
+void exact_mstep_stats_rows(const T *X, i64 row0, i64 n, i64 rps, const T *q, const T *oldMeans, i64 K,
+                            i64 D, double *pmass, double *ps1, double *ps2, cudaStream_t s);
+template <typename T>
+void exact_mstep_finalize_slabs(int nslab, const double *pmass, const double *ps1, const double *ps2,
+                                const double *lb, T *means, T *covs, T *priors, i64 K, i64 D,
+                                cudaStream_t s);
 
 // Rand initialisation pieces (vl/gmm.c:1376-1443), bit-exact with the
 // reference.  global_variance: sigma (D) from X (N x D).  kmeanspp: K centres
@@ -159,6 +173,21 @@ i64 tc_estep_em(const float *X, i64 N, const DevModel<float> &m, float *q, doubl
                 int precision, cudaStream_t s);
 void tc_mstep(const float *X, i64 N, float *means, float *covs, float *priors, i64 K, i64 D,
               const double *lb, int precision, cudaStream_t s);
+// Streaming EM, one chunk of rows at a time (N x K never resident).  After
+// tc_estep_em on a chunk (or tc_em_image_from_rows, which makes the chunk's
+// thresholded fp16 image from row-major posteriors), tc_em_stats adds the
+// chunk's statistics (rows [row0, row0 + n) of X; split 2: fp16x3 from the
+// FP32 mode's image, 1: one fp16 q part) as tc_em_items(n) item partials
+// starting at item0 of `partial` (tc_em_partial_floats(K, D) floats each);
+// tc_em_finalize then applies the M-step from all nitems partials, in f64.
+// Every call of a pass uses the same model, on the same thread.
+void tc_em_image_from_rows(const float *qrows, i64 n, const DevModel<float> &m, cudaStream_t s);
+i64 tc_em_items(i64 n);
+size_t tc_em_partial_floats(i64 K, i64 D);
+void tc_em_stats(const float *X, i64 row0, i64 n, i64 K, i64 D, int split, float *partial, int item0,
+                 cudaStream_t s);
+void tc_em_finalize(int nitems, const float *partial, float *means, float *covs, float *priors, i64 K,
+                    i64 D, const double *lb, cudaStream_t s);
 void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages,
                      const DevModel<float> &m, float *enc, unsigned long long *nterms, int flags,
                      int precision, cudaStream_t s);

@@ -7,6 +7,8 @@
 // device during the loop and are copied back at the end; posteriors are
 // copied back lazily on the first vl_gmm_get_posteriors() call.
 #include <algorithm>
+#include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -51,7 +53,26 @@ struct _VlGMM {
   // entry t holds means, covariances and priors after t M-steps, in double.
   bool traceParams = false;
   std::vector<std::vector<double>> paramTrace;
+  // Streamed EM (vlb200_gmm_em_stream_device): one report row per E-step, and
+  // what the posteriors are recomputed from when they are asked for (they are
+  // never resident: N x K can exceed the device's memory).
+  std::vector<std::array<double, 6>> streamReport;
+  bool postLazy = false;
+  const void *lazyX = nullptr;
+  int lazyPrec = 0;
+  VlB200Router *lazyRouter = nullptr;
+  vl_size lazyM = 8;
+  float lazyThr = 0.99f;
+  vl_size lazyChunk = 0;
+  vlb::DevBuf dpart, dpm, dp1, dp2, dqr, dpe;
 };
+
+namespace vlb {
+double router_estep(VlB200Router *r, const float *X, i64 n, const DevModel<float> &m, float *q,
+                    size_t mcand, float thr, unsigned long long *fallback, cudaStream_t s);
+double router_missed_sum(const float *qfull, const float *qc, i64 n, i64 K, cudaStream_t s);
+void router_fit(VlB200Router *r, const float *X, i64 n, const float *q, int epochs, float lr, cudaStream_t s);
+}  // namespace vlb
 
 namespace {
 
@@ -74,8 +95,56 @@ auto guarded(F &&f, decltype(f()) sentinel) -> decltype(f()) {
   return sentinel;
 }
 
+template <typename T>
+double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int precision,
+                    bool fast, cudaStream_t s, bool em_image = false);
+
+// Posteriors of a streamed EM, recomputed chunk by chunk from the data and
+// the final parameters with the final E-step's arithmetic (the loop ends
+// after an E-step, so they are that E-step's posteriors, vl/gmm.c:1220-1308).
+template <typename T>
+void lazy_posteriors(VlGMM *self) {
+  cudaStream_t s = vlb::thread_stream();
+  const i64 K = (i64)self->numClusters, D = (i64)self->dimension, N = (i64)self->numData;
+  const i64 chunk = std::max<i64>(1, (i64)self->lazyChunk);
+  vlb::DevModel<T> m;
+  m.means = self->dmeans.get<T>(K * D);
+  m.covs = self->dcovs.get<T>(K * D);
+  m.priors = self->dpriors.get<T>(K);
+  m.K = K;
+  m.D = D;
+  T *dq = self->dq.get<T>((size_t)std::min(chunk, N) * K);
+  const T *X = (const T *)self->lazyX;
+  for (i64 r0 = 0; r0 < N; r0 += chunk) {
+    const i64 n = std::min(chunk, N - r0);
+    bool done = false;
+    if constexpr (sizeof(T) == 4) {
+      if (self->lazyRouter) {
+        vlb::router_estep(self->lazyRouter, X + r0 * D, n, m, dq, self->lazyM, self->lazyThr, nullptr, s);
+        done = true;
+      }
+    }
+    if (!done) device_estep<T>(X + r0 * D, n, m, dq, self->lazyPrec, false, s, false);
+    VLB_CUDA(cudaMemcpyAsync((T *)self->posteriors + r0 * K, dq, sizeof(T) * n * K, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
 // Host copy of the posteriors, refreshed from the device when stale.
 void sync_posteriors(VlGMM *self) {
+  if (self->postLazy) {
+    const size_t bytes = tsize(self->dataType) * self->numData * self->numClusters;
+    if (self->posteriorsCap < self->numData || !self->posteriors) {
+      vl_free(self->posteriors);
+      self->posteriors = vl_malloc(bytes ? bytes : 1);
+      VLB_CHECK(self->posteriors != nullptr, VL_ERR_ALLOC, "vl_gmm_get_posteriors: host allocation failed");
+      self->posteriorsCap = self->numData;
+    }
+    if (self->dataType == VL_TYPE_FLOAT) lazy_posteriors<float>(self);
+    else lazy_posteriors<double>(self);
+    self->postLazy = false;
+    return;
+  }
   if (!self->postOnDevice) return;
   const size_t bytes = tsize(self->dataType) * self->numData * self->numClusters;
   if (self->posteriorsCap < self->numData || !self->posteriors) {
@@ -93,7 +162,7 @@ void sync_posteriors(VlGMM *self) {
 // image (EM with the tensor-core path; see vlb::tc_estep_em).
 template <typename T>
 double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int precision,
-                    bool fast, cudaStream_t s, bool em_image = false) {
+                    bool fast, cudaStream_t s, bool em_image) {
   vlb::Scratch &sc = vlb::thread_scratch();
   double *llp = sc.slot[15].get<double>(vlb::estep_ll_parts(N));
   double *dll = sc.slot[16].get<double>(1);
@@ -191,11 +260,25 @@ vl_size restart_empty_modes(VlGMM *self, const T *dX, i64 N, T *dq, T *dmeans, T
   return nsplit;
 }
 
-// The EM loop, vl/gmm.c:1220-1308, on device-resident data dX (N x D).
+struct StreamCfg;
+template <typename T>
+double em_stream_device(VlGMM *self, const T *dX, i64 N, int precision, const StreamCfg &cfg);
+template <typename T>
+double em_stream_default(VlGMM *self, const T *dX, i64 N, int precision);
+
+// The EM loop, vl/gmm.c:1220-1308, on device-resident data dX (N x D).  When
+// the N x K posteriors (and the tensor-core M-step's operand image) would not
+// fit in free device memory, the streamed loop runs instead.
 template <typename T>
 double em_device(VlGMM *self, const T *dX, i64 N, int precision) {
   cudaStream_t s = vlb::thread_stream();
   const i64 K = (i64)self->numClusters, D = (i64)self->dimension;
+  {
+    size_t freeB = 0, totalB = 0;
+    VLB_CUDA(cudaMemGetInfo(&freeB, &totalB));
+    const double need = (double)N * (double)K * (sizeof(T) + 4.0);
+    if (need > 0.8 * (double)(freeB + self->dq.cap)) return em_stream_default<T>(self, dX, N, precision);
+  }
   T *dmeans = self->dmeans.get<T>(K * D);
   T *dcovs = self->dcovs.get<T>(K * D);
   T *dpriors = self->dpriors.get<T>(K);
@@ -276,7 +359,261 @@ double em_device(VlGMM *self, const T *dX, i64 N, int precision) {
   VLB_CUDA(cudaMemcpyAsync(self->priors, dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
   VLB_CUDA(cudaStreamSynchronize(s));
   self->postOnDevice = true;
+  self->postLazy = false;
   return LL;
+}
+
+// ------------------------------------------------------------ streamed EM
+// The EM loop of vl/gmm.c:1220-1308 over data whose N x K posteriors do not
+// stay on the device: each pass runs the E-step chunk by chunk (rows
+// [r0, r0 + n)), and while a chunk's posteriors exist it adds their column
+// masses (for the restart check, vl/gmm.c:814-999), the chunk's log-
+// likelihood and its M-step statistics (vl/gmm.c:1036-1213: tensor-core item
+// partials, or the exact path's slab partials) to the pass's totals; the
+// M-step is finalised from all of them in f64 once the loop's checks allow it.
+// With a router, the E-steps of iterations that are not multiples of
+// `judgeEvery` evaluate the exact posteriors of each row's router candidates
+// only (full E-step on rows whose predicted candidate mass is below thr);
+// every judgeEvery-th iteration runs the full E-step, re-fits the router on
+// the first rows' posteriors, and measures the router's missed posterior
+// mass on the other rows against it.  Restarts re-derive the iteration's
+// posteriors chunk by chunk (the same E-step on the same parameters, then
+// the splits so far in order) for each M-step they need, as the reference
+// re-runs its M-step on the modified posteriors.
+struct StreamCfg {
+  i64 chunk = 0;
+  VlB200Router *router = nullptr;
+  vl_size m = 8;
+  float thr = 0.99f;
+  vl_size judgeEvery = 5;
+  i64 fitRows = 1 << 20;
+};
+
+template <typename T>
+double em_stream_device(VlGMM *self, const T *dX, i64 N, int precision, const StreamCfg &cfg) {
+  using clk = std::chrono::steady_clock;
+  cudaStream_t s = vlb::thread_stream();
+  const i64 K = (i64)self->numClusters, D = (i64)self->dimension;
+  VLB_CHECK(N >= 1, VL_ERR_BAD_ARG, "streamed EM: no data");
+  T *dmeans = self->dmeans.get<T>(K * D);
+  T *dcovs = self->dcovs.get<T>(K * D);
+  T *dpriors = self->dpriors.get<T>(K);
+  double *dlb = self->dlb.get<double>(D);
+  VLB_CUDA(cudaMemcpyAsync(dmeans, self->means, sizeof(T) * K * D, cudaMemcpyHostToDevice, s));
+  VLB_CUDA(cudaMemcpyAsync(dcovs, self->covariances, sizeof(T) * K * D, cudaMemcpyHostToDevice, s));
+  VLB_CUDA(cudaMemcpyAsync(dpriors, self->priors, sizeof(T) * K, cudaMemcpyHostToDevice, s));
+  VLB_CUDA(cudaMemcpyAsync(dlb, self->sigmaLowBound, sizeof(double) * D, cudaMemcpyHostToDevice, s));
+  self->numData = (vl_size)N;
+  self->llTrace.clear();
+  self->paramTrace.clear();
+  self->streamReport.clear();
+  self->numRestarts = 0;
+  self->postOnDevice = false;
+  self->postLazy = false;
+
+  vlb::DevModel<T> m;
+  m.means = dmeans; m.covs = dcovs; m.priors = dpriors; m.K = K; m.D = D;
+  vlb::apply_bounds<T>(dcovs, K, D, dlb, s);  // vl/gmm.c:1233
+
+  bool tcm = false;
+  if constexpr (sizeof(T) == 4) tcm = precision != VLB200_PREC_EXACT && vlb::tc_supported(K, D);
+  VlB200Router *router = nullptr;
+  if constexpr (sizeof(T) == 4) router = cfg.router;
+  const vl_size judgeEvery = std::max<vl_size>(1, cfg.judgeEvery);
+  // Chunks start on the exact M-step's slab boundaries (its partition of all
+  // N rows), so restarts can use the exact M-step chunk by chunk.
+  const i64 rps = vlb::exact_mstep_slab_rows(N);
+  const int nslab = (int)((N + rps - 1) / rps);
+  i64 want = cfg.chunk > 0 ? cfg.chunk : std::max<i64>(rps, (i64)((1ll << 33) / (K * (i64)sizeof(T))));
+  const i64 chunk = std::min<i64>(N + rps - 1, (want + rps - 1) / rps * rps) / rps * rps;
+  T *dq = self->dq.get<T>((size_t)chunk * K);
+  T *dqr = router ? self->dqr.get<T>((size_t)chunk * K) : nullptr;
+  double *dmass = self->dtmp.get<double>(K);
+  i64 nitems = 0;
+  for (i64 r0 = 0; r0 < N; r0 += chunk) nitems += vlb::tc_em_items(std::min(chunk, N - r0));
+  float *dpart = tcm ? self->dpart.get<float>((size_t)nitems * vlb::tc_em_partial_floats(K, D)) : nullptr;
+  double *pm = self->dpm.get<double>((size_t)nslab * K);
+  double *p1 = self->dp1.get<double>((size_t)nslab * K * D);
+  double *p2 = self->dp2.get<double>((size_t)nslab * K * D);
+  // The parameters an iteration's E-step used (restarts re-derive from them).
+  T *pe = self->dpe.get<T>((size_t)(2 * K * D + K));
+
+  // E-step of one chunk into q (row-major): full (tensor-core image for the
+  // M-step when tcm) or through the router.  Returns the chunk's LL.
+  auto chunk_estep = [&](const vlb::DevModel<T> &mm, i64 r0, i64 n, bool viaRouter, T *q,
+                         unsigned long long *fb) -> double {
+    if constexpr (sizeof(T) == 4) {
+      if (viaRouter) {
+        const double ll = vlb::router_estep(router, dX + r0 * D, n, mm, q, cfg.m, cfg.thr, fb, s);
+        if (tcm) vlb::tc_em_image_from_rows(q, n, mm, s);
+        return ll;
+      }
+    }
+    return device_estep<T>(dX + r0 * D, n, mm, q, precision, false, s, tcm);
+  };
+
+  double prevLL = -INFINITY, LL = -INFINITY;
+  std::vector<T> snap;
+  for (vl_size it = 0;; ++it) {
+    const auto t0 = clk::now();
+    const bool judged = router && it % judgeEvery == 0;
+    const bool viaRouter = router && !judged;
+    if (self->traceParams) {
+      snap.resize((size_t)(2 * K * D + K));
+      VLB_CUDA(cudaMemcpyAsync(snap.data(), dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaMemcpyAsync(snap.data() + K * D, dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaMemcpyAsync(snap.data() + 2 * K * D, dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaStreamSynchronize(s));
+      self->paramTrace.emplace_back(snap.begin(), snap.end());
+    }
+    std::vector<double> mass(K, 0.0), mchunk(K);
+    double missed = 0, missedRows = 0;
+    unsigned long long fb = 0, fbJudge = 0;
+    LL = 0;
+    int item0 = 0;
+    for (i64 r0 = 0; r0 < N; r0 += chunk) {
+      const i64 n = std::min(chunk, N - r0);
+      LL += chunk_estep(m, r0, n, viaRouter, dq, &fb);
+      if constexpr (sizeof(T) == 4) {
+        if (judged) {
+          // Re-fit the router on this pass's first rows, then judge it on the rest.
+          const i64 skip = r0 == 0 ? std::min<i64>(n, cfg.fitRows) : 0;
+          if (r0 == 0) vlb::router_fit(router, dX, skip, dq, it == 0 ? 4 : 1, 2e-3f, s);
+          if (n > skip) {
+            vlb::router_estep(router, dX + (r0 + skip) * D, n - skip, m, dqr, cfg.m, cfg.thr, &fbJudge, s);
+            missed += vlb::router_missed_sum(dq + skip * K, dqr, n - skip, K, s);
+            missedRows += (double)(n - skip);
+          }
+        }
+      }
+      if (it > 1) {
+        vlb::column_mass<T>(dq, n, K, dmass, s);
+        VLB_CUDA(cudaMemcpyAsync(mchunk.data(), dmass, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+        VLB_CUDA(cudaStreamSynchronize(s));
+        for (i64 k = 0; k < K; ++k) mass[k] += mchunk[k];
+      }
+      bool tcStats = false;
+      if constexpr (sizeof(T) == 4) {
+        if (tcm) {
+          const int split = (!viaRouter && precision == VLB200_PREC_FP32) ? 2 : 1;
+          vlb::tc_em_stats((const float *)dX, r0, n, K, D, split, dpart, item0, s);
+          item0 += (int)vlb::tc_em_items(n);
+          tcStats = true;
+        }
+      }
+      if (!tcStats) vlb::exact_mstep_stats_rows<T>(dX, r0, n, rps, dq, dmeans, K, D, pm, p1, p2, s);
+    }
+    self->llTrace.push_back(LL);
+    const double ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+    self->streamReport.push_back({LL, judged ? 1.0 : 0.0, viaRouter ? 1.0 : 0.0,
+                                  missedRows > 0 ? missed / missedRows : (judged ? 0.0 : NAN),
+                                  (double)(viaRouter ? fb : fbJudge), ms});
+    if (self->verbosity)
+      VLB_PRINTF("gmm: em: iteration %d: loglikelihood = %f (variation = %f)\n", (int)it, LL, LL - prevLL);
+    if (it >= self->maxNumIterations) break;
+    const double eps = fabs((LL - prevLL) / LL);
+    if (it > 0 && eps < 0.00001) break;
+    prevLL = LL;
+
+    // Restarts (vl/gmm.c:1292, 814-999) with the masses of this pass.
+    vl_size nsplit = 0;
+    if (it > 1 && K > 1) {
+      const double cutoff = 1e-2 * std::max(1.0, (double)N / (double)K);
+      std::vector<std::array<double, 4>> splits;  // (empty mode, split mode, dimension, cut)
+      std::vector<T> pr(K), cv(K * D), mu(K * D);
+      bool saved = false;
+      auto rederive_mstep = [&]() {
+        vlb::DevModel<T> me;
+        me.means = pe; me.covs = pe + K * D; me.priors = pe + 2 * K * D; me.K = K; me.D = D;
+        for (i64 r0 = 0; r0 < N; r0 += chunk) {
+          const i64 n = std::min(chunk, N - r0);
+          chunk_estep(me, r0, n, viaRouter, dq, nullptr);
+          for (auto &sp : splits)
+            vlb::restart_split<T>(dq, dX + r0 * D, n, K, D, (i64)sp[0], (i64)sp[1], (i64)sp[2], (T)sp[3], s);
+          vlb::exact_mstep_stats_rows<T>(dX, r0, n, rps, dq, dmeans, K, D, pm, p1, p2, s);
+        }
+        vlb::exact_mstep_finalize_slabs<T>(nslab, pm, p1, p2, dlb, dmeans, dcovs, dpriors, K, D, s);
+        VLB_CUDA(cudaMemcpyAsync(pr.data(), dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+        VLB_CUDA(cudaMemcpyAsync(cv.data(), dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+        VLB_CUDA(cudaMemcpyAsync(mu.data(), dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+        VLB_CUDA(cudaStreamSynchronize(s));
+      };
+      for (i64 icl = 0; icl < K; ++icl) {
+        if (mass[icl] >= cutoff) continue;
+        if (self->verbosity) VLB_PRINTF("gmm: mode %d is nearly empty (mass %f)\n", (int)icl, mass[icl]);
+        if (!saved) {
+          VLB_CUDA(cudaMemcpyAsync(pe, dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToDevice, s));
+          VLB_CUDA(cudaMemcpyAsync(pe + K * D, dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToDevice, s));
+          VLB_CUDA(cudaMemcpyAsync(pe + 2 * K * D, dpriors, sizeof(T) * K, cudaMemcpyDeviceToDevice, s));
+          VLB_CUDA(cudaMemcpyAsync(pr.data(), dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+          VLB_CUDA(cudaMemcpyAsync(cv.data(), dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+          VLB_CUDA(cudaMemcpyAsync(mu.data(), dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+          VLB_CUDA(cudaStreamSynchronize(s));
+          saved = true;
+        }
+        double bestScore = -INFINITY;
+        i64 best = -1;
+        for (i64 j = 0; j < K; ++j) {
+          if ((double)pr[j] < 1e-6) continue;
+          double sc = 0.5 * (double)D * (1.0 + log(2 * 3.141592653589793));
+          for (i64 d = 0; d < D; ++d) sc += 0.5 * log((double)cv[j * D + d]);
+          sc = (double)pr[j] * (sc - log((double)pr[j]));
+          if (sc > bestScore) {
+            bestScore = sc;
+            best = j;
+          }
+        }
+        if (best == icl || best < 0) continue;
+        double bv = -INFINITY;
+        i64 bd = -1;
+        for (i64 d = 0; d < D; ++d)
+          if ((double)cv[best * D + d] > bv) {
+            bv = (double)cv[best * D + d];
+            bd = d;
+          }
+        if (bd < 0) continue;
+        if (self->verbosity)
+          VLB_PRINTF("gmm: reinitializing empty mode %d with mode %d (prior %f, mass %f, score %f)\n",
+                     (int)icl, (int)best, (double)pr[best], mass[best], bestScore);
+        splits.push_back({(double)icl, (double)best, (double)bd, (double)mu[best * D + bd]});
+        rederive_mstep();
+        ++nsplit;
+      }
+      if (nsplit > 0) {
+        self->numRestarts += nsplit;
+        rederive_mstep();  // the iteration's own M-step on the modified posteriors
+      }
+    }
+    if (nsplit == 0) {
+      bool done = false;
+      if constexpr (sizeof(T) == 4) {
+        if (tcm) {
+          vlb::tc_em_finalize(item0, dpart, dmeans, dcovs, dpriors, K, D, dlb, s);
+          done = true;
+        }
+      }
+      if (!done) vlb::exact_mstep_finalize_slabs<T>(nslab, pm, p1, p2, dlb, dmeans, dcovs, dpriors, K, D, s);
+    }
+  }
+  VLB_CUDA(cudaMemcpyAsync(self->means, dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaMemcpyAsync(self->covariances, dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaMemcpyAsync(self->priors, dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  // The final E-step's posteriors are recomputed on demand from the data.
+  const vl_size last = self->llTrace.size() - 1;
+  self->postLazy = true;
+  self->lazyX = dX;
+  self->lazyPrec = precision;
+  self->lazyRouter = (router && last % judgeEvery != 0) ? router : nullptr;
+  self->lazyM = cfg.m;
+  self->lazyThr = cfg.thr;
+  self->lazyChunk = (vl_size)chunk;
+  return LL;
+}
+
+template <typename T>
+double em_stream_default(VlGMM *self, const T *dX, i64 N, int precision) {
+  return em_stream_device<T>(self, dX, N, precision, StreamCfg());
 }
 
 template <typename T>
@@ -378,6 +715,7 @@ void init_kmeans(VlGMM *self, const T *dX, i64 N) {
   VLB_CUDA(cudaMemcpyAsync(self->priors, dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
   VLB_CUDA(cudaStreamSynchronize(s));
   self->postOnDevice = true;
+  self->postLazy = false;
 }
 
 double em_host(VlGMM *self, const void *data, vl_size N) {
@@ -433,6 +771,7 @@ void vl_gmm_reset(VlGMM *self) {
   }
   self->numData = 0;
   self->postOnDevice = false;
+  self->postLazy = false;
   drop_kmeans(self);
 }
 
@@ -595,7 +934,9 @@ double vl_gmm_cluster(VlGMM *self, void const *data, vl_size numData) {
           memcpy(self->covariances, bc.data(), bc.size());
           memcpy(self->priors, bp.data(), bp.size());
         }
-        self->postOnDevice = bestOnDevice;  // else the host copy holds the winner's
+        // The host copy holds an earlier winner's posteriors; a streamed run
+        // (posteriors never resident) recomputes them when they are asked for.
+        self->postOnDevice = bestOnDevice && !self->postLazy;
         self->LL = bestLL;
         if (self->verbosity)
           VLB_PRINTF("gmm: all repetitions terminated with final loglikelihood %f\n", self->LL);
@@ -693,6 +1034,34 @@ vl_size vlb200_gmm_get_ll_trace(VlGMM const *self, double *trace, vl_size maxEnt
 }
 
 vl_size vlb200_gmm_get_num_restarts(VlGMM const *self) { return self->numRestarts; }
+
+double vlb200_gmm_em_stream_device(VlGMM *self, float const *data, vl_size numData, int precision,
+                                   vl_size chunkRows, VlB200Router *router, vl_size m, float threshold,
+                                   vl_size judgeEvery) {
+  return guarded(
+      [&]() -> double {
+        VLB_CHECK(self->dataType == VL_TYPE_FLOAT, VL_ERR_BAD_ARG,
+                  "vlb200_gmm_em_stream_device: the model must be VL_TYPE_FLOAT");
+        StreamCfg cfg;
+        cfg.chunk = (i64)chunkRows;
+        cfg.router = router;
+        cfg.m = m;
+        cfg.thr = threshold;
+        cfg.judgeEvery = judgeEvery;
+        const double ll = em_stream_device<float>(self, data, (i64)numData,
+                                                  vlb::resolve_precision(precision, false), cfg);
+        self->LL = ll;
+        return ll;
+      },
+      (double)NAN);
+}
+
+vl_size vlb200_gmm_get_stream_report(VlGMM const *self, double *rows, vl_size maxIterations) {
+  const vl_size n = std::min<vl_size>(maxIterations, self->streamReport.size());
+  for (vl_size i = 0; i < n; ++i)
+    for (int j = 0; j < 6; ++j) rows[6 * i + j] = self->streamReport[i][j];
+  return n;
+}
 
 void vlb200_gmm_set_param_trace(VlGMM *self, int on) {
   self->traceParams = on != 0;

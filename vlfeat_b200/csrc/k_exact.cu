@@ -726,6 +726,32 @@ void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i6
   VLB_LAUNCH("normalize_priors", s, k_normalize_priors<T><<<1, kThreads, 0, s>>>(priors, (int)K));
 }
 
+i64 exact_mstep_slab_rows(i64 N) { return pick_slab_rows(N > 0 ? N : 1); }
+
+template <typename T>
+void exact_mstep_stats_rows(const T *X, i64 row0, i64 n, i64 rps, const T *q, const T *oldMeans, i64 K,
+                            i64 D, double *pmass, double *ps1, double *ps2, cudaStream_t s) {
+  constexpr int TKC = 32, RC = 32, JMAX = sizeof(T) == 8 ? 8 : 16, DB = 8 * JMAX;
+  if (n <= 0) return;
+  VLB_CHECK(row0 % rps == 0, VL_ERR_BAD_ARG, "M-step chunk must start on a slab boundary");
+  const i64 s0 = row0 / rps, nslab = (n + rps - 1) / rps;
+  dim3 g((unsigned)nslab, grid1(K, TKC), grid1(D, DB));
+  VLB_LAUNCH("exact_mstep_stats", s,
+             (k_mstep_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
+                 X + row0 * D, q, n, (int)K, (int)D, rps, oldMeans, pmass + s0 * K, ps1 + s0 * K * D,
+                 ps2 + s0 * K * D)));
+}
+
+template <typename T>
+void exact_mstep_finalize_slabs(int nslab, const double *pmass, const double *ps1, const double *ps2,
+                                const double *lb, T *means, T *covs, T *priors, i64 K, i64 D,
+                                cudaStream_t s) {
+  VLB_LAUNCH("exact_mstep_finalize", s,
+             k_mstep_finalize<T><<<grid1(K * D, kThreads), kThreads, 0, s>>>(
+                 nslab, (int)K, (int)D, pmass, ps1, ps2, lb, means, covs, priors));
+  VLB_LAUNCH("normalize_priors", s, k_normalize_priors<T><<<1, kThreads, 0, s>>>(priors, (int)K));
+}
+
 template <typename T>
 void normalize_priors(T *priors, i64 K, cudaStream_t s) {
   VLB_LAUNCH("normalize_priors", s, k_normalize_priors<T><<<1, kThreads, 0, s>>>(priors, (int)K));
@@ -1065,6 +1091,10 @@ void kmeanspp(const T *X, i64 N, i64 D, i64 K, T *centers, i64 x0, const std::ve
   template void exact_mstep<T>(const T *, i64, const T *, T *, T *, T *, i64, i64,           \
                                const double *, cudaStream_t);                                \
   template void column_mass<T>(const T *, i64, i64, double *, cudaStream_t);                 \
+  template void exact_mstep_stats_rows<T>(const T *, i64, i64, i64, const T *, const T *, i64, i64, \
+                                          double *, double *, double *, cudaStream_t);       \
+  template void exact_mstep_finalize_slabs<T>(int, const double *, const double *, const double *, \
+                                              const double *, T *, T *, T *, i64, i64, cudaStream_t); \
   template void normalize_priors<T>(T *, i64, cudaStream_t);                                 \
   template void global_variance<T>(const T *, i64, i64, T *, cudaStream_t);                  \
   template void kmeanspp<T>(const T *, i64, i64, i64, T *, i64, const std::vector<T> &, int,  \

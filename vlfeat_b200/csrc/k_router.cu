@@ -276,7 +276,8 @@ __global__ void k_candidate_estep(const float *__restrict__ X, i64 n, int D, int
                                   const float *__restrict__ means, const float *__restrict__ inv,
                                   const double *__restrict__ cst, const int *__restrict__ cand,
                                   const float *__restrict__ cmass, int m, float thr,
-                                  float *__restrict__ q, unsigned char *__restrict__ fell) {
+                                  float *__restrict__ q, unsigned char *__restrict__ fell,
+                                  double *__restrict__ llrow) {
   const i64 row = (i64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   if (row >= n) return;
@@ -331,6 +332,9 @@ __global__ void k_candidate_estep(const float *__restrict__ X, i64 n, int D, int
     qr[k] = expf(qr[k] - mx) / s;
   }
   if (lane == 0) fell[row] = fb ? 1 : 0;
+  // The row's log-likelihood over the components evaluated (all of them on
+  // fallback rows): the E-step's log-sum-exp restricted to the candidates.
+  if (lane == 0 && llrow) llrow[row] = (double)mx + log((double)s);
 }
 
 // Missed posterior mass of each row: sum of the full-E-step posteriors that
@@ -654,7 +658,7 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
       VLB_LAUNCH("router_candidate_estep", s,
                  vlb::k_candidate_estep<<<vlb::gridn(B, 8), 256, 0, s>>>(
                      X + i0 * D, B, D, K, means, der.inv, der.cst, cand, cm, (int)m, threshold,
-                     posteriors + i0 * K, fell));
+                     posteriors + i0 * K, fell, nullptr));
       if (fallbackRows) {
         std::vector<unsigned char> h(B);
         VLB_CUDA(cudaMemcpyAsync(h.data(), fell, B, cudaMemcpyDeviceToHost, s));
@@ -704,6 +708,84 @@ extern "C" int vlb200_router_set_default(VlB200Router *router, vl_size m, float 
 }
 
 namespace vlb {
+// Router E-step of n rows for streamed EM: posteriors q (n x K, zeros off the
+// candidates), the rows' log-likelihood over the evaluated components
+// (returned), and the number of rows that fell back to the full E-step.
+double router_estep(VlB200Router *r, const float *X, i64 n, const DevModel<float> &m, float *q,
+                    size_t mcand, float thr, unsigned long long *fallback, cudaStream_t s) {
+  VLB_CHECK(r->K == m.K && r->D == m.D, VL_ERR_BAD_ARG, "router does not match the model's K and D");
+  VLB_CHECK(mcand >= 1 && mcand <= 32 && (int)mcand <= r->K, VL_ERR_BAD_ARG, "router: m must be in [1, 32]");
+  VLB_CHECK(r->K <= 1024, VL_ERR_BAD_ARG, "router: at most 1024 components");
+  Scratch &sc = thread_scratch(kArenaRouter);
+  const int L = nlayers(r), K = r->K, D = r->D;
+  DevDerived<float> der;
+  der.inv = sc.slot[22].get<float>((size_t)K * D);
+  der.sis = sc.slot[23].get<float>((size_t)K * D);
+  der.cst = sc.slot[24].get<double>(K);
+  exact_prepare(m, der, s);
+  const i64 chunk = 1 << 17;
+  double ll = 0;
+  unsigned long long nfb = 0;
+  for (i64 i0 = 0; i0 < n; i0 += chunk) {
+    const i64 B = std::min<i64>(chunk, n - i0);
+    std::vector<float *> act(L + 1);
+    for (int l = 0; l <= L; ++l) act[l] = sc.slot[l].get<float>((size_t)chunk * r->sizes[l]);
+    int *cand = sc.slot[25].get<int>((size_t)chunk * mcand);
+    float *cm = sc.slot[26].get<float>(chunk);
+    unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
+    double *llrow = sc.slot[28].get<double>(chunk);
+    double *llsum = sc.slot[29].get<double>(1);
+    forward(r, X + i0 * D, B, act, s);
+    if (K <= 256)
+      VLB_LAUNCH("router_select", s, k_select<8><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+    else if (K <= 512)
+      VLB_LAUNCH("router_select", s, k_select<16><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+    else
+      VLB_LAUNCH("router_select", s, k_select<32><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+    VLB_LAUNCH("router_candidate_estep", s,
+               k_candidate_estep<<<gridn(B, 8), 256, 0, s>>>(X + i0 * D, B, D, K, m.means, der.inv, der.cst, cand,
+                                                             cm, (int)mcand, thr, q + i0 * K, fell, llrow));
+    sum_doubles(llrow, B, llsum, s);
+    double h = 0;
+    std::vector<unsigned char> hf(B);
+    VLB_CUDA(cudaMemcpyAsync(&h, llsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaMemcpyAsync(hf.data(), fell, B, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+    ll += h;
+    for (auto v : hf) nfb += v;
+  }
+  if (fallback) *fallback += nfb;
+  return ll;
+}
+
+// Sum over n rows of the posterior mass of qfull that qc leaves out.
+double router_missed_sum(const float *qfull, const float *qc, i64 n, i64 K, cudaStream_t s) {
+  if (n <= 0) return 0.0;
+  Scratch &sc = thread_scratch(kArenaRouter);
+  double *rows = sc.slot[30].get<double>(n), *tot = sc.slot[31].get<double>(1);
+  VLB_LAUNCH("router_missed", s, k_missed<<<gridn(n, 8), 256, 0, s>>>(qfull, qc, n, (int)K, rows));
+  sum_doubles(rows, n, tot, s);
+  double h = 0;
+  VLB_CUDA(cudaMemcpyAsync(&h, tot, sizeof(double), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+// Top-8 targets of full-E-step posteriors q (n x K) and `epochs` epochs of
+// training on them (batch 1024, Adam).
+void router_fit(VlB200Router *r, const float *X, i64 n, const float *q, int epochs, float lr, cudaStream_t s) {
+  if (n <= 0 || epochs <= 0) return;
+  DevBuf ti, tw;
+  int *tidx = ti.get<int>((size_t)n * 8);
+  float *twt = tw.get<float>((size_t)n * 8);
+  VLB_CUDA(cudaStreamSynchronize(s));
+  if (vlb200_router_targets(q, (vl_size)n, (vl_size)r->K, tidx, twt))
+    throw Error(vl_get_last_error(), vl_get_last_error_message());
+  double loss = 0;
+  if (vlb200_router_train(r, X, (vl_size)n, tidx, twt, (vl_size)epochs, 1024, lr, &loss))
+    throw Error(vl_get_last_error(), vl_get_last_error_message());
+}
+
 void router_default_posteriors(const float *X, i64 N, const DevModel<float> &m, float *q,
                                cudaStream_t s) {
   VlB200Router *r;

@@ -1661,6 +1661,8 @@ i64 tc_estep_em(const float *X, i64 N, const DevModel<float> &m, float *q, doubl
   return n;
 }
 
+constexpr i64 kEmItemRows = 8192;  // rows per statistics work item in EM
+
 void tc_mstep(const float *X, i64 N, float *means, float *covs, float *priors, i64 K, i64 D,
               const double *lb, int precision, cudaStream_t s) {
   Scratch &sc = thread_scratch(kArenaTc);
@@ -1695,6 +1697,67 @@ void tc_mstep(const float *X, i64 N, float *means, float *covs, float *priors, i
   normalize_priors<float>(priors, K, s);
   check_err(err, s);
 }
+
+// ------------------------------------------------- streaming EM pieces
+// EM over data too large for resident N x K posteriors runs chunk by chunk:
+// each chunk's q image lives in this arena's slot 4, its statistics go to
+// the caller's item partials (items never straddle chunks), and one
+// finalize reduces all items of the pass in f64, in item order.
+
+void tc_em_image_from_rows(const float *qrows, i64 n, const DevModel<float> &m, cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaTc);
+  TcPrep tp;
+  tc_prepare(m, tp, true, sc, s);
+  const int Kq = padQ(tp.Kp);
+  const i64 ntiles = (n + 127) / 128, rowsPad = ntiles * 128;
+  __half *img = sc.slot[4].get<__half>((size_t)std::max<i64>(1, ntiles) * 128 * Kq);
+  if (rowsPad > 0)
+    VLB_LAUNCH("tc_rows_to_image", s,
+               k_rows_to_image16<<<(unsigned)((rowsPad + 7) / 8), 256, 0, s>>>(
+                   qrows, n, (int)m.K, Kq, float_at_least(1e-2 / (double)m.K), img, nullptr, rowsPad, false));
+}
+
+i64 tc_em_items(i64 n) { return (n + kEmItemRows - 1) / kEmItemRows; }
+
+void tc_em_stats(const float *X, i64 row0, i64 n, i64 K, i64 D, int split, float *partial, int item0,
+                 cudaStream_t s) {
+  if (n <= 0) return;
+  Scratch &sc = thread_scratch(kArenaTc);
+  const int Kp = padK(K), Kq = padQ(Kp);
+  const i64 ntiles = (n + 127) / 128;
+  std::vector<SItem> items;
+  for (i64 r = 0; r < n; r += kEmItemRows)
+    items.push_back({row0 + r, row0 + std::min(n, r + kEmItemRows), item0 + (int)items.size(), 0});
+  const int nitems = (int)items.size();
+  const int gx = std::max(1, std::min(nitems, num_sms()));
+  std::vector<int> order, beg;
+  lpt_assign(items, gx, order, beg);
+  SItem *ditems = upload(sc.slot[7], items, s);
+  int *dorder = upload(sc.slot[8], order, s);
+  int *dbeg = upload(sc.slot[9], beg, s);
+  int *err = sc.slot[3].get<int>(1);
+  VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  SParams sp;
+  sp.X = X; sp.qimg = (const uint8_t *)sc.slot[4].p; sp.qpart = ntiles * 128 * (i64)Kq * 2; sp.qbase = row0;
+  sp.K = (int)K; sp.Kp = Kp; sp.Kq = Kq; sp.nst = 0;
+  sp.ctr = (const float *)sc.slot[0].p; sp.scale = (const float *)sc.slot[12].p;
+  sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg; sp.partial = partial; sp.err = err;
+  stats_dispatch((int)D, split, sp, gx, 0, 0, s);
+  check_err(err, s);
+}
+
+void tc_em_finalize(int nitems, const float *partial, float *means, float *covs, float *priors, i64 K, i64 D,
+                    const double *lb, cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaTc);
+  const int Kp = padK(K);
+  VLB_LAUNCH("tc_mstep_finalize", s,
+             k_tc_mstep_finalize<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
+                 nitems, (int)K, Kp, (int)D, partial, (const float *)sc.slot[0].p,
+                 (const float *)sc.slot[12].p, lb, means, covs, priors));
+  normalize_priors<float>(priors, K, s);
+}
+
+size_t tc_em_partial_floats(i64 K, i64 D) { return (size_t)padK(K) * (size_t)(2 * D + 16); }
 
 // ------------------------------------------------- batched Fisher encoding
 namespace {

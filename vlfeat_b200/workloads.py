@@ -124,3 +124,74 @@ def config1(N: int = 1_000_000, K: int = 256, iters: int = 20):
 
 def config2_counts(num_images: int = 4096):
     return image_counts(num_images, seed=300)
+
+
+def config3_params(K: int = 1024, D: int = 80, seed: int = 500):
+    """Learned-router configuration: a seeded K-component diagonal mixture with
+    the config-0 generator and sigma ~ U[0.3, 1.5] (means ~ N(0, 4 I), priors
+    ~ Dirichlet(1)); the GMM of the E-step is the mixture itself.  Returns
+    float32 (priors, means, variances)."""
+    means, sigma, priors = mixture_params(K, D, seed, 0.3, 1.5)
+    return (priors.astype(np.float32), means.astype(np.float32), (sigma ** 2).astype(np.float32))
+
+
+def config3_data_device(n: int, params, seed: int, device="cuda", chunk: int = 1 << 22):
+    """n float32 rows of the config-3 mixture drawn on the GPU with a seeded
+    torch generator (component ~ priors, then mean + sigma * N(0, 1))."""
+    import torch
+    pr, mu, cv = params
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    p = torch.from_numpy(pr.astype(np.float64)).to(device)
+    m = torch.from_numpy(mu).to(device)
+    s = torch.from_numpy(np.sqrt(cv)).to(device)
+    out = torch.empty((n, mu.shape[1]), dtype=torch.float32, device=device)
+    for i in range(0, n, chunk):
+        b = min(chunk, n - i)
+        c = torch.multinomial(p, b, replacement=True, generator=g)
+        out[i:i + b] = m[c] + s[c] * torch.randn((b, mu.shape[1]), generator=g, device=device)
+    return out
+
+
+def sift_like_device(n: int, D: int = 128, seed: int = 0, device="cuda", chunk: int = 1 << 21):
+    """SIFT-shaped descriptors as :func:`sift_like` (Gamma(0.5, 1) bins,
+    L2-normalise, clip at 0.2, renormalise, x512, round, clamp to [0, 255]),
+    drawn on the GPU from torch's generator seeded with `seed` (for sizes
+    where NumPy on the host is too slow; not the same bytes as sift_like)."""
+    import torch
+    out = torch.empty((n, D), dtype=torch.float32, device=device)
+    torch.cuda.manual_seed(seed)
+    conc = torch.full((min(chunk, n), D), 0.5, device=device)
+    for i in range(0, n, chunk):
+        b = min(chunk, n - i)
+        x = torch._standard_gamma(conc[:b])
+        x /= x.norm(dim=1, keepdim=True).clamp_min(1e-12)
+        x.clamp_(max=0.2)
+        x /= x.norm(dim=1, keepdim=True).clamp_min(1e-12)
+        out[i:i + b] = (x * 512.0).round_().clamp_(0, 255)
+    return out
+
+
+def custom_init_device(x, K: int, seed: int):
+    """:func:`custom_init` for a CUDA tensor: K seeded distinct rows as means,
+    the unbiased global variance (N - 1, vl/gmm.c:1409, accumulated in f64)
+    for every component, uniform priors.  Returns float32 NumPy arrays and
+    the variance floor 1e-4 x the largest global variance."""
+    N, D = x.shape
+    idx = _rng(seed).choice(N, size=K, replace=False)
+    means = x[idx].cpu().numpy().astype(np.float32)
+    s1 = np.zeros(D)
+    s2 = np.zeros(D)
+    step = 1 << 22
+    for i in range(0, N, step):
+        xb = x[i:i + step].double()
+        s1 += xb.sum(0).cpu().numpy()
+    mean = s1 / N
+    import torch
+    mt = torch.from_numpy(mean).to(x.device)
+    for i in range(0, N, step):
+        s2 += ((x[i:i + step].double() - mt) ** 2).sum(0).cpu().numpy()
+    var = s2 / (N - 1)
+    covs = np.tile(var.astype(np.float32), (K, 1))
+    priors = np.full(K, 1.0 / K, np.float32)
+    return priors, means, covs, 1e-4 * float(var.max())
