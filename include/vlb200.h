@@ -289,6 +289,15 @@ VL_EXPORT int vlb200_router_posteriors(VlB200Router *router, float *posteriors,
 VL_EXPORT int vlb200_router_missed_mass(float const *fullPosteriors,
                                         float const *candidatePosteriors, vl_size numData,
                                         vl_size numClusters, double *meanMissedMass);
+/* Inference engine: 1 (default) runs the network's layers as tcgen05 dense
+ * layers (bf16 features, activations and weights, fp32 accumulation, TMA-
+ * staged tiles) when every layer width is a multiple of 8; 0 runs the
+ * training forward (fp32 activations, bf16-rounded weights) on the CUDA
+ * cores.  vlb200_router_logits returns the inference logits (N x K fp32,
+ * device) of rows X (N x D, device). */
+VL_EXPORT int vlb200_router_set_tensor_core_inference(VlB200Router *router, int on);
+VL_EXPORT int vlb200_router_logits(VlB200Router *router, float const *data, vl_size numData,
+                                   float *logits, void *stream);
 /* Router used by VLB200_PREC_BF16_ROUTER calls (not owned; NULL clears). */
 VL_EXPORT int vlb200_router_set_default(VlB200Router *router, vl_size m, float threshold);
 

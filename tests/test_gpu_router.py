@@ -140,3 +140,52 @@ def test_nan_descriptor_falls_back_without_touching_other_rows(vl):
     assert np.array_equal(qh[keep], ch[keep])
     for row in (100, 200):
         assert np.all(np.isnan(qh[row]) | np.isfinite(qh[row]))
+
+
+def _emulated_logits(layers, x, centre, scale):
+    """FP64 forward with the tensor-core path's roundings: bf16 features,
+    weights and hidden activations, exact sums."""
+    import torch
+    bf = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(torch.bfloat16).double().numpy()
+    h = bf((x - centre) * scale)
+    for i, (W, b) in enumerate(layers):
+        z = h @ bf(W).T + b.astype(np.float64)
+        h = bf(np.maximum(z, 0.0)) if i + 1 < len(layers) else z
+    return h
+
+
+@pytest.mark.parametrize("shape", [(80, (256, 256), 1024, 4000), (16, (24,), 40, 300), (128, (256, 256), 256, 1000)])
+def test_tensor_core_dense_layers(vl, shape):
+    """The router's inference on tcgen05 dense layers (TMA-staged bf16 tiles,
+    fp32 accumulation) against an FP64 forward with the same bf16 roundings,
+    and against the CUDA-core forward (fp32 activations); row counts that are
+    not multiples of the 128-row tile and widths below one 256-column tile."""
+    import torch
+    from vlfeat_b200.router import Router
+    D, hidden, K, N = shape
+    rng = np.random.default_rng(D + K)
+    r = Router(D, K, hidden=hidden, seed=11)
+    centre = rng.normal(size=D).astype(np.float32)
+    scale = rng.uniform(0.5, 2.0, size=D).astype(np.float32)
+    r.set_input_transform(centre, scale)
+    # Non-zero biases so that the epilogue's bias is exercised.
+    p = r.get_params()
+    o = 0
+    for i in range(len(hidden) + 1):
+        n_in, n_out = ([D, *hidden, K])[i], ([D, *hidden, K])[i + 1]
+        o += n_in * n_out
+        p[o:o + n_out] = rng.normal(scale=0.1, size=n_out)
+        o += n_out
+    r.set_params(p)
+    x = rng.normal(size=(N, D)).astype(np.float32)
+    got = torch.zeros((N, K), device="cuda")
+    r.logits(got, _t(x))
+    r.set_tensor_core_inference(False)
+    cc = torch.zeros((N, K), device="cuda")
+    r.logits(cc, _t(x))
+    r.set_tensor_core_inference(True)
+    want = _emulated_logits(r.layers(), x.astype(np.float64), centre.astype(np.float64),
+                            scale.astype(np.float64))
+    g = got.cpu().numpy()
+    assert rel_err(g, want) < 5e-3
+    assert rel_err(g, cc.cpu().numpy()) < 3e-2

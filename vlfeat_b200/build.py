@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
           "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 SOURCES = ["runtime.cpp", "gmm_api.cpp", "fisher_api.cpp", "fisher_plan.cpp", "k_exact.cu", "k_tc.cu", "k_noalloc.cu",
-           "k_router.cu", "k_vlad.cu", "k_pca.cu", "k_kmeans.cu"]
+           "k_router.cu", "k_mlp.cu", "k_vlad.cu", "k_pca.cu", "k_kmeans.cu"]
 HEADERS = ["common.h", "engine.h", "tc_common.cuh", "exact_math.cuh"]
 
 

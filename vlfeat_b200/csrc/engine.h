@@ -9,6 +9,8 @@
 #include <cstdint>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "common.h"
 
 namespace vlb {
@@ -157,6 +159,16 @@ void router_default_posteriors(const float *X, i64 N, const DevModel<float> &m, 
 // ------------------------------------------------------- tensor-core path
 // Implemented in k_tc.cu.  Available for float data only.
 bool tc_supported(i64 K, i64 D);
+// Dense layer on the tensor cores (k_mlp.cu): C (M x N) = act(A (M x Ka) .
+// W (N x Ka)^T + bias), A and W bf16 row-major, fp32 accumulation, ReLU when
+// relu, C fp32 when outF32 else bf16; N and Ka multiples of 8.  An expired
+// wait writes its code to *err (device).
+bool tc_dense_supported(int N, int Ka);
+void tc_dense(const __nv_bfloat16 *A, long long M, int Ka, const __nv_bfloat16 *W, int N, const float *bias,
+              bool relu, bool outF32, void *C, int *err, cudaStream_t s);
+void features_bf16(const float *X, long long n, int D, int Ka, const float *ctr, const float *scl,
+                   __nv_bfloat16 *Z, cudaStream_t s);
+void weights_bf16(const float *W, int out, int in, int inPad, __nv_bfloat16 *Wb, cudaStream_t s);
 // Runs the bounded-wait self-test kernel with a wait limit of limit_ms and
 // raises the error a kernel's expired wait raises.
 void wait_selftest(double limit_ms, cudaStream_t s);

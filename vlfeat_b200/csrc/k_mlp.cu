@@ -1,0 +1,284 @@
+// Dense layers of the learned router on the tensor cores.
+//
+// One persistent tcgen05 kernel computes C = act(A . B^T + bias) for a layer:
+// A (M x Ka) the activations and B (N x Ka) the weights, both bf16 and
+// row-major (K-major), fp32 accumulation in TMEM, the bias and ReLU applied
+// in the epilogue, C stored as bf16 (hidden layers, the next layer's A) or
+// fp32 (logits).  Operand tiles are staged by TMA (cp.async.bulk.tensor.2d,
+// 128-byte swizzle, zero fill past the matrix edges) into a ring of shared
+// memory stages:
+//   warp 0     TMA producer (one thread),
+//   warp 1     TMEM allocation and, from one lane, tcgen05.mma issue,
+//   warps 2-5  epilogue: TMEM -> registers -> bias, ReLU -> global.
+// Tiles are 128 rows x BN columns (BN = N rounded up to 16, at most 256),
+// 64-element k-blocks (4 MMAs of K = 16 each), two TMEM accumulators so that
+// one tile's epilogue overlaps the next tile's MMAs.  Every mbarrier wait is
+// bounded (tc_common.cuh); an expired wait records its code in the error word.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "engine.h"
+#include "tc_common.cuh"
+
+namespace vlb {
+namespace {
+
+using namespace tc;
+
+constexpr int kMlpThreads = 192;
+constexpr int kBM = 128, kBK = 64;
+constexpr int kMlpSmemLimit = 232448;
+
+struct MlpParams {
+  CUtensorMap ta, tb;  // A: {Ka, M}, box {64, 128};  B: {Ka, N}, box {64, BN}
+  const float *bias;
+  void *c;
+  int M, N, Ka, BN, nst, relu, out_f32;
+  int *err;
+};
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_constant__ MlpParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t aBytes = kBM * kBK * 2, bBytes = (uint32_t)p.BN * kBK * 2, stageBytes = aBytes + bBytes;
+  uint64_t *bars = (uint64_t *)(base + (size_t)p.nst * stageBytes);
+  uint64_t *full = bars, *empty = bars + 8, *accf = bars + 16, *acce = bars + 18;
+  uint32_t *s_tmem = (uint32_t *)(bars + 20);
+  volatile int *s_abort = (volatile int *)(s_tmem + 1);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int mtiles = (p.M + kBM - 1) / kBM, ntiles = (p.N + p.BN - 1) / p.BN;
+  const int tiles = mtiles * ntiles, nkb = (p.Ka + kBK - 1) / kBK;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < p.nst; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 128);
+    }
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    tmem_alloc(s_tmem, 512);
+    tmem_relinquish();
+  }
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------------------------------------------------- producer
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&p.ta)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&p.tb)) : "memory");
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+      const int mt = t / ntiles, nt = t % ntiles;
+      bool ok = true;
+      for (int kb = 0; kb < nkb; ++kb, ++it) {
+        const int st = it % p.nst;
+        if (!mbar_wait(&empty[st], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 31)) {
+          ok = false;
+          break;
+        }
+        const uint32_t sa = smem_u32(base + (size_t)st * stageBytes);
+        mbar_arrive_expect_tx(&full[st], stageBytes);
+        tma_load_2d(sa, &p.ta, kb * kBK, mt * kBM, &full[st]);
+        tma_load_2d(sa + aBytes, &p.tb, kb * kBK, nt * p.BN, &full[st]);
+      }
+      if (!ok) break;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // --------------------------------------------------------------- MMA
+    const uint32_t idesc = idesc_bf16(kBM, p.BN, false, false);
+    int it = 0, tt = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++tt) {
+      const int buf = tt & 1;
+      if (!mbar_wait(&acce[buf], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 32)) break;
+      tc_fence_after();
+      const uint32_t d = tmem + (uint32_t)(buf * 256);
+      for (int kb = 0; kb < nkb; ++kb, ++it) {
+        const int st = it % p.nst;
+        if (!mbar_wait(&full[st], (it / p.nst) & 1, s_abort, p.err, 33)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(base + (size_t)st * stageBytes), sb = sa + aBytes;
+#pragma unroll
+        for (int ks = 0; ks < kBK / 16; ++ks) {
+          const uint64_t ad = sdesc(sa + ks * 32, 16, 1024, kSw128);
+          const uint64_t bd = sdesc(sb + ks * 32, 16, 1024, kSw128);
+          mma_bf16(d, ad, bd, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+        }
+        mma_commit(&empty[st]);
+      }
+      if (ok) mma_commit(&accf[buf]);
+    }
+  } else if (warp >= 2) {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int r = q * 32 + lane;
+    int tt = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tt) {
+      const int mt = t / ntiles, nt = t % ntiles, buf = tt & 1;
+      if (!mbar_wait(&accf[buf], (tt >> 1) & 1, s_abort, p.err, 34)) break;
+      tc_fence_after();
+      const long long row = (long long)mt * kBM + r;
+      const bool valid = row < p.M;
+      const uint32_t tb = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 256);
+      for (int c0 = 0; c0 < p.BN; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(tb + (uint32_t)c0, v);
+        tmem_wait_ld();
+        const int n0 = nt * p.BN + c0;
+        if (!valid) continue;
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const int n = n0 + 8 * g;
+          if (n >= p.N) break;  // N is a multiple of 8: a group is wholly in or out
+          float y[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            float a = __uint_as_float(v[8 * g + j]) + __ldg(p.bias + n + j);
+            y[j] = (p.relu && !(a > 0.f)) ? 0.f : a;
+          }
+          if (p.out_f32) {
+            float4 *dst = (float4 *)((float *)p.c + row * p.N + n);
+            dst[0] = make_float4(y[0], y[1], y[2], y[3]);
+            dst[1] = make_float4(y[4], y[5], y[6], y[7]);
+          } else {
+            uint4 w;
+            w.x = pack2<false>(y[0], y[1]);
+            w.y = pack2<false>(y[2], y[3]);
+            w.z = pack2<false>(y[4], y[5]);
+            w.w = pack2<false>(y[6], y[7]);
+            *(uint4 *)((__nv_bfloat16 *)p.c + row * p.N + n) = w;
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[buf]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// x (n x D, fp32) -> bf16 features (x - centre) * scale, rows padded with
+// zeros to Ka columns.
+__global__ void k_features_bf16(const float *__restrict__ X, long long n, int D, int Ka,
+                                const float *__restrict__ ctr, const float *__restrict__ scl,
+                                __nv_bfloat16 *__restrict__ Z) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * Ka) return;
+  const long long row = i / Ka;
+  const int d = (int)(i % Ka);
+  Z[i] = __float2bfloat16_rn(d < D ? (X[row * D + d] - ctr[d]) * scl[d] : 0.f);
+}
+
+// fp32 weights (out x in) -> bf16 (out x inPad), zero padding columns.
+__global__ void k_weights_bf16(const float *__restrict__ W, int out, int in, int inPad,
+                               __nv_bfloat16 *__restrict__ Wb) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)out * inPad) return;
+  const int o = (int)(i / inPad), k = (int)(i % inPad);
+  Wb[i] = __float2bfloat16_rn(k < in ? W[(long long)o * in + k] : 0.f);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  VLB_CHECK(fn != nullptr, VL_ERR_BAD_ARG, "cuTensorMapEncodeTiled is not available from the driver");
+  return fn;
+}
+
+// 2-D bf16 row-major matrix (rows x cols, cols contiguous) for TMA boxes of
+// 64 columns x boxRows rows with the 128-byte swizzle.
+void make_map(CUtensorMap *m, const void *ptr, long long rows, int cols, int boxRows) {
+  VLB_CHECK(((uintptr_t)ptr & 15) == 0 && (cols * 2) % 16 == 0, VL_ERR_BAD_ARG,
+            "dense layer: operands must be 16-byte aligned rows");
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)boxRows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides,
+                                 box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  VLB_CHECK(r == CUDA_SUCCESS, VL_ERR_BAD_ARG, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
+}  // namespace
+
+bool tc_dense_supported(int N, int Ka) { return N >= 8 && N % 8 == 0 && Ka >= 8 && Ka % 8 == 0; }
+
+void tc_dense(const __nv_bfloat16 *A, long long M, int Ka, const __nv_bfloat16 *W, int N, const float *bias,
+              bool relu, bool outF32, void *C, int *err, cudaStream_t s) {
+  if (M <= 0) return;
+  VLB_CHECK(tc_dense_supported(N, Ka), VL_ERR_BAD_ARG, "dense layer: widths must be multiples of 8");
+  MlpParams p;
+  const int BN = std::min(256, (N + 15) / 16 * 16);
+  make_map(&p.ta, A, M, Ka, kBM);
+  make_map(&p.tb, W, N, Ka, BN);
+  p.bias = bias;
+  p.c = C;
+  p.M = (int)M;
+  p.N = N;
+  p.Ka = Ka;
+  p.BN = BN;
+  p.relu = relu ? 1 : 0;
+  p.out_f32 = outF32 ? 1 : 0;
+  p.err = err;
+  const size_t stageBytes = (size_t)(kBM + BN) * kBK * 2;
+  const size_t fixed = 1024 /*alignment*/ + 256 /*barriers, TMEM base, abort flag*/;
+  p.nst = (int)std::min<size_t>(8, (kMlpSmemLimit - fixed) / stageBytes);
+  VLB_CHECK(p.nst >= 2, VL_ERR_BAD_ARG, "dense layer: operand stages exceed shared memory");
+  const size_t smem = fixed + (size_t)p.nst * stageBytes;
+  VLB_CUDA(cudaFuncSetAttribute(k_tc_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long tiles = ((M + kBM - 1) / kBM) * ((N + BN - 1) / BN);
+  int nsm = 0, dev = 0;
+  VLB_CUDA(cudaGetDevice(&dev));
+  VLB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int grid = (int)std::min<long long>(tiles, nsm);
+  VLB_LAUNCH("router_dense_tc", s, k_tc_dense<<<grid, kMlpThreads, smem, s>>>(p));
+}
+
+void features_bf16(const float *X, long long n, int D, int Ka, const float *ctr, const float *scl,
+                   __nv_bfloat16 *Z, cudaStream_t s) {
+  const long long total = n * Ka;
+  if (total <= 0) return;
+  VLB_LAUNCH("router_features_bf16", s,
+             k_features_bf16<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(X, n, D, Ka, ctr, scl, Z));
+}
+
+void weights_bf16(const float *W, int out, int in, int inPad, __nv_bfloat16 *Wb, cudaStream_t s) {
+  const long long total = (long long)out * inPad;
+  VLB_LAUNCH("router_weights_bf16", s,
+             k_weights_bf16<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(W, out, in, inPad, Wb));
+}
+
+}  // namespace vlb

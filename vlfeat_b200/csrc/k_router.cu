@@ -360,10 +360,14 @@ struct _VlB200Router {
   std::vector<int> sizes;  // D, hidden..., K
   // Parameters (device): per layer W (out x in), b (out); Adam moments.
   std::vector<vlb::DevBuf *> W, b, Wq, mW, vW, mb, vb, gW, gb;
+  // bf16 weights for the tensor-core inference (layer l: out x in8(in), the
+  // input width rounded up to a multiple of 8 with zero columns).
+  std::vector<vlb::DevBuf *> Wb;
+  bool tcInfer = true;  // inference on the tensor cores when the widths allow
   vlb::DevBuf ctr, scl;
   long step = 0;
   ~_VlB200Router() {
-    for (auto *v : {&W, &b, &Wq, &mW, &vW, &mb, &vb, &gW, &gb})
+    for (auto *v : {&W, &b, &Wq, &mW, &vW, &mb, &vb, &gW, &gb, &Wb})
       for (auto *p : *v) delete p;
   }
 };
@@ -397,12 +401,60 @@ void gemm(bool relu, bool bias, const float *A, i64 sam, i64 sak, const float *B
     VLB_LAUNCH("router_gemm", s, (vlb::k_gemm<false, false><<<g, vlb::kT, 0, s>>>(A, sam, sak, B, sbn, sbk, bvec, C, ldc, M, N, Kd)));
 }
 
+int in8(int n) { return (n + 7) / 8 * 8; }
+
 void refresh_bf16(VlB200Router *r, cudaStream_t s) {
   for (int l = 0; l < nlayers(r); ++l) {
     const i64 n = (i64)r->sizes[l + 1] * r->sizes[l];
     VLB_LAUNCH("router_round", s,
                vlb::k_round_bf16<<<vlb::gridn(n, 256), 256, 0, s>>>((float *)r->W[l]->p, (float *)r->Wq[l]->p, n));
+    const int in = r->sizes[l], out = r->sizes[l + 1];
+    while ((int)r->Wb.size() <= l) r->Wb.push_back(new DevBuf());
+    vlb::weights_bf16((const float *)r->W[l]->p, out, in, in8(in),
+                      r->Wb[l]->get<__nv_bfloat16>((size_t)out * in8(in)), s);
   }
+}
+
+// Inference on the tensor cores: every layer's output width a multiple of 8.
+bool tc_infer_ok(const VlB200Router *r) {
+  if (!r->tcInfer || nlayers(r) > 6) return false;
+  for (size_t l = 1; l < r->sizes.size(); ++l)
+    if (!vlb::tc_dense_supported(r->sizes[l], in8(r->sizes[l - 1]))) return false;
+  return true;
+}
+
+void forward(VlB200Router *r, const float *X, i64 B, std::vector<float *> &act, cudaStream_t s);
+
+// Logits (B x K, fp32) of a batch for inference: on the tensor cores (bf16
+// features and activations, bf16 weights, fp32 accumulation; tcgen05 dense
+// layers), else the training forward on the CUDA cores.  act: the forward's
+// buffers (act[L] receives the logits).
+void forward_infer(VlB200Router *r, const float *X, i64 B, std::vector<float *> &act, vlb::Scratch &sc,
+                   cudaStream_t s) {
+  if (!tc_infer_ok(r)) {
+    forward(r, X, B, act, s);
+    return;
+  }
+  const int L = nlayers(r);
+  int *err = sc.slot[9].get<int>(1);
+  VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  // Ping-pong bf16 activation buffers (slots 7 and 8; slots 0 .. L hold the
+  // fp32 activations, so L <= 6).
+  int wmax = 0;
+  for (int l = 0; l < L; ++l) wmax = std::max(wmax, in8(r->sizes[l]));
+  __nv_bfloat16 *buf[2] = {sc.slot[7].get<__nv_bfloat16>((size_t)B * wmax),
+                           sc.slot[8].get<__nv_bfloat16>((size_t)B * wmax)};
+  vlb::features_bf16(X, B, r->D, in8(r->D), (const float *)r->ctr.p, (const float *)r->scl.p, buf[0], s);
+  for (int l = 0; l < L; ++l) {
+    const int out = r->sizes[l + 1];
+    const bool last = l + 1 == L;
+    vlb::tc_dense(buf[l & 1], B, in8(r->sizes[l]), (const __nv_bfloat16 *)r->Wb[l]->p, out,
+                  (const float *)r->b[l]->p, !last, last, last ? (void *)act[L] : (void *)buf[(l + 1) & 1], err, s);
+  }
+  int h = 0;
+  VLB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  if (h) throw vlb::Error(VL_ERR_BAD_ARG, "router dense layer gave up waiting (code " + std::to_string(h) + ")");
 }
 
 // Activations of a batch: act[0] = features, act[l+1] = layer l output.
@@ -645,7 +697,7 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
       int *cand = sc.slot[25].get<int>((size_t)chunk * m);
       float *cm = sc.slot[26].get<float>(chunk);
       unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
-      forward(r, X + i0 * D, B, act, s);
+      forward_infer(r, X + i0 * D, B, act, sc, s);
       if (K <= 256)
         VLB_LAUNCH("router_select", s,
                    vlb::k_select<8><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
@@ -667,6 +719,30 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
       }
     }
     if (fallbackRows) *fallbackRows = nfb;
+  });
+}
+
+// Inference engine of the router: 1 = tcgen05 dense layers (default, when
+// every width allows), 0 = the training forward on the CUDA cores.
+int vlb200_router_set_tensor_core_inference(VlB200Router *r, int on) {
+  return guarded([&] { r->tcInfer = on != 0; });
+}
+
+// Inference logits (N x K, fp32, device) of the rows X (N x D, device).
+int vlb200_router_logits(VlB200Router *r, float const *X, vl_size N, float *logits, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = vlb::pick_stream(stream);
+    vlb::Scratch &sc = vlb::thread_scratch(vlb::kArenaRouter);
+    const int L = nlayers(r);
+    const i64 chunk = 1 << 17;
+    for (i64 i0 = 0; i0 < (i64)N; i0 += chunk) {
+      const i64 B = std::min<i64>(chunk, (i64)N - i0);
+      std::vector<float *> act(L + 1);
+      for (int l = 0; l < L; ++l) act[l] = sc.slot[l].get<float>((size_t)chunk * r->sizes[l]);
+      act[L] = logits + i0 * r->K;
+      forward_infer(r, X + i0 * r->D, B, act, sc, s);
+    }
+    VLB_CUDA(cudaStreamSynchronize(s));
   });
 }
 
@@ -735,7 +811,7 @@ double router_estep(VlB200Router *r, const float *X, i64 n, const DevModel<float
     unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
     double *llrow = sc.slot[28].get<double>(chunk);
     double *llsum = sc.slot[29].get<double>(1);
-    forward(r, X + i0 * D, B, act, s);
+    forward_infer(r, X + i0 * D, B, act, sc, s);
     if (K <= 256)
       VLB_LAUNCH("router_select", s, k_select<8><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
     else if (K <= 512)

@@ -41,6 +41,8 @@ def _lib():
           C.POINTER(C.c_uint64), _vp)
         f("vlb200_router_missed_mass", C.c_int, _vp, _vp, _sz, _sz, C.POINTER(C.c_double))
         f("vlb200_router_set_default", C.c_int, _vp, _sz, C.c_float)
+        f("vlb200_router_set_tensor_core_inference", C.c_int, _vp, C.c_int)
+        f("vlb200_router_logits", C.c_int, _vp, _vp, _sz, _vp, _vp)
         _DECLARED = True
     return L
 
@@ -122,6 +124,14 @@ class Router:
                                                x_t.shape[0], m, threshold, C.byref(fb),
                                                capi._stream(None)), "router_posteriors")
         return int(fb.value)
+
+    def set_tensor_core_inference(self, on=True):
+        _check(_lib().vlb200_router_set_tensor_core_inference(self._h, 1 if on else 0),
+               "set_tensor_core_inference")
+
+    def logits(self, logits_t, x_t):
+        _check(_lib().vlb200_router_logits(self._h, x_t.data_ptr(), x_t.shape[0], logits_t.data_ptr(),
+                                           capi._stream(None)), "logits")
 
     def set_default(self, m=8, threshold=0.99):
         _check(_lib().vlb200_router_set_default(self._h, m, threshold), "set_default")
