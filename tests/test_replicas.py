@@ -1,6 +1,9 @@
-"""The multi-GPU host logic of the benchmark (vlfeat_b200.replicas) with two
-gloo ranks on the CPU: every rank encodes its own data, the step time is the
-slowest rank's, and the job's work is the sum of the ranks' descriptors."""
+"""The multi-GPU host logic (vlfeat_b200.replicas) with two gloo ranks on the
+CPU: every rank encodes its own data, the step time is the slowest rank's, and
+the job's work is the sum of the ranks' descriptors; a batch split into blocks
+of whole images, encoded rank by rank (the C restatement standing in for the
+GPU on these CPU ranks) and gathered on rank 0, equals the single-process
+encoding of the whole batch."""
 import multiprocessing as mp
 import os
 import socket
@@ -49,3 +52,67 @@ def test_two_ranks_gloo():
 def test_single_process_without_group():
     from vlfeat_b200 import replicas
     assert replicas.whole_job_rate(500.0, 2.0, None) == (250000.0, 2.0)
+
+
+def _shard_worker(rank, world, port, out):
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from oracle.oracle import FLAG_IMPROVED, Restatement
+        from vlfeat_b200 import replicas
+        from vlfeat_b200 import workloads as W
+        offs, x, (pr, mu, cv) = _batch()
+        j0, j1, local = replicas.image_shard(offs, rank, world)
+        R = Restatement()
+        rows = x[offs[j0]:offs[j1]]
+        enc = np.zeros((j1 - j0, 2 * 16 * 8), np.float32)
+        for j in range(j1 - j0):
+            enc[j] = R.fisher(rows[local[j]:local[j + 1]], mu, cv, pr, FLAG_IMPROVED)[0]
+        allenc = replicas.gather_encodings(torch.from_numpy(enc), len(offs) - 1, dist)
+        out.put((rank, None if allenc is None else allenc.numpy(), (j0, j1)))
+    finally:
+        dist.destroy_process_group()
+
+
+def _batch():
+    import numpy as np
+    from vlfeat_b200 import workloads as W
+    counts = np.array([5, 0, 130, 17, 1, 64, 300])
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    x = W.pca_like(int(offs[-1]), 8, seed=77)
+    return offs, x, W.fv_gmm(16, 8, seed=78)
+
+
+def test_sharded_batch_gathers_to_single_process_result():
+    import numpy as np
+    from oracle.oracle import FLAG_IMPROVED, Restatement
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((out.get(timeout=120) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    offs, x, (pr, mu, cv) = _batch()
+    assert res[0][2] == (0, 3) and res[1][2] == (3, 7)
+    assert res[1][1] is None
+    R = Restatement()
+    want = np.stack([R.fisher(x[offs[j]:offs[j + 1]], mu, cv, pr, FLAG_IMPROVED)[0] for j in range(len(offs) - 1)])
+    assert np.array_equal(res[0][1], want)
+
+
+def test_image_shard_blocks():
+    from vlfeat_b200 import replicas
+    offs = [0, 3, 3, 10, 11]
+    blocks = [replicas.image_shard(offs, r, 3) for r in range(3)]
+    assert [(b[0], b[1]) for b in blocks] == [(0, 1), (1, 2), (2, 4)]
+    assert list(blocks[2][2]) == [0, 7, 8]
