@@ -329,3 +329,56 @@ def test_config1_full_size_em_per_iteration(vl):
             assert rel_err(tr[t][1], tr64[t][1]) < bc, (mode, t)
             assert rel_err(tr[t][2], tr64[t][2]) < bp, (mode, t)
             assert abs(ll[t] - ll64[t]) < bl * abs(ll64[t]), (mode, t)
+
+
+# ------------------------------------------------- zero-padded dimensions
+# Dimensions other than 64, 80 and 128 (up to 128) run on the tensor cores
+# zero-padded to the next of them: D = 82 is the recognition app's encoder
+# input (PCA-80 plus the 'xy' frame extension, apps/recognition/
+# encodeImage.m:91-103).
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+@pytest.mark.parametrize("D", [82, 32, 100])
+def test_fv_padded_dimension(vl, restatement, vlfeat_float, mode, D):
+    import torch
+    from vlfeat_b200 import workloads as W
+    K = 256
+    pr, mu, cv = W.fv_gmm(K, D, seed=41)
+    counts = np.array([3000, 0, 200, 1377])
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    x = W.pca_like(int(offs[-1]), D, seed=42)
+    enc = torch.zeros((len(counts), 2 * K * D), device="cuda")
+    vl.fisher_encode_batch_device(enc, _t(mu), _t(cv), _t(pr), _t(x), offs, FLAG_IMPROVED, mode)
+    assert vl.last_precision() == mode
+    enc = enc.cpu().numpy()
+    for j in range(len(counts)):
+        xj = x[offs[j]:offs[j + 1]]
+        e, _ = restatement.fisher(xj.astype(np.float64), mu.astype(np.float64), cv.astype(np.float64),
+                                  pr.astype(np.float64), FLAG_IMPROVED)
+        if counts[j] == 0:
+            assert np.all(enc[j] == 0)
+        else:
+            assert rel_err(enc[j], e) < fv_bound(mode, e, vlfeat_float, xj, mu, cv, pr, FLAG_IMPROVED), j
+
+
+def test_posteriors_padded_dimension(vl, restatement):
+    from vlfeat_b200 import workloads as W
+    D = 82
+    pr, mu, cv = W.fv_gmm(256, D, seed=43)
+    x = W.pca_like(5000, D, seed=44)
+    q64, ll64 = restatement.posteriors(x.astype(np.float64), pr.astype(np.float64),
+                                       mu.astype(np.float64), cv.astype(np.float64))
+    vl.set_precision("fp32")
+    q, ll = vl.get_gmm_data_posteriors(x, pr, mu, cv)
+    assert vl.last_precision() == "fp32"
+    assert np.max(np.abs(q - q64)) < 4e-5
+    assert abs(ll - ll64) < 4e-6 * abs(ll64)
+
+
+def test_em_on_padded_dimension_reports_exact(vl):
+    """EM keeps the CUDA-core path for dimensions the tensor-core M-step is not
+    built for, and says so."""
+    from vlfeat_b200 import workloads as W
+    c = W.config0(scale=0.1)
+    c = dict(c, data=c["data"][:, :50].copy(), means=c["means"][:, :50].copy(), covs=c["covs"][:, :50].copy(), D=50)
+    _em(vl, c, 2, "fp32")
+    assert vl.last_precision() == "exact"

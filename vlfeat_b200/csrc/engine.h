@@ -174,6 +174,12 @@ void weights_bf16(const float *W, int out, int in, int inPad, __nv_bfloat16 *Wb,
 void wait_selftest(double limit_ms, cudaStream_t s);
 // The tensor-core Fisher encoder (E-step, statistics and the cluster finalize).
 bool tc_fv_supported(i64 K, i64 D);
+// Shapes the tensor-core E-step (posteriors) and Fisher encoding take with
+// the dimension zero-padded to the next one the kernels are built for (64,
+// 80 or 128; any D <= 128).
+int tc_pad_dim(i64 D);
+bool tc_supported_padded(i64 K, i64 D);
+bool tc_fv_supported_padded(i64 K, i64 D);
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
              bool fast, int precision, cudaStream_t s);
 // EM with the tensor-core M-step.  tc_estep_em is the E-step of tc_estep that

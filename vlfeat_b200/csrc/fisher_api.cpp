@@ -32,7 +32,7 @@ void encode_batch(T *enc, const vlb::DevModel<T> &m, const T *X, const i64 *h_of
                   i64 numImages, int flags, int precision, unsigned long long *nterms,
                   cudaStream_t s) {
   if constexpr (sizeof(T) == 4) {
-    if (precision != VLB200_PREC_EXACT && vlb::tc_fv_supported(m.K, m.D)) {
+    if (precision != VLB200_PREC_EXACT && vlb::tc_fv_supported_padded(m.K, m.D)) {
       vlb::tc_fisher_batch(X, h_offsets, numImages, m, enc, nterms, flags, precision, s);
       vlb::note_precision(precision);
       return;

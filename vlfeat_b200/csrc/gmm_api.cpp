@@ -169,7 +169,10 @@ double device_estep(const T *dX, i64 N, const vlb::DevModel<T> &m, T *dq, int pr
   bool done = false;
   i64 nparts = 0;
   if constexpr (sizeof(T) == 4) {
-    if (precision != VLB200_PREC_EXACT && vlb::tc_supported(m.K, m.D)) {
+    // The EM image format needs a dimension the kernels are built for; the
+    // posteriors alone also run zero-padded (vlb::tc_supported_padded).
+    if (precision != VLB200_PREC_EXACT &&
+        (em_image ? vlb::tc_supported(m.K, m.D) : vlb::tc_supported_padded(m.K, m.D))) {
       nparts = em_image ? vlb::tc_estep_em(dX, N, m, dq, llp, precision, s)
                         : vlb::tc_estep(dX, N, m, dq, llp, fast, precision, s);
       done = true;

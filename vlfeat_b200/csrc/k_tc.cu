@@ -1122,9 +1122,11 @@ __global__ void k_tc_fv_consts(const float *__restrict__ means, const float *__r
 constexpr int kFinThreads = 256;
 constexpr int kFinCluster = 4;  // divides K (a multiple of 8 on this path)
 
+// DIM: the dimension the statistics were taken in; Dr <= DIM: the model's own
+// dimension (dimensions past it are zero padding, left out of the vector).
 template <int DIM>
 __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThreads) k_tc_fv_finalize(
-    int K, int Kp, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
+    int K, int Kp, int Dr, const float *__restrict__ partial, const int *__restrict__ imgSlot0,
     const i64 *__restrict__ imgRow0, const double *__restrict__ cmu, const double *__restrict__ cis2,
     const double *__restrict__ cisd, const double *__restrict__ cup, const double *__restrict__ cvp,
     const float *__restrict__ scale, const unsigned *__restrict__ rowcnt, i64 rowcntBase, int flags,
@@ -1142,7 +1144,7 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
   const int img = blockIdx.x / kFinCluster;
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const int Kc = K / kFinCluster, k0 = rank * Kc;
-  const int E = Kc * DIM, KD = K * DIM, eBase = k0 * DIM;
+  const int E = Kc * Dr, KD = K * Dr, eBase = k0 * Dr;
   const int s0 = imgSlot0[img], s1 = imgSlot0[img + 1];
   const i64 r0 = imgRow0[img], r1 = imgRow0[img + 1];
   const i64 n = r1 - r0;
@@ -1153,7 +1155,7 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
   __syncthreads();
   double sq = 0;
   for (int el = tid; el < E; el += kFinThreads) {
-    const int kl = el / DIM, d = el - kl * DIM, k = k0 + kl, e = eBase + el;
+    const int kl = el / Dr, d = el - kl * Dr, k = k0 + kl, e = eBase + el;
     double S0 = 0, S1 = 0, S2 = 0;
     const float *pp = partial + ((size_t)s0 * Kp + k) * NST;
     for (int s = s0; s < s1; ++s, pp += slotStride) {
@@ -1325,6 +1327,30 @@ __global__ void k_rows_to_image16(const float *__restrict__ q, i64 n, int K, int
   }
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane == 0 && valid && rowcnt) rowcnt[row] = cnt;
+}
+
+// ============================================================ padding
+// Dimensions the kernels are built for take the data as it is; any other
+// dimension up to 128 runs zero-padded to the next of them: each row gets
+// zero columns, each component mean 0 and variance 1 there, which adds 0 to
+// every (x - mu)^2 / sigma^2 and to every sum of log sigma^2, so the
+// posteriors and the Fisher statistics of the real dimensions are unchanged
+// (the log-likelihood's D/2 log(2 pi) term is corrected for the padding).
+__global__ void k_pad_rows(const float *__restrict__ X, i64 N, int D, int Dp, float *__restrict__ Xp) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * Dp) return;
+  const i64 r = i / Dp;
+  const int d = (int)(i - r * Dp);
+  Xp[i] = d < D ? X[r * D + d] : 0.f;
+}
+__global__ void k_pad_model(const float *__restrict__ means, const float *__restrict__ covs, int K, int D, int Dp,
+                            float *__restrict__ mp, float *__restrict__ cp) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (i64)K * Dp) return;
+  const i64 k = i / Dp;
+  const int d = (int)(i - k * Dp);
+  mp[i] = d < D ? means[k * D + d] : 0.f;
+  cp[i] = d < D ? covs[k * D + d] : 1.f;
 }
 
 // ================================================================ host
@@ -1614,6 +1640,38 @@ bool tc_supported(i64 K, i64 D) {
   return D == 64 ? ELayout<64, false, true>::max_stages(Kb) >= 2 : ELayout<80, false, true>::max_stages(Kb) >= 2;
 }
 
+int tc_pad_dim(i64 D) { return D <= 64 ? 64 : D <= 80 ? 80 : D <= 128 ? 128 : 0; }
+
+bool tc_supported_padded(i64 K, i64 D) { return tc_pad_dim(D) > 0 && tc_supported(K, tc_pad_dim(D)); }
+
+bool tc_fv_supported_padded(i64 K, i64 D) {
+  const int Dp = tc_pad_dim(D);
+  return Dp > 0 && tc_supported(K, Dp) && K % kFinCluster == 0 &&
+         sizeof(float) * 2 * (size_t)(K / kFinCluster) * D <= (size_t)kSmemLimit;
+}
+
+// Zero-padded copies of rows and model in `sc` (slots 22-24).
+struct Padded {
+  DevModel<float> m;
+  const float *X = nullptr;
+};
+Padded pad_inputs(const float *X, i64 N, const DevModel<float> &m, Scratch &sc, cudaStream_t s) {
+  Padded P;
+  const int Dp = tc_pad_dim(m.D), D = (int)m.D;
+  float *xp = sc.slot[22].get<float>((size_t)std::max<i64>(1, N) * Dp);
+  float *mp = sc.slot[23].get<float>((size_t)m.K * Dp), *cp = sc.slot[24].get<float>((size_t)m.K * Dp);
+  if (N > 0)
+    VLB_LAUNCH("pad_rows", s, k_pad_rows<<<(unsigned)((N * Dp + 255) / 256), 256, 0, s>>>(X, N, D, Dp, xp));
+  VLB_LAUNCH("pad_model", s,
+             k_pad_model<<<(unsigned)((m.K * Dp + 255) / 256), 256, 0, s>>>(m.means, m.covs, (int)m.K, D, Dp, mp, cp));
+  P.X = xp;
+  P.m = m;
+  P.m.means = mp;
+  P.m.covs = cp;
+  P.m.D = Dp;
+  return P;
+}
+
 bool tc_fv_supported(i64 K, i64 D) {
   // The finalize keeps 2 (K / kFinCluster) D floats per CTA in shared memory.
   return tc_supported(K, D) && K % kFinCluster == 0 &&
@@ -1624,6 +1682,18 @@ i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *
              int precision, cudaStream_t s) {
   (void)precision;
   Scratch &sc = thread_scratch(kArenaTc);
+  if (!tc_supported(m.K, m.D)) {
+    // Zero-padded dimension: the same posteriors; the log-likelihood's
+    // -D/2 log(2 pi) per row was taken with the padded D, so one more
+    // partial adds (Dp - D)/2 log(2 pi) for each row back.
+    const Padded P = pad_inputs(X, N, m, sc, s);
+    const i64 n = tc_estep(P.X, N, P.m, q, ll_part, fast, precision, s);
+    if (!ll_part) return n;
+    const double fix = 0.5 * (double)(P.m.D - m.D) * log(2.0 * 3.141592653589793) * (double)N;
+    VLB_CUDA(cudaMemcpyAsync(ll_part + n, &fix, sizeof(double), cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+    return n + 1;
+  }
   TcPrep tp;
   tc_prepare(m, tp, false, sc, s);
   int *err = sc.slot[3].get<int>(1);
@@ -1845,9 +1915,12 @@ using ChunkHook = std::function<void(size_t)>;
 
 // All launches of one batched encode; no host copies, no synchronisation and,
 // once the scratch is sized by fv_upload and one earlier run, no allocation.
+// m: the model the kernels run on; mreal (or null): the caller's model when m
+// is its zero-padded copy (tc_pad_dim), whose dimension the vectors take.
 void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float> &m, float *enc,
             unsigned long long *nterms, int flags, int precision, const TcFvConfig &cfg, cudaStream_t s,
-            const ChunkHook &before = nullptr, const ChunkHook &after = nullptr) {
+            const ChunkHook &before = nullptr, const ChunkHook &after = nullptr,
+            const DevModel<float> *mreal = nullptr) {
   const bool fp32 = (precision == VLB200_PREC_FP32);
   TcPrep tp;
   tc_prepare(m, tp, !fp32, sc, s);
@@ -1860,9 +1933,11 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
   double *cmu = sc.slot[13].get<double>(K * D), *cis2 = sc.slot[14].get<double>(K * D);
   double *cisd = sc.slot[15].get<double>(K * D), *cup = sc.slot[16].get<double>(K);
   double *cvp = sc.slot[17].get<double>(K);
+  const DevModel<float> &mr = mreal ? *mreal : m;
+  const i64 Dr = mr.D;
   VLB_LAUNCH("tc_fv_consts", s,
-             k_tc_fv_consts<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
-                 m.means, m.covs, m.priors, tp.ctr, (int)K, (int)D, cmu, cis2, cisd, cup, cvp));
+             k_tc_fv_consts<<<(unsigned)((K * Dr + 255) / 256), 256, 0, s>>>(
+                 mr.means, mr.covs, mr.priors, tp.ctr, (int)K, (int)Dr, cmu, cis2, cisd, cup, cvp));
   void *q = sc.slot[4].p;
   unsigned *rowcnt = (unsigned *)sc.slot[5].p;
   float *partial = (float *)sc.slot[6].p;
@@ -1871,7 +1946,7 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
   const int *dslot0 = (const int *)sc.slot[10].p;
   const i64 *drow0 = (const i64 *)sc.slot[11].p;
   auto fin = D == 64 ? k_tc_fv_finalize<64> : D == 80 ? k_tc_fv_finalize<80> : k_tc_fv_finalize<128>;
-  const size_t finSmem = sizeof(float) * 2 * (K / kFinCluster) * D;
+  const size_t finSmem = sizeof(float) * 2 * (K / kFinCluster) * Dr;
   VLB_CUDA(cudaFuncSetAttribute(fin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)finSmem));
   for (size_t ci = 0; ci < L.chunks.size(); ++ci) {
     const FvChunk &c = L.chunks[ci];
@@ -1900,7 +1975,7 @@ void fv_run(const FvLayout &L, Scratch &sc, const float *X, const DevModel<float
     }
     VLB_LAUNCH("tc_fv_finalize", s,
                fin<<<(unsigned)(c.nimg * kFinCluster), kFinThreads, finSmem, s>>>(
-                   (int)K, tp.Kp, partial, dslot0 + c.img, drow0 + c.img, cmu, cis2, cisd, cup, cvp,
+                   (int)K, tp.Kp, (int)Dr, partial, dslot0 + c.img, drow0 + c.img, cmu, cis2, cisd, cup, cvp,
                    tp.scale, c.nrows > 0 ? rowcnt : nullptr, c.row0, flags, c.img0, enc,
                    nterms));
     if (after) after(ci);
@@ -1917,6 +1992,17 @@ void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages, const 
   TcFvConfig cfg;
   FvLayout L;
   fv_layout(h_offsets, numImages, default_row_budget(Kp, fp32), cfg.itemRows, num_sms(), L);
+  if (!tc_fv_supported(m.K, m.D)) {
+    const i64 N = h_offsets[numImages] - h_offsets[0];
+    const Padded P = pad_inputs(X + h_offsets[0] * m.D, N, m, sc, s);
+    std::vector<i64> offs(h_offsets, h_offsets + numImages + 1);
+    for (auto &o : offs) o -= h_offsets[0];
+    fv_layout(offs.data(), numImages, default_row_budget(Kp, fp32), cfg.itemRows, num_sms(), L);
+    fv_upload(L, Kp, padQ(Kp), (int)(2 * P.m.D + 16), fp32, sc, s);
+    fv_run(L, sc, P.X, P.m, enc, nterms, flags, precision, cfg, s, nullptr, nullptr, &m);
+    check_err((int *)sc.slot[3].p, s);
+    return;
+  }
   fv_upload(L, Kp, padQ(Kp), (int)(2 * m.D + 16), fp32, sc, s);
   fv_run(L, sc, X, m, enc, nterms, flags, precision, cfg, s);
   check_err((int *)sc.slot[3].p, s);
