@@ -971,6 +971,10 @@ def main():
                     help="skip the GMM KMeans-initialisation measurement")
     ap.add_argument("--no-router-eval", action="store_true",
                     help="skip the learned router's evaluation at K=1024 (train 2M, evaluate 10M)")
+    ap.add_argument("--router-train", type=int, default=2_000_000,
+                    help="training descriptors of the router evaluation (smaller for profiling cases)")
+    ap.add_argument("--router-eval", type=int, default=10_000_000,
+                    help="held-out descriptors of the router evaluation (smaller for profiling cases)")
     ap.add_argument("--images", type=int, default=4096,
                     help="encode only the first IMAGES images of the workload (small profiling cases)")
     ap.add_argument("--plan", default=None,
@@ -1086,7 +1090,7 @@ def main():
             if router is not None:
                 capi.lib().vlb200_router_set_default(None, 8, 0.99)
                 del router
-            out["router_config3"] = router_config3(capi)
+            out["router_config3"] = router_config3(capi, n_train=args.router_train, n_eval=args.router_eval)
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

@@ -189,3 +189,50 @@ def test_tensor_core_dense_layers(vl, shape):
     g = got.cpu().numpy()
     assert rel_err(g, want) < 5e-3
     assert rel_err(g, cc.cpu().numpy()) < 3e-2
+
+
+def test_config3_network_reduced(vl):
+    """The config-3 setting at reduced size: K = 1,024, D = 80, the 1,024-
+    component mixture with sigma ~ U[0.3, 1.5], the MLP 80 -> 256 -> 256 ->
+    1024 trained on 200,000 descriptors' full-E-step top-8 posteriors, judged
+    on 50,000 held-out descriptors at m = 8: the missed posterior mass without
+    fallback is small, the fallback at 0.99 predicted candidate mass leaves
+    less, and Fisher vectors through the router path stay within the metric's
+    1e-3 of the FP32 path."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    from vlfeat_b200.router import Router, missed_mass, targets
+    params = W.config3_params(1024, 80)
+    pr, mu, cv = (_t(a) for a in params)
+    xtr = W.config3_data_device(200_000, params, seed=601)
+    xte = W.config3_data_device(50_000, params, seed=602)
+    q = torch.empty((xtr.shape[0], 1024), device="cuda")
+    vl.gmm_posteriors_device(q, pr, mu, cv, xtr, "fp32")
+    tidx = torch.empty((xtr.shape[0], 8), dtype=torch.int32, device="cuda")
+    tw = torch.empty((xtr.shape[0], 8), dtype=torch.float32, device="cuda")
+    targets(q, tidx, tw)
+    r = Router(80, 1024, hidden=(256, 256), seed=3)
+    r.set_input_transform(xtr.mean(0).cpu().numpy(), (1.0 / xtr.std(0)).cpu().numpy())
+    r.train(xtr, tidx, tw, epochs=6, batch=1024, lr=2e-3)
+    qf = torch.empty((xte.shape[0], 1024), device="cuda")
+    vl.gmm_posteriors_device(qf, pr, mu, cv, xte, "fp32")
+    qc = torch.empty_like(qf)
+    r.posteriors(qc, pr, mu, cv, xte, m=8, threshold=0.0)
+    mm0 = missed_mass(qf, qc)
+    fb = r.posteriors(qc, pr, mu, cv, xte, m=8, threshold=0.99)
+    mm1 = missed_mass(qf, qc)
+    assert mm0 < 2e-2, mm0
+    assert mm1 <= mm0 and fb < 0.5 * xte.shape[0], (mm1, fb)
+    offs = np.arange(11, dtype=np.int64) * 3000
+    xi = xte[:30000].contiguous()
+    ref = torch.empty((10, 2 * 1024 * 80), device="cuda")
+    vl.fisher_encode_batch_device(ref, mu, cv, pr, xi, offs, 3, "fp32")
+    enc = torch.empty_like(ref)
+    r.set_default(m=8, threshold=0.99)
+    try:
+        vl.fisher_encode_batch_device(enc, mu, cv, pr, xi, offs, 3, "bf16_router")
+    finally:
+        r.set_default(m=8, threshold=0.99)
+        vl.lib().vlb200_router_set_default(None, 8, 0.99)
+    e = ((enc.double() - ref.double()).norm(dim=1) / ref.double().norm(dim=1)).max().item()
+    assert e < 1e-3, e
