@@ -374,11 +374,18 @@ def test_posteriors_padded_dimension(vl, restatement):
     assert abs(ll - ll64) < 4e-6 * abs(ll64)
 
 
-def test_em_on_padded_dimension_reports_exact(vl):
-    """EM keeps the CUDA-core path for dimensions the tensor-core M-step is not
-    built for, and says so."""
+def test_em_on_padded_dimension(vl, restatement):
+    """EM at a dimension the tensor-core M-step is not built for (D = 50): the
+    E-steps run zero-padded on the tensor cores (the record says FP32), the
+    M-steps on the CUDA cores; the result stays within the FP32 mode's EM
+    bound of the FP64 restatement."""
     from vlfeat_b200 import workloads as W
     c = W.config0(scale=0.1)
     c = dict(c, data=c["data"][:, :50].copy(), means=c["means"][:, :50].copy(), covs=c["covs"][:, :50].copy(), D=50)
-    _em(vl, c, 2, "fp32")
-    assert vl.last_precision() == "exact"
+    r = restatement.em(c["data"].astype(np.float64), c["priors"], c["means"], c["covs"], c["lower_bound"], 3)
+    m, ll = _em(vl, c, 3, "fp32")
+    assert vl.last_precision() == "fp32"
+    assert abs(ll - r["ll"]) <= 2e-5 * abs(r["ll"])
+    assert rel_err(m.means, r["means"]) < EM_TOL["fp32"]
+    assert rel_err(m.covariances, r["covs"]) < EM_TOL["fp32"]
+    assert rel_err(m.priors, r["priors"]) < EM_TOL["fp32"]

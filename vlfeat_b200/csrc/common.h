@@ -121,7 +121,8 @@ enum ScratchArena {
   kArenaRouter = 3,
   kArenaVlad = 4,
   kArenaKMeans = 5,
-  kNumArenas = 6
+  kArenaRouterTc = 6,  // the router's fallback rows on the tensor-core E-step
+  kNumArenas = 7
 };
 Scratch &thread_scratch(int arena = kArenaApi);
 

@@ -181,7 +181,7 @@ int tc_pad_dim(i64 D);
 bool tc_supported_padded(i64 K, i64 D);
 bool tc_fv_supported_padded(i64 K, i64 D);
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part,
-             bool fast, int precision, cudaStream_t s);
+             bool fast, int precision, cudaStream_t s, Scratch *arena = nullptr);
 // EM with the tensor-core M-step.  tc_estep_em is the E-step of tc_estep that
 // also writes the posteriors as the statistics operand image, thresholded at
 // the M-step's skip (vl/gmm.c:1099); tc_mstep then runs the M-step

@@ -277,13 +277,21 @@ __global__ void k_candidate_estep(const float *__restrict__ X, i64 n, int D, int
                                   const double *__restrict__ cst, const int *__restrict__ cand,
                                   const float *__restrict__ cmass, int m, float thr,
                                   float *__restrict__ q, unsigned char *__restrict__ fell,
-                                  double *__restrict__ llrow) {
+                                  double *__restrict__ llrow, bool deferFallback) {
   const i64 row = (i64)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   if (row >= n) return;
   const float *x = X + row * D;
   float *qr = q + row * K;
   const bool fb = !(cmass[row] >= thr);  // a NaN mass (NaN logits) falls back too
+  if (fb && deferFallback) {
+    // The row goes to the tensor-core E-step with the other fallback rows.
+    if (lane == 0) {
+      fell[row] = 1;
+      if (llrow) llrow[row] = 0.0;
+    }
+    return;
+  }
   const int nc = fb ? K : m;
   for (int k = lane; k < K; k += 32) qr[k] = 0.f;
   __syncwarp();
@@ -337,6 +345,55 @@ __global__ void k_candidate_estep(const float *__restrict__ X, i64 n, int D, int
   if (lane == 0 && llrow) llrow[row] = (double)mx + log((double)s);
 }
 
+// Stable list of the rows that fell back (their order kept): per-block
+// counts, one exclusive scan, then each block writes its rows' indices.
+__global__ void k_fb_count(const unsigned char *__restrict__ fell, i64 n, int *__restrict__ counts) {
+  const i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = __syncthreads_count(row < n && fell[row]);
+  if (threadIdx.x == 0) counts[blockIdx.x] = c;
+}
+__global__ void k_fb_scan(int *__restrict__ counts, int nb, int *__restrict__ total) {
+  if (threadIdx.x != 0) return;
+  int acc = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int c = counts[b];
+    counts[b] = acc;
+    acc += c;
+  }
+  *total = acc;
+}
+__global__ void k_fb_scatter(const unsigned char *__restrict__ fell, i64 n, const int *__restrict__ offs,
+                             int *__restrict__ idx) {
+  __shared__ int warpBase[32];
+  const i64 row = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  const bool f = row < n && fell[row];
+  const unsigned bal = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) warpBase[warp] = __popc(bal);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+      const int c = warpBase[w];
+      warpBase[w] = acc;
+      acc += c;
+    }
+  }
+  __syncthreads();
+  if (f) idx[offs[blockIdx.x] + warpBase[warp] + __popc(bal & ((1u << lane) - 1u))] = (int)row;
+}
+// Rows idx[j] of src (width w floats) -> row j of dst, or back (scatter).
+__global__ void k_rows_gather(const float *__restrict__ src, const int *__restrict__ idx, int cnt, int w,
+                              float *__restrict__ dst, bool scatter) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (i64)cnt * w) return;
+  const i64 j = i / w;
+  const int c = (int)(i - j * w);
+  const i64 r = idx[j];
+  if (scatter) dst[r * w + c] = src[i];
+  else dst[i] = src[r * w + c];
+}
+
 // Missed posterior mass of each row: sum of the full-E-step posteriors that
 // the candidate rows set to zero.
 __global__ void k_missed(const float *__restrict__ qfull, const float *__restrict__ qc, i64 n, int K,
@@ -355,6 +412,11 @@ __global__ void k_missed(const float *__restrict__ qfull, const float *__restric
 }  // namespace vlb
 
 // ====================================================================== host
+namespace vlb {
+double tc_fallback(const float *X, i64 B, const DevModel<float> &m, const unsigned char *fell, float *q,
+                   unsigned long long *nfb, cudaStream_t s);
+}
+
 struct _VlB200Router {
   int D = 0, K = 0;
   std::vector<int> sizes;  // D, hidden..., K
@@ -707,11 +769,14 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
       else
         VLB_LAUNCH("router_select", s,
                    vlb::k_select<32><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+      const bool tcfb = vlb::tc_supported_padded(K, D);
       VLB_LAUNCH("router_candidate_estep", s,
                  vlb::k_candidate_estep<<<vlb::gridn(B, 8), 256, 0, s>>>(
                      X + i0 * D, B, D, K, means, der.inv, der.cst, cand, cm, (int)m, threshold,
-                     posteriors + i0 * K, fell, nullptr));
-      if (fallbackRows) {
+                     posteriors + i0 * K, fell, nullptr, tcfb));
+      if (tcfb) {
+        vlb::tc_fallback(X + i0 * D, B, md, fell, posteriors + i0 * K, &nfb, s);
+      } else if (fallbackRows) {
         std::vector<unsigned char> h(B);
         VLB_CUDA(cudaMemcpyAsync(h.data(), fell, B, cudaMemcpyDeviceToHost, s));
         VLB_CUDA(cudaStreamSynchronize(s));
@@ -784,6 +849,42 @@ extern "C" int vlb200_router_set_default(VlB200Router *router, vl_size m, float 
 }
 
 namespace vlb {
+// The rows that fell back (fell[i] = 1) go through the tensor-core E-step
+// together: their indices listed in row order, the rows gathered into one
+// block, their posteriors computed there (fp16x3 split, FP32-grade, every
+// component), and scattered back into q.  Returns their log-likelihood and
+// adds their count to *nfb.
+double tc_fallback(const float *X, i64 B, const DevModel<float> &m, const unsigned char *fell, float *q,
+                   unsigned long long *nfb, cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaRouterTc);
+  const int K = (int)m.K, D = (int)m.D;
+  const int nb = (int)((B + 1023) / 1024);
+  int *counts = sc.slot[25].get<int>((size_t)nb + 1);
+  int *idx = sc.slot[26].get<int>((size_t)B);
+  VLB_LAUNCH("router_fallback_list", s, k_fb_count<<<nb, 1024, 0, s>>>(fell, B, counts));
+  VLB_LAUNCH("router_fallback_list", s, k_fb_scan<<<1, 32, 0, s>>>(counts, nb, counts + nb));
+  VLB_LAUNCH("router_fallback_list", s, k_fb_scatter<<<nb, 1024, 0, s>>>(fell, B, counts, idx));
+  int cnt = 0;
+  VLB_CUDA(cudaMemcpyAsync(&cnt, counts + nb, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  if (nfb) *nfb += (unsigned long long)cnt;
+  if (cnt == 0) return 0.0;
+  float *xg = sc.slot[27].get<float>((size_t)cnt * D);
+  float *qg = sc.slot[28].get<float>((size_t)cnt * K);
+  double *llp = sc.slot[29].get<double>(estep_ll_parts(cnt));
+  double *tot = sc.slot[30].get<double>(1);
+  VLB_LAUNCH("router_fallback_gather", s,
+             k_rows_gather<<<gridn((i64)cnt * D, 256), 256, 0, s>>>(X, idx, cnt, D, xg, false));
+  const i64 np = tc_estep(xg, cnt, m, qg, llp, false, VLB200_PREC_FP32, s, &sc);
+  sum_doubles(llp, np, tot, s);
+  VLB_LAUNCH("router_fallback_scatter", s,
+             k_rows_gather<<<gridn((i64)cnt * K, 256), 256, 0, s>>>(qg, idx, cnt, K, q, true));
+  double h = 0;
+  VLB_CUDA(cudaMemcpyAsync(&h, tot, sizeof(double), cudaMemcpyDeviceToHost, s));
+  VLB_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
 // Router E-step of n rows for streamed EM: posteriors q (n x K, zeros off the
 // candidates), the rows' log-likelihood over the evaluated components
 // (returned), and the number of rows that fell back to the full E-step.
@@ -818,17 +919,23 @@ double router_estep(VlB200Router *r, const float *X, i64 n, const DevModel<float
       VLB_LAUNCH("router_select", s, k_select<16><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
     else
       VLB_LAUNCH("router_select", s, k_select<32><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+    const bool tcfb = tc_supported_padded(K, D);
     VLB_LAUNCH("router_candidate_estep", s,
                k_candidate_estep<<<gridn(B, 8), 256, 0, s>>>(X + i0 * D, B, D, K, m.means, der.inv, der.cst, cand,
-                                                             cm, (int)mcand, thr, q + i0 * K, fell, llrow));
+                                                             cm, (int)mcand, thr, q + i0 * K, fell, llrow, tcfb));
     sum_doubles(llrow, B, llsum, s);
     double h = 0;
-    std::vector<unsigned char> hf(B);
     VLB_CUDA(cudaMemcpyAsync(&h, llsum, sizeof(double), cudaMemcpyDeviceToHost, s));
-    VLB_CUDA(cudaMemcpyAsync(hf.data(), fell, B, cudaMemcpyDeviceToHost, s));
     VLB_CUDA(cudaStreamSynchronize(s));
     ll += h;
-    for (auto v : hf) nfb += v;
+    if (tcfb) {
+      ll += tc_fallback(X + i0 * D, B, m, fell, q + i0 * K, &nfb, s);
+    } else {
+      std::vector<unsigned char> hf(B);
+      VLB_CUDA(cudaMemcpyAsync(hf.data(), fell, B, cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaStreamSynchronize(s));
+      for (auto v : hf) nfb += v;
+    }
   }
   if (fallback) *fallback += nfb;
   return ll;

@@ -1679,15 +1679,15 @@ bool tc_fv_supported(i64 K, i64 D) {
 }
 
 i64 tc_estep(const float *X, i64 N, const DevModel<float> &m, float *q, double *ll_part, bool fast,
-             int precision, cudaStream_t s) {
+             int precision, cudaStream_t s, Scratch *arena) {
   (void)precision;
-  Scratch &sc = thread_scratch(kArenaTc);
+  Scratch &sc = arena ? *arena : thread_scratch(kArenaTc);
   if (!tc_supported(m.K, m.D)) {
     // Zero-padded dimension: the same posteriors; the log-likelihood's
     // -D/2 log(2 pi) per row was taken with the padded D, so one more
     // partial adds (Dp - D)/2 log(2 pi) for each row back.
     const Padded P = pad_inputs(X, N, m, sc, s);
-    const i64 n = tc_estep(P.X, N, P.m, q, ll_part, fast, precision, s);
+    const i64 n = tc_estep(P.X, N, P.m, q, ll_part, fast, precision, s, &sc);
     if (!ll_part) return n;
     const double fix = 0.5 * (double)(P.m.D - m.D) * log(2.0 * 3.141592653589793) * (double)N;
     VLB_CUDA(cudaMemcpyAsync(ll_part + n, &fix, sizeof(double), cudaMemcpyHostToDevice, s));
