@@ -9,7 +9,9 @@
 // memory stages:
 //   warp 0     TMA producer (one thread),
 //   warp 1     TMEM allocation and, from one lane, tcgen05.mma issue,
-//   warps 2-5  epilogue: TMEM -> registers -> bias, ReLU -> global.
+//   warps 2-9  epilogue: TMEM -> registers -> bias, ReLU -> global; two
+//              warps per TMEM lane quarter, each taking half of the tile's
+//              columns, the bias staged in shared memory.
 // Tiles are 128 rows x BN columns (BN = N rounded up to 16, at most 256),
 // 64-element k-blocks (4 MMAs of K = 16 each), two TMEM accumulators so that
 // one tile's epilogue overlaps the next tile's MMAs.  Every mbarrier wait is
@@ -28,7 +30,9 @@ namespace {
 
 using namespace tc;
 
-constexpr int kMlpThreads = 192;
+constexpr int kMlpThreads = 320;
+constexpr int kMlpEpiThreads = 256;
+constexpr int kMlpMaxN = 4096;  // bias entries staged in shared memory
 constexpr int kBM = 128, kBK = 64;
 constexpr int kMlpSmemLimit = 232448;
 
@@ -56,6 +60,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
   uint64_t *full = bars, *empty = bars + 8, *accf = bars + 16, *acce = bars + 18;
   uint32_t *s_tmem = (uint32_t *)(bars + 20);
   volatile int *s_abort = (volatile int *)(s_tmem + 1);
+  float *s_bias = (float *)(bars + 32);  // N floats
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int mtiles = (p.M + kBM - 1) / kBM, ntiles = (p.N + p.BN - 1) / p.BN;
   const int tiles = mtiles * ntiles, nkb = (p.Ka + kBK - 1) / kBK;
@@ -66,7 +71,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 128);
+      mbar_init(&acce[b], kMlpEpiThreads);
     }
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -75,6 +80,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
     tmem_alloc(s_tmem, 512);
     tmem_relinquish();
   }
+  for (int n = threadIdx.x; n < p.N; n += kMlpThreads) s_bias[n] = p.bias[n];
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
@@ -131,7 +137,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
   } else if (warp >= 2) {
     // ---------------------------------------------------------- epilogue
     const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int half = (warp - 2) >> 2;  // which half of the tile's 32-column chunks
     const int r = q * 32 + lane;
+    const int nch = (p.BN + 31) / 32, ch0 = half ? (nch + 1) / 2 : 0, ch1 = half ? nch : (nch + 1) / 2;
     int tt = 0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tt) {
       const int mt = t / ntiles, nt = t % ntiles, buf = tt & 1;
@@ -140,7 +148,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
       const long long row = (long long)mt * kBM + r;
       const bool valid = row < p.M;
       const uint32_t tb = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 256);
-      for (int c0 = 0; c0 < p.BN; c0 += 32) {
+      for (int c0 = 32 * ch0; c0 < 32 * ch1; c0 += 32) {
         uint32_t v[32];
         tmem_ld32(tb + (uint32_t)c0, v);
         tmem_wait_ld();
@@ -153,7 +161,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
           float y[8];
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
-            float a = __uint_as_float(v[8 * g + j]) + __ldg(p.bias + n + j);
+            float a = __uint_as_float(v[8 * g + j]) + s_bias[n + j];
             y[j] = (p.relu && !(a > 0.f)) ? 0.f : a;
           }
           if (p.out_f32) {
@@ -234,12 +242,14 @@ void make_map(CUtensorMap *m, const void *ptr, long long rows, int cols, int box
 
 }  // namespace
 
-bool tc_dense_supported(int N, int Ka) { return N >= 8 && N % 8 == 0 && Ka >= 8 && Ka % 8 == 0; }
+bool tc_dense_supported(int N, int Ka) {
+  return N >= 8 && N % 8 == 0 && N <= kMlpMaxN && Ka >= 8 && Ka % 8 == 0;
+}
 
 void tc_dense(const __nv_bfloat16 *A, long long M, int Ka, const __nv_bfloat16 *W, int N, const float *bias,
               bool relu, bool outF32, void *C, int *err, cudaStream_t s) {
   if (M <= 0) return;
-  VLB_CHECK(tc_dense_supported(N, Ka), VL_ERR_BAD_ARG, "dense layer: widths must be multiples of 8");
+  VLB_CHECK(tc_dense_supported(N, Ka), VL_ERR_BAD_ARG, "dense layer: widths must be multiples of 8, N <= 4096");
   MlpParams p;
   const int BN = std::min(256, (N + 15) / 16 * 16);
   make_map(&p.ta, A, M, Ka, kBM);
@@ -254,7 +264,7 @@ void tc_dense(const __nv_bfloat16 *A, long long M, int Ka, const __nv_bfloat16 *
   p.out_f32 = outF32 ? 1 : 0;
   p.err = err;
   const size_t stageBytes = (size_t)(kBM + BN) * kBK * 2;
-  const size_t fixed = 1024 /*alignment*/ + 256 /*barriers, TMEM base, abort flag*/;
+  const size_t fixed = 1024 /*alignment*/ + 256 /*barriers, TMEM base, abort flag*/ + 4 * (size_t)N /*bias*/;
   p.nst = (int)std::min<size_t>(8, (kMlpSmemLimit - fixed) / stageBytes);
   VLB_CHECK(p.nst >= 2, VL_ERR_BAD_ARG, "dense layer: operand stages exceed shared memory");
   const size_t smem = fixed + (size_t)p.nst * stageBytes;
