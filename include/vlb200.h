@@ -30,7 +30,12 @@ struct _VlB200Router; /* the learned router, declared below */
  *             on the candidates only; fp16 statistics; full E-step fallback
  *             for descriptors whose predicted candidate mass is < 0.99.
  * DEFAULT resolves to the process-wide mode (vlb200_set_precision), which
- * starts as EXACT.  VL_TYPE_DOUBLE calls always run EXACT in double. */
+ * starts as EXACT -- VLFeat's own float arithmetic, so that a relinked
+ * program gets the reference's float results -- unless the environment
+ * variable VLB200_PRECISION names fp32 or bf16 at load time.  (FP32 is the
+ * faster and, against FP64, the more accurate of the two float modes; EXACT
+ * is the one that reproduces VLFeat's float roundings.)  VL_TYPE_DOUBLE calls
+ * always run EXACT in double. */
 #define VLB200_PREC_DEFAULT 0
 #define VLB200_PREC_EXACT 1
 #define VLB200_PREC_FP32 2

@@ -153,3 +153,20 @@ def test_pca_argument_checks(libpath):
     assert L.vlb200_pca_project_device(None, 80, None, 128, 10, None, None, 1, C.c_void_p(16), None, None, 1,
                                        C.c_void_p(1)) == 3
     assert L.vlb200_pca_learn_device(None, None, 81, None, 80, 10, 0, 0.0, None, C.c_void_p(1)) == 3
+
+
+def test_precision_default_from_environment():
+    """The process-wide mode starts as EXACT; VLB200_PRECISION=fp32 or bf16 in
+    the environment selects another mode when the library is loaded."""
+    import os
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); from vlfeat_b200 import capi; "
+            "print(capi.get_precision())" % ROOT)
+    for env, want in ((None, 1), ("fp32", 2), ("bf16", 3), ("bogus", 1)):
+        e = dict(os.environ)
+        e.pop("VLB200_PRECISION", None)
+        if env:
+            e["VLB200_PRECISION"] = env
+        out = subprocess.run([sys.executable, "-c", code], env=e, capture_output=True, text=True, check=True)
+        assert int(out.stdout.strip()) == want, (env, out.stdout)

@@ -23,7 +23,18 @@ thread_local int g_last_error = VL_ERR_OK;
 thread_local char g_last_msg[1024] = "";
 std::atomic<vl_size> g_num_threads{1};
 std::atomic<int> g_simd{1};
-std::atomic<int> g_precision{VLB200_PREC_EXACT};
+// The process-wide mode starts as EXACT, VLFeat's own float arithmetic, so a
+// program relinked against this library gets the reference's float results;
+// the environment variable VLB200_PRECISION (exact, fp32, bf16) selects
+// another mode without a code change.
+int initial_precision() {
+  const char *e = getenv("VLB200_PRECISION");
+  if (!e) return VLB200_PREC_EXACT;
+  if (!strcmp(e, "fp32") || !strcmp(e, "FP32")) return VLB200_PREC_FP32;
+  if (!strcmp(e, "bf16") || !strcmp(e, "BF16")) return VLB200_PREC_BF16;
+  return VLB200_PREC_EXACT;
+}
+std::atomic<int> g_precision{initial_precision()};
 printf_func_t g_printf = (printf_func_t)&printf;
 
 int silent_printf(char const *, ...) { return 0; }
