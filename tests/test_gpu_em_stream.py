@@ -116,3 +116,21 @@ def test_router_pruned_streamed_em_against_fp64(vl):
     for t in range(11):
         if rep[t]["routed"]:
             assert 0 <= rep[t]["fallback_rows"] <= 300_000
+
+
+def test_streamed_restarts_in_fp32_mode_match_resident(vl):
+    """Config 0 (restarts fire at iteration 2) in FP32 mode: the streamed loop's
+    restarts re-derive the tensor-core E-step's posteriors chunk by chunk and
+    land where the resident loop does."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    c = W.config0()
+    x = torch.from_numpy(c["data"]).cuda()
+    a = _model(vl, c, 6)
+    lla = a.em_device(x, "fp32")
+    b = _model(vl, c, 6)
+    llb = b.em_stream_device(x, "fp32", chunk_rows=10_000)
+    assert a.num_restarts == b.num_restarts and a.num_restarts >= 1
+    assert abs(lla - llb) <= 1e-6 * abs(lla)
+    for got, want in ((b.means, a.means), (b.covariances, a.covariances), (b.priors, a.priors)):
+        assert rel_err(got, want) < 1e-5
