@@ -485,7 +485,23 @@ bool tc_infer_ok(const VlB200Router *r) {
   return true;
 }
 
+i64 infer_chunk(const VlB200Router *r) { return tc_infer_ok(r) ? (1 << 20) : (1 << 17); }
+
 void forward(VlB200Router *r, const float *X, i64 B, std::vector<float *> &act, cudaStream_t s);
+
+// Rows per inference chunk and the forward's buffers for it: the tensor-core
+// path needs only the logits (its activations are bf16, in slots 7 and 8),
+// so it takes 2^20 rows at a time; the CUDA-core path 2^17 with every layer's
+// fp32 activations.
+i64 infer_chunk(const VlB200Router *r);
+std::vector<float *> infer_buffers(VlB200Router *r, vlb::Scratch &sc, i64 chunk) {
+  const int L = nlayers(r);
+  std::vector<float *> act(L + 1, nullptr);
+  const bool tc = infer_chunk(r) == (1 << 20);
+  for (int l = 0; l <= L; ++l)
+    if (!tc || l == L) act[l] = sc.slot[l].get<float>((size_t)chunk * r->sizes[l]);
+  return act;
+}
 
 // Logits (B x K, fp32) of a batch for inference: on the tensor cores (bf16
 // features and activations, bf16 weights, fp32 accumulation; tcgen05 dense
@@ -750,12 +766,11 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
     der.sis = sc.slot[23].get<float>((size_t)K * D);
     der.cst = sc.slot[24].get<double>(K);
     vlb::exact_prepare(md, der, s);
-    const i64 chunk = 1 << 17;
+    const i64 chunk = infer_chunk(r);
     unsigned long long nfb = 0;
     for (i64 i0 = 0; i0 < (i64)N; i0 += chunk) {
       const i64 B = std::min<i64>(chunk, (i64)N - i0);
-      std::vector<float *> act(L + 1);
-      for (int l = 0; l <= L; ++l) act[l] = sc.slot[l].get<float>((size_t)chunk * r->sizes[l]);
+      std::vector<float *> act = infer_buffers(r, sc, chunk);
       int *cand = sc.slot[25].get<int>((size_t)chunk * m);
       float *cm = sc.slot[26].get<float>(chunk);
       unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
@@ -900,13 +915,12 @@ double router_estep(VlB200Router *r, const float *X, i64 n, const DevModel<float
   der.sis = sc.slot[23].get<float>((size_t)K * D);
   der.cst = sc.slot[24].get<double>(K);
   exact_prepare(m, der, s);
-  const i64 chunk = 1 << 17;
+  const i64 chunk = infer_chunk(r);
   double ll = 0;
   unsigned long long nfb = 0;
   for (i64 i0 = 0; i0 < n; i0 += chunk) {
     const i64 B = std::min<i64>(chunk, n - i0);
-    std::vector<float *> act(L + 1);
-    for (int l = 0; l <= L; ++l) act[l] = sc.slot[l].get<float>((size_t)chunk * r->sizes[l]);
+    std::vector<float *> act = infer_buffers(r, sc, chunk);
     int *cand = sc.slot[25].get<int>((size_t)chunk * mcand);
     float *cm = sc.slot[26].get<float>(chunk);
     unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
