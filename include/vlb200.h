@@ -303,6 +303,13 @@ VL_EXPORT int vlb200_router_missed_mass(float const *fullPosteriors,
 VL_EXPORT int vlb200_router_set_tensor_core_inference(VlB200Router *router, int on);
 VL_EXPORT int vlb200_router_logits(VlB200Router *router, float const *data, vl_size numData,
                                    float *logits, void *stream);
+/* Top-m candidates (numData x m int, descending logits, ties: lowest index)
+ * and their predicted softmax mass (numData floats) of rows `data`, device
+ * arrays.  fused = 1: selected in the last dense layer's epilogue (tensor-core
+ * inference, m <= 16, numClusters >= 32), else by the selection kernel on
+ * the logits; both are what vlb200_router_posteriors uses. */
+VL_EXPORT int vlb200_router_candidates(VlB200Router *router, float const *data, vl_size numData, vl_size m,
+                                       int *candidates, float *mass, int fused, void *stream);
 /* Router used by VLB200_PREC_BF16_ROUTER calls (not owned; NULL clears). */
 VL_EXPORT int vlb200_router_set_default(VlB200Router *router, vl_size m, float threshold);
 

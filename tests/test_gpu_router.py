@@ -236,3 +236,34 @@ def test_config3_network_reduced(vl):
         vl.lib().vlb200_router_set_default(None, 8, 0.99)
     e = ((enc.double() - ref.double()).norm(dim=1) / ref.double().norm(dim=1)).max().item()
     assert e < 1e-3, e
+
+
+@pytest.mark.parametrize("K,m", [(1024, 16), (256, 8), (40, 4)])
+def test_fused_selection_matches_selection_kernel(vl, K, m):
+    """Top-m selection in the last dense layer's epilogue (running top-16 per
+    row across the column tiles, two half-rows merged, online softmax mass)
+    against the selection kernel on the same tensor-core logits: the same
+    candidates in the same order, the same mass within 1e-4; NaN rows get
+    valid candidates and a NaN mass (so they fall back)."""
+    import torch
+    from vlfeat_b200.router import Router
+    rng = np.random.default_rng(K)
+    D = 80
+    r = Router(D, K, hidden=(256, 256), seed=13)
+    r.set_input_transform(np.zeros(D, np.float32), np.ones(D, np.float32))
+    N = 5000
+    x = rng.normal(size=(N, D)).astype(np.float32)
+    x[17] = np.nan
+    a_c = torch.zeros((N, m), dtype=torch.int32, device="cuda")
+    a_m = torch.zeros(N, device="cuda")
+    b_c = torch.zeros_like(a_c)
+    b_m = torch.zeros_like(a_m)
+    r.candidates(a_c, a_m, _t(x), m=m, fused=True)
+    r.candidates(b_c, b_m, _t(x), m=m, fused=False)
+    ac, bc = a_c.cpu().numpy(), b_c.cpu().numpy()
+    am, bm = a_m.cpu().numpy(), b_m.cpu().numpy()
+    keep = np.arange(N) != 17
+    assert np.array_equal(ac[keep], bc[keep])
+    assert np.max(np.abs(am[keep] - bm[keep])) < 1e-4
+    assert np.all((ac[17] >= 0) & (ac[17] < K)) and len(set(ac[17].tolist())) == m
+    assert np.isnan(am[17])

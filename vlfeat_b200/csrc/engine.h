@@ -164,8 +164,12 @@ bool tc_supported(i64 K, i64 D);
 // relu, C fp32 when outF32 else bf16; N and Ka multiples of 8.  An expired
 // wait writes its code to *err (device).
 bool tc_dense_supported(int N, int Ka);
+// With selM in 1..16 (N >= 32) the last layer's epilogue does not write C:
+// it keeps each row's selM largest outputs (ties: lowest index) in cand
+// (rows x selM) and their softmax mass over all N in cmass (rows).
 void tc_dense(const __nv_bfloat16 *A, long long M, int Ka, const __nv_bfloat16 *W, int N, const float *bias,
-              bool relu, bool outF32, void *C, int *err, cudaStream_t s);
+              bool relu, bool outF32, void *C, int *err, cudaStream_t s, int selM = 0, int *cand = nullptr,
+              float *cmass = nullptr);
 void features_bf16(const float *X, long long n, int D, int Ka, const float *ctr, const float *scl,
                    __nv_bfloat16 *Z, cudaStream_t s);
 void weights_bf16(const float *W, int out, int in, int inPad, __nv_bfloat16 *Wb, cudaStream_t s);

@@ -36,13 +36,37 @@ constexpr int kMlpMaxN = 4096;  // bias entries staged in shared memory
 constexpr int kBM = 128, kBK = 64;
 constexpr int kMlpSmemLimit = 232448;
 
+constexpr int kSelList = 16;  // the selecting epilogue keeps each row's 16 largest logits
+
 struct MlpParams {
   CUtensorMap ta, tb;  // A: {Ka, M}, box {64, 128};  B: {Ka, N}, box {64, BN}
   const float *bias;
   void *c;
   int M, N, Ka, BN, nst, relu, out_f32;
+  // Selecting epilogue (sel = 1): instead of writing C, keep each row's m
+  // largest logits (ties: lowest index) and their softmax mass.
+  int sel, m;
+  int *cand;
+  float *cmass;
   int *err;
 };
+
+// The j-th tile of this CTA as (mt, nt); false past the last one.  With the
+// selecting epilogue a CTA takes whole rows of tiles (every n-tile of an
+// m-tile, in order), so each row's logits pass through one thread pair.
+__device__ __forceinline__ bool tile_at(const MlpParams &p, int mtiles, int ntiles, int j, int &mt, int &nt) {
+  if (p.sel) {
+    mt = (int)blockIdx.x + (j / ntiles) * (int)gridDim.x;
+    nt = j % ntiles;
+    return mt < mtiles;
+  }
+  const long long t = (long long)blockIdx.x + (long long)j * gridDim.x;
+  mt = (int)(t / ntiles);
+  nt = (int)(t % ntiles);
+  return t < (long long)mtiles * ntiles;
+}
+
+
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
   asm volatile(
@@ -60,10 +84,16 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
   uint64_t *full = bars, *empty = bars + 8, *accf = bars + 16, *acce = bars + 18;
   uint32_t *s_tmem = (uint32_t *)(bars + 20);
   volatile int *s_abort = (volatile int *)(s_tmem + 1);
+  uint64_t *xbar = bars + 24;  // selecting epilogue: one per TMEM lane quarter (64 arrivals)
   float *s_bias = (float *)(bars + 32);  // N floats
+  // Selecting epilogue's exchange: per TMEM lane quarter and lane, the second
+  // half's list (values, indices) and its (max, sum).
+  float *s_xv = s_bias + ((p.N + 3) & ~3);
+  int *s_xi = (int *)(s_xv + 4 * 32 * kSelList);
+  float *s_xm = (float *)(s_xi + 4 * 32 * kSelList);
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int mtiles = (p.M + kBM - 1) / kBM, ntiles = (p.N + p.BN - 1) / p.BN;
-  const int tiles = mtiles * ntiles, nkb = (p.Ka + kBK - 1) / kBK;
+  const int nkb = (p.Ka + kBK - 1) / kBK;
   if (threadIdx.x == 0) {
     for (int s = 0; s < p.nst; ++s) {
       mbar_init(&full[s], 1);
@@ -73,6 +103,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], kMlpEpiThreads);
     }
+    for (int b = 0; b < 4; ++b) mbar_init(&xbar[b], 64);
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -89,9 +120,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
     // ---------------------------------------------------------- producer
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&p.ta)) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&p.tb)) : "memory");
-    int it = 0;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-      const int mt = t / ntiles, nt = t % ntiles;
+    int it = 0, mt, nt;
+    for (int j = 0; tile_at(p, mtiles, ntiles, j, mt, nt); ++j) {
       bool ok = true;
       for (int kb = 0; kb < nkb; ++kb, ++it) {
         const int st = it % p.nst;
@@ -109,9 +139,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
   } else if (warp == 1 && lane == 0) {
     // --------------------------------------------------------------- MMA
     const uint32_t idesc = idesc_bf16(kBM, p.BN, false, false);
-    int it = 0, tt = 0;
+    int it = 0, tt = 0, mt, nt;
     bool ok = true;
-    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++tt) {
+    for (; ok && tile_at(p, mtiles, ntiles, tt, mt, nt); ++tt) {
       const int buf = tt & 1;
       if (!mbar_wait(&acce[buf], ((tt >> 1) & 1) ^ 1, s_abort, p.err, 32)) break;
       tc_fence_after();
@@ -140,20 +170,67 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
     const int half = (warp - 2) >> 2;  // which half of the tile's 32-column chunks
     const int r = q * 32 + lane;
     const int nch = (p.BN + 31) / 32, ch0 = half ? (nch + 1) / 2 : 0, ch1 = half ? nch : (nch + 1) / 2;
-    int tt = 0;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tt) {
-      const int mt = t / ntiles, nt = t % ntiles, buf = tt & 1;
+    int tt = 0, mt, nt;
+    // Selecting epilogue state of this thread's row and half: the 16 largest
+    // logits seen (descending; ties keep the lower index first, as columns
+    // arrive in increasing order) and the online softmax (max, sum).
+    float lv[kSelList], smx = -INFINITY, ssum = 0.f;
+    int li[kSelList];
+    int xph = 0;  // uses of this quarter's exchange barrier so far
+    for (; tile_at(p, mtiles, ntiles, tt, mt, nt); ++tt) {
+      const int buf = tt & 1;
       if (!mbar_wait(&accf[buf], (tt >> 1) & 1, s_abort, p.err, 34)) break;
       tc_fence_after();
       const long long row = (long long)mt * kBM + r;
       const bool valid = row < p.M;
       const uint32_t tb = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 256);
+      if (p.sel && nt == 0) {
+#pragma unroll
+        for (int i = 0; i < kSelList; ++i) {
+          lv[i] = -INFINITY;
+          li[i] = half * kSelList + i;  // distinct valid indices (N >= 32) if nothing beats -inf
+        }
+        smx = -INFINITY;
+        ssum = 0.f;
+      }
       for (int c0 = 32 * ch0; c0 < 32 * ch1; c0 += 32) {
         uint32_t v[32];
         tmem_ld32(tb + (uint32_t)c0, v);
         tmem_wait_ld();
         const int n0 = nt * p.BN + c0;
         if (!valid) continue;
+        if (p.sel) {
+          float cm = -INFINITY;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const float a = __uint_as_float(v[j]) + (n0 + j < p.N ? s_bias[n0 + j] : 0.f);
+            v[j] = __float_as_uint(n0 + j < p.N ? a : -INFINITY);
+            cm = fmaxf(cm, __uint_as_float(v[j]));
+          }
+          if (cm > smx) {
+            ssum = smx == -INFINITY ? 0.f : ssum * __expf(smx - cm);
+            smx = cm;
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            float cv = __uint_as_float(v[j]);
+            ssum += cv == -INFINITY ? 0.f : __expf(cv - smx);
+            if (cv > lv[kSelList - 1]) {
+              int ci = n0 + j;
+#pragma unroll
+              for (int i = 0; i < kSelList; ++i)
+                if (cv > lv[i]) {
+                  const float tv = lv[i];
+                  const int ti = li[i];
+                  lv[i] = cv;
+                  li[i] = ci;
+                  cv = tv;
+                  ci = ti;
+                }
+            }
+          }
+          continue;
+        }
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
           const int n = n0 + 8 * g;
@@ -180,6 +257,62 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_consta
       }
       tc_fence_before();
       mbar_arrive(&acce[buf]);
+      if (p.sel && nt == ntiles - 1) {
+        // Merge the two halves of each row (the warps of a lane quarter pair
+        // up through shared memory), then write the row's m candidates and
+        // their softmax mass.
+        const int slot = q * 32 + lane;
+        if (half == 1) {
+#pragma unroll
+          for (int i = 0; i < kSelList; ++i) {
+            s_xv[slot * kSelList + i] = lv[i];
+            s_xi[slot * kSelList + i] = li[i];
+          }
+          s_xm[2 * slot] = smx;
+          s_xm[2 * slot + 1] = ssum;
+        }
+        // Bounded waits: a partner that left on an abort cannot strand this warp.
+        mbar_arrive(&xbar[q]);
+        if (!mbar_wait(&xbar[q], xph & 1, s_abort, p.err, 35)) break;
+        ++xph;
+        if (half == 0 && valid) {
+          const float omx = s_xm[2 * slot], osum = s_xm[2 * slot + 1];
+          const float MX = fmaxf(smx, omx);
+          const float S = (smx == -INFINITY ? 0.f : ssum * __expf(smx - MX)) +
+                          (omx == -INFINITY ? 0.f : osum * __expf(omx - MX));
+          int a = 0, b = 0;
+          float mass = 0.f;
+          for (int i = 0; i < p.m; ++i) {
+            const float bv = b < kSelList ? s_xv[slot * kSelList + b] : -INFINITY;
+            const int bi = b < kSelList ? s_xi[slot * kSelList + b] : 0x7fffffff;
+            // First list wins ties unless the other's index is lower.
+            const bool takeA = a < kSelList && (b >= kSelList || lv[0] > bv || (lv[0] == bv && li[0] < bi));
+            float val;
+            int idx;
+            if (takeA) {
+              val = lv[0];
+              idx = li[0];
+              ++a;
+#pragma unroll
+              for (int k = 0; k < kSelList - 1; ++k) {
+                lv[k] = lv[k + 1];
+                li[k] = li[k + 1];
+              }
+              lv[kSelList - 1] = -INFINITY;
+            } else {
+              val = bv;
+              idx = bi;
+              ++b;
+            }
+            p.cand[row * p.m + i] = idx;
+            mass += __expf(val - MX);
+          }
+          p.cmass[row] = mass / S;
+        }
+        mbar_arrive(&xbar[q]);
+        if (!mbar_wait(&xbar[q], xph & 1, s_abort, p.err, 36)) break;
+        ++xph;
+      }
     }
   }
   tc_fence_before();
@@ -247,9 +380,11 @@ bool tc_dense_supported(int N, int Ka) {
 }
 
 void tc_dense(const __nv_bfloat16 *A, long long M, int Ka, const __nv_bfloat16 *W, int N, const float *bias,
-              bool relu, bool outF32, void *C, int *err, cudaStream_t s) {
+              bool relu, bool outF32, void *C, int *err, cudaStream_t s, int selM, int *cand, float *cmass) {
   if (M <= 0) return;
   VLB_CHECK(tc_dense_supported(N, Ka), VL_ERR_BAD_ARG, "dense layer: widths must be multiples of 8, N <= 4096");
+  VLB_CHECK(selM == 0 || (selM >= 1 && selM <= kSelList && N >= 32 && cand && cmass), VL_ERR_BAD_ARG,
+            "dense layer: selection of 1..16 candidates from at least 32 outputs");
   MlpParams p;
   const int BN = std::min(256, (N + 15) / 16 * 16);
   make_map(&p.ta, A, M, Ka, kBM);
@@ -262,14 +397,19 @@ void tc_dense(const __nv_bfloat16 *A, long long M, int Ka, const __nv_bfloat16 *
   p.BN = BN;
   p.relu = relu ? 1 : 0;
   p.out_f32 = outF32 ? 1 : 0;
+  p.sel = selM > 0 ? 1 : 0;
+  p.m = selM;
+  p.cand = cand;
+  p.cmass = cmass;
   p.err = err;
   const size_t stageBytes = (size_t)(kBM + BN) * kBK * 2;
-  const size_t fixed = 1024 /*alignment*/ + 256 /*barriers, TMEM base, abort flag*/ + 4 * (size_t)N /*bias*/;
+  const size_t fixed = 1024 /*alignment*/ + 256 /*barriers, TMEM base, abort flag*/ +
+                       4 * (size_t)((N + 3) & ~3) /*bias*/ + (size_t)(2 * 4 * 32 * kSelList + 256) * 4 /*exchange*/;
   p.nst = (int)std::min<size_t>(8, (kMlpSmemLimit - fixed) / stageBytes);
   VLB_CHECK(p.nst >= 2, VL_ERR_BAD_ARG, "dense layer: operand stages exceed shared memory");
   const size_t smem = fixed + (size_t)p.nst * stageBytes;
   VLB_CUDA(cudaFuncSetAttribute(k_tc_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const long long tiles = ((M + kBM - 1) / kBM) * ((N + BN - 1) / BN);
+  const long long tiles = p.sel ? (M + kBM - 1) / kBM : ((M + kBM - 1) / kBM) * ((N + BN - 1) / BN);
   int nsm = 0, dev = 0;
   VLB_CUDA(cudaGetDevice(&dev));
   VLB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));

@@ -507,12 +507,16 @@ std::vector<float *> infer_buffers(VlB200Router *r, vlb::Scratch &sc, i64 chunk)
 // features and activations, bf16 weights, fp32 accumulation; tcgen05 dense
 // layers), else the training forward on the CUDA cores.  act: the forward's
 // buffers (act[L] receives the logits).
-void forward_infer(VlB200Router *r, const float *X, i64 B, std::vector<float *> &act, vlb::Scratch &sc,
-                   cudaStream_t s) {
+// With selM > 0 (and at most 16 of at least 32 outputs) the last layer's
+// epilogue selects each row's candidates itself (cand, cmass) instead of
+// writing the logits; returns whether it did.
+bool forward_infer(VlB200Router *r, const float *X, i64 B, std::vector<float *> &act, vlb::Scratch &sc,
+                   cudaStream_t s, int selM = 0, int *cand = nullptr, float *cmass = nullptr) {
   if (!tc_infer_ok(r)) {
     forward(r, X, B, act, s);
-    return;
+    return false;
   }
+  const bool sel = selM >= 1 && selM <= 16 && r->K >= 32;
   const int L = nlayers(r);
   int *err = sc.slot[9].get<int>(1);
   VLB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
@@ -527,12 +531,14 @@ void forward_infer(VlB200Router *r, const float *X, i64 B, std::vector<float *> 
     const int out = r->sizes[l + 1];
     const bool last = l + 1 == L;
     vlb::tc_dense(buf[l & 1], B, in8(r->sizes[l]), (const __nv_bfloat16 *)r->Wb[l]->p, out,
-                  (const float *)r->b[l]->p, !last, last, last ? (void *)act[L] : (void *)buf[(l + 1) & 1], err, s);
+                  (const float *)r->b[l]->p, !last, last, last ? (void *)act[L] : (void *)buf[(l + 1) & 1], err, s,
+                  last && sel ? selM : 0, cand, cmass);
   }
   int h = 0;
   VLB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
   VLB_CUDA(cudaStreamSynchronize(s));
   if (h) throw vlb::Error(VL_ERR_BAD_ARG, "router dense layer gave up waiting (code " + std::to_string(h) + ")");
+  return sel;
 }
 
 // Activations of a batch: act[0] = features, act[l+1] = layer l output.
@@ -774,16 +780,17 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
       int *cand = sc.slot[25].get<int>((size_t)chunk * m);
       float *cm = sc.slot[26].get<float>(chunk);
       unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
-      forward_infer(r, X + i0 * D, B, act, sc, s);
-      if (K <= 256)
-        VLB_LAUNCH("router_select", s,
-                   vlb::k_select<8><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
-      else if (K <= 512)
-        VLB_LAUNCH("router_select", s,
-                   vlb::k_select<16><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
-      else
-        VLB_LAUNCH("router_select", s,
-                   vlb::k_select<32><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+      if (!forward_infer(r, X + i0 * D, B, act, sc, s, (int)m, cand, cm)) {
+        if (K <= 256)
+          VLB_LAUNCH("router_select", s,
+                     vlb::k_select<8><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+        else if (K <= 512)
+          VLB_LAUNCH("router_select", s,
+                     vlb::k_select<16><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+        else
+          VLB_LAUNCH("router_select", s,
+                     vlb::k_select<32><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, cand, cm));
+      }
       const bool tcfb = vlb::tc_supported_padded(K, D);
       VLB_LAUNCH("router_candidate_estep", s,
                  vlb::k_candidate_estep<<<vlb::gridn(B, 8), 256, 0, s>>>(
@@ -806,6 +813,36 @@ int vlb200_router_posteriors(VlB200Router *r, float *posteriors, float const *pr
 // every width allows), 0 = the training forward on the CUDA cores.
 int vlb200_router_set_tensor_core_inference(VlB200Router *r, int on) {
   return guarded([&] { r->tcInfer = on != 0; });
+}
+
+// Top-m candidates (N x m int) and their predicted softmax mass (N float) of
+// rows X, all device arrays.  fused: selected in the last dense layer's
+// epilogue when that applies, else by the selection kernel on the logits.
+int vlb200_router_candidates(VlB200Router *r, float const *X, vl_size N, vl_size m, int *cand, float *cmass,
+                             int fused, void *stream) {
+  return guarded([&] {
+    VLB_CHECK(m >= 1 && m <= 32 && (int)m <= r->K, VL_ERR_BAD_ARG, "router: m must be in [1, 32]");
+    VLB_CHECK(r->K <= 1024, VL_ERR_BAD_ARG, "router: at most 1024 components");
+    cudaStream_t s = vlb::pick_stream(stream);
+    vlb::Scratch &sc = vlb::thread_scratch(vlb::kArenaRouter);
+    const int L = nlayers(r), K = r->K;
+    const i64 chunk = infer_chunk(r);
+    for (i64 i0 = 0; i0 < (i64)N; i0 += chunk) {
+      const i64 B = std::min<i64>(chunk, (i64)N - i0);
+      std::vector<float *> act = infer_buffers(r, sc, chunk);
+      int *c = cand + i0 * m;
+      float *cm = cmass + i0;
+      if (!forward_infer(r, X + i0 * r->D, B, act, sc, s, fused ? (int)m : 0, c, cm)) {
+        if (K <= 256)
+          VLB_LAUNCH("router_select", s, vlb::k_select<8><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, c, cm));
+        else if (K <= 512)
+          VLB_LAUNCH("router_select", s, vlb::k_select<16><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, c, cm));
+        else
+          VLB_LAUNCH("router_select", s, vlb::k_select<32><<<vlb::gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)m, c, cm));
+      }
+    }
+    VLB_CUDA(cudaStreamSynchronize(s));
+  });
 }
 
 // Inference logits (N x K, fp32, device) of the rows X (N x D, device).
@@ -926,13 +963,14 @@ double router_estep(VlB200Router *r, const float *X, i64 n, const DevModel<float
     unsigned char *fell = sc.slot[27].get<unsigned char>(chunk);
     double *llrow = sc.slot[28].get<double>(chunk);
     double *llsum = sc.slot[29].get<double>(1);
-    forward_infer(r, X + i0 * D, B, act, sc, s);
-    if (K <= 256)
-      VLB_LAUNCH("router_select", s, k_select<8><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
-    else if (K <= 512)
-      VLB_LAUNCH("router_select", s, k_select<16><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
-    else
-      VLB_LAUNCH("router_select", s, k_select<32><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+    if (!forward_infer(r, X + i0 * D, B, act, sc, s, (int)mcand, cand, cm)) {
+      if (K <= 256)
+        VLB_LAUNCH("router_select", s, k_select<8><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+      else if (K <= 512)
+        VLB_LAUNCH("router_select", s, k_select<16><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+      else
+        VLB_LAUNCH("router_select", s, k_select<32><<<gridn(B, 8), 256, 0, s>>>(act[L], B, K, (int)mcand, cand, cm));
+    }
     const bool tcfb = tc_supported_padded(K, D);
     VLB_LAUNCH("router_candidate_estep", s,
                k_candidate_estep<<<gridn(B, 8), 256, 0, s>>>(X + i0 * D, B, D, K, m.means, der.inv, der.cst, cand,

@@ -43,6 +43,7 @@ def _lib():
         f("vlb200_router_set_default", C.c_int, _vp, _sz, C.c_float)
         f("vlb200_router_set_tensor_core_inference", C.c_int, _vp, C.c_int)
         f("vlb200_router_logits", C.c_int, _vp, _vp, _sz, _vp, _vp)
+        f("vlb200_router_candidates", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, C.c_int, _vp)
         _DECLARED = True
     return L
 
@@ -132,6 +133,11 @@ class Router:
     def logits(self, logits_t, x_t):
         _check(_lib().vlb200_router_logits(self._h, x_t.data_ptr(), x_t.shape[0], logits_t.data_ptr(),
                                            capi._stream(None)), "logits")
+
+    def candidates(self, cand_t, mass_t, x_t, m=8, fused=True):
+        _check(_lib().vlb200_router_candidates(self._h, x_t.data_ptr(), x_t.shape[0], m, cand_t.data_ptr(),
+                                               mass_t.data_ptr(), 1 if fused else 0, capi._stream(None)),
+               "candidates")
 
     def set_default(self, m=8, threshold=0.99):
         _check(_lib().vlb200_router_set_default(self._h, m, threshold), "set_default")
