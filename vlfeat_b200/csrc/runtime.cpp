@@ -11,6 +11,8 @@
 #include <map>
 #include <mutex>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.h"
 
 extern "C" {
@@ -280,8 +282,10 @@ int resolve_precision(int p, bool is_double) {
   return p;
 }
 
+// Each launch is also an NVTX range named after its kernel, so a timeline
+// tool shows the library's kernels by name (a no-op without one attached).
 void launch_begin(const char *name, cudaStream_t s) {
-  (void)name;
+  nvtxRangePushA(name);
   if (g_profile.load()) {
     VLB_CUDA(cudaEventCreate(&g_open_event));
     VLB_CUDA(cudaEventRecord(g_open_event, s));
@@ -293,6 +297,7 @@ void count_launches(unsigned long long n) { g_launches.fetch_add(n); }
 bool profile_swap(bool on) { return g_profile.exchange(on ? 1 : 0) != 0; }
 
 void launch_end(const char *name, cudaStream_t s) {
+  nvtxRangePop();
   g_launches.fetch_add(1);
   if (g_profile.load() && g_open_event) {
     cudaEvent_t e1;
