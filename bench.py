@@ -163,6 +163,37 @@ def train_router(capi, wl, n_train=200_000, m=16, threshold=0.99):
     return r, report
 
 
+def router_sweep(capi, wl, router, enc, nt, ref, m=16, thresholds=(0.999, 0.99999, 1.0), steps=3):
+    """The BF16+router path at fallback thresholds above the default 0.99:
+    rate (CUDA events, batched call), Fisher-vector error over all images,
+    and the fraction of rows that fall back (on 100,000 rows)."""
+    import torch
+    s = torch.cuda.current_stream()
+    xe = wl["x"][:100_000].contiguous()
+    qc = torch.zeros((xe.shape[0], K), device="cuda")
+    out = {}
+    for thr in thresholds:
+        router.set_default(m=m, threshold=thr)
+        fb = router.posteriors(qc, wl["priors"], wl["means"], wl["covs"], xe, m=m, threshold=thr)
+        encode(capi, wl, enc, nt, "bf16_router", s)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            encode(capi, wl, enc, nt, "bf16_router", s)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        err = rel_errs(enc, ref)
+        err.pop("per_image")
+        out[str(thr)] = {"value": wl["total"] / (ms * 1e-3), "ms_per_step": ms, "fallback_fraction": fb / xe.shape[0],
+                         "rel_err_max": err["max"], "rel_err_p50": err["p50"],
+                         "images_over_1e-3": err["images_over_1e-3"]}
+    router.set_default(m=m, threshold=0.99)
+    del qc
+    return out
+
+
 def encode(capi, wl, enc, nt, prec, stream):
     capi.fisher_encode_batch_device(enc, wl["means"], wl["covs"], wl["priors"], wl["x"], wl["offs"],
                                     FLAGS, prec, nt, stream)
@@ -1079,6 +1110,7 @@ def main():
             out["bf16_vs_fp32"] = results["bf16"]["value"] / results["fp32"]["value"]
         if router is not None:
             out.update(router_report)
+            out["router_threshold_sweep"] = router_sweep(capi, wl, router, enc, nt, ref)
         if not args.no_e2e:
             out["e2e"] = e2e(capi, wl, head, results[head].get("plan_config"))
         if not args.no_cpu and world == 1:
