@@ -68,14 +68,6 @@ __device__ __forceinline__ bool tile_at(const MlpParams &p, int mtiles, int ntil
 
 
 
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
 __global__ void __launch_bounds__(kMlpThreads, 1) k_tc_dense(const __grid_constant__ MlpParams p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -361,19 +353,41 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // 2-D bf16 row-major matrix (rows x cols, cols contiguous) for TMA boxes of
 // 64 columns x boxRows rows with the 128-byte swizzle.
 void make_map(CUtensorMap *m, const void *ptr, long long rows, int cols, int boxRows) {
-  VLB_CHECK(((uintptr_t)ptr & 15) == 0 && (cols * 2) % 16 == 0, VL_ERR_BAD_ARG,
-            "dense layer: operands must be 16-byte aligned rows");
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)boxRows};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides,
-                                 box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  VLB_CHECK(r == CUDA_SUCCESS, VL_ERR_BAD_ARG, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  tc::tma_map_2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, rows, cols, kBK, boxRows, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 }  // namespace
+
+namespace tc {
+void tma_map(CUtensorMap *m, CUtensorMapDataType type, int rank, const void *ptr, const unsigned long long *dims,
+             const unsigned long long *strides, const unsigned *box, CUtensorMapSwizzle swizzle) {
+  VLB_CHECK(rank >= 1 && rank <= 5 && ((uintptr_t)ptr & 15) == 0, VL_ERR_BAD_ARG,
+            "tensor map: the tensor must start 16-byte aligned");
+  cuuint64_t d[5], st[4];
+  cuuint32_t bx[5], estr[5];
+  for (int i = 0; i < rank; ++i) {
+    d[i] = (cuuint64_t)dims[i];
+    bx[i] = (cuuint32_t)box[i];
+    estr[i] = 1;
+    if (i + 1 < rank) {
+      VLB_CHECK(strides[i] % 16 == 0, VL_ERR_BAD_ARG, "tensor map: strides must be multiples of 16 bytes");
+      st[i] = (cuuint64_t)strides[i];
+    }
+  }
+  const CUresult r = encode_fn()(m, type, (cuuint32_t)rank, const_cast<void *>(ptr), d, st, bx, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  VLB_CHECK(r == CUDA_SUCCESS, VL_ERR_BAD_ARG, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
+void tma_map_2d(CUtensorMap *m, CUtensorMapDataType type, int esize, const void *ptr, long long rows, int cols,
+                int boxCols, int boxRows, CUtensorMapSwizzle swizzle) {
+  const unsigned long long dims[2] = {(unsigned long long)cols, (unsigned long long)rows};
+  const unsigned long long strides[1] = {(unsigned long long)cols * (unsigned long long)esize};
+  const unsigned box[2] = {(unsigned)boxCols, (unsigned)boxRows};
+  tma_map(m, type, 2, ptr, dims, strides, box, swizzle);
+}
+}  // namespace tc
 
 bool tc_dense_supported(int N, int Ka) {
   return N >= 8 && N % 8 == 0 && N <= kMlpMaxN && Ka >= 8 && Ka % 8 == 0;

@@ -56,7 +56,9 @@ namespace {
 using namespace tc;
 namespace cg = cooperative_groups;
 
-constexpr int kTcThreads = 416;  // E-step: 4 producer, 8 epilogue, 1 MMA warp
+// E-step block: 4 producer, 8 epilogue and 1 MMA warp; with W streamed (SW)
+// one more warp loads the descriptor rows and the W k-atoms.
+__host__ __device__ constexpr int tc_threads(bool sw) { return sw ? 448 : 416; }
 constexpr int kSmemLimit = 232448;  // 227 KB opt-in per block
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr double kLn2 = 0.6931471805599453;
@@ -259,26 +261,35 @@ constexpr float kQScale = 16384.f;
 
 // Output layouts of the posteriors written by the E-step.
 //   kQRow    fp32, row-major q[i * ldq + k] (VLFeat's layout; EM and API).
-//   kQImg16  fp16 operand image of q^T (times 2^14) for the statistics GEMM: per 8-row
-//            group g of a 128-row tile, Kq/64 MN-major 128-byte-swizzled
-//            1 KB atoms (64 components x 8 rows), so that a run of 8-row
-//            groups is exactly the MMA's A operand and moves with one bulk
-//            copy per group.
+//   kQImg16  fp16 operand image of q^T (times 2^14) for the statistics GEMM: per
+//            32-component block, the 8-row groups of all rows in order, each
+//            an MN-major 64-byte-swizzled 512-byte atom (32 components x 8
+//            rows; qimg_off).  An E-step warp's 32 rows x 32 components are
+//            one 2 KB block, written by one bulk copy from shared memory, and
+//            the statistics' A operand for 32 rows (4 groups of each of its
+//            blocks) is one 4-D TMA box of the image.
 //   kQImg32  the same image as two fp16 parts (hi, lo) for fp16x3 statistics.
 //   kQRowImg16, kQRowImg32  both: the row-major posteriors (unthresholded)
 //            and the image (thresholded), for EM with the tensor-core M-step.
 constexpr int kQRow = 0, kQImg16 = 1, kQImg32 = 2, kQRowImg16 = 3, kQRowImg32 = 4;
+// Byte offset in an image part of `ngroups` 8-row groups of the 16-byte chunk
+// with components [8 k8, 8 k8 + 8) of row r.
+__host__ __device__ __forceinline__ size_t qimg_off(i64 ngroups, i64 r, uint32_t k8) {
+  return ((size_t)(k8 >> 2) * (size_t)ngroups + (size_t)(r >> 3)) * 512u + mnmajor_sw64_off((uint32_t)(r & 7), k8 & 3u);
+}
 __host__ __device__ constexpr bool q_rows(int qf) { return qf == kQRow || qf == kQRowImg16 || qf == kQRowImg32; }
 __host__ __device__ constexpr bool q_image(int qf) { return qf != kQRow; }
 __host__ __device__ constexpr bool q_image32(int qf) { return qf == kQImg32 || qf == kQRowImg32; }
 
 struct EParams {
+  CUtensorMap xmap;  // SW: X as a {D, N} fp32 tensor, boxes of 16 dimensions x 128 rows
   const float *X;
   i64 N;
   // Kp: this CTA's components (at most 256); Kg: all padded components (the
   // W image's and cst2's extent; Kp times the cluster size); Kq: components in
   // the q image (Kg rounded up to 128).
   int K, Kp, Kg, Kq, nst;
+  int nxs;    // SW: boxes in the ring of descriptor rows
   i64 qpart;  // bytes of one part of the q image
   const uint4 *wimg;
   const float *cst2;
@@ -299,29 +310,37 @@ struct EParams {
 };
 
 // Shared-memory layout of the E-step.  With W resident (SW false) the W
-// image (hi + lo) is copied in once; with W streamed (SW true: W does not fit,
-// e.g. D=128 at K=256) each operand stage also holds the k-atom of W its
-// MMAs read, bulk-copied from global memory (L2) when the stage is filled.
+// image (hi + lo) is copied in once and the producers load the descriptor
+// rows into registers.  With W streamed (SW true) each operand stage also
+// holds the k-atom of W its MMAs read, bulk-copied from global memory (L2)
+// when the stage is filled, and the freed space holds a ring of TMA boxes of
+// descriptor rows (128 rows x 16 dimensions, fp32) that the producers read.
 template <int DIM, bool SW = false, bool CL = false>
 struct ELayout {
   static constexpr int KD2 = 2 * DIM;
   static constexpr int NKA = KD2 / 32;
   static constexpr int kStage = 2 * 8192;  // hi + lo parts of one 128 x 32 chunk
-  // Epilogue staging: each of the 8 epilogue warps transposes its 32 rows x
-  // 32 components (64 B per row) of q through 2 KB before the global stores.
-  static constexpr int kStaging = 8 * 2048;
+  // Epilogue staging: each of the 8 epilogue warps lays out its 32 rows x 32
+  // components of the q image (one 2 KB block) in shared memory for one bulk
+  // copy to global memory; two buffers per warp (one with W resident) so the
+  // next block is formed while the previous copy reads its buffer.
+  static constexpr int kStageBufs = SW ? 2 : 1;
+  static constexpr int kStaging = 8 * 2048 * kStageBufs;
   __host__ __device__ static size_t wbytes(int Kp) { return (size_t)NKA * Kp * 64; }
   __host__ __device__ static size_t wstage(int Kp) { return SW ? (size_t)2 * Kp * 64 : 0; }
   __host__ __device__ static size_t stage(int Kp) { return kStage + wstage(Kp); }
   // Cluster exchange slots: per TMEM buffer, 128 rows of (max, sum, argmax).
   static constexpr int kXch = CL ? 2 * 128 * 16 : 0;
+  static constexpr int kXBox = 128 * 16 * 4;  // one box of descriptor rows
+  static constexpr int kMaxXs = 8;            // boxes in the ring, at most
   static size_t fixed(int Kp) {
-    return (SW ? 0 : 2 * wbytes(Kp)) + 1024 /*cst*/ + 1024 /*ctr, bars*/ + kStaging + kXch + 1024 /*alignment*/;
+    return (SW ? 0 : 2 * wbytes(Kp)) + 1024 /*cst*/ + 2048 /*ctr, bars*/ + kStaging + kXch + 1024 /*alignment*/;
   }
-  static int max_stages(int Kp) {
-    return fixed(Kp) >= (size_t)kSmemLimit ? 0 : (int)((kSmemLimit - fixed(Kp)) / stage(Kp));
+  static int max_stages(int Kp, int nxs = 0) {
+    const size_t f = fixed(Kp) + (size_t)nxs * kXBox;
+    return f >= (size_t)kSmemLimit ? 0 : (int)((kSmemLimit - f) / stage(Kp));
   }
-  static size_t bytes(int Kp, int nst) { return fixed(Kp) + (size_t)nst * stage(Kp); }
+  static size_t bytes(int Kp, int nst, int nxs = 0) { return fixed(Kp) + (size_t)nst * stage(Kp) + (size_t)nxs * kXBox; }
 };
 
 // CL: the components are split over the CTAs of a thread-block cluster (K
@@ -330,9 +349,10 @@ struct ELayout {
 // running maximum and sum through distributed shared memory, so that pass B
 // normalises with the row's log-sum-exp over all K.
 template <int DIM, int QF, bool FAST, bool SW = false, bool CL = false>
-__global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
+__global__ void __launch_bounds__(tc_threads(SW), 1) k_tc_estep(const __grid_constant__ EParams p) {
   using L = ELayout<DIM, SW, CL>;
   constexpr int NKA = L::NKA;
+  constexpr int NT = tc_threads(SW);
   extern __shared__ uint8_t smem_raw[];
   uint8_t *base = align1024(smem_raw);
   const uint32_t wbytes = (uint32_t)L::wbytes(p.Kp);
@@ -340,14 +360,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   const uint32_t wpart = (uint32_t)p.Kp * 64;  // one k-atom of one W part
   uint8_t *sW = base;
   uint8_t *sA = sW + (SW ? 0 : 2 * wbytes);
-  float *s_cst = (float *)(sA + (size_t)p.nst * stageBytes);
+  uint8_t *sX = sA + (size_t)p.nst * stageBytes;  // SW: ring of nxs boxes of descriptor rows
+  float *s_cst = (float *)(sX + (SW ? (size_t)p.nxs * L::kXBox : 0));
   float *s_ctr = s_cst + 256;                     // DIM <= 128 floats
-  uint64_t *bars = (uint64_t *)(s_ctr + 128);     // 52 barriers, then TMEM base and abort flag
+  uint64_t *bars = (uint64_t *)(s_ctr + 128);     // 84 barriers, then TMEM base and abort flag
   uint64_t *full = bars, *empty = bars + 16, *accf = bars + 32, *acce = bars + 34;
   uint64_t *xready = bars + 36, *xcons = bars + 44;  // cluster exchange: [buffer][epilogue warp]
-  uint32_t *s_tmem = (uint32_t *)(bars + 52);
+  uint64_t *xfull = bars + 52, *xempty = bars + 60;  // SW: descriptor-row boxes
+  uint64_t *wfull = bars + 68;                       // SW: W k-atoms, per stage
+  uint32_t *s_tmem = (uint32_t *)(bars + 84);
   volatile int *s_abort = (volatile int *)(s_tmem + 1);
-  uint8_t *s_stage = (uint8_t *)(s_cst + 512);   // 8 x 2 KB epilogue staging
+  uint8_t *s_stage = (uint8_t *)(s_cst + 768);   // 8 x 2 KB epilogue staging
   float4 *s_xch = (float4 *)(s_stage + L::kStaging);  // [buffer][row] (max, sum, argmax) when CL
   // This CTA's components and tiles: with CL the cluster shares each tile.
   const int crank = CL ? (int)cluster_rank() : 0, ncta = CL ? (int)cluster_size() : 1;
@@ -358,9 +381,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
   const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   if (tid == 0) {
     for (int s = 0; s < p.nst; ++s) {
-      mbar_init(&full[s], SW ? 129 : 128);  // + the W copy's expect-tx arrival
+      mbar_init(&full[s], 128);
       mbar_init(&empty[s], 1);
+      if (SW) mbar_init(&wfull[s], 1);
     }
+    if (SW)
+      for (int b = 0; b < p.nxs; ++b) {
+        mbar_init(&xfull[b], 1);
+        mbar_init(&xempty[b], 128);
+      }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 128);
@@ -384,11 +413,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     uint4 *dst = (uint4 *)sW;
     const int n16 = SW ? 0 : (int)(2 * wbytes / 16);
     const int part16 = (int)(wbytes / 16), atom16 = (int)(wpart / 16);
-    for (int i = tid; i < n16; i += kTcThreads) {
+    for (int i = tid; i < n16; i += NT) {
       const int part = i / part16, rem = i % part16, c = rem / atom16, o = rem % atom16;
       dst[i] = src[(part * wbytesG + (size_t)c * p.Kg * 64 + (size_t)kbase * 64) / 16 + o];
     }
-    for (int k = tid; k < 256; k += kTcThreads) s_cst[k] = k < p.Kp ? p.cst2[kbase + k] : -INFINITY;
+    for (int k = tid; k < 256; k += NT) s_cst[k] = k < p.Kp ? p.cst2[kbase + k] : -INFINITY;
     fence_proxy_async_smem();
   }
   __syncthreads();
@@ -403,11 +432,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     // 32w + 8s + rr, s = 0..3, once and writes both the x' and the x'^2
     // elements: each load instruction reads 8 rows x 64 contiguous bytes.
     // rr permutes rg so that the 16 lanes of each half-warp store to 16
-    // distinct bank groups of the 64-byte-swizzled stage.  The next chunks'
-    // rows are prefetched into registers while the current chunk is converted.
+    // distinct bank groups of the 64-byte-swizzled stage.  With W resident
+    // the rows come from global memory, the next chunks' rows prefetched into
+    // registers while the current chunk is converted; with W streamed they
+    // come from the loader warp's ring of TMA boxes (one box per chunk: 128
+    // rows x 64 bytes, rows past N zero-filled), read 8 rows x 64 contiguous
+    // bytes per instruction.
     const int part = lane & 3, rg = lane >> 2;
     const int rr = (rg & 1) | ((rg & 2) << 1) | ((rg & 4) >> 1);
-    float4 b0[4], b1[4], b2[4];
     auto load = [&](float4(&buf)[4], i64 t, int c) {
       const int d0 = 16 * c + 4 * part;
 #pragma unroll
@@ -416,8 +448,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         buf[s] = row < p.N ? __ldg((const float4 *)(p.X + row * DIM + d0)) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     };
-    // Positions (tile, chunk) of the chunk being converted and the next two,
-    // whose rows are already in flight (a 3-deep register prefetch ring).
+    // Position (tile, chunk) of the chunk being converted and, with W
+    // resident, of the next two, whose rows are already in flight (a 3-deep
+    // register prefetch ring).
     i64 t0 = tile0, t1, t2;
     int c0 = 0, c1, c2, it = 0;
     // Log-likelihood: the common parts taken out of the logits, per row
@@ -436,23 +469,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         tn += tstep;
       }
     };
-    adv(t0, c0, t1, c1);
-    adv(t1, c1, t2, c2);
-    if (t0 < p.ntiles) load(b0, t0, c0);
-    if (t1 < p.ntiles) load(b1, t1, c1);
-    auto step = [&](float4(&cur)[4], float4(&fut)[4]) -> bool {
-      if (t0 >= p.ntiles) return false;
-      if (t2 < p.ntiles) load(fut, t2, c2);
+    // Converts chunk (t0, c0), whose rows are in cur, into operand stage it % nst.
+    auto put = [&](const float4(&cur)[4]) -> bool {
       const int stage = it % p.nst;
       if (!mbar_wait(&empty[stage], ((it / p.nst) & 1) ^ 1, s_abort, p.err, 1)) return false;
       const uint32_t a_hi = smem_u32(sA + (size_t)stage * stageBytes);
-      if (SW && warp == 0 && lane == 0) {
-        // This stage's k-atom of W: its hi and lo parts, complete on full[stage].
-        const uint8_t *w = (const uint8_t *)p.wimg + (size_t)c0 * p.Kg * 64 + (size_t)kbase * 64;
-        mbar_arrive_expect_tx(&full[stage], 2 * wpart);
-        bulk_g2s(a_hi + L::kStage, w, wpart, &full[stage]);
-        bulk_g2s(a_hi + L::kStage + wpart, w + wbytesG, wpart, &full[stage]);
-      }
       const int d0 = 16 * c0 + 4 * part;
       const float4 mm = __ldg((const float4 *)(p.ctr + d0)), sc = __ldg((const float4 *)(p.scl + d0));
       const float4 wb = want_ll ? __ldg((const float4 *)(p.wbar + d0)) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -489,13 +510,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
         }
         cacc = 0.0;
       }
-      ++it;
-      t0 = t1; c0 = c1;
-      t1 = t2; c1 = c2;
-      adv(t1, c1, t2, c2);
       return true;
     };
-    while (step(b0, b2) && step(b1, b0) && step(b2, b1)) {
+    if constexpr (SW) {
+      while (t0 < p.ntiles) {
+        const int xs = it % p.nxs;
+        if (!mbar_wait(&xfull[xs], (it / p.nxs) & 1, s_abort, p.err, 9)) break;
+        float4 cur[4];
+        const uint8_t *xb = sX + (size_t)xs * L::kXBox + (size_t)(32 * warp + rr) * 64 + part * 16;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) cur[s] = *(const float4 *)(xb + s * 8 * 64);
+        if (!put(cur)) break;
+        // The slot is released after put()'s proxy fence: these generic reads
+        // of the box must be ordered before the loader's next TMA (async
+        // proxy) write into it, which the mbarrier alone does not do.
+        mbar_arrive(&xempty[xs]);
+        ++it;
+        adv(t0, c0, t0, c0);
+      }
+    } else {
+      float4 b0[4], b1[4], b2[4];
+      adv(t0, c0, t1, c1);
+      adv(t1, c1, t2, c2);
+      if (t0 < p.ntiles) load(b0, t0, c0);
+      if (t1 < p.ntiles) load(b1, t1, c1);
+      auto step = [&](float4(&cur)[4], float4(&fut)[4]) -> bool {
+        if (t0 >= p.ntiles) return false;
+        if (t2 < p.ntiles) load(fut, t2, c2);
+        if (!put(cur)) return false;
+        ++it;
+        t0 = t1; c0 = c1;
+        t1 = t2; c1 = c2;
+        adv(t1, c1, t2, c2);
+        return true;
+      };
+      while (step(b0, b2) && step(b1, b0) && step(b2, b1)) {
+      }
     }
   } else if (warp < 12) {
     // ----------------------------------------------------- epilogue
@@ -513,7 +563,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
     const unsigned long long *cst2v = (const unsigned long long *)s_cst;
     const float wsc = *p.wsc;
     const unsigned long long wsc2 = f2u(wsc, wsc);
-    uint8_t *stg = s_stage + (warp - 4) * 2048;
+    uint8_t *stg = s_stage + (warp - 4) * 2048 * L::kStageBufs;
+    int sb = 0;  // staging buffer the next image block is formed in
     int tt = 0;
     for (i64 tile = tile0; tile < p.ntiles; tile += tstep, ++tt) {
       const int buf = tt & 1;
@@ -639,27 +690,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       constexpr float kPack = kImgOnly ? 1.f : kQScale;  // still to apply when packing the image
       // -prev(qthr) * 2^64 (times the scale), prev(qthr) the largest float below qthr (> 0).
       const float nthr = -__uint_as_float(__float_as_uint(p.qthr) - 1u) * (0x1p64f * kQs);
-      // q image of this tile; this warp's rows are its 8-row groups 4 ew .. 4 ew + 3.
-      uint8_t *ib = (uint8_t *)(q_rows(QF) ? p.qimg : p.q) + (size_t)tile * 128 * p.Kq * 2;
-      // Image stores go through this warp's staging (32 rows x 64 B, 16-byte
-      // chunks swizzled by row so that both sides are free of bank conflicts):
-      // lane = row on the way in; on the way out lane (a, b) moves chunk b of
-      // row 8i + a, so one store instruction writes 8 rows x 64 contiguous
-      // bytes of the image instead of 32 scattered 16-byte pieces.
-      auto stage_out = [&](const uint4(&w)[4], int cc, size_t part_off) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) *(uint4 *)(stg + lane * 64 + ((j ^ ((lane >> 1) & 3)) << 4)) = w[j];
+      // q image; this warp's rows are the tile's 8-row groups 4 ew .. 4 ew + 3.
+      uint8_t *ib = (uint8_t *)(q_rows(QF) ? p.qimg : p.q);
+      const size_t blockBytes = (size_t)p.ntiles * 16 * 512;  // one 32-component block of all rows
+      // Image blocks: lane = row writes its 64 bytes (four 16-byte chunks)
+      // into the staging buffer in the image's own layout (the 64-byte
+      // swizzle keeps each 8-lane group on distinct banks), then lane 0 copies
+      // the 2 KB block to the image with one bulk copy (component block
+      // kbase / 32 + cc, the tile's row groups 4 ew .. 4 ew + 3).  Before a
+      // buffer is refilled, the copy that last read it has finished reading.
+      auto stage_put = [&](int j, const uint4 &w) {
+        *(uint4 *)(stg + sb * 2048 + (lane >> 3) * 512 + mnmajor_sw64_off((uint32_t)(lane & 7), (uint32_t)j)) = w;
+      };
+      auto stage_out = [&](int cc, size_t part_off) {
+        fence_proxy_async_smem();  // this lane's staging writes, before the copy reads them
         __syncwarp();
-        const int a = lane >> 2, b = lane & 3;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const uint4 v = *(const uint4 *)(stg + (8 * i + a) * 64 + ((b ^ ((a >> 1) & 3)) << 4));
-          const int gc = kbase / 32 + cc;  // chunk of the whole image
-          const size_t off = (size_t)(4 * ew + i) * (p.Kq / 64) * 1024 + (size_t)(gc >> 1) * 1024 +
-                             mnmajor_sw128_off((uint32_t)a, (uint32_t)((gc & 1) * 4 + b));
-          *(uint4 *)(ib + part_off + off) = v;
+        if (lane == 0) {
+          bulk_s2g(ib + part_off + (size_t)(kbase / 32 + cc) * blockBytes + ((size_t)tile * 16 + 4 * ew) * 512,
+                   smem_u32(stg + sb * 2048), 2048);
+          bulk_commit();
+          bulk_wait_read<L::kStageBufs - 1>();
         }
         __syncwarp();
+        sb = sb + 1 == L::kStageBufs ? 0 : sb + 1;
       };
       // Pass B: q = e * 2^(m_g - m) / sum, thresholded, one 32-column chunk at
       // a time.  TMEM loads and staging stay warp-uniform; rows past N (tile
@@ -727,23 +780,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
 #pragma unroll
             for (int j = 0; j < 32; ++j) qv[j] *= __saturatef(fmaf(qv[j], 0x1p64f, nthr));
           }
-          uint4 wh[4], wl[4];
+          // The hi part goes to the staging as it is formed; the lo part
+          // waits in registers for the next buffer.
+          uint4 wl[4];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
+            uint4 wh;
             if (!q_image32(QF)) {
-              wh[j].x = pack2<true>(qv[8 * j + 0] * kPack, qv[8 * j + 1] * kPack);
-              wh[j].y = pack2<true>(qv[8 * j + 2] * kPack, qv[8 * j + 3] * kPack);
-              wh[j].z = pack2<true>(qv[8 * j + 4] * kPack, qv[8 * j + 5] * kPack);
-              wh[j].w = pack2<true>(qv[8 * j + 6] * kPack, qv[8 * j + 7] * kPack);
+              wh.x = pack2<true>(qv[8 * j + 0] * kPack, qv[8 * j + 1] * kPack);
+              wh.y = pack2<true>(qv[8 * j + 2] * kPack, qv[8 * j + 3] * kPack);
+              wh.z = pack2<true>(qv[8 * j + 4] * kPack, qv[8 * j + 5] * kPack);
+              wh.w = pack2<true>(qv[8 * j + 6] * kPack, qv[8 * j + 7] * kPack);
             } else {
-              split2<true>(qv[8 * j + 0] * kPack, qv[8 * j + 1] * kPack, wh[j].x, wl[j].x);
-              split2<true>(qv[8 * j + 2] * kPack, qv[8 * j + 3] * kPack, wh[j].y, wl[j].y);
-              split2<true>(qv[8 * j + 4] * kPack, qv[8 * j + 5] * kPack, wh[j].z, wl[j].z);
-              split2<true>(qv[8 * j + 6] * kPack, qv[8 * j + 7] * kPack, wh[j].w, wl[j].w);
+              split2<true>(qv[8 * j + 0] * kPack, qv[8 * j + 1] * kPack, wh.x, wl[j].x);
+              split2<true>(qv[8 * j + 2] * kPack, qv[8 * j + 3] * kPack, wh.y, wl[j].y);
+              split2<true>(qv[8 * j + 4] * kPack, qv[8 * j + 5] * kPack, wh.z, wl[j].z);
+              split2<true>(qv[8 * j + 6] * kPack, qv[8 * j + 7] * kPack, wh.w, wl[j].w);
             }
+            stage_put(j, wh);
           }
-          stage_out(wh, cc, 0);
-          if (q_image32(QF)) stage_out(wl, cc, (size_t)p.qpart);
+          stage_out(cc, 0);
+          if (q_image32(QF)) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) stage_put(j, wl[j]);
+            stage_out(cc, (size_t)p.qpart);
+          }
         }
       }
       tc_fence_before();
@@ -759,6 +820,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       for (int o = 16; o > 0; o >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, o);
       if (lane == 0 && p.ll_part && crank == 0) p.ll_part[tile * 4 + ew] = ll;
     }
+    // The image blocks' copies complete before the block exits.
+    if (q_image(QF) && lane == 0) bulk_wait_all();
   } else if (warp == 12 && lane == 0) {
     // ---------------------------------------------------------- MMA
     const uint32_t idesc = idesc_f16(128, p.Kp, false, false);
@@ -772,7 +835,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       const uint32_t d = tmem + (uint32_t)(buf * 256);
       for (int c = 0; c < NKA; ++c) {
         const int stage = it % p.nst;
-        if (!mbar_wait(&full[stage], (it / p.nst) & 1, s_abort, p.err, 4)) {
+        if (!mbar_wait(&full[stage], (it / p.nst) & 1, s_abort, p.err, 4) ||
+            (SW && !mbar_wait(&wfull[stage], (it / p.nst) & 1, s_abort, p.err, 20))) {
           ok = false;
           break;
         }
@@ -795,6 +859,44 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_estep(const EParams p) {
       }
       if (ok) mma_commit(&accf[buf]);
     }
+  } else if (SW && warp == 13 && lane == 0) {
+    // ------------------------------------------------------- loader
+    // Chunk j of this CTA (tile tile0 + (j / NKA) tstep, chunk j % NKA): its
+    // box of descriptor rows goes to ring slot j % nxs, up to nxs chunks
+    // ahead of the operand stages, and its k-atom of W (hi and lo parts) to
+    // stage j % nst once the MMAs have released the stage.
+    const i64 ntl = tile0 < p.ntiles ? (p.ntiles - tile0 + tstep - 1) / tstep : 0;
+    const i64 nchunks = ntl * NKA;
+    i64 jx = 0, jw = 0;  // boxes and W atoms issued
+    bool ok = true;
+    for (; jw < nchunks && ok; ++jw) {
+      for (; jx < nchunks && jx < jw + p.nxs; ++jx) {
+        const int xs = (int)(jx % p.nxs);
+        if (!mbar_wait(&xempty[xs], (uint32_t)((jx / p.nxs) & 1) ^ 1u, s_abort, p.err, 10)) {
+          ok = false;
+          break;
+        }
+        mbar_arrive_expect_tx(&xfull[xs], L::kXBox);
+        tma_load_2d(smem_u32(sX + (size_t)xs * L::kXBox), &p.xmap, 16 * (int)(jx % NKA),
+                    (int)((tile0 + (jx / NKA) * tstep) * 128), &xfull[xs]);
+      }
+      if (!ok) break;
+      const int stage = (int)(jw % p.nst);
+      if (!mbar_wait(&empty[stage], (uint32_t)((jw / p.nst) & 1) ^ 1u, s_abort, p.err, 17)) break;
+      const uint32_t a_hi = smem_u32(sA + (size_t)stage * stageBytes);
+      const uint8_t *w = (const uint8_t *)p.wimg + (size_t)(jw % NKA) * p.Kg * 64 + (size_t)kbase * 64;
+      mbar_arrive_expect_tx(&wfull[stage], 2 * wpart);
+      bulk_g2s(a_hi + L::kStage, w, wpart, &wfull[stage]);
+      bulk_g2s(a_hi + L::kStage + wpart, w + wbytesG, wpart, &wfull[stage]);
+    }
+    // After an abort, copies still in flight land before the block exits:
+    // wait (bounded, whatever the abort flag says) for the last box of each
+    // ring slot and the last W atom of each stage.
+    volatile int never = 0;
+    for (i64 j = jx - 1; j >= 0 && j >= jx - p.nxs; --j)
+      mbar_wait(&xfull[j % p.nxs], (uint32_t)((j / p.nxs) & 1), &never, p.err, 18);
+    for (i64 j = jw - 1; j >= 0 && j >= jw - p.nst; --j)
+      mbar_wait(&wfull[j % p.nst], (uint32_t)((j / p.nst) & 1), &never, p.err, 19);
   }
   tc_fence_before();
   __syncthreads();
@@ -814,6 +916,7 @@ struct SItem {
 };
 
 struct SParams {
+  CUtensorMap qmap;     // the image as {256 (one atom, u16), groups, 32-component blocks, parts}
   const float *X;
   const uint8_t *qimg;  // q^T operand image written by the E-step
   i64 qpart;            // bytes of one image part
@@ -838,7 +941,7 @@ struct SLayout {
   static constexpr int NCH = (NST + 255) / 256;        // MMA N chunks
   static constexpr int NPA = SPLIT == 2 ? 2 : 1;       // q^T parts
   static constexpr int NPB = 2;                        // [x'', x''^2, 1] parts
-  static constexpr int A_PART = MT * 2 * 4 * 1024;     // [kgroup 4][mnblk 2MT][1 KB]
+  static constexpr int A_PART = MT * 4 * 4 * 512;      // [mnblk 4MT][kgroup 4][512 B atom]
   static constexpr int B_PART = NB * 4 * 1024;         // [kgroup 4][nblk NB][1 KB]
   static constexpr int XST = (32 * DIM * 4 + 1023) / 1024 * 1024;  // staged x rows
   static constexpr int kStage = NPA * A_PART + NPB * B_PART + XST;
@@ -857,7 +960,7 @@ constexpr int kStatsThreads = 320;  // + one loader warp
 // operand [x'', x''^2, 1] (zero rows outside the item); one thread issues the
 // MMAs; the epilogue drains the item's accumulators to its partial.
 template <int DIM, int MT, int SPLIT>
-__global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) {
+__global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const __grid_constant__ SParams p) {
   using L = SLayout<DIM, MT, SPLIT>;
   constexpr int NST = L::NST, NB = L::NB, NPA = L::NPA;
   constexpr bool F16 = true;  // fp16 operands: the q image and x'' = x' scale
@@ -920,18 +1023,13 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) 
           }
           const uint32_t sa = smem_u32(sS + (size_t)stage * L::kStage);
           const uint32_t sx = sa + NPA * L::A_PART + L::NPB * L::B_PART;
-          const int nkg = (int)min((i64)4, (item.row1 - cb + 7) / 8);
           const int nx = (int)min((i64)32, item.row1 - cb);
-          const uint32_t gbytes = MT * 2 * 1024;
-          mbar_arrive_expect_tx(&xfull[stage], (uint32_t)(NPA * nkg) * gbytes + (uint32_t)nx * DIM * 4);
-          for (int part = 0; part < NPA; ++part) {
-            for (int kg = 0; kg < nkg; ++kg) {
-              const i64 rel = cb - p.qbase + 8 * kg;  // row of the image
-              const uint8_t *src = p.qimg + part * p.qpart + (size_t)(rel >> 7) * 128 * p.Kq * 2 +
-                                   (size_t)((rel & 127) >> 3) * (p.Kq / 64) * 1024 + (size_t)(comp0 / 64) * 1024;
-              bulk_g2s(sa + part * L::A_PART + kg * gbytes, src, gbytes, &xfull[stage]);
-            }
-          }
+          mbar_arrive_expect_tx(&xfull[stage], (uint32_t)(NPA * L::A_PART) + (uint32_t)nx * DIM * 4);
+          // q^T for the chunk: groups (cb - qbase) / 8 .. +3 of this CTA's
+          // 4 MT blocks, all parts, as one box laid out [part][block][group]
+          // (groups past the image read as zero; groups past the item are
+          // finite and meet zero x-side rows).
+          tma_load_4d(sa, &p.qmap, 0, (int)((cb - p.qbase) >> 3), comp0 / 32, 0, &xfull[stage]);
           bulk_g2s(sx, p.X + cb * DIM, (uint32_t)nx * DIM * 4, &xfull[stage]);
           ++it;
         }
@@ -1056,8 +1154,10 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) 
         for (int ks = 0; ks < 2; ++ks) {
 #pragma unroll
           for (int mt = 0; mt < MT; ++mt) {
-            const uint32_t a0 = sa + ks * 2 * (MT * 2 * 1024) + mt * 2 * 1024;
-            const uint64_t ah = sdesc(a0, 1024, MT * 2 * 1024, kSw128);
+            // q^T: MN-major 64-byte-swizzled atoms, 32-component blocks 2 KB
+            // apart (LBO), 8-row groups 512 B apart (SBO).
+            const uint32_t a0 = sa + mt * 4 * 2048 + ks * 2 * 512;
+            const uint64_t ah = sdesc(a0, 2048, 512, kSw64);
 #pragma unroll
             for (int nc = 0; nc < L::NCH; ++nc) {
               const int nn = (NST - nc * 256) < 256 ? (NST - nc * 256) : 256;
@@ -1068,7 +1168,7 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const SParams p) 
               const uint32_t d = tmem + (uint32_t)(mt * NST + nc * 256);
               mma_bf16(d, ah, bh, idesc, (chunk > 0 || ks > 0) ? 1u : 0u);
               mma_bf16(d, ah, bl, idesc, 1u);
-              if (NPA == 2) mma_bf16(d, sdesc(a0 + L::A_PART, 1024, MT * 2 * 1024, kSw128), bh, idesc, 1u);
+              if (NPA == 2) mma_bf16(d, sdesc(a0 + L::A_PART, 2048, 512, kSw64), bh, idesc, 1u);
             }
           }
         }
@@ -1303,8 +1403,6 @@ __global__ void k_rows_to_image16(const float *__restrict__ q, i64 n, int K, int
     }
     am = bi;
   }
-  uint8_t *tb = (uint8_t *)img + (size_t)(row >> 7) * 128 * Kq * 2;
-  const int r = (int)(row & 127);
   unsigned cnt = 0;
   for (int g = lane; g < Kq / 8; g += 32) {
     float v[8];
@@ -1321,9 +1419,7 @@ __global__ void k_rows_to_image16(const float *__restrict__ q, i64 n, int K, int
     w.y = pack2<true>(v[2] * kQScale, v[3] * kQScale);
     w.z = pack2<true>(v[4] * kQScale, v[5] * kQScale);
     w.w = pack2<true>(v[6] * kQScale, v[7] * kQScale);
-    const int kk = g * 8;
-    const uint32_t off = (uint32_t)((r >> 3) * (Kq / 64) * 1024 + (kk >> 6) * 1024) + mnmajor_sw128_off(r & 7, (kk & 63) >> 3);
-    *(uint4 *)(tb + off) = w;
+    *(uint4 *)((uint8_t *)img + qimg_off(rowsPad / 8, row, (uint32_t)g)) = w;
   }
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane == 0 && valid && rowcnt) rowcnt[row] = cnt;
@@ -1433,9 +1529,18 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   const i64 ntiles = (N + 127) / 128;
   if (ntiles == 0) return 0;
   const int nb = CL ? kblocks(tp.Kp) : 1, Kb = tp.Kp / nb;
-  const int nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(Kb));
-  VLB_CHECK(nst >= 2, VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
-  const size_t smem = L::bytes(Kb, nst);
+  VLB_CHECK(((uintptr_t)X & 15) == 0, VL_ERR_BAD_ARG, "tensor-core E-step: the data must start 16-byte aligned");
+  // W streamed: 3 operand stages unless requested, beside a ring of up to 8
+  // (at least 2) boxes of descriptor rows.  W resident: up to 8 stages.
+  int nst, nxs = 0;
+  if constexpr (SW) {
+    nst = std::min(nst_req > 0 ? nst_req : 3, L::max_stages(Kb, 2));
+    if (nst >= 2) nxs = std::min<int>(L::kMaxXs, (int)((kSmemLimit - L::bytes(Kb, nst)) / L::kXBox));
+  } else {
+    nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(Kb));
+  }
+  VLB_CHECK(nst >= 2 && (!SW || nxs >= 2), VL_ERR_BAD_ARG, "tensor-core E-step: operands exceed shared memory");
+  const size_t smem = L::bytes(Kb, nst, nxs);
   auto kern = k_tc_estep<DIM, QF, false, SW, CL>;
   if constexpr (!q_rows(QF) || QF == kQRow) {
     if (fast) kern = k_tc_estep<DIM, QF, true, SW, CL>;
@@ -1444,7 +1549,15 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   }
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   EParams p;
-  p.X = X; p.N = N; p.K = tp.K; p.Kp = Kb; p.Kg = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst;
+  p.X = X; p.N = N; p.K = tp.K; p.Kp = Kb; p.Kg = tp.Kp; p.Kq = padQ(tp.Kp); p.nst = nst; p.nxs = nxs;
+  if constexpr (SW) {
+    // Boxes of 16 dimensions (64 bytes, 16-byte aligned) x 128 rows; the row
+    // coordinate is a 32-bit TMA coordinate.
+    VLB_CHECK(ntiles * 128 <= (i64)INT32_MAX, VL_ERR_BAD_ARG, "tensor-core E-step: at most 2^31 - 128 rows per launch");
+    tc::tma_map_2d(&p.xmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, X, N, DIM, 16, 128, CU_TENSOR_MAP_SWIZZLE_NONE);
+  } else {
+    std::memset(&p.xmap, 0, sizeof p.xmap);
+  }
   p.qpart = ntiles * 128 * (i64)p.Kq * 2;
   p.wimg = (const uint4 *)tp.wimg; p.cst2 = tp.cst2; p.ctr = tp.ctr; p.scl = tp.scale; p.wsc = tp.wsc;
   p.wbar = tp.wbar; p.cbar = tp.cbar;
@@ -1453,7 +1566,7 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   p.err = err; p.ntiles = ntiles;
   if constexpr (!CL) {
     const int grid = (int)std::min<i64>(ntiles, num_sms());
-    VLB_LAUNCH("tc_estep_f16x3", s, kern<<<grid, kTcThreads, smem, s>>>(p));
+    VLB_LAUNCH("tc_estep_f16x3", s, kern<<<grid, tc_threads(SW), smem, s>>>(p));
   } else {
     // One cluster of nb CTAs per tile, as many clusters as fit at once
     // (persistent: each cluster strides over the tiles).
@@ -1464,7 +1577,7 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
     attr[0].val.clusterDim.x = (unsigned)nb;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(kTcThreads);
+    cfg.blockDim = dim3(tc_threads(SW));
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cfg.attrs = attr;
@@ -1479,9 +1592,10 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   return ll_part ? ntiles * 8 : ntiles * 4;  // LL partials written: epilogue's, then the common parts
 }
 
-// W resident in shared memory when two operand stages fit beside it, else
-// streamed through the stages (D=128 at 256 components per CTA).  Above 256
-// components the E-step runs as clusters of CTAs.
+// Up to 256 components W is streamed through the operand stages (it costs
+// L2 reads only) and the freed shared memory stages the descriptor rows by
+// TMA.  Above 256 components the E-step runs as clusters of CTAs, with W
+// resident when two operand stages fit beside it (else streamed).
 template <int DIM, int QF>
 i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool fast,
                  unsigned *rowcnt, double *ll_part, int *err, int nst_req, cudaStream_t s,
@@ -1494,11 +1608,7 @@ i64 launch_estep(const float *X, i64 N, const TcPrep &tp, void *q, int ldq, bool
     }
     return launch_estep_impl<DIM, QF, false, true>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
   }
-  if constexpr (DIM == 128) {
-    if (ELayout<DIM, false>::max_stages(tp.Kp) < 2)
-      return launch_estep_impl<DIM, QF, true, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
-  }
-  return launch_estep_impl<DIM, QF, false, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
+  return launch_estep_impl<DIM, QF, true, false>(X, N, tp, q, ldq, fast, rowcnt, ll_part, err, nst_req, s, eo);
 }
 
 template <int DIM, int MT, int SPLIT>
@@ -1510,6 +1620,17 @@ void launch_stats(const SParams &p0, int grid_x, int grid_y, int nst_req, cudaSt
   const size_t smem = L::bytes(p.nst);
   auto kern = k_tc_stats<DIM, MT, SPLIT>;
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  {
+    // The image (parts of ngroups 8-row groups per 32-component block) for
+    // boxes of 4 groups x this CTA's 4 MT blocks x all parts.
+    const i64 ngroups = p.qpart / ((i64)p.Kq * 16);
+    VLB_CHECK(ngroups <= (i64)INT32_MAX, VL_ERR_BAD_ARG, "tensor-core statistics: image too large for one launch");
+    const unsigned long long dims[4] = {256, (unsigned long long)ngroups, (unsigned long long)(p.Kq / 32),
+                                        (unsigned long long)L::NPA};
+    const unsigned long long strides[3] = {512, (unsigned long long)ngroups * 512, (unsigned long long)p.qpart};
+    const unsigned box[4] = {256, 4, 4 * MT, L::NPA};
+    tc::tma_map(&p.qmap, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, p.qimg, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_NONE);
+  }
   VLB_LAUNCH(SPLIT == 2 ? "tc_stats_f16x3" : "tc_stats_f16x2", s,
              kern<<<dim3(grid_x, grid_y), kStatsThreads, smem, s>>>(p));
 }
@@ -1627,16 +1748,17 @@ void wait_selftest(double limit_ms, cudaStream_t s) {
 bool tc_supported(i64 K, i64 D) {
   if (!(D == 64 || D == 80 || D == 128)) return false;
   if (K < 8 || K > 2048 || K % 8) return false;
-  // Per CTA: W resident beside two operand stages, or (D=128) streamed through
-  // them; TMEM holds two accumulators of the CTA's components.  Above 256
-  // components, clusters of up to 8 CTAs.
+  // Per CTA: W streamed through two operand stages beside a ring of two boxes
+  // of descriptor rows (up to 256 components), or, in clusters of up to 8
+  // CTAs above 256, resident beside two stages (D=128: streamed); TMEM holds
+  // two accumulators of the CTA's components.
   const int Kp = padK(K), nb = kblocks(Kp), Kb = Kp / nb;
   if (nb > 8) return false;
   if (nb == 1) {
-    if (D == 128) return ELayout<128, true>::max_stages(Kb) >= 2;
-    return D == 64 ? ELayout<64, false>::max_stages(Kb) >= 2 : ELayout<80, false>::max_stages(Kb) >= 2;
+    if (D == 128) return ELayout<128, true>::max_stages(Kb, 2) >= 2;
+    return D == 64 ? ELayout<64, true>::max_stages(Kb, 2) >= 2 : ELayout<80, true>::max_stages(Kb, 2) >= 2;
   }
-  if (D == 128) return ELayout<128, true, true>::max_stages(Kb) >= 2;
+  if (D == 128) return ELayout<128, true, true>::max_stages(Kb, 2) >= 2;
   return D == 64 ? ELayout<64, false, true>::max_stages(Kb) >= 2 : ELayout<80, false, true>::max_stages(Kb) >= 2;
 }
 

@@ -8,6 +8,7 @@
 // context usable.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cstdint>
@@ -246,6 +247,13 @@ __host__ __device__ __forceinline__ uint32_t mnmajor_sw128_off(uint32_t kr, uint
   return kr * 128u + ((c ^ kr) & 7u) * 16u;
 }
 
+// Byte offset of the 16-byte chunk holding MN-elements [8c, 8c+8) (c in
+// 0..3 within a 32-element block) of K-row kr (0..7) in an MN-major atom with
+// the 64-byte swizzle (K-rows 64 B apart; atom 512-byte aligned).
+__host__ __device__ __forceinline__ uint32_t mnmajor_sw64_off(uint32_t kr, uint32_t c) {
+  return kr * 64u + ((c ^ (kr >> 1)) & 3u) * 16u;
+}
+
 // bf16 hi/lo split: x ~= hi + lo with hi = bf16(x), lo = bf16(x - hi).
 __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
   hi = __float2bfloat16_rn(x);
@@ -314,6 +322,54 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst_smem, const void *src, uin
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+
+// Non-tensor bulk copy shared (this CTA) -> global in the thread's bulk
+// async-group; both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_s2g(void *dst, uint32_t src_smem, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src_smem), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until at most N of the thread's bulk groups still read their source.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// Waits until all of the thread's bulk groups are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Tiled 2-D tensor copy global -> shared (this CTA) of the box at (x, y)
+// (x the inner coordinate, in elements), completing on `bar`; rows and
+// columns outside the tensor read as zero.  x times the element size must be
+// a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// 4-D variant: box at (x, y, z, w), x the innermost coordinate.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int x, int y, int z, int w,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Host: a tensor map of `rank` dimensions (dims[0] innermost, contiguous;
+// strides[i] the byte stride of dimension i + 1) for boxes of box[] elements,
+// no swizzle unless given, zero fill outside; `ptr` and the strides 16-byte
+// aligned (checked).
+void tma_map(CUtensorMap *m, CUtensorMapDataType type, int rank, const void *ptr, const unsigned long long *dims,
+             const unsigned long long *strides, const unsigned *box, CUtensorMapSwizzle swizzle);
+// A 2-D row-major matrix (rows x cols elements of `esize` bytes, rows
+// contiguous) for boxes of boxCols x boxRows.
+void tma_map_2d(CUtensorMap *m, CUtensorMapDataType type, int esize, const void *ptr, long long rows, int cols,
+                int boxCols, int boxRows, CUtensorMapSwizzle swizzle);
 
 __device__ __forceinline__ void st_shared_v2(uint32_t addr, uint32_t a, uint32_t b) {
   asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(a), "r"(b) : "memory");
