@@ -477,20 +477,32 @@ __global__ void __launch_bounds__(tc_threads(SW), 1) k_tc_estep(const __grid_con
       const int d0 = 16 * c0 + 4 * part;
       const float4 mm = __ldg((const float4 *)(p.ctr + d0)), sc = __ldg((const float4 *)(p.scl + d0));
       const float4 wb = want_ll ? __ldg((const float4 *)(p.wbar + d0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const unsigned long long m01 = f2u(mm.x, mm.y), m23 = f2u(mm.z, mm.w);
+      const unsigned long long s01 = f2u(sc.x, sc.y), s23 = f2u(sc.z, sc.w);
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
-        // x'' = (x - ctr) scale, kept inside fp16's range (an x'' beyond it
-        // is more than 255 model scales from the centre).
-        const float v0 = clamp_f16((cur[s].x - mm.x) * sc.x), v1 = clamp_f16((cur[s].y - mm.y) * sc.y);
-        const float v2 = clamp_f16((cur[s].z - mm.z) * sc.z), v3 = clamp_f16((cur[s].w - mm.w) * sc.w);
+        // x'' = (x - ctr) scale (packed pairs, the scalar roundings), clamped
+        // to fp16's finite range (an x'' beyond it is more than 255 model
+        // scales from the centre); NaN passes.
+        const unsigned long long d01 = mul2(sub2(f2u(cur[s].x, cur[s].y), m01), s01);
+        const unsigned long long d23 = mul2(sub2(f2u(cur[s].z, cur[s].w), m23), s23);
+        const float v0 = clamp_f16n(lo32(d01)), v1 = clamp_f16n(hi32(d01));
+        const float v2 = clamp_f16n(lo32(d23)), v3 = clamp_f16n(hi32(d23));
         if (want_ll && t0 * 128 + 32 * warp + 8 * s + rr < p.N)
           cacc += (double)wb.x * ((double)v0 * v0) + (double)wb.y * ((double)v1 * v1) +
                   (double)wb.z * ((double)v2 * v2) + (double)wb.w * ((double)v3 * v3);
+        // x''^2, at most fp16's max; plus d * 0, which is +-0 for a finite
+        // difference and NaN for an infinite one, so that a non-finite x
+        // still makes the row's logits NaN (as the reference's arithmetic
+        // makes its posteriors).
+        const unsigned long long p01 = mul2(f2u(v0, v1), f2u(v0, v1)), p23 = mul2(f2u(v2, v3), f2u(v2, v3));
+        const unsigned long long q01 = add2(f2u(fminf(lo32(p01), 65504.f), fminf(hi32(p01), 65504.f)), mul2(d01, 0ull));
+        const unsigned long long q23 = add2(f2u(fminf(lo32(p23), 65504.f), fminf(hi32(p23), 65504.f)), mul2(d23, 0ull));
         uint32_t h0, l0, h1, l1, h2, l2, h3, l3;
         split2<true>(v0, v1, h0, l0);
         split2<true>(v2, v3, h1, l1);
-        split2<true>(clamp_f16(v0 * v0), clamp_f16(v1 * v1), h2, l2);
-        split2<true>(clamp_f16(v2 * v2), clamp_f16(v3 * v3), h3, l3);
+        split2<true>(lo32(q01), hi32(q01), h2, l2);
+        split2<true>(lo32(q23), hi32(q23), h3, l3);
         const uint32_t row = (uint32_t)(32 * warp + 8 * s + rr);
         const uint32_t o1 = kmajor_sw64_off(row, (uint32_t)(part >> 1)) + (part & 1) * 8;
         const uint32_t o2 = kmajor_sw64_off(row, (uint32_t)(2 + (part >> 1))) + (part & 1) * 8;

@@ -279,7 +279,13 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
   if (F16) {
     const __half2 h = __floats2half2_rn(a, b);
     const float2 hf = __half22float2(h);
-    const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+    // (a - hi_a, b - hi_b) in one packed subtraction (the same roundings).
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(r)
+        : "l"((unsigned long long)__float_as_uint(a) | ((unsigned long long)__float_as_uint(b) << 32)),
+          "l"((unsigned long long)__float_as_uint(hf.x) | ((unsigned long long)__float_as_uint(hf.y) << 32)));
+    const __half2 l = __floats2half2_rn(__uint_as_float((uint32_t)r), __uint_as_float((uint32_t)(r >> 32)));
     hi = *(const uint32_t *)&h;
     lo = *(const uint32_t *)&l;
   } else {
@@ -397,6 +403,19 @@ __device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigne
                                                    unsigned long long c) {
   unsigned long long r;
   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+// v clamped to fp16's finite range [-65504, 65504]; NaN stays NaN.
+__device__ __forceinline__ float clamp_f16n(float v) {
+  float r;
+  asm("{\n\t.reg .f32 t;\n\tmax.NaN.f32 t, %1, 0fC77FE000;\n\tmin.NaN.f32 %0, t, 0f477FE000;\n\t}"
+      : "=f"(r)
+      : "f"(v));
   return r;
 }
 __device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
