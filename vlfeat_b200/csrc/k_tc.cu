@@ -963,7 +963,10 @@ struct SLayout {
   static_assert(MT * NST <= 512, "accumulators exceed TMEM");
 };
 
-constexpr int kStatsThreads = 320;  // + one loader warp
+// Statistics block: converter warps 0-3 and 10-13, epilogue warps 4-7, MMA
+// warp 8, loader warp 9.
+constexpr int kStatsThreads = 448;
+constexpr int kStatsConv = 256;  // converter threads
 
 // Statistics over work items (runs of rows of one image): for each 32-row
 // chunk, the loader warp bulk-copies the chunk's q^T operand (four 8-row
@@ -991,7 +994,7 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const __grid_cons
   const int comp0 = blockIdx.y * MT * 128;  // first component of this CTA's M tiles
   if (tid == 0) {
     for (int s = 0; s < p.nst; ++s) {
-      mbar_init(&full[s], 128);
+      mbar_init(&full[s], kStatsConv);
       mbar_init(&empty[s], 1);
       mbar_init(&xfull[s], 1);
     }
@@ -1047,8 +1050,9 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const __grid_cons
         }
       }
     }
-  } else if (warp < 4) {
+  } else if (warp < 4 || warp >= 10) {
     // ---------------------------------------------------- converters
+    const int ctid = (warp < 4 ? warp : warp - 6) * 32 + lane;
     int it = 0;
     bool ok = true;
     for (int ii = ib; ii < ie && ok; ++ii) {
@@ -1063,8 +1067,8 @@ __global__ void __launch_bounds__(kStatsThreads, 1) k_tc_stats(const __grid_cons
         const uint32_t sb = sa + NPA * L::A_PART;
         const float *xs = (const float *)(sS + (size_t)stage * L::kStage + NPA * L::A_PART + L::NPB * L::B_PART);
 #pragma unroll
-        for (int j = 0; j < (32 * NF4 + 127) / 128; ++j) {
-          const int i = tid + 128 * j;
+        for (int j = 0; j < (32 * NF4 + kStatsConv - 1) / kStatsConv; ++j) {
+          const int i = ctid + kStatsConv * j;
           if (i >= 32 * NF4) break;
           const int rs = i / NF4, pp = i % NF4;
           const i64 row = cb + rs;
