@@ -130,6 +130,62 @@ def test_posteriors_fp32(vl, restatement, D):
     assert abs(ll - ll64) < ll_tol * abs(ll64)
 
 
+@pytest.mark.parametrize("mode", ["fp32", "bf16"])
+def test_batched_many_tiles_per_block(vl, mode):
+    """64 images of the benchmark's count distribution (about 300,000 rows, a
+    dozen row tiles per block in one launch): every block refills its ring
+    of descriptor-row boxes and its q-image staging many times, and the
+    statistics read q^T boxes across tile and image boundaries.  Each image
+    against the exact CUDA-core path (the FP32 path within 1e-4, the BF16 path
+    within 2e-3 of it, term counts within 1e-3 of its) and two runs
+    bit-identical."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    K, D = 256, 80
+    pr, mu, cv = W.fv_gmm(K, D, seed=11)
+    counts = W.config2_counts(4096)[:64]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    x = _t(W.pca_like(int(offs[-1]), D, seed=16))
+    out = {}
+    for name, m in (("exact", "exact"), ("a", mode), ("b", mode)):
+        enc = torch.zeros((len(counts), 2 * K * D), device="cuda")
+        nt = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+        vl.fisher_encode_batch_device(enc, _t(mu), _t(cv), _t(pr), x, offs, FLAG_IMPROVED, m, nt)
+        torch.cuda.synchronize()
+        out[name] = (enc.cpu().numpy(), nt.cpu().numpy())
+    assert np.array_equal(out["a"][0], out["b"][0]) and np.array_equal(out["a"][1], out["b"][1])
+    tol = 1e-4 if mode == "fp32" else 2e-3
+    for j in range(len(counts)):
+        assert rel_err(out["a"][0][j], out["exact"][0][j]) < tol, j
+        n = int(out["exact"][1][j])
+        assert abs(int(out["a"][1][j]) - n) <= max(2, 1e-3 * n), j
+
+
+@pytest.mark.parametrize("KD", [(256, 64), (256, 80), (256, 128), (200, 80), (64, 128)])
+def test_posteriors_many_tiles_per_block(vl, KD):
+    """120,000 rows (938 row tiles, six or seven per block): every block
+    reuses its ring of descriptor-row boxes and its operand stages many
+    times.  Tensor-core posteriors against the exact CUDA-core path on every
+    row, and two runs bit-identical (a box refilled before all its readers
+    were done showed up as wrong, run-dependent rows from each block's second
+    tile on)."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    K, D = KD
+    N = 120_000
+    x = W.sift_like(N, D, seed=200) if D == 128 else W.pca_like(N, D, seed=15)
+    pr, mu, cv = W.custom_init(x, K, seed=201)
+    X, P, M, C = _t(x), _t(pr), _t(mu), _t(cv)
+    q = {}
+    for name, mode in (("exact", "exact"), ("a", "fp32"), ("b", "fp32")):
+        out = torch.zeros((N, K), device="cuda")
+        vl.gmm_posteriors_device(out, P, M, C, X, mode)
+        torch.cuda.synchronize()
+        q[name] = out.cpu().numpy()
+    assert np.array_equal(q["a"], q["b"])
+    assert np.max(np.abs(q["a"] - q["exact"])) < 1e-4
+
+
 # EM in the tensor-core modes: E-step and M-step statistics on tcgen05
 # (the M-step from the E-step's posterior image, thresholded at 1e-2/K).
 # Bounds on the relative L2 error of every parameter against the FP64
