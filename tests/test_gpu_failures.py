@@ -171,3 +171,37 @@ def test_em_on_nan_data_gives_nan_loglikelihood(vl, vlfeat_float, mode):
     if vlfeat_float is not None:
         r = vlfeat_float.em(data, c["priors"], c["means"], c["covs"], c["lower_bound"], 3)
         assert np.isnan(r["ll"])
+
+
+def test_misaligned_device_buffers_are_rejected(vl):
+    """The tensor-core paths read the data with TMA and bulk copies and store
+    row-major posteriors 16 bytes at a time, so device data or posterior
+    buffers that do not start 16-byte aligned are refused on the host with
+    VL_ERR_BAD_ARG before any launch (never a misaligned access on the GPU);
+    the same call on aligned buffers then succeeds, and the exact path, which
+    reads and writes element-wise, takes the misaligned buffers."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    K, D, N = 64, 80, 3000
+    pr, mu, cv = W.fv_gmm(K, D, seed=21)
+    x = W.pca_like(N, D, seed=22)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    P, M, Cv = t(pr), t(mu), t(cv)
+    xbuf = torch.zeros(N * D + 4, device="cuda")
+    xbuf[1:1 + N * D] = t(x).reshape(-1)
+    xm = xbuf[1:1 + N * D].view(N, D)  # starts 4 bytes past a 16-byte boundary
+    qbuf = torch.zeros(N * K + 4, device="cuda")
+    qm = qbuf[1:1 + N * K].view(N, K)
+    q = torch.zeros((N, K), device="cuda")
+    with pytest.raises(vl.VLError, match="16-byte aligned"):
+        vl.gmm_posteriors_device(q, P, M, Cv, xm, "fp32")
+    with pytest.raises(vl.VLError, match="16-byte aligned"):
+        vl.gmm_posteriors_device(qm, P, M, Cv, t(x), "fp32")
+    ll = vl.gmm_posteriors_device(q, P, M, Cv, t(x), "fp32")
+    ref = torch.zeros((N, K), device="cuda")
+    ll_exact = vl.gmm_posteriors_device(ref, P, M, Cv, xm, "exact")
+    vl.gmm_posteriors_device(qm, P, M, Cv, xm, "exact")
+    torch.cuda.synchronize()
+    assert np.array_equal(qm.cpu().numpy(), ref.cpu().numpy())
+    assert np.max(np.abs(q.cpu().numpy() - ref.cpu().numpy())) < 1e-4
+    assert abs(ll - ll_exact) <= 1e-5 * abs(ll_exact)

@@ -1546,6 +1546,9 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   if (ntiles == 0) return 0;
   const int nb = CL ? kblocks(tp.Kp) : 1, Kb = tp.Kp / nb;
   VLB_CHECK(((uintptr_t)X & 15) == 0, VL_ERR_BAD_ARG, "tensor-core E-step: the data must start 16-byte aligned");
+  // Row-major posteriors are stored 16 bytes at a time.
+  VLB_CHECK(!q_rows(QF) || (((uintptr_t)q & 15) == 0 && ldq % 4 == 0), VL_ERR_BAD_ARG,
+            "tensor-core E-step: the posteriors must start 16-byte aligned");
   // W streamed: 3 operand stages unless requested, beside a ring of up to 8
   // (at least 2) boxes of descriptor rows.  W resident: up to 8 stages.
   int nst, nxs = 0;
