@@ -70,7 +70,10 @@ VL_EXPORT void vlb200_profile_reset(void);
 
 /* E-step on device data (vl_get_gmm_data_posteriors_f, vl/gmm.h:94-103, with
  * device pointers).  posteriors: numData x numClusters, device.  *ll receives
- * the log-likelihood (host pointer). */
+ * the log-likelihood (host pointer).  The tensor-core modes read the data with
+ * TMA and store the posteriors 16 bytes at a time: both device arrays must
+ * start 16-byte aligned there (else VL_ERR_BAD_ARG, nothing launched); the
+ * exact mode takes any float alignment. */
 VL_EXPORT int vlb200_gmm_posteriors_device(float *posteriors, vl_size numClusters,
                                            vl_size numData, float const *priors,
                                            float const *means, vl_size dimension,
