@@ -109,6 +109,26 @@ VL_EXPORT double vlb200_gmm_em_stream_device(VlGMM *self, float const *data, vl_
                                              int precision, vl_size chunkRows,
                                              struct _VlB200Router *router, vl_size m,
                                              float threshold, vl_size judgeEvery);
+/* Sums `count` doubles in place over all ranks of a sharded EM.  Every rank
+ * calls it with the same counts in the same order (the rank's C-ABI call
+ * below makes the calls); it returns when the sums are complete. */
+typedef void (*vlb200_allreduce_fn)(double *values, vl_size count, void *context);
+
+/* EM with the rows sharded over ranks (one process and device each): this
+ * rank holds numData rows of data (device, VL_TYPE_FLOAT or VL_TYPE_DOUBLE as
+ * the model, at least one row) of totalData in all.  Every rank sets the same
+ * initial parameters and options.  The loop is the streamed EM's
+ * (vlb200_gmm_em_stream_device, no router) on the rank's rows; each sum over
+ * rows is completed by `allreduce` before it is used: per iteration the
+ * log-likelihood and (from iteration 2) the component masses of the restart
+ * check (vl/gmm.c:814-999, with totalData in its cut-off), and the M-step
+ * sums ((2 D + 1) numClusters doubles, vl/gmm.c:1036-1213), once more per
+ * restart.  All ranks end with the same parameters and log-likelihood
+ * (returned; NaN on error).  vl_gmm_get_posteriors gives this rank's rows. */
+VL_EXPORT double vlb200_gmm_em_sharded_device(VlGMM *self, void const *data, vl_size numData,
+                                              vl_size totalData, int precision, vl_size chunkRows,
+                                              vlb200_allreduce_fn allreduce, void *context);
+
 /* One row of 6 doubles per E-step of the last streamed EM: log-likelihood,
  * judged (1: full E-step with the router judged), routed (1: router E-step),
  * mean missed posterior mass of the router on the judged rows (NaN when not

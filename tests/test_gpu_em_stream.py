@@ -136,3 +136,71 @@ def test_streamed_restarts_in_fp32_mode_match_resident(vl):
     # restarts' discontinuous choices carry that on (measured 1.1e-5 priors).
     for got, want in ((b.means, a.means), (b.covariances, a.covariances), (b.priors, a.priors)):
         assert rel_err(got, want) < 5e-5
+
+
+def _sharded(vl, c, T, x_t, world, mode, dt):
+    """EM with the rows of x_t sharded over `world` ranks, run as threads of
+    this process on one GPU (each with its own model object and the library's
+    per-thread stream); the all-reduce sums through host barriers (bounded),
+    so no kernel ever waits for another."""
+    import threading
+    from vlfeat_b200 import replicas
+    N = x_t.shape[0]
+    bar = threading.Barrier(world, timeout=60)
+    slots = [None] * world
+    res, errs = [None] * world, []
+
+    def make_reduce(r):
+        def reduce(values):
+            slots[r] = values.copy()
+            bar.wait()
+            total = np.sum(np.stack(slots), axis=0)  # every rank adds in rank order
+            bar.wait()
+            values[...] = total
+        return reduce
+
+    def run(r):
+        try:
+            r0, r1 = replicas.row_shard(N, r, world)
+            m = _model(vl, c, T, dt)
+            ll = m.em_sharded_device(x_t[r0:r1], N, make_reduce(r), mode)
+            res[r] = (ll, m.means, m.covariances, m.priors, m.num_restarts)
+        except BaseException as e:  # noqa: BLE001
+            errs.append(e)
+            bar.abort()
+
+    th = [threading.Thread(target=run, args=(r,)) for r in range(world)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=600)
+    assert not errs, errs
+    return res
+
+
+@pytest.mark.parametrize("mode,dt,tol", [("exact", np.float64, 1e-10), ("exact", np.float32, 2e-5),
+                                         ("fp32", np.float32, 5e-5)])
+def test_sharded_em_matches_one_process(vl, mode, dt, tol):
+    """Config-0 data (restarts fire at iteration 2) sharded over two ranks:
+    every rank ends with the same parameters and log-likelihood, equal to the
+    single-process streamed EM's within the precision's summation-order
+    tolerance (the ranks' partial sums are added across ranks), with the same
+    number of restarts."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    c = W.config0(scale=0.3)
+    x = torch.from_numpy(c["data"].astype(dt)).cuda()
+    one = _model(vl, c, 5, dt)
+    if dt == np.float32:
+        ll1 = one.em_stream_device(x, mode)
+    else:  # the double model's loop through vl_gmm_cluster (custom initialisation: no init)
+        vl.set_precision(mode)
+        ll1 = one.cluster(c["data"].astype(dt))
+    res = _sharded(vl, c, 5, x, 2, mode, dt)
+    (lla, mua, cva, pra, ra), (llb, mub, cvb, prb, rb) = res
+    assert lla == llb and ra == rb
+    assert np.array_equal(mua, mub) and np.array_equal(cva, cvb) and np.array_equal(pra, prb)
+    assert ra == one.num_restarts and ra > 0
+    assert abs(lla - ll1) <= tol * abs(ll1)
+    for got, want in ((mua, one.means), (cva, one.covariances), (pra, one.priors)):
+        assert rel_err(got, want) < tol

@@ -116,3 +116,47 @@ def test_image_shard_blocks():
     blocks = [replicas.image_shard(offs, r, 3) for r in range(3)]
     assert [(b[0], b[1]) for b in blocks] == [(0, 1), (1, 2), (2, 4)]
     assert list(blocks[2][2]) == [0, 7, 8]
+
+
+def _allreduce_worker(rank, world, port, out):
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from vlfeat_b200 import replicas
+        reduce = replicas.allreduce_sum(dist)
+        r0, r1 = replicas.row_shard(1001, rank, world)
+        # The sums sharded EM completes: a log-likelihood, then (2D+1)K M-step sums.
+        vals = np.arange(r0, r1, dtype=np.float64)
+        ll = np.array([vals.sum()])
+        reduce(ll)
+        stats = np.full(7, float(rank + 1))
+        reduce(stats)
+        out.put((rank, r0, r1, float(ll[0]), stats.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_em_sums_over_two_ranks():
+    """The host side of sharded EM on two gloo ranks: row_shard cuts the rows
+    into contiguous blocks covering all of them, and allreduce_sum (the
+    library's all-reduce callback) sums a float64 array in place on every
+    rank."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_allreduce_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, a0, a1, ll0, s0), (_, b0, b1, ll1, s1) = res
+    assert (a0, a1, b0, b1) == (0, 500, 500, 1001)
+    assert ll0 == ll1 == float(sum(range(1001)))
+    assert s0 == s1 == [3.0] * 7

@@ -42,6 +42,9 @@ class VLError(RuntimeError):
 
 _LIB = None
 
+# vlb200_allreduce_fn: void (*)(double *values, vl_size count, void *context)
+ALLREDUCE_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_size_t, C.c_void_p)
+
 
 def _decl(L):
     def f(name, res, *args):
@@ -106,6 +109,7 @@ def _decl(L):
     f("vlb200_gmm_get_num_restarts", _sz, _vp)
     f("vlb200_gmm_set_param_trace", None, _vp, C.c_int)
     f("vlb200_gmm_em_stream_device", C.c_double, _vp, _vp, _sz, C.c_int, _sz, _vp, _sz, C.c_float, _sz)
+    f("vlb200_gmm_em_sharded_device", C.c_double, _vp, _vp, _sz, _sz, C.c_int, _sz, ALLREDUCE_FN, _vp)
     f("vlb200_gmm_get_stream_report", _sz, _vp, _vp, _sz)
     f("vlb200_gmm_get_param_trace", _sz, _vp, _sz, _vp, _vp, _vp)
     f("vlb200_fisher_encode_device", C.c_int, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _sz, C.c_int,
@@ -313,6 +317,34 @@ class GMM:
                                                int(m), float(threshold), int(judge_every))
         if lib().vl_get_last_error():
             _raise_last("vlb200_gmm_em_stream_device")
+        return ll
+
+    def em_sharded_device(self, data_t, total_rows, allreduce, precision="default", chunk_rows=0) -> float:
+        """EM over rows sharded across ranks (vlb200_gmm_em_sharded_device):
+        `data_t` this rank's (n, D) CUDA tensor of the model's dtype, at least
+        one row, of `total_rows` in all; `allreduce(values)` sums a float64
+        NumPy array in place over all ranks (replicas.allreduce_sum builds one
+        on a torch.distributed group).  Returns the log-likelihood over all
+        rows, the same on every rank."""
+        err = []
+
+        def cb(ptr, count, _ctx):
+            # Every call is passed on, also after a failure, so that the ranks
+            # keep making the same collective calls; the first error is
+            # raised once the library call returns.
+            try:
+                allreduce(np.ctypeslib.as_array(ptr, shape=(int(count),)))
+            except BaseException as e:  # noqa: BLE001
+                err.append(e)
+
+        fn = ALLREDUCE_FN(cb)
+        _clear()
+        ll = lib().vlb200_gmm_em_sharded_device(self._h, data_t.data_ptr(), data_t.shape[0], int(total_rows),
+                                                 _prec(precision), int(chunk_rows), fn, None)
+        if err:
+            raise err[0]
+        if lib().vl_get_last_error():
+            _raise_last("vlb200_gmm_em_sharded_device")
         return ll
 
     def stream_report(self):

@@ -69,6 +69,11 @@ template <typename T>
 void exact_mstep_finalize_slabs(int nslab, const double *pmass, const double *ps1, const double *ps2,
                                 const double *lb, T *means, T *covs, T *priors, i64 K, i64 D,
                                 cudaStream_t s);
+// Sums the nslab slabs' partials into slab 0 (in slab order): the
+// finalize over that one slab then gives the same parameters, and the sums
+// ((2D + 1) K doubles: pmass[0..K), ps1[0..KD), ps2[0..KD)) can be added
+// across ranks first.
+void exact_sum_slabs(int nslab, double *pmass, double *ps1, double *ps2, i64 K, i64 D, cudaStream_t s);
 
 // Rand initialisation pieces (vl/gmm.c:1376-1443), bit-exact with the
 // reference.  global_variance: sigma (D) from X (N x D).  kmeanspp: K centres
@@ -210,6 +215,14 @@ void tc_em_stats(const float *X, i64 row0, i64 n, i64 K, i64 D, int split, float
                  cudaStream_t s);
 void tc_em_finalize(int nitems, const float *partial, float *means, float *covs, float *priors, i64 K,
                     i64 D, const double *lb, cudaStream_t s);
+// The same M-step in two parts: tc_em_sums writes the f64 sums of the
+// partials (S0: K, S1 and S2: K x D, scale factors taken out), which can be
+// added across ranks, and tc_em_apply updates the parameters from them
+// (using the centre of the last tc_prepare on this thread).
+void tc_em_sums(int nitems, const float *partial, i64 K, i64 D, double *S0, double *S1, double *S2,
+                cudaStream_t s);
+void tc_em_apply(const double *S0, const double *S1, const double *S2, float *means, float *covs, float *priors,
+                 i64 K, i64 D, const double *lb, cudaStream_t s);
 void tc_fisher_batch(const float *X, const i64 *h_offsets, i64 numImages,
                      const DevModel<float> &m, float *enc, unsigned long long *nterms, int flags,
                      int precision, cudaStream_t s);

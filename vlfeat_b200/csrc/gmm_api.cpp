@@ -390,6 +390,12 @@ struct StreamCfg {
   float thr = 0.99f;
   vl_size judgeEvery = 5;
   i64 fitRows = 1 << 20;
+  // Sharded EM: this rank's rows are part of totalN; every sum over rows
+  // (log-likelihood, restart masses, M-step sums) is completed across ranks
+  // by allreduce before it is used.
+  vlb200_allreduce_fn allreduce = nullptr;
+  void *arctx = nullptr;
+  i64 totalN = 0;
 };
 
 template <typename T>
@@ -423,6 +429,30 @@ double em_stream_device(VlGMM *self, const T *dX, i64 N, int precision, const St
   VlB200Router *router = nullptr;
   if constexpr (sizeof(T) == 4) router = cfg.router;
   const vl_size judgeEvery = std::max<vl_size>(1, cfg.judgeEvery);
+  const bool sharded = cfg.allreduce != nullptr;
+  VLB_CHECK(!sharded || (!router && cfg.totalN >= N), VL_ERR_BAD_ARG,
+            "sharded EM: no router, and totalData at least this rank's rows");
+  const i64 Ntot = sharded ? cfg.totalN : N;
+  std::vector<double> hsum;
+  // Completes the exact M-step's slab partials across ranks (summed into slab
+  // 0 first) and finalises from them; unsharded, the finalize over all slabs.
+  auto exact_finalize = [&](int nsl, double *qm, double *q1, double *q2) {
+    if (!sharded) {
+      vlb::exact_mstep_finalize_slabs<T>(nsl, qm, q1, q2, dlb, dmeans, dcovs, dpriors, K, D, s);
+      return;
+    }
+    vlb::exact_sum_slabs(nsl, qm, q1, q2, K, D, s);
+    hsum.resize((size_t)(2 * D + 1) * K);
+    VLB_CUDA(cudaMemcpyAsync(hsum.data(), qm, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaMemcpyAsync(hsum.data() + K, q1, sizeof(double) * K * D, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaMemcpyAsync(hsum.data() + K + K * D, q2, sizeof(double) * K * D, cudaMemcpyDeviceToHost, s));
+    VLB_CUDA(cudaStreamSynchronize(s));
+    cfg.allreduce(hsum.data(), (vl_size)hsum.size(), cfg.arctx);
+    VLB_CUDA(cudaMemcpyAsync(qm, hsum.data(), sizeof(double) * K, cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(q1, hsum.data() + K, sizeof(double) * K * D, cudaMemcpyHostToDevice, s));
+    VLB_CUDA(cudaMemcpyAsync(q2, hsum.data() + K + K * D, sizeof(double) * K * D, cudaMemcpyHostToDevice, s));
+    vlb::exact_mstep_finalize_slabs<T>(1, qm, q1, q2, dlb, dmeans, dcovs, dpriors, K, D, s);
+  };
   // Chunks start on the exact M-step's slab boundaries (its partition of all
   // N rows), so restarts can use the exact M-step chunk by chunk.
   const i64 rps = vlb::exact_mstep_slab_rows(N);
@@ -506,6 +536,15 @@ double em_stream_device(VlGMM *self, const T *dX, i64 N, int precision, const St
       }
       if (!tcStats) vlb::exact_mstep_stats_rows<T>(dX, r0, n, rps, dq, dmeans, K, D, pm, p1, p2, s);
     }
+    if (sharded) {
+      // This pass's log-likelihood and (for the restart check) masses, over all ranks.
+      hsum.assign(1 + (it > 1 ? K : 0), 0.0);
+      hsum[0] = LL;
+      for (i64 k = 0; k < (it > 1 ? K : 0); ++k) hsum[1 + k] = mass[k];
+      cfg.allreduce(hsum.data(), (vl_size)hsum.size(), cfg.arctx);
+      LL = hsum[0];
+      for (i64 k = 0; k < (it > 1 ? K : 0); ++k) mass[k] = hsum[1 + k];
+    }
     self->llTrace.push_back(LL);
     const double ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
     self->streamReport.push_back({LL, judged ? 1.0 : 0.0, viaRouter ? 1.0 : 0.0,
@@ -521,7 +560,7 @@ double em_stream_device(VlGMM *self, const T *dX, i64 N, int precision, const St
     // Restarts (vl/gmm.c:1292, 814-999) with the masses of this pass.
     vl_size nsplit = 0;
     if (it > 1 && K > 1) {
-      const double cutoff = 1e-2 * std::max(1.0, (double)N / (double)K);
+      const double cutoff = 1e-2 * std::max(1.0, (double)Ntot / (double)K);
       std::vector<std::array<double, 4>> splits;  // (empty mode, split mode, dimension, cut)
       std::vector<T> pr(K), cv(K * D), mu(K * D);
       bool saved = false;
@@ -535,7 +574,7 @@ double em_stream_device(VlGMM *self, const T *dX, i64 N, int precision, const St
             vlb::restart_split<T>(dq, dX + r0 * D, n, K, D, (i64)sp[0], (i64)sp[1], (i64)sp[2], (T)sp[3], s);
           vlb::exact_mstep_stats_rows<T>(dX, r0, n, rps, dq, dmeans, K, D, pm, p1, p2, s);
         }
-        vlb::exact_mstep_finalize_slabs<T>(nslab, pm, p1, p2, dlb, dmeans, dcovs, dpriors, K, D, s);
+        exact_finalize(nslab, pm, p1, p2);
         VLB_CUDA(cudaMemcpyAsync(pr.data(), dpriors, sizeof(T) * K, cudaMemcpyDeviceToHost, s));
         VLB_CUDA(cudaMemcpyAsync(cv.data(), dcovs, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
         VLB_CUDA(cudaMemcpyAsync(mu.data(), dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
@@ -590,12 +629,27 @@ double em_stream_device(VlGMM *self, const T *dX, i64 N, int precision, const St
     if (nsplit == 0) {
       bool done = false;
       if constexpr (sizeof(T) == 4) {
-        if (tcm) {
+        if (tcm && !sharded) {
           vlb::tc_em_finalize(item0, dpart, dmeans, dcovs, dpriors, K, D, dlb, s);
+          done = true;
+        } else if (tcm) {
+          // The item sums (f64, into slab 0 of the exact partials), completed
+          // across ranks, then the update.
+          vlb::tc_em_sums(item0, dpart, K, D, pm, p1, p2, s);
+          hsum.resize((size_t)(2 * D + 1) * K);
+          VLB_CUDA(cudaMemcpyAsync(hsum.data(), pm, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+          VLB_CUDA(cudaMemcpyAsync(hsum.data() + K, p1, sizeof(double) * K * D, cudaMemcpyDeviceToHost, s));
+          VLB_CUDA(cudaMemcpyAsync(hsum.data() + K + K * D, p2, sizeof(double) * K * D, cudaMemcpyDeviceToHost, s));
+          VLB_CUDA(cudaStreamSynchronize(s));
+          cfg.allreduce(hsum.data(), (vl_size)hsum.size(), cfg.arctx);
+          VLB_CUDA(cudaMemcpyAsync(pm, hsum.data(), sizeof(double) * K, cudaMemcpyHostToDevice, s));
+          VLB_CUDA(cudaMemcpyAsync(p1, hsum.data() + K, sizeof(double) * K * D, cudaMemcpyHostToDevice, s));
+          VLB_CUDA(cudaMemcpyAsync(p2, hsum.data() + K + K * D, sizeof(double) * K * D, cudaMemcpyHostToDevice, s));
+          vlb::tc_em_apply(pm, p1, p2, dmeans, dcovs, dpriors, K, D, dlb, s);
           done = true;
         }
       }
-      if (!done) vlb::exact_mstep_finalize_slabs<T>(nslab, pm, p1, p2, dlb, dmeans, dcovs, dpriors, K, D, s);
+      if (!done) exact_finalize(nslab, pm, p1, p2);
     }
   }
   VLB_CUDA(cudaMemcpyAsync(self->means, dmeans, sizeof(T) * K * D, cudaMemcpyDeviceToHost, s));
@@ -1053,6 +1107,29 @@ double vlb200_gmm_em_stream_device(VlGMM *self, float const *data, vl_size numDa
         cfg.judgeEvery = judgeEvery;
         const double ll = em_stream_device<float>(self, data, (i64)numData,
                                                   vlb::resolve_precision(precision, false), cfg);
+        self->LL = ll;
+        return ll;
+      },
+      (double)NAN);
+}
+
+double vlb200_gmm_em_sharded_device(VlGMM *self, void const *data, vl_size numData, vl_size totalData,
+                                    int precision, vl_size chunkRows, vlb200_allreduce_fn allreduce,
+                                    void *context) {
+  return guarded(
+      [&]() -> double {
+        VLB_CHECK(allreduce != nullptr && data != nullptr && numData >= 1 && totalData >= numData &&
+                      totalData <= (vl_size)INT64_MAX,
+                  VL_ERR_BAD_ARG, "vlb200_gmm_em_sharded_device: bad arguments");
+        StreamCfg cfg;
+        cfg.chunk = (i64)chunkRows;
+        cfg.allreduce = allreduce;
+        cfg.arctx = context;
+        cfg.totalN = (i64)totalData;
+        const bool isFloat = self->dataType == VL_TYPE_FLOAT;
+        const int prec = vlb::resolve_precision(precision, !isFloat);
+        const double ll = isFloat ? em_stream_device<float>(self, (const float *)data, (i64)numData, prec, cfg)
+                                  : em_stream_device<double>(self, (const double *)data, (i64)numData, prec, cfg);
         self->LL = ll;
         return ll;
       },

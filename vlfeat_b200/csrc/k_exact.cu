@@ -752,6 +752,28 @@ void exact_mstep_finalize_slabs(int nslab, const double *pmass, const double *ps
   VLB_LAUNCH("normalize_priors", s, k_normalize_priors<T><<<1, kThreads, 0, s>>>(priors, (int)K));
 }
 
+// Slab partials summed into slab 0 in slab order (the order the finalize
+// kernel uses), so that the finalize over one slab gives the same values.
+__global__ void k_sum_slabs(int nslab, i64 K, i64 KD, double *__restrict__ pmass, double *__restrict__ ps1,
+                            double *__restrict__ ps2) {
+  const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= KD) return;
+  double a = 0, b = 0, c = 0;
+  for (int sl = 0; sl < nslab; ++sl) {
+    if (i < K) a += pmass[(i64)sl * K + i];
+    b += ps1[(i64)sl * KD + i];
+    c += ps2[(i64)sl * KD + i];
+  }
+  if (i < K) pmass[i] = a;
+  ps1[i] = b;
+  ps2[i] = c;
+}
+
+void exact_sum_slabs(int nslab, double *pmass, double *ps1, double *ps2, i64 K, i64 D, cudaStream_t s) {
+  VLB_LAUNCH("sum_slabs", s,
+             k_sum_slabs<<<grid1(K * D, kThreads), kThreads, 0, s>>>(nslab, K, K * D, pmass, ps1, ps2));
+}
+
 template <typename T>
 void normalize_priors(T *priors, i64 K, cudaStream_t s) {
   VLB_LAUNCH("normalize_priors", s, k_normalize_priors<T><<<1, kThreads, 0, s>>>(priors, (int)K));

@@ -1358,28 +1358,43 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
 // S2 - 2 a S1 + a^2 S0 with a = mu_old - c.  Then the reference's update:
 // mean, variance about the new mean, the variance floor, and the mass as
 // the unnormalised prior.
-__global__ void k_tc_mstep_finalize(int nitems, int K, int Kp, int D, const float *__restrict__ partial,
-                                    const float *__restrict__ ctr, const float *__restrict__ scale,
-                                    const double *__restrict__ lb, float *__restrict__ means,
-                                    float *__restrict__ covs, float *__restrict__ priors) {
+// Sums of the item partials in f64, item order: S0[k] = sum q, S1[k][d] =
+// sum q x'', S2[k][d] = sum q x''^2, with the q 2^14 and x'' = x' scale
+// factors (powers of two, so exact) taken out.
+__global__ void k_tc_mstep_sums(int nitems, int K, int Kp, int D, const float *__restrict__ partial,
+                                const float *__restrict__ scale, double *__restrict__ S0,
+                                double *__restrict__ S1, double *__restrict__ S2) {
   const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (i64)K * D) return;
   const int k = (int)(idx / D), d = (int)(idx % D);
   const int NST = 2 * D + 16;
-  double S0 = 0, S1 = 0, S2 = 0;
+  double s0 = 0, s1 = 0, s2 = 0;
   for (int it = 0; it < nitems; ++it) {
     const float *pp = partial + ((size_t)it * Kp + k) * NST;
-    S0 += (double)pp[2 * D];
-    S1 += (double)pp[d];
-    S2 += (double)pp[D + d];
+    s0 += (double)pp[2 * D];
+    s1 += (double)pp[d];
+    s2 += (double)pp[D + d];
   }
   const double is = scale ? 1.0 / (double)scale[d] : 1.0, iq = 1.0 / (double)kQScale;
-  S0 *= iq;
-  S1 *= is * iq;
-  S2 *= is * is * iq;
+  if (d == 0) S0[k] = s0 * iq;
+  S1[idx] = s1 * (is * iq);
+  S2[idx] = s2 * (is * is * iq);
+}
+
+// The M-step from those sums: the reference's mean and variance about the
+// new mean (sum q x = S1 + c S0, sum q (x - mu_old)^2 = S2 - 2 a S1 + a^2 S0
+// with a = mu_old - c), the variance floor, the mass as the unnormalised prior.
+__global__ void k_tc_mstep_apply(int K, int D, const double *__restrict__ S0, const double *__restrict__ S1,
+                                 const double *__restrict__ S2, const float *__restrict__ ctr,
+                                 const double *__restrict__ lb, float *__restrict__ means,
+                                 float *__restrict__ covs, float *__restrict__ priors) {
+  const i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (i64)K * D) return;
+  const int k = (int)(idx / D), d = (int)(idx % D);
+  const double s0 = S0[k], s1 = S1[idx], s2 = S2[idx];
   const double c = (double)ctr[d], oldmu = (double)means[idx], a = oldmu - c;
-  const double mass = S0;
-  double mu = S1 + c * S0, v = S2 - 2.0 * a * S1 + a * a * S0;
+  const double mass = s0;
+  double mu = s1 + c * s0, v = s2 - 2.0 * a * s1 + a * a * s0;
   if (mass >= 1e-6 / (double)K) {
     mu /= mass;
     v /= mass;
@@ -1901,11 +1916,7 @@ void tc_mstep(const float *X, i64 N, float *means, float *covs, float *priors, i
     sp.items = ditems; sp.order = dorder; sp.cta_beg = dbeg; sp.partial = partial; sp.err = err;
     stats_dispatch((int)D, fp32 ? 2 : 1, sp, gx, 0, 0, s);
   }
-  VLB_LAUNCH("tc_mstep_finalize", s,
-             k_tc_mstep_finalize<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
-                 nitems, (int)K, Kp, (int)D, partial, (const float *)sc.slot[0].p,
-                 (const float *)sc.slot[12].p, lb, means, covs, priors));
-  normalize_priors<float>(priors, K, s);
+  tc_em_finalize(nitems, partial, means, covs, priors, K, D, lb, s);
   check_err(err, s);
 }
 
@@ -1957,15 +1968,29 @@ void tc_em_stats(const float *X, i64 row0, i64 n, i64 K, i64 D, int split, float
   check_err(err, s);
 }
 
+void tc_em_sums(int nitems, const float *partial, i64 K, i64 D, double *S0, double *S1, double *S2,
+                cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaTc);
+  VLB_LAUNCH("tc_mstep_sums", s,
+             k_tc_mstep_sums<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
+                 nitems, (int)K, padK(K), (int)D, partial, (const float *)sc.slot[12].p, S0, S1, S2));
+}
+
+void tc_em_apply(const double *S0, const double *S1, const double *S2, float *means, float *covs, float *priors,
+                 i64 K, i64 D, const double *lb, cudaStream_t s) {
+  Scratch &sc = thread_scratch(kArenaTc);
+  VLB_LAUNCH("tc_mstep_apply", s,
+             k_tc_mstep_apply<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
+                 (int)K, (int)D, S0, S1, S2, (const float *)sc.slot[0].p, lb, means, covs, priors));
+  normalize_priors<float>(priors, K, s);
+}
+
 void tc_em_finalize(int nitems, const float *partial, float *means, float *covs, float *priors, i64 K, i64 D,
                     const double *lb, cudaStream_t s) {
   Scratch &sc = thread_scratch(kArenaTc);
-  const int Kp = padK(K);
-  VLB_LAUNCH("tc_mstep_finalize", s,
-             k_tc_mstep_finalize<<<(unsigned)((K * D + 255) / 256), 256, 0, s>>>(
-                 nitems, (int)K, Kp, (int)D, partial, (const float *)sc.slot[0].p,
-                 (const float *)sc.slot[12].p, lb, means, covs, priors));
-  normalize_priors<float>(priors, K, s);
+  double *S = sc.slot[25].get<double>((size_t)(2 * D + 1) * K);
+  tc_em_sums(nitems, partial, K, D, S, S + K, S + K + K * D, s);
+  tc_em_apply(S, S + K, S + K + K * D, means, covs, priors, K, D, lb, s);
 }
 
 size_t tc_em_partial_floats(i64 K, i64 D) { return (size_t)padK(K) * (size_t)(2 * D + 16); }

@@ -1,4 +1,5 @@
-"""Multi-GPU Fisher encoding as independent replicas (one process per GPU).
+"""Multi-GPU Fisher encoding as independent replicas (one process per GPU),
+and EM with its rows sharded over ranks.
 
 Images are independent, so N GPUs run N replicas, each on its own batch, with
 no exchange on the data path (weak scaling).  A batch that one caller owns is
@@ -79,3 +80,24 @@ def gather_encodings(local, num_images: int, dist):
         return None
     rows = [parts[r][: (r + 1) * num_images // world - r * num_images // world] for r in range(world)]
     return torch.cat(rows, 0)
+
+
+def row_shard(n_rows: int, rank: int, world: int) -> tuple[int, int]:
+    """This rank's contiguous rows [r0, r1) of n_rows for sharded EM (sizes
+    differ by at most one row)."""
+    return rank * n_rows // world, (rank + 1) * n_rows // world
+
+
+def allreduce_sum(dist, group=None):
+    """A sum over the ranks of `group` for capi.GMM.em_sharded_device: the
+    returned function adds a float64 NumPy array in place over all ranks
+    (through a CUDA tensor on an NCCL group, a CPU tensor on gloo)."""
+    import numpy as np
+    import torch
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+
+    def reduce(values: np.ndarray) -> None:
+        t = torch.from_numpy(np.ascontiguousarray(values, dtype=np.float64)).to(dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        values[...] = t.cpu().numpy()
+    return reduce
