@@ -15,6 +15,7 @@
 // [offsets[j], offsets[j+1]) of the data and of the assignments (row-major,
 // numClusters per row, vl/vlad.c:173-176).
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "engine.h"
@@ -226,6 +227,7 @@ struct VsParams {
   i64 img0;
   int D, K, flags, R;
   int *err;
+  const int *only;  // when set, the images with only[img] != 0 (the others are done elsewhere)
 };
 
 template <typename T>
@@ -318,6 +320,7 @@ __global__ void __launch_bounds__(kVsThreads, sizeof(T) == 4 && JD <= 3 ? 2 : 1)
   const int D = p.D, K = p.K, R = p.R;
   const int k0 = blockIdx.x * (kVsWarps * CPW), nkb = min(kVsWarps * CPW, K - k0);
   const i64 img = p.img0 + blockIdx.y;
+  if (p.only && !p.only[img]) return;
   const i64 r0 = p.offs[img], r1 = p.offs[img + 1];
   const int ntiles = (int)((r1 - r0 + R - 1) / R);
   const uint32_t aBytes = (uint32_t)(R * nkb * sizeof(T)), stageBytes = aBytes + (uint32_t)(R * D * sizeof(T));
@@ -462,6 +465,242 @@ __global__ void __launch_bounds__(kVsThreads, sizeof(T) == 4 && JD <= 3 ? 2 : 1)
     for (int d = lane; d < D; d += 32) out[(i64)c * D + d] = zs[c * ld + d];
 }
 
+// -------------------------------------------- grouped path (one weight per row)
+// When each row has at most one positive weight (hard assignments), the rows
+// of an image are first grouped by that component, in row order; then one
+// warp per (image, component) walks its rows.  Every chain sees the same
+// rows in the same order as in the reference's loop, so the bits are the
+// same; the assignment matrix is read once, by a streaming pass.
+
+// Per row: its only positive weight's component and value (comp -1: no
+// positive weight; -2: more than one, and its image takes the streaming
+// kernel).  One warp per row, 16-byte loads.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vlad_pick(const T *__restrict__ A, i64 N, int K, int *__restrict__ comp,
+                                                    T *__restrict__ wgt) {
+  constexpr int V = 16 / (int)sizeof(T);
+  using L = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  const int lane = threadIdx.x & 31;
+  const i64 w0 = ((i64)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((i64)gridDim.x * blockDim.x) >> 5;
+  // Two rows per warp and pass, their loads in flight together.
+  for (i64 i0 = 2 * w0; i0 < N; i0 += 2 * nw) {
+    int cnt[2] = {0, 0}, kk[2] = {-1, -1};
+    T av[2] = {(T)0, (T)0};
+    for (int k0 = lane * V; k0 < K; k0 += 32 * V) {
+      L v[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (i0 + h < N) v[h] = *reinterpret_cast<const L *>(A + (i0 + h) * K + k0);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (i0 + h >= N) continue;
+        const T *e = reinterpret_cast<const T *>(&v[h]);
+#pragma unroll
+        for (int u = 0; u < V; ++u)
+          if (e[u] > (T)0) {  // vl/vlad.c:182
+            ++cnt[h];
+            kk[h] = k0 + u;
+            av[h] = e[u];
+          }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const i64 i = i0 + h;
+      const int tot = __reduce_add_sync(0xffffffffu, cnt[h]);
+      if (i >= N) continue;
+      if (tot == 1 && cnt[h] == 1) {
+        comp[i] = kk[h];
+        wgt[i] = av[h];
+      }
+      if (lane == 0 && tot != 1) comp[i] = tot == 0 ? -1 : -2;
+    }
+  }
+}
+
+constexpr int kSortWarps = 16;
+
+// Per image (one block): a stable counting sort of its rows by component.
+// Warp w takes a contiguous run of the rows; per-warp counts give each
+// (warp, component) its first slot, so rows keep their order within a
+// component.  cstart[img][k] .. cstart[img][k + 1]: the component's slots in
+// sorted (rows relative to the image's first); soft[img]: a row with more
+// than one positive weight.
+__global__ void __launch_bounds__(kSortWarps * 32) k_vlad_sort(const i64 *__restrict__ offs, const int *__restrict__ comp,
+                                                              int K, int *__restrict__ sorted, int *__restrict__ cstart,
+                                                              int *__restrict__ soft) {
+  extern __shared__ int sh[];
+  int *hist = sh;                   // [warp][K]: counts, then first slots
+  int *base = sh + kSortWarps * K;  // [K + 1]
+  __shared__ int s_soft;
+  const i64 img = blockIdx.x;
+  const i64 r0 = offs[img], n = offs[img + 1] - r0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < kSortWarps * K; i += kSortWarps * 32) hist[i] = 0;
+  if (tid == 0) s_soft = 0;
+  __syncthreads();
+  const i64 w0 = r0 + n * warp / kSortWarps, w1 = r0 + n * (warp + 1) / kSortWarps;
+  for (i64 r = w0 + lane; r < w1; r += 32) {
+    const int c = comp[r];
+    if (c >= 0) atomicAdd(&hist[warp * K + c], 1);
+    else if (c == -2) s_soft = 1;
+  }
+  __syncthreads();
+  for (int k = tid; k < K; k += kSortWarps * 32) {
+    int t = 0;
+    for (int w = 0; w < kSortWarps; ++w) {
+      const int h = hist[w * K + k];
+      hist[w * K + k] = t;
+      t += h;
+    }
+    base[k] = t;
+  }
+  __syncthreads();
+  if (warp == 0) {  // exclusive prefix of the component totals
+    const int per = (K + 31) / 32;
+    int sum = 0;
+    for (int j = 0; j < per; ++j) {
+      const int k = lane * per + j;
+      if (k < K) sum += base[k];
+    }
+    int pre = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, pre, o);
+      if (lane >= o) pre += v;
+    }
+    int run = pre - sum;
+    for (int j = 0; j < per; ++j) {
+      const int k = lane * per + j;
+      if (k < K) {
+        const int t = base[k];
+        base[k] = run;
+        run += t;
+      }
+    }
+    if (lane == 31) base[K] = run;
+  }
+  __syncthreads();
+  for (int k = tid; k <= K; k += kSortWarps * 32) cstart[img * (K + 1) + k] = base[k];
+  if (tid == 0) soft[img] = s_soft;
+  // Stable scatter: 32 consecutive rows at a time; lanes with the same
+  // component take consecutive slots in lane order.
+  for (i64 rb = w0; rb < w1; rb += 32) {
+    const i64 r = rb + lane;
+    const int c = r < w1 ? comp[r] : -1;
+    const unsigned same = __match_any_sync(0xffffffffu, c);
+    const int first = c >= 0 ? base[c] + hist[warp * K + c] : 0;
+    __syncwarp();
+    if (c >= 0) {
+      sorted[r0 + first + __popc(same & ((1u << lane) - 1u))] = (int)(r - r0);
+      if ((same >> lane) == 1u) hist[warp * K + c] += __popc(same);  // the group's last lane
+    }
+    __syncwarp();
+  }
+}
+
+struct VgParams {
+  void *enc;
+  const void *means, *X, *wgt;
+  const i64 *offs;
+  const int *sorted, *cstart, *soft;
+  i64 img0;
+  int D, K, flags;
+};
+
+constexpr int kVgWarps = 8;
+constexpr int kVgPrefetch = 8;  // rows whose descriptors are loaded together
+
+// One warp per (image, component): the component's rows in order (lane l
+// holds dimensions l + 32 j), the chain step and the mass as in the
+// reference's loop, then the mass step, the signed square root and the
+// component norm (a sum of squares in dimension order, by lane 0 through
+// shared memory), and the coalesced store.  Images with a multi-weight row
+// are left to the streaming kernel.
+template <typename T, int JD>
+__global__ void __launch_bounds__(kVgWarps * 32) k_vlad_group(const VgParams p) {
+  __shared__ T zs[kVgWarps][128];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const i64 img = p.img0 + blockIdx.y;
+  if (p.soft[img]) return;
+  const int K = p.K, D = p.D, k = blockIdx.x * kVgWarps + warp;
+  if (k >= K) return;
+  const T *X = (const T *)p.X, *W = (const T *)p.wgt;
+  const i64 r0 = p.offs[img];
+  const int b = p.cstart[img * (K + 1) + k], e = p.cstart[img * (K + 1) + k + 1];
+  const int *rows = p.sorted + r0;
+  T acc[JD];
+#pragma unroll
+  for (int j = 0; j < JD; ++j) acc[j] = (T)0;
+  double mass = 0.0;
+  // 32 of the component's rows at a time: lane j loads the j-th row index and
+  // weight; the rows' descriptors are loaded kVgPrefetch rows ahead.
+  for (int t = b; t < e; t += 32) {
+    const int cnt = min(32, e - t);
+    const int myrow = lane < cnt ? rows[t + lane] : 0;
+    const T mya = lane < cnt ? W[r0 + myrow] : (T)0;
+    for (int u0 = 0; u0 < cnt; u0 += kVgPrefetch) {
+      T av[kVgPrefetch], xv[kVgPrefetch][JD];
+#pragma unroll
+      for (int u = 0; u < kVgPrefetch; ++u) {
+        const int rr = __shfl_sync(0xffffffffu, myrow, (u0 + u) & 31);
+        av[u] = __shfl_sync(0xffffffffu, mya, (u0 + u) & 31);
+        if (u0 + u < cnt) {
+          const i64 row = r0 + rr;
+#pragma unroll
+          for (int j = 0; j < JD; ++j) {
+            const int d = lane + 32 * j;
+            xv[u][j] = d < D ? X[row * D + d] : (T)0;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kVgPrefetch; ++u) {
+        if (u0 + u < cnt) {
+          mass += (double)av[u];
+          if (sizeof(T) == 4 && av[u] == (T)1) {
+#pragma unroll
+            for (int j = 0; j < JD; ++j) acc[j] = add_t(acc[j], xv[u][j]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < JD; ++j) acc[j] = acc_step(acc[j], av[u], xv[u][j]);
+          }
+        }
+      }
+    }
+  }
+  const T *mu = (const T *)p.means + (i64)k * D;
+  T z[JD];
+#pragma unroll
+  for (int j = 0; j < JD; ++j) {
+    const int d = lane + 32 * j;
+    z[j] = (T)0;
+    if (d < D) {
+      T v = vlad_mass_step<T>(acc[j], mu[d], mass, p.flags);
+      if (p.flags & VL_VLAD_FLAG_SQUARE_ROOT) v = v >= (T)0 ? sqrt_t(v) : -sqrt_t(-v);
+      z[j] = v;
+      zs[warp][d] = v;
+    }
+  }
+  if (p.flags & VL_VLAD_FLAG_NORMALIZE_COMPONENTS) {
+    __syncwarp();
+    T nrm = (T)0;
+    if (lane == 0) {
+      for (int d = 0; d < D; ++d) nrm = add_t(nrm, mul_t(zs[warp][d], zs[warp][d]));
+      nrm = (T)fmax((double)sqrt_t(nrm), 1e-12);
+    }
+    nrm = __shfl_sync(0xffffffffu, nrm, 0);
+#pragma unroll
+    for (int j = 0; j < JD; ++j) z[j] = div_t(z[j], nrm);
+  }
+  T *out = (T *)p.enc + img * (i64)K * D + (i64)k * D;
+#pragma unroll
+  for (int j = 0; j < JD; ++j) {
+    const int d = lane + 32 * j;
+    if (d < D) out[d] = z[j];
+  }
+}
+
 // Components per consumer warp.  16 (two rows per step) keeps float
 // accumulators within the register budget of two blocks per SM.
 constexpr int kVsCpw = 16;
@@ -499,11 +738,46 @@ void launch_stream_cpw(const VsParams &p0, i64 nimg, cudaStream_t s) {
 
 template <typename T, int JD>
 void launch_stream(T *enc, const T *means, int D, int K, const T *X, const T *A, const i64 *doffs, i64 nimg,
-                   int flags, int *derr, cudaStream_t s) {
+                   int flags, int *derr, const int *only, cudaStream_t s) {
   VsParams p;
   p.enc = enc; p.means = means; p.X = X; p.A = A; p.offs = doffs;
-  p.D = D; p.K = K; p.flags = flags; p.R = vs_rows<T>(D, K); p.err = derr;
+  p.D = D; p.K = K; p.flags = flags; p.R = vs_rows<T>(D, K); p.err = derr; p.only = only;
   launch_stream_cpw<T, JD, kVsCpw>(p, nimg, s);
+}
+
+template <typename T, int JD>
+void launch_group(const VgParams &p0, i64 nimg, cudaStream_t s) {
+  VgParams p = p0;
+  for (i64 img0 = 0; img0 < nimg; img0 += 65535) {
+    p.img0 = img0;
+    dim3 grid((unsigned)((p.K + kVgWarps - 1) / kVgWarps), (unsigned)std::min<i64>(65535, nimg - img0));
+    VLB_LAUNCH("vlad_group", s, (k_vlad_group<T, JD><<<grid, kVgWarps * 32, 0, s>>>(p)));
+  }
+}
+
+// The grouped path's pre-passes: per row its one positive weight, then per
+// image the rows sorted by component (scratch slots 7-11 of the VLAD arena).
+// Returns the per-image flags of images that need the streaming kernel.
+template <typename T>
+const int *group_rows(Scratch &sc, const T *A, i64 N, int K, const i64 *doffs, i64 nimg, VgParams &g,
+                      cudaStream_t s) {
+  int *comp = sc.slot[7].get<int>((size_t)std::max<i64>(1, N));
+  T *wgt = sc.slot[8].get<T>((size_t)std::max<i64>(1, N));
+  int *sorted = sc.slot[9].get<int>((size_t)std::max<i64>(1, N));
+  int *cstart = sc.slot[10].get<int>((size_t)nimg * (K + 1));
+  int *soft = sc.slot[11].get<int>((size_t)nimg);
+  if (N > 0) {
+    const unsigned blocks = (unsigned)std::min<i64>((N + 7) / 8, 16 * 148);
+    VLB_LAUNCH("vlad_pick", s, k_vlad_pick<T><<<blocks, 256, 0, s>>>(A, N, K, comp, wgt));
+  }
+  const size_t smem = sizeof(int) * ((size_t)kSortWarps * K + K + 1);
+  VLB_CUDA(cudaFuncSetAttribute(k_vlad_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  VLB_LAUNCH("vlad_sort", s, k_vlad_sort<<<(unsigned)nimg, kSortWarps * 32, smem, s>>>(doffs, comp, K, sorted, cstart, soft));
+  g.wgt = wgt;
+  g.sorted = sorted;
+  g.cstart = cstart;
+  g.soft = soft;
+  return soft;
 }
 
 template <typename T, int JD>
@@ -539,8 +813,14 @@ void vlad_batch(T *enc, const T *means, i64 D, i64 K, const T *X, const T *A, co
   // VLAD arena slots: 0 offsets, 6 error word (here); 2-5 the
   // host entry point's staged inputs and output.
   Scratch &sc = thread_scratch(kArenaVlad);
+  // Offsets relative to the first image's first row (data and assignments
+  // rebased with them), so that the per-row scratch starts at the batch.
+  const i64 base0 = h_offsets[0];
   std::vector<i64> rel(nimg + 1);
-  for (i64 j = 0; j <= nimg; ++j) rel[j] = h_offsets[j];
+  for (i64 j = 0; j <= nimg; ++j) rel[j] = h_offsets[j] - base0;
+  X += base0 * D;
+  A += base0 * K;
+  const i64 N = rel[nimg];
   i64 *doffs = sc.slot[0].get<i64>(nimg + 1);
   VLB_CUDA(cudaMemcpyAsync(doffs, rel.data(), sizeof(i64) * (nimg + 1), cudaMemcpyHostToDevice, s));
   int *herr = (int *)pinned_host(sizeof(int));
@@ -549,10 +829,23 @@ void vlad_batch(T *enc, const T *means, i64 D, i64 K, const T *X, const T *A, co
     int *derr = sc.slot[6].get<int>(1);
     VLB_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), s));
     const int jd = (int)((D + 31) / 32);
-    if (jd <= 1) launch_stream<T, 1>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
-    else if (jd == 2) launch_stream<T, 2>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
-    else if (jd == 3) launch_stream<T, 3>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
-    else launch_stream<T, 4>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, s);
+    // Up to 1,024 components, rows with one positive weight are grouped by
+    // component first; the streaming kernel takes only the images with a
+    // row of several.
+    const int *only = nullptr;
+    if (K <= 1024 && N < (i64)INT32_MAX) {
+      VgParams g;
+      g.enc = enc; g.means = means; g.X = X; g.offs = doffs; g.D = (int)D; g.K = (int)K; g.flags = flags;
+      only = group_rows<T>(sc, A, N, (int)K, doffs, nimg, g, s);
+      if (jd <= 1) launch_group<T, 1>(g, nimg, s);
+      else if (jd == 2) launch_group<T, 2>(g, nimg, s);
+      else if (jd == 3) launch_group<T, 3>(g, nimg, s);
+      else launch_group<T, 4>(g, nimg, s);
+    }
+    if (jd <= 1) launch_stream<T, 1>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, only, s);
+    else if (jd == 2) launch_stream<T, 2>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, only, s);
+    else if (jd == 3) launch_stream<T, 3>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, only, s);
+    else launch_stream<T, 4>(enc, means, (int)D, (int)K, X, A, doffs, nimg, flags, derr, only, s);
     VLB_CUDA(cudaMemcpyAsync(herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
   } else {
     vlad_tiles<T>(enc, means, D, K, X, A, doffs, nimg, flags, s);
