@@ -198,7 +198,20 @@ __global__ void __launch_bounds__(256) k_vlad_global_norm(T *__restrict__ enc, i
   if (lane == 0) s_n[w] = (T)fmax((double)sqrt_t(n), 1e-12);
   __syncwarp();
   n = s_n[w];
-  for (i64 i = lane; i < KD; i += 32) e[i] = div_t(e[i], n);
+  // Eight loads in flight before their divisions and stores.
+  for (i64 i0 = lane; i0 < KD; i0 += 32 * 8) {
+    T v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const i64 i = i0 + 32 * u;
+      v[u] = i < KD ? e[i] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const i64 i = i0 + 32 * u;
+      if (i < KD) e[i] = div_t(v[u], n);
+    }
+  }
 }
 
 // ------------------------------------------------------------ streaming path
