@@ -109,3 +109,49 @@ def test_noalloc_rejects_sizes_that_wrap_when_signed(vl):
     for n, k, d in ((1 << 63, 8, 8), (16, (1 << 64) - 1, 8), (16, 8, 1 << 63)):
         rc = noalloc(None, None, d, k, None, None, None, n, vl.FLAG_IMPROVED, None, None)
         assert rc == 3  # VL_ERR_BAD_ARG
+
+
+def test_noalloc_call_is_captured_and_replayed_in_a_cuda_graph(vl):
+    """After a first call, the entry point allocates nothing and copies nothing
+    from the host: a call captured into a CUDA graph replays on new descriptor
+    values and matches the allocating entry point, and a direct call leaves the
+    device's free memory unchanged."""
+    import torch
+    lib = vl.lib()
+    noalloc = _bind(lib)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    K, D, N = 128, 64, 2500
+    pr, mu, cv, x = _case(11, K, D, N)
+    mu_t, cv_t, pr_t, x_t = t(mu), t(cv), t(pr), t(x)
+    enc = torch.zeros(2 * K * D, device="cuda")
+    nt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    flags = vl.FLAG_IMPROVED
+
+    def call(stream):
+        return noalloc(enc.data_ptr(), mu_t.data_ptr(), D, K, cv_t.data_ptr(), pr_t.data_ptr(),
+                       x_t.data_ptr(), N, flags, nt.data_ptr(), C.c_void_p(stream.cuda_stream))
+
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        assert call(side) == 0, lib.vl_get_last_error_message()  # first call: module loading
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    with torch.cuda.stream(side):
+        assert call(side) == 0, lib.vl_get_last_error_message()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        rc = call(torch.cuda.current_stream())
+    assert rc == 0, lib.vl_get_last_error_message()
+    stream = torch.cuda.current_stream()
+    for seed in (12, 13):
+        x_t.copy_(t(_case(seed, K, D, N)[3]))
+        enc.fill_(float("nan"))
+        graph.replay()
+        ref = torch.zeros(2 * K * D, device="cuda")
+        nt_ref = vl.fisher_encode_device(ref, mu_t, cv_t, pr_t, x_t, flags, "exact", stream)
+        torch.cuda.synchronize()
+        assert rel_err(enc.cpu().numpy(), ref.cpu().numpy()) < 2e-5
+        assert int(nt.item()) == nt_ref

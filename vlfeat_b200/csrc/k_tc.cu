@@ -1269,36 +1269,56 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
   for (int d = tid; d < DIM; d += kFinThreads) s_is[d] = scale ? 1.0 / (double)scale[d] : 1.0;
   const double iq = 1.0 / (double)kQScale;
   __syncthreads();
+  // Element (component kl, dimension d) is el = kl Dr + d.  Warp w takes the
+  // components w, w + NW, ...; lane l the dimensions l, l + 32, ... below Dr,
+  // so no element index is divided and a component's S0 is one broadcast load.
+  constexpr int DPL = (DIM + 31) / 32;
   double sq = 0;
-  for (int el = tid; el < E; el += kFinThreads) {
-    const int kl = el / Dr, d = el - kl * Dr, k = k0 + kl, e = eBase + el;
-    double S0 = 0, S1 = 0, S2 = 0;
+#pragma unroll 2
+  for (int kl = warp; kl < Kc; kl += NW) {
+    const int k = k0 + kl;
+    double S0 = 0, S1[DPL], S2[DPL];
+#pragma unroll
+    for (int j = 0; j < DPL; ++j) S1[j] = S2[j] = 0;
     const float *pp = partial + ((size_t)s0 * Kp + k) * NST;
     for (int s = s0; s < s1; ++s, pp += slotStride) {
       S0 += (double)pp[2 * DIM];
-      S1 += (double)pp[d];
-      S2 += (double)pp[DIM + d];
+#pragma unroll
+      for (int j = 0; j < DPL; ++j) {
+        const int d = lane + 32 * j;
+        if (d < Dr) {
+          S1[j] += (double)pp[d];
+          S2[j] += (double)pp[DIM + d];
+        }
+      }
     }
     // Statistics were taken on q 2^14 and x'' = x' * scale.
-    const double is = s_is[d];
     S0 *= iq;
-    S1 *= is * iq;
-    S2 *= is * is * iq;
-    const double mup = cmu[e];
-    const double u = cisd[e] * (S1 - mup * S0) * (cup[k] * in);
-    const double v = ((S2 - 2.0 * mup * S1 + mup * mup * S0) * cis2[e] - S0) * (cvp[k] * in);
-    float uf = (float)u, vf = (float)v;
-    if (flags & 1) {
-      uf = uf >= 0.f ? sqrtf(uf) : -sqrtf(-uf);
-      vf = vf >= 0.f ? sqrtf(vf) : -sqrtf(-vf);
+    const double cu = cup[k] * in, cv = cvp[k] * in;
+#pragma unroll
+    for (int j = 0; j < DPL; ++j) {
+      const int d = lane + 32 * j;
+      if (d >= Dr) continue;
+      const int el = kl * Dr + d, e = eBase + el;
+      const double is = s_is[d];
+      const double s1 = S1[j] * (is * iq), s2 = S2[j] * (is * is * iq);
+      const double mup = cmu[e];
+      const double u = cisd[e] * (s1 - mup * S0) * cu;
+      const double v = ((s2 - 2.0 * mup * s1 + mup * mup * S0) * cis2[e] - S0) * cv;
+      float uf = (float)u, vf = (float)v;
+      if (flags & 1) {
+        uf = uf >= 0.f ? sqrtf(uf) : -sqrtf(-uf);
+        vf = vf >= 0.f ? sqrtf(vf) : -sqrtf(-vf);
+      }
+      s_fv[el] = uf;
+      s_fv[E + el] = vf;
+      sq += (double)uf * uf + (double)vf * vf;
     }
-    s_fv[el] = uf;
-    s_fv[E + el] = vf;
-    sq += (double)uf * uf + (double)vf * vf;
   }
   // Term counts: the image's rows are split over the cluster's CTAs.
   unsigned long long nt = 0;
   if (rowcnt)
+#pragma unroll 4
     for (i64 r = r0 + rank * kFinThreads + tid; r < r1; r += kFinThreads * kFinCluster)
       nt += rowcnt[r - rowcntBase];
   sq = warp_sum(sq);
@@ -1332,18 +1352,28 @@ __global__ void __cluster_dims__(kFinCluster, 1, 1) __launch_bounds__(kFinThread
   }
   __syncthreads();
   float *out = enc + (imgBase + img) * 2 * (i64)KD + eBase;
-  if (flags & 2) {
+  const bool nrmz = (flags & 2) != 0;
+  float nf = 1.f;
+  if (nrmz) {
     double nrm = sqrt(s_tot);
     if (nrm < 1e-12) nrm = 1e-12;
-    const float nf = (float)nrm;
-    for (int el = tid; el < E; el += kFinThreads) {
-      out[el] = s_fv[el] / nf;
-      out[KD + el] = s_fv[E + el] / nf;
+    nf = (float)nrm;
+  }
+  // Both halves in 16-byte pieces where E and the output allow it.
+  if (E % 4 == 0 && (((uintptr_t)out | (uintptr_t)(out + KD)) & 15) == 0) {
+    for (int el = 4 * tid; el < E; el += 4 * kFinThreads) {
+      float4 a = *(const float4 *)(s_fv + el), b = *(const float4 *)(s_fv + E + el);
+      if (nrmz) {
+        a = make_float4(a.x / nf, a.y / nf, a.z / nf, a.w / nf);
+        b = make_float4(b.x / nf, b.y / nf, b.z / nf, b.w / nf);
+      }
+      *(float4 *)(out + el) = a;
+      *(float4 *)(out + KD + el) = b;
     }
   } else {
     for (int el = tid; el < E; el += kFinThreads) {
-      out[el] = s_fv[el];
-      out[KD + el] = s_fv[E + el];
+      out[el] = nrmz ? s_fv[el] / nf : s_fv[el];
+      out[KD + el] = nrmz ? s_fv[E + el] / nf : s_fv[E + el];
     }
   }
   cluster.sync();  // the partials stay readable until every CTA has read them
