@@ -593,6 +593,165 @@ __global__ void __launch_bounds__(kThreads) k_fisher_stats(
   }
 }
 
+// Asynchronous global -> shared copies (16 or 4 bytes; bytes past srcBytes
+// are zero-filled and nothing is read for them).
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t srcBytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(srcBytes) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void *src, uint32_t srcBytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(srcBytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The same statistics as k_fisher_stats (float, D <= 128), visiting only the
+// (row, component) pairs that pass the skips.  A block takes one segment and
+// kFsKB components, all dimensions; 32-row chunks of x and of the block's
+// posterior columns are double-buffered in shared memory by cp.async.  Warp w
+// owns the components w, w + 16, ...: per chunk and component it ballots the
+// rows with q >= 1e-6 and walks them in row order, lanes over dimensions, with
+// the accumulators in registers.  Per (component, dimension) the operations
+// and their order are k_fisher_stats' (u += q df, v += q (df^2 - 1) as fused
+// multiply-adds, df = (x - mu) s, rows ascending), so the partials are the
+// same bits; the dense kernel spends its time on the ~94% of pairs the skip
+// removes on typical posteriors.
+constexpr int kFsThreads = 512, kFsRC = 32;
+
+// KB: components per block (128, or 64 above 96 dimensions, where the
+// accumulators of 8 components per warp would not fit in registers).
+size_t fisher_sparse_smem(int D, int KB) {
+  return sizeof(float) * ((size_t)2 * KB * D + (size_t)2 * kFsRC * D + (size_t)2 * kFsRC * (KB + 4));
+}
+
+template <int DPL, int kFsKB>
+__global__ void __launch_bounds__(kFsThreads, 1) k_fisher_stats_sparse(
+    const float *__restrict__ X, const float *__restrict__ q, i64 qbase, int K, int D,
+    const Segment *__restrict__ segs, const float *__restrict__ means, const float *__restrict__ sis,
+    const float *__restrict__ priors, double *__restrict__ pu, double *__restrict__ pv,
+    unsigned long long *__restrict__ pnt, int vec16) {
+  constexpr int NW = kFsThreads / 32, CPW = kFsKB / NW, kFsQP = kFsKB + 4;
+  extern __shared__ __align__(16) float fs_smem[];
+  float *smu = fs_smem;               // [KB][D]
+  float *ssi = smu + kFsKB * D;       // [KB][D]
+  float *sx = ssi + kFsKB * D;        // [2][RC][D]
+  float *sq = sx + 2 * kFsRC * D;     // [2][RC][QP]
+  const int tid = threadIdx.x, w = tid / 32, lane = tid % 32;
+  const int sidx = blockIdx.x, k0 = blockIdx.y * kFsKB;
+  const Segment sg = segs[sidx];
+  const i64 rows = sg.row1 - sg.row0;
+  const int nch = (int)((rows + kFsRC - 1) / kFsRC);
+
+  auto issue = [&](int ch) {
+    const int b = ch & 1;
+    const i64 rb = sg.row0 + (i64)ch * kFsRC;
+    const int rc = (int)min((i64)kFsRC, sg.row1 - rb);
+    float *bx = sx + b * kFsRC * D, *bq = sq + b * kFsRC * kFsQP;
+    if (vec16) {
+      const int d4 = D / 4;
+      for (int e = tid; e < kFsRC * d4; e += kFsThreads) {
+        const int r = e / d4, c4 = e - r * d4;
+        const bool ok = r < rc;
+        cp_async16(tc::smem_u32(bx + r * D + 4 * c4), ok ? X + (rb + r) * D + 4 * c4 : X, ok ? 16u : 0u);
+      }
+      for (int e = tid; e < kFsRC * (kFsKB / 4); e += kFsThreads) {
+        const int r = e / (kFsKB / 4), c4 = e % (kFsKB / 4), kk = k0 + 4 * c4;
+        const bool ok = r < rc && kk < K;
+        cp_async16(tc::smem_u32(bq + r * kFsQP + 4 * c4), ok ? q + (rb + r - qbase) * K + kk : q, ok ? 16u : 0u);
+      }
+    } else {
+      for (int e = tid; e < kFsRC * D; e += kFsThreads) {
+        const int r = e / D, d = e - r * D;
+        const bool ok = r < rc;
+        cp_async4(tc::smem_u32(bx + r * D + d), ok ? X + (rb + r) * D + d : X, ok ? 4u : 0u);
+      }
+      for (int e = tid; e < kFsRC * kFsKB; e += kFsThreads) {
+        const int r = e / kFsKB, c = e % kFsKB, kk = k0 + c;
+        const bool ok = r < rc && kk < K;
+        cp_async4(tc::smem_u32(bq + r * kFsQP + c), ok ? q + (rb + r - qbase) * K + kk : q, ok ? 4u : 0u);
+      }
+    }
+    cp_async_commit();
+  };
+
+  if (nch > 0) issue(0);
+  for (int e = tid; e < kFsKB * D; e += kFsThreads) {
+    const int kl = e / D, d = e - kl * D, k = k0 + kl;
+    smu[e] = k < K ? means[(i64)k * D + d] : 0.f;
+    ssi[e] = k < K ? sis[(i64)k * D + d] : 0.f;
+  }
+  bool act[CPW];
+  float u[CPW][DPL], v[CPW][DPL];
+  unsigned nt[CPW];  // at most the segment's rows
+#pragma unroll
+  for (int c = 0; c < CPW; ++c) {
+    const int k = k0 + w + NW * c;
+    act[c] = k < K && (double)priors[k] >= 1e-6;
+    nt[c] = 0;
+#pragma unroll
+    for (int j = 0; j < DPL; ++j) u[c][j] = v[c][j] = 0.f;
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) {
+      issue(ch + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const float *bx = sx + (ch & 1) * kFsRC * D, *bq = sq + (ch & 1) * kFsRC * kFsQP;
+    const int rc = (int)min((i64)kFsRC, rows - (i64)ch * kFsRC);
+#pragma unroll
+    for (int c = 0; c < CPW; ++c) {
+      if (!act[c]) continue;  // warp-uniform
+      const int kl = w + NW * c;
+      const float val = bq[lane * kFsQP + kl];
+      // k_fisher_stats' skip: values below 1e-6 (compared in double) and zeros.
+      unsigned m = __ballot_sync(0xffffffffu, lane < rc && !((double)val < 1e-6) && val != 0.f);
+      nt[c] += (unsigned)__popc(m);
+      float mu[DPL], si[DPL];
+#pragma unroll
+      for (int j = 0; j < DPL; ++j) {
+        const int d = lane + 32 * j;
+        mu[j] = d < D ? smu[kl * D + d] : 0.f;
+        si[j] = d < D ? ssi[kl * D + d] : 0.f;
+      }
+      while (m) {
+        const int r = __ffs(m) - 1;
+        m &= m - 1;
+        const float p = bq[r * kFsQP + kl];
+#pragma unroll
+        for (int j = 0; j < DPL; ++j) {
+          const int d = lane + 32 * j;
+          if (d < D) {
+            const float df = (bx[r * D + d] - mu[j]) * si[j];
+            u[c][j] = fmaf(p, df, u[c][j]);
+            v[c][j] = fmaf(p, fmaf(df, df, -1.f), v[c][j]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < CPW; ++c) {
+    const int k = k0 + w + NW * c;
+    if (k >= K) continue;
+    const i64 base = ((i64)sidx * K + k) * D;
+#pragma unroll
+    for (int j = 0; j < DPL; ++j) {
+      const int d = lane + 32 * j;
+      if (d < D) {
+        pu[base + d] = (double)u[c][j];
+        pv[base + d] = (double)v[c][j];
+      }
+    }
+    if (lane == 0) pnt[(i64)sidx * K + k] = (unsigned long long)nt[c];
+  }
+}
+
 // Per-image Fisher finalisation (vl/fisher.c:450-485): sum the image's
 // segment partials, scale u by 1/(N sqrt pi) and v by 1/(N sqrt(2 pi)),
 // signed square root, global L2 normalisation.  One block per image.
@@ -885,10 +1044,31 @@ void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const D
     VLB_CUDA(cudaMemcpyAsync(dsegs, segs.data(), sizeof(Segment) * nseg, cudaMemcpyHostToDevice, s));
     VLB_CUDA(cudaMemcpyAsync(dbeg, segBegin.data(), sizeof(int) * (nimg + 1), cudaMemcpyHostToDevice, s));
     VLB_CUDA(cudaMemcpyAsync(drows, rows.data(), sizeof(i64) * nimg, cudaMemcpyHostToDevice, s));
-    dim3 g((unsigned)nseg, grid1(K, TKC), grid1(D, DB));
-    VLB_LAUNCH("exact_fisher_stats", s,
-               (k_fisher_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
-                   X, q, row0, (int)K, (int)D, dsegs, m.means, der.sis, m.priors, pu, pv, pnt)));
+    bool sparse = false;
+    if constexpr (sizeof(T) == 4) {
+      if (D <= 128) {
+        // The sparse statistics kernel (same partials, float data up to 128 dimensions).
+        const int dpl = (int)((D + 31) / 32), kb = dpl == 4 ? 64 : 128;
+        auto kern = dpl == 1 ? k_fisher_stats_sparse<1, 128>
+                    : dpl == 2 ? k_fisher_stats_sparse<2, 128>
+                    : dpl == 3 ? k_fisher_stats_sparse<3, 128>
+                               : k_fisher_stats_sparse<4, 64>;
+        const size_t smem = fisher_sparse_smem((int)D, kb);
+        VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int vec16 = (D % 4 == 0 && K % 4 == 0 && ((uintptr_t)X & 15) == 0 && ((uintptr_t)q & 15) == 0) ? 1 : 0;
+        dim3 g((unsigned)nseg, grid1(K, kb));
+        VLB_LAUNCH("exact_fisher_stats", s,
+                   kern<<<g, kFsThreads, smem, s>>>(X, q, row0, (int)K, (int)D, dsegs, m.means, der.sis,
+                                                     m.priors, pu, pv, pnt, vec16));
+        sparse = true;
+      }
+    }
+    if (!sparse) {
+      dim3 g((unsigned)nseg, grid1(K, TKC), grid1(D, DB));
+      VLB_LAUNCH("exact_fisher_stats", s,
+                 (k_fisher_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
+                     X, q, row0, (int)K, (int)D, dsegs, m.means, der.sis, m.priors, pu, pv, pnt)));
+    }
     VLB_LAUNCH("exact_fisher_finalize", s,
                k_fisher_finalize<T><<<(unsigned)nimg, kThreads, 0, s>>>(
                    (int)K, (int)D, dbeg, drows, pu, pv, pnt, m.priors, flags, chunkImg0, enc,
