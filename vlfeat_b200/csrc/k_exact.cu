@@ -607,49 +607,79 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// The same statistics as k_fisher_stats (float, D <= 128), visiting only the
-// (row, component) pairs that pass the skips.  A block takes one segment and
-// kFsKB components, all dimensions; 32-row chunks of x and of the block's
-// posterior columns are double-buffered in shared memory by cp.async.  Warp w
-// owns the components w, w + 16, ...: per chunk and component it ballots the
-// rows with q >= 1e-6 and walks them in row order, lanes over dimensions, with
-// the accumulators in registers.  Per (component, dimension) the operations
-// and their order are k_fisher_stats' (u += q df, v += q (df^2 - 1) as fused
-// multiply-adds, df = (x - mu) s, rows ascending), so the partials are the
-// same bits; the dense kernel spends its time on the ~94% of pairs the skip
-// removes on typical posteriors.
+// Thresholded statistics visiting only the (row, component) pairs that pass
+// the skip, for float data up to 128 dimensions:
+//  - kSpFisher: k_fisher_stats' statistics (vl/fisher.c:419-449): per segment,
+//    for pi_k >= 1e-6 and q >= 1e-6, u += q df, v += q (df^2 - 1) with
+//    df = (x - mu) s, and the term counts;
+//  - kSpMstep: k_mstep_stats' statistics (vl/gmm.c:1093-1149): per slab, for
+//    q >= 1e-2/K, mass += q, S1 += q x, S2 += q (x - mu_old)^2.
+// A block takes one segment (or slab) and KB components, all dimensions;
+// 32-row chunks of x and of the block's posterior columns are double-buffered
+// in shared memory by cp.async.  Warp w owns the components w, w + 16, ...:
+// per chunk and component it ballots the rows that pass and walks them in row
+// order, lanes over dimensions, with the accumulators in registers.  Per
+// (component, dimension) the operations and their order are the dense
+// kernels' (fused multiply-adds as there, rows ascending), so the partials are
+// the same bits; the dense kernels spend their time on the pairs the skip
+// removes (about 94% of them on typical posteriors).
 constexpr int kFsThreads = 512, kFsRC = 32;
+enum { kSpFisher = 0, kSpMstep = 1 };
+
+struct SparseStatsArgs {
+  const float *X;        // rows indexed from the call's first row
+  const float *q;        // N x K posteriors, row (r - qbase)
+  i64 qbase;
+  int K, D;
+  const Segment *segs;   // kSpFisher: the segments
+  i64 N, rowsPerSlab;    // kSpMstep: slab s is rows [s rps, min(N, (s + 1) rps))
+  const float *mu;       // means (kSpFisher) or old means (kSpMstep)
+  const float *sis;      // kSpFisher: 1 / sigma
+  const float *priors;   // kSpFisher
+  double *p1, *p2;       // u, v (kSpFisher) or S1, S2 (kSpMstep): [block][K][D]
+  unsigned long long *pnt;  // kSpFisher: term counts [segment][K]
+  double *pmass;            // kSpMstep: [slab][K]
+  int vec16;
+};
 
 // KB: components per block (128, or 64 above 96 dimensions, where the
 // accumulators of 8 components per warp would not fit in registers).
-size_t fisher_sparse_smem(int D, int KB) {
+size_t sparse_stats_smem(int D, int KB) {
   return sizeof(float) * ((size_t)2 * KB * D + (size_t)2 * kFsRC * D + (size_t)2 * kFsRC * (KB + 4));
 }
 
-template <int DPL, int kFsKB>
-__global__ void __launch_bounds__(kFsThreads, 1) k_fisher_stats_sparse(
-    const float *__restrict__ X, const float *__restrict__ q, i64 qbase, int K, int D,
-    const Segment *__restrict__ segs, const float *__restrict__ means, const float *__restrict__ sis,
-    const float *__restrict__ priors, double *__restrict__ pu, double *__restrict__ pv,
-    unsigned long long *__restrict__ pnt, int vec16) {
+template <int MODE, int DPL, int kFsKB>
+__global__ void __launch_bounds__(kFsThreads, 1) k_stats_sparse(const SparseStatsArgs a) {
   constexpr int NW = kFsThreads / 32, CPW = kFsKB / NW, kFsQP = kFsKB + 4;
   extern __shared__ __align__(16) float fs_smem[];
+  const int K = a.K, D = a.D;
+  const float *__restrict__ X = a.X;
+  const float *__restrict__ q = a.q;
   float *smu = fs_smem;               // [KB][D]
-  float *ssi = smu + kFsKB * D;       // [KB][D]
+  float *ssi = smu + kFsKB * D;       // [KB][D] (kSpFisher)
   float *sx = ssi + kFsKB * D;        // [2][RC][D]
   float *sq = sx + 2 * kFsRC * D;     // [2][RC][QP]
   const int tid = threadIdx.x, w = tid / 32, lane = tid % 32;
   const int sidx = blockIdx.x, k0 = blockIdx.y * kFsKB;
-  const Segment sg = segs[sidx];
-  const i64 rows = sg.row1 - sg.row0;
+  i64 row0, row1;
+  if constexpr (MODE == kSpFisher) {
+    const Segment sg = a.segs[sidx];
+    row0 = sg.row0;
+    row1 = sg.row1;
+  } else {
+    row0 = (i64)sidx * a.rowsPerSlab;
+    row1 = min(a.N, row0 + a.rowsPerSlab);
+  }
+  const i64 rows = row1 - row0;
   const int nch = (int)((rows + kFsRC - 1) / kFsRC);
+  const i64 qbase = a.qbase;
 
   auto issue = [&](int ch) {
     const int b = ch & 1;
-    const i64 rb = sg.row0 + (i64)ch * kFsRC;
-    const int rc = (int)min((i64)kFsRC, sg.row1 - rb);
+    const i64 rb = row0 + (i64)ch * kFsRC;
+    const int rc = (int)min((i64)kFsRC, row1 - rb);
     float *bx = sx + b * kFsRC * D, *bq = sq + b * kFsRC * kFsQP;
-    if (vec16) {
+    if (a.vec16) {
       const int d4 = D / 4;
       for (int e = tid; e < kFsRC * d4; e += kFsThreads) {
         const int r = e / d4, c4 = e - r * d4;
@@ -679,17 +709,21 @@ __global__ void __launch_bounds__(kFsThreads, 1) k_fisher_stats_sparse(
   if (nch > 0) issue(0);
   for (int e = tid; e < kFsKB * D; e += kFsThreads) {
     const int kl = e / D, d = e - kl * D, k = k0 + kl;
-    smu[e] = k < K ? means[(i64)k * D + d] : 0.f;
-    ssi[e] = k < K ? sis[(i64)k * D + d] : 0.f;
+    smu[e] = k < K ? a.mu[(i64)k * D + d] : 0.f;
+    if constexpr (MODE == kSpFisher) ssi[e] = k < K ? a.sis[(i64)k * D + d] : 0.f;
   }
+  // The skip: values below thr (compared in double) and zeros.
+  const double thr = MODE == kSpFisher ? 1e-6 : 1e-2 / (double)K;
   bool act[CPW];
-  float u[CPW][DPL], v[CPW][DPL];
+  float u[CPW][DPL], v[CPW][DPL], mass[CPW];
   unsigned nt[CPW];  // at most the segment's rows
 #pragma unroll
   for (int c = 0; c < CPW; ++c) {
     const int k = k0 + w + NW * c;
-    act[c] = k < K && (double)priors[k] >= 1e-6;
+    if constexpr (MODE == kSpFisher) act[c] = k < K && (double)a.priors[k] >= 1e-6;
+    else act[c] = k < K;
     nt[c] = 0;
+    mass[c] = 0.f;
 #pragma unroll
     for (int j = 0; j < DPL; ++j) u[c][j] = v[c][j] = 0.f;
   }
@@ -708,27 +742,34 @@ __global__ void __launch_bounds__(kFsThreads, 1) k_fisher_stats_sparse(
       if (!act[c]) continue;  // warp-uniform
       const int kl = w + NW * c;
       const float val = bq[lane * kFsQP + kl];
-      // k_fisher_stats' skip: values below 1e-6 (compared in double) and zeros.
-      unsigned m = __ballot_sync(0xffffffffu, lane < rc && !((double)val < 1e-6) && val != 0.f);
+      unsigned m = __ballot_sync(0xffffffffu, lane < rc && !((double)val < thr) && val != 0.f);
       nt[c] += (unsigned)__popc(m);
       float mu[DPL], si[DPL];
 #pragma unroll
       for (int j = 0; j < DPL; ++j) {
         const int d = lane + 32 * j;
         mu[j] = d < D ? smu[kl * D + d] : 0.f;
-        si[j] = d < D ? ssi[kl * D + d] : 0.f;
+        if constexpr (MODE == kSpFisher) si[j] = d < D ? ssi[kl * D + d] : 0.f;
       }
       while (m) {
         const int r = __ffs(m) - 1;
         m &= m - 1;
         const float p = bq[r * kFsQP + kl];
+        if constexpr (MODE == kSpMstep) mass[c] += p;
 #pragma unroll
         for (int j = 0; j < DPL; ++j) {
           const int d = lane + 32 * j;
           if (d < D) {
-            const float df = (bx[r * D + d] - mu[j]) * si[j];
-            u[c][j] = fmaf(p, df, u[c][j]);
-            v[c][j] = fmaf(p, fmaf(df, df, -1.f), v[c][j]);
+            const float x = bx[r * D + d];
+            if constexpr (MODE == kSpFisher) {
+              const float df = (x - mu[j]) * si[j];
+              u[c][j] = fmaf(p, df, u[c][j]);
+              v[c][j] = fmaf(p, fmaf(df, df, -1.f), v[c][j]);
+            } else {
+              const float df = x - mu[j];
+              u[c][j] = fmaf(p, x, u[c][j]);
+              v[c][j] = fmaf(p, df * df, v[c][j]);
+            }
           }
         }
       }
@@ -744,12 +785,34 @@ __global__ void __launch_bounds__(kFsThreads, 1) k_fisher_stats_sparse(
     for (int j = 0; j < DPL; ++j) {
       const int d = lane + 32 * j;
       if (d < D) {
-        pu[base + d] = (double)u[c][j];
-        pv[base + d] = (double)v[c][j];
+        a.p1[base + d] = (double)u[c][j];
+        a.p2[base + d] = (double)v[c][j];
       }
     }
-    if (lane == 0) pnt[(i64)sidx * K + k] = (unsigned long long)nt[c];
+    if (lane == 0) {
+      if constexpr (MODE == kSpFisher) a.pnt[(i64)sidx * K + k] = (unsigned long long)nt[c];
+      else a.pmass[(i64)sidx * K + k] = (double)mass[c];
+    }
   }
+}
+
+// Launches k_stats_sparse over nblk segments (or slabs); false when the shape
+// is outside it (the dense kernel runs instead).
+template <int MODE>
+bool launch_stats_sparse(SparseStatsArgs a, i64 nblk, cudaStream_t s) {
+  if (a.D > 128 || nblk <= 0) return false;
+  const int dpl = (a.D + 31) / 32, kb = dpl == 4 ? 64 : 128;
+  auto kern = dpl == 1 ? k_stats_sparse<MODE, 1, 128>
+              : dpl == 2 ? k_stats_sparse<MODE, 2, 128>
+              : dpl == 3 ? k_stats_sparse<MODE, 3, 128>
+                         : k_stats_sparse<MODE, 4, 64>;
+  const size_t smem = sparse_stats_smem(a.D, kb);
+  VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  a.vec16 = (a.D % 4 == 0 && a.K % 4 == 0 && ((uintptr_t)a.X & 15) == 0 && ((uintptr_t)a.q & 15) == 0) ? 1 : 0;
+  dim3 g((unsigned)nblk, (unsigned)((a.K + kb - 1) / kb));
+  VLB_LAUNCH(MODE == kSpFisher ? "exact_fisher_stats" : "exact_mstep_stats", s,
+             kern<<<g, kFsThreads, smem, s>>>(a));
+  return true;
 }
 
 // Per-image Fisher finalisation (vl/fisher.c:450-485): sum the image's
@@ -859,6 +922,20 @@ i64 pick_slab_rows(i64 N) {
 }
 }  // namespace
 
+// The M-step statistics of nslab slabs of rows by the sparse kernel (float
+// data up to 128 dimensions); false when the dense kernel is to run.
+template <typename T>
+bool mstep_stats_sparse(const T *X, const T *q, i64 N, i64 K, i64 D, i64 rps, i64 nslab, const T *oldMeans,
+                        double *pmass, double *ps1, double *ps2, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    SparseStatsArgs a{};
+    a.X = X; a.q = q; a.qbase = 0; a.K = (int)K; a.D = (int)D; a.N = N; a.rowsPerSlab = rps;
+    a.mu = oldMeans; a.p1 = ps1; a.p2 = ps2; a.pmass = pmass;
+    return launch_stats_sparse<kSpMstep>(a, nslab, s);
+  }
+  return false;
+}
+
 template <typename T>
 void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i64 K, i64 D,
                  const double *lb, cudaStream_t s) {
@@ -870,10 +947,12 @@ void exact_mstep(const T *X, i64 N, const T *q, T *means, T *covs, T *priors, i6
   double *ps1 = sc.slot[11].get<double>((size_t)nslab * K * D);
   double *ps2 = sc.slot[12].get<double>((size_t)nslab * K * D);
   if (N > 0) {
-    dim3 g(nslab, grid1(K, TKC), grid1(D, DB));
-    VLB_LAUNCH("exact_mstep_stats", s,
-               (k_mstep_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
-                   X, q, N, (int)K, (int)D, rps, means, pmass, ps1, ps2)));
+    if (!mstep_stats_sparse<T>(X, q, N, K, D, rps, nslab, means, pmass, ps1, ps2, s)) {
+      dim3 g(nslab, grid1(K, TKC), grid1(D, DB));
+      VLB_LAUNCH("exact_mstep_stats", s,
+                 (k_mstep_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
+                     X, q, N, (int)K, (int)D, rps, means, pmass, ps1, ps2)));
+    }
   } else {
     VLB_CUDA(cudaMemsetAsync(pmass, 0, sizeof(double) * nslab * K, s));
     VLB_CUDA(cudaMemsetAsync(ps1, 0, sizeof(double) * nslab * K * D, s));
@@ -894,6 +973,9 @@ void exact_mstep_stats_rows(const T *X, i64 row0, i64 n, i64 rps, const T *q, co
   if (n <= 0) return;
   VLB_CHECK(row0 % rps == 0, VL_ERR_BAD_ARG, "M-step chunk must start on a slab boundary");
   const i64 s0 = row0 / rps, nslab = (n + rps - 1) / rps;
+  if (mstep_stats_sparse<T>(X + row0 * D, q, n, K, D, rps, nslab, oldMeans, pmass + s0 * K, ps1 + s0 * K * D,
+                            ps2 + s0 * K * D, s))
+    return;
   dim3 g((unsigned)nslab, grid1(K, TKC), grid1(D, DB));
   VLB_LAUNCH("exact_mstep_stats", s,
              (k_mstep_stats<T, TKC, RC, JMAX><<<g, kThreads, 0, s>>>(
@@ -1046,22 +1128,11 @@ void exact_fisher_batch(const T *X, const i64 *h_offsets, i64 numImages, const D
     VLB_CUDA(cudaMemcpyAsync(drows, rows.data(), sizeof(i64) * nimg, cudaMemcpyHostToDevice, s));
     bool sparse = false;
     if constexpr (sizeof(T) == 4) {
-      if (D <= 128) {
-        // The sparse statistics kernel (same partials, float data up to 128 dimensions).
-        const int dpl = (int)((D + 31) / 32), kb = dpl == 4 ? 64 : 128;
-        auto kern = dpl == 1 ? k_fisher_stats_sparse<1, 128>
-                    : dpl == 2 ? k_fisher_stats_sparse<2, 128>
-                    : dpl == 3 ? k_fisher_stats_sparse<3, 128>
-                               : k_fisher_stats_sparse<4, 64>;
-        const size_t smem = fisher_sparse_smem((int)D, kb);
-        VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int vec16 = (D % 4 == 0 && K % 4 == 0 && ((uintptr_t)X & 15) == 0 && ((uintptr_t)q & 15) == 0) ? 1 : 0;
-        dim3 g((unsigned)nseg, grid1(K, kb));
-        VLB_LAUNCH("exact_fisher_stats", s,
-                   kern<<<g, kFsThreads, smem, s>>>(X, q, row0, (int)K, (int)D, dsegs, m.means, der.sis,
-                                                     m.priors, pu, pv, pnt, vec16));
-        sparse = true;
-      }
+      // The sparse statistics kernel (same partials, float data up to 128 dimensions).
+      SparseStatsArgs a{};
+      a.X = X; a.q = q; a.qbase = row0; a.K = (int)K; a.D = (int)D; a.segs = dsegs;
+      a.mu = m.means; a.sis = der.sis; a.priors = m.priors; a.p1 = pu; a.p2 = pv; a.pnt = pnt;
+      sparse = launch_stats_sparse<kSpFisher>(a, nseg, s);
     }
     if (!sparse) {
       dim3 g((unsigned)nseg, grid1(K, TKC), grid1(D, DB));
