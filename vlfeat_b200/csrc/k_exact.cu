@@ -826,25 +826,45 @@ __global__ void __launch_bounds__(kThreads) k_fisher_finalize(
     i64 imgBase, T *__restrict__ enc, unsigned long long *__restrict__ nterms) {
   __shared__ double sh[kThreads];
   __shared__ unsigned long long shn[kThreads];
+  // Per-component factors 1 / (n sqrt(pi_k)) and 1 / (n sqrt(2 pi_k)), formed
+  // once per image (-1: the component is skipped, its entries are 0).
+  constexpr int kFinK = 2048;
+  __shared__ double sfu[kFinK], sfv[kFinK];
   const int img = blockIdx.x;
   const int s0 = imgSegBegin[img], s1 = imgSegBegin[img + 1];
   const i64 n = imgRows[img];
   const i64 KD = (i64)K * D;
   T *out = enc + (imgBase + img) * 2 * KD;
+  auto factor = [&](int k, bool isv) -> double {
+    const double pk = (double)priors[k];
+    if (!(pk >= 1e-6 && n > 0)) return -1.0;
+    return isv ? 1.0 / ((double)n * sqrt(2.0 * pk)) : 1.0 / ((double)n * sqrt(pk));
+  };
+  const bool cached = K <= kFinK;
+  if (cached) {
+    for (int k = threadIdx.x; k < K; k += kThreads) {
+      sfu[k] = factor(k, false);
+      sfv[k] = factor(k, true);
+    }
+    __syncthreads();
+  }
+  const bool small = KD <= (i64)INT32_MAX;
   double sq = 0;
   for (i64 e = threadIdx.x; e < 2 * KD; e += kThreads) {
     const bool isv = e >= KD;
     const i64 kd = isv ? e - KD : e;
-    const int k = (int)(kd / D);
+    const int k = small ? (int)((unsigned)kd / (unsigned)D) : (int)(kd / D);
     double acc = 0;
     for (int s = s0; s < s1; ++s) acc += isv ? pv[(i64)s * KD + kd] : pu[(i64)s * KD + kd];
-    const double pk = (double)priors[k];
-    double z = 0;
-    if (pk >= 1e-6 && n > 0) {
-      z = isv ? acc * (1.0 / ((double)n * sqrt(2.0 * pk))) : acc * (1.0 / ((double)n * sqrt(pk)));
-    }
+    const double f = cached ? (isv ? sfv[k] : sfu[k]) : factor(k, isv);
+    const double z = f >= 0.0 ? acc * f : 0.0;
     T zt = (T)z;
-    if (flags & 1) zt = zt >= (T)0 ? (T)sqrt((double)zt) : -(T)sqrt(-(double)zt);
+    // For float, sqrtf is the float rounding of the double square root (double
+    // rounding is innocuous for sqrt with 53 >= 2 x 24 + 2 bits).
+    if (flags & 1) {
+      if constexpr (sizeof(T) == 4) zt = zt >= 0.f ? sqrtf(zt) : -sqrtf(-zt);
+      else zt = zt >= (T)0 ? (T)sqrt((double)zt) : -(T)sqrt(-(double)zt);
+    }
     out[e] = zt;
     sq += (double)zt * (double)zt;
   }
