@@ -159,6 +159,32 @@ def test_batched_matches_single(vl, restatement):
         assert nt[j] == n
 
 
+@pytest.mark.parametrize("K,D", [(200, 128), (130, 80), (7, 3), (257, 33)])
+def test_batched_statistics_layouts(vl, restatement, K, D):
+    """Batched exact encoding at shapes that reach every layout of the sparse
+    statistics kernel: 64-component blocks (D = 128) and 128-component ones, a
+    partial last block, 16-byte and 4-byte copies (K or D not a multiple of
+    4), one to four dimensions per lane, an empty image and images cut into
+    several 2,048-row segments; per image against the C restatement."""
+    import torch
+    from vlfeat_b200 import workloads as W
+    pr, mu, cv = W.fv_gmm(K, D, seed=K + D)
+    counts = np.array([0, 5, 1500, 4100, 37])
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    x = W.pca_like(int(offs[-1]), D, seed=K * D)
+    dev = torch.device("cuda")
+    enc = torch.zeros((len(counts), 2 * K * D), device=dev)
+    nt = torch.zeros(len(counts), dtype=torch.int64, device=dev)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    vl.fisher_encode_batch_device(enc, t(mu), t(cv), t(pr), t(x), offs, FLAG_IMPROVED, "exact", nt)
+    enc = enc.cpu().numpy()
+    nt = nt.cpu().numpy()
+    for j in range(len(counts)):
+        e, n = restatement.fisher(x[offs[j]:offs[j + 1]], mu, cv, pr, FLAG_IMPROVED)
+        assert rel_err(enc[j], e) < 2e-5, j
+        assert nt[j] == n
+
+
 def test_deterministic(vl, golden):
     g = golden
     a = _em(vl, g, np.float32, 5)[0]
