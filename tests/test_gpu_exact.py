@@ -185,6 +185,31 @@ def test_batched_statistics_layouts(vl, restatement, K, D):
         assert nt[j] == n
 
 
+@pytest.mark.parametrize("K,D", [(96, 128), (70, 33)])
+def test_em_statistics_layouts(vl, restatement, K, D):
+    """Exact float EM at shapes that reach the sparse M-step statistics'
+    64-component blocks (D = 128) and its 4-byte copies with a partial block
+    (K = 70, D = 33): 4 iterations from the same custom initialisation against
+    the C restatement in float."""
+    from vlfeat_b200 import workloads as W
+    pr, mu, cv = W.fv_gmm(K, D, seed=3 * K + D)
+    x = W.pca_like(12000, D, seed=K + 7 * D)
+    ref = restatement.em(x, pr, mu, cv, 1e-4, 4)
+    m = vl.GMM(D, K, np.float32)
+    m.set_initialization("custom")
+    m.set_max_num_iterations(4)
+    m.set_covariance_lower_bound(1e-4)
+    m.set_means(mu)
+    m.set_covariances(cv)
+    m.set_priors(pr)
+    ll = m.cluster(x)
+    tol = 5e-5
+    assert abs(ll - ref["ll"]) <= tol * abs(ref["ll"])
+    assert m.num_restarts == ref["restarts"]
+    for name, got in (("priors", m.priors), ("means", m.means), ("covs", m.covariances)):
+        assert rel_err(got, ref[name]) < tol, name
+
+
 def test_deterministic(vl, golden):
     g = golden
     a = _em(vl, g, np.float32, 5)[0]
