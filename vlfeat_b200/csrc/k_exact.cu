@@ -64,7 +64,7 @@ __global__ void k_prepare(const T *__restrict__ priors, const T *__restrict__ co
 // updates acc += (x - mu)^2 / sigma^2.  Per (descriptor, component) the sum
 // runs over the dimensions in ascending order.
 template <typename T, int TM, int TK, int DC>
-__global__ void __launch_bounds__(kThreads) k_logp(const T *__restrict__ X, i64 N, int D, int K,
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 2) k_logp(const T *__restrict__ X, i64 N, int D, int K,
                                                   const T *__restrict__ means,
                                                   const T *__restrict__ inv,
                                                   const double *__restrict__ cst,
@@ -150,6 +150,22 @@ __global__ void __launch_bounds__(kThreads) k_logp(const T *__restrict__ X, i64 
       }
     }
     __syncthreads();
+  }
+  if constexpr (sizeof(T) == 4 && CC == 4) {
+    // The thread's 4 components of a row in one 16-byte store.
+    const int kb = k0 + tc * CC;
+    if ((K & 3) == 0 && kb + CC <= K && ((uintptr_t)q & 15) == 0) {
+      const double c0 = cst[kb], c1 = cst[kb + 1], c2 = cst[kb + 2], c3 = cst[kb + 3];
+#pragma unroll
+      for (int r = 0; r < RR; ++r) {
+        const i64 i = i0 + tr * RR + r;
+        if (i < N)
+          *reinterpret_cast<float4 *>(q + i * K + kb) =
+              make_float4((float)(c0 - 0.5 * (double)acc[r][0]), (float)(c1 - 0.5 * (double)acc[r][1]),
+                          (float)(c2 - 0.5 * (double)acc[r][2]), (float)(c3 - 0.5 * (double)acc[r][3]));
+      }
+      return;
+    }
   }
 #pragma unroll
   for (int c = 0; c < CC; ++c) {
@@ -630,6 +646,7 @@ struct SparseStatsArgs {
   const float *X;        // rows indexed from the call's first row
   const float *q;        // N x K posteriors, row (r - qbase)
   i64 qbase;
+  float thr;             // the smallest float >= the skip threshold
   int K, D;
   const Segment *segs;   // kSpFisher: the segments
   i64 N, rowsPerSlab;    // kSpMstep: slab s is rows [s rps, min(N, (s + 1) rps))
@@ -679,24 +696,17 @@ __global__ void __launch_bounds__(kFsThreads, 1) k_stats_sparse(const SparseStat
     const i64 rb = row0 + (i64)ch * kFsRC;
     const int rc = (int)min((i64)kFsRC, row1 - rb);
     float *bx = sx + b * kFsRC * D, *bq = sq + b * kFsRC * kFsQP;
+    // The chunk's x rows are one contiguous range (rows past rc are never read).
+    const float *xs = X + rb * D;
     if (a.vec16) {
-      const int d4 = D / 4;
-      for (int e = tid; e < kFsRC * d4; e += kFsThreads) {
-        const int r = e / d4, c4 = e - r * d4;
-        const bool ok = r < rc;
-        cp_async16(tc::smem_u32(bx + r * D + 4 * c4), ok ? X + (rb + r) * D + 4 * c4 : X, ok ? 16u : 0u);
-      }
+      for (int e = tid; e < rc * D / 4; e += kFsThreads) cp_async16(tc::smem_u32(bx + 4 * e), xs + 4 * e, 16u);
       for (int e = tid; e < kFsRC * (kFsKB / 4); e += kFsThreads) {
         const int r = e / (kFsKB / 4), c4 = e % (kFsKB / 4), kk = k0 + 4 * c4;
         const bool ok = r < rc && kk < K;
         cp_async16(tc::smem_u32(bq + r * kFsQP + 4 * c4), ok ? q + (rb + r - qbase) * K + kk : q, ok ? 16u : 0u);
       }
     } else {
-      for (int e = tid; e < kFsRC * D; e += kFsThreads) {
-        const int r = e / D, d = e - r * D;
-        const bool ok = r < rc;
-        cp_async4(tc::smem_u32(bx + r * D + d), ok ? X + (rb + r) * D + d : X, ok ? 4u : 0u);
-      }
+      for (int e = tid; e < rc * D; e += kFsThreads) cp_async4(tc::smem_u32(bx + e), xs + e, 4u);
       for (int e = tid; e < kFsRC * kFsKB; e += kFsThreads) {
         const int r = e / kFsKB, c = e % kFsKB, kk = k0 + c;
         const bool ok = r < rc && kk < K;
@@ -712,8 +722,9 @@ __global__ void __launch_bounds__(kFsThreads, 1) k_stats_sparse(const SparseStat
     smu[e] = k < K ? a.mu[(i64)k * D + d] : 0.f;
     if constexpr (MODE == kSpFisher) ssi[e] = k < K ? a.sis[(i64)k * D + d] : 0.f;
   }
-  // The skip: values below thr (compared in double) and zeros.
-  const double thr = MODE == kSpFisher ? 1e-6 : 1e-2 / (double)K;
+  // The skip: values below thr (compared in double, i.e. below a.thr as
+  // floats; NaN passes in both) and zeros.
+  const float thr = a.thr;
   bool act[CPW];
   float u[CPW][DPL], v[CPW][DPL], mass[CPW];
   unsigned nt[CPW];  // at most the segment's rows
@@ -742,7 +753,7 @@ __global__ void __launch_bounds__(kFsThreads, 1) k_stats_sparse(const SparseStat
       if (!act[c]) continue;  // warp-uniform
       const int kl = w + NW * c;
       const float val = bq[lane * kFsQP + kl];
-      unsigned m = __ballot_sync(0xffffffffu, lane < rc && !((double)val < thr) && val != 0.f);
+      unsigned m = __ballot_sync(0xffffffffu, lane < rc && !(val < thr) && val != 0.f);
       nt[c] += (unsigned)__popc(m);
       float mu[DPL], si[DPL];
 #pragma unroll
@@ -809,6 +820,11 @@ bool launch_stats_sparse(SparseStatsArgs a, i64 nblk, cudaStream_t s) {
   const size_t smem = sparse_stats_smem(a.D, kb);
   VLB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   a.vec16 = (a.D % 4 == 0 && a.K % 4 == 0 && ((uintptr_t)a.X & 15) == 0 && ((uintptr_t)a.q & 15) == 0) ? 1 : 0;
+  // (double)v < t for a float v exactly when v < tf, tf the smallest float >= t.
+  const double t = MODE == kSpFisher ? 1e-6 : 1e-2 / (double)a.K;
+  float tf = (float)t;
+  if ((double)tf < t) tf = std::nextafter(tf, INFINITY);
+  a.thr = tf;
   dim3 g((unsigned)nblk, (unsigned)((a.K + kb - 1) / kb));
   VLB_LAUNCH(MODE == kSpFisher ? "exact_fisher_stats" : "exact_mstep_stats", s,
              kern<<<g, kFsThreads, smem, s>>>(a));
