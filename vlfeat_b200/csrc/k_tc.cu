@@ -60,7 +60,7 @@ namespace cg = cooperative_groups;
 // one more warp loads the descriptor rows and the W k-atoms.
 __host__ __device__ constexpr int tc_threads(bool sw) { return sw ? 448 : 416; }
 constexpr int kSmemLimit = 232448;  // 227 KB opt-in per block
-constexpr float kLog2e = 1.4426950408889634f;
+constexpr int kMaxXs = 8;           // E-step ring of descriptor-row boxes: at most 8
 constexpr double kLn2 = 0.6931471805599453;
 
 int num_sms() {
@@ -332,7 +332,6 @@ struct ELayout {
   // Cluster exchange slots: per TMEM buffer, 128 rows of (max, sum, argmax).
   static constexpr int kXch = CL ? 2 * 128 * 16 : 0;
   static constexpr int kXBox = 128 * 16 * 4;  // one box of descriptor rows
-  static constexpr int kMaxXs = 8;            // boxes in the ring, at most
   static size_t fixed(int Kp) {
     return (SW ? 0 : 2 * wbytes(Kp)) + 1024 /*cst*/ + 2048 /*ctr, bars*/ + kStaging + kXch + 1024 /*alignment*/;
   }
@@ -1599,7 +1598,7 @@ i64 launch_estep_impl(const float *X, i64 N, const TcPrep &tp, void *q, int ldq,
   int nst, nxs = 0;
   if constexpr (SW) {
     nst = std::min(nst_req > 0 ? nst_req : 3, L::max_stages(Kb, 2));
-    if (nst >= 2) nxs = std::min<int>(L::kMaxXs, (int)((kSmemLimit - L::bytes(Kb, nst)) / L::kXBox));
+    if (nst >= 2) nxs = std::min<int>(kMaxXs, (int)((kSmemLimit - L::bytes(Kb, nst)) / L::kXBox));
   } else {
     nst = std::min(nst_req > 0 ? nst_req : 8, L::max_stages(Kb));
   }
